@@ -1,0 +1,124 @@
+/*
+ * qcbc_gpu.h -- C ABI of the B200 likelihood engine for QuickCBC.
+ *
+ * Plain C types only (pointers, sizes, doubles); no CUDA or torch types.
+ * Every function returns a status code (QCBC_OK on success) unless noted;
+ * qcbc_last_error() gives the message of the calling thread's last failure.
+ *
+ * Data conventions are the QuickCBC reference's:
+ *   D      [nifo][N]          half-complex FFT rows (Re at i, Im at N-i),
+ *                             scaled by sqrt(Tobs)/N (QuickCBC.c:254-313)
+ *   SN     [nifo][sn_stride]  one-sided PSD per bin, sn_stride >= N/2
+ *   params [B][11]            ln(Mc kg), ln(Mt kg), chi1, chi2, phi0, tc,
+ *                             ln(DL m), alpha, sin(delta), psi, cos(iota)
+ *                             (QuickCBC.c:1867)
+ *   lnL                       sum_ifo <d|h> - <h|h>/2 over
+ *                             [Tobs*fmin, min(Tobs*fmax, N/2))  (QuickCBC.c:4236-4273)
+ *
+ * Reentrancy: calls on different events, or on the same event from different
+ * host threads, may run concurrently (each thread has its own CUDA stream and
+ * scratch).  Opening/closing an event or replacing its heterodyne tables must
+ * not race with likelihood calls on that event.
+ */
+#ifndef QCBC_GPU_H
+#define QCBC_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QCBC_OK 0
+#define QCBC_EINVAL (-1)   /* bad argument */
+#define QCBC_ECUDA (-2)    /* CUDA runtime error */
+#define QCBC_ENOMEM (-3)   /* device or host allocation failed */
+#define QCBC_EBUDGET (-4)  /* admission refused by the device-memory budget */
+#define QCBC_ETIMEOUT (-5) /* a bounded device wait ran out */
+#define QCBC_EDOM 33       /* some parameter sets were outside the waveform's domain;
+                              their lnL is -1e20 (IMRPhenomD.c:208-242 would exit) */
+
+#define QCBC_FP64 0        /* plain form: every step in FP64 */
+#define QCBC_MIXED 1       /* FP64 phase and 2 pi f tc shift, FP32 amplitude/sincos/accumulate */
+
+typedef struct qcbc_event qcbc_event;
+
+/* Heterodyne summary tables, flat row-major (the reference's struct Het,
+ * QuickCBC.h:27-51, with its row-pointer arrays flattened):
+ *   fgrid[M], freq[M], amp[nifo][M], phase[nifo][M], IP[NR][J+1][J+1],
+ *   SL/lc/ls[NR][nifo][J+1], aa/rc/rs[nifo][NR], NR = (M-1)/J. */
+typedef struct {
+  int M, MN, MM, J, NR;
+  double logLb;
+  const int* fgrid;
+  const double *freq, *amp, *phase, *IP, *SL, *lc, *ls, *aa, *rc, *rs;
+} qcbc_het_tables;
+
+const char* qcbc_last_error(void);
+const char* qcbc_version(void);
+
+/* Select the CUDA device for the calling thread and load the model tables
+ * there (idempotent).  Every entry point calls it for device 0 if needed. */
+int qcbc_init(int device);
+
+/* QNM table override: final spin a[n] (strictly increasing), fring[n], fdamp[n].
+ * The library ships the table of IMRPhenomD_internals.h:176-640. */
+int qcbc_set_qnm_table(const double* a, const double* fring, const double* fdamp, int n);
+
+/* ---- events: one analysis resident on the device ---- */
+/* Copies D and SN to the device once (replaces QuickCBC.c:4254-4266's per-call
+ * template and two inner-product passes).  d_stride / sn_stride are row strides. */
+qcbc_event* qcbc_event_open(int nifo, const int* labels, double Tobs, double GMST, int N, const double* D,
+                            int d_stride, const double* SN, int sn_stride, double fmin, double fmax);
+int qcbc_event_close(qcbc_event* ev);
+/* Device bytes held by an event (data, tables). */
+long long qcbc_event_device_bytes(const qcbc_event* ev);
+
+/* Full likelihood for B parameter sets (host arrays).  rho may be NULL
+ * ([B][nifo] otherwise, rho = <d|h>/sqrt(<h|h>) per detector). */
+int qcbc_lnl_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int precision);
+/* Same with device pointers on a caller stream (cudaStream_t passed as void*, NULL = the thread's stream). */
+int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho, int precision,
+                      void* stream);
+
+/* ---- heterodyned likelihood ---- */
+/* Upload tables computed elsewhere (e.g. by the reference's heterodyne()). */
+int qcbc_het_set(qcbc_event* ev, const qcbc_het_tables* t);
+/* Compute the tables on the device in FP64 for reference parameters pref[11] and
+ * grid fgrid[M] (bin indices, from het_space, QuickCBC.c:4570-4910); replaces
+ * heterodyne(), QuickCBC.c:5112-5299. */
+int qcbc_het_setup(qcbc_event* ev, const double* pref, const int* fgrid, int M, int MN, int MM, int J);
+/* Copy the event's tables back: caller buffers sized from qcbc_het_sizes(). */
+int qcbc_het_sizes(const qcbc_event* ev, int* M, int* J, int* NR, int* MN, int* MM);
+int qcbc_het_export(const qcbc_event* ev, int* fgrid, double* freq, double* amp, double* phase, double* IP,
+                    double* SL, double* lc, double* ls, double* aa, double* rc, double* rs, double* logLb);
+int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double* lnl, int precision);
+int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, int precision, void* stream);
+
+/* ---- launch tuning ---- */
+/* Blocks per parameter set and threads per block for the full likelihood
+ * (0 = automatic: measured once per (bins, nifo, B, precision) and cached). */
+int qcbc_set_full_launch(qcbc_event* ev, int tiles, int threads);
+int qcbc_get_full_launch(qcbc_event* ev, int B, int precision, int* tiles, int* threads);
+
+/* ---- device memory for callers that stage parameters themselves ---- */
+void* qcbc_device_alloc(long long bytes);
+int qcbc_device_free(void* p);
+int qcbc_memcpy_h2d(void* dst, const void* src, long long bytes);
+int qcbc_memcpy_d2h(void* dst, const void* src, long long bytes);
+int qcbc_synchronize(void);
+
+/* ---- measurement helpers (CUDA events on the launching stream) ---- */
+/* Runs `iters` likelihood launches on device-resident params; between launches
+ * writes a scratch buffer larger than L2 when flush_l2 != 0 (outside the timed
+ * span).  ms[iters] receives each launch's device time; kernel_ms[iters] the
+ * time of the fused inner-product kernel alone (may be NULL). */
+int qcbc_time_lnl_full(qcbc_event* ev, const double* d_params, int B, int precision, int iters, int flush_l2,
+                       float* ms, float* kernel_ms);
+int qcbc_time_lnl_het(qcbc_event* ev, const double* d_params, int B, int precision, int iters, int flush_l2,
+                      float* ms);
+/* Kernel launches issued by this library in the calling thread so far. */
+long long qcbc_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,121 @@
+/*
+ * qcbc_quickcbc.h -- drop-in replacements for the QuickCBC reference's
+ * waveform and likelihood entry points, executed on the GPU.
+ *
+ * The functions keep the reference's names and signatures so the unchanged
+ * host C (PT-MCMC, proposals, Fisher updates, heterodyne grid search) links
+ * against them.  The struct layouts below are byte-compatible with the
+ * reference's declarations; a program that already includes the reference's
+ * QuickCBC.h / IMRPhenomD_internals.h uses its own definitions and only needs
+ * the prototypes (define QCBC_HAVE_REFERENCE_TYPES before including this).
+ *
+ * Device residency: D, SN and freq are host arrays owned by the caller.  A
+ * call uploads them unless they were registered with qcbc_bind_data(), in
+ * which case the device copies made at registration are used (register again
+ * after changing their contents).  No caller pointer is kept beyond a call
+ * except as the registration key.
+ *
+ * Errors: the double-returning functions cannot report errors in-band; on a
+ * failure they return -1e20 (the reference's rejected-sample value,
+ * QuickCBC.c:2366) and qcbc_last_error() tells why.
+ */
+#ifndef QCBC_QUICKCBC_H
+#define QCBC_QUICKCBC_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#ifndef QCBC_HAVE_REFERENCE_TYPES
+/* QuickCBC.h:13-25 */
+struct Net {
+  int Nifo;
+  double Tobs;
+  double tmax;
+  double tmin;
+  double GMST;
+  int* labels;
+  double* tds;
+  double** delays;
+  int* lstart;
+  int* lstop;
+};
+
+/* IMRPhenomD_internals.h:662-665 */
+typedef struct tagRealVector {
+  double* data;
+  size_t length;
+} RealVector;
+
+/* IMRPhenomD_internals.h:649-654 */
+typedef struct tagAmpPhaseFDWaveform {
+  double* freq;
+  double* amp;
+  double* phase;
+  size_t length;
+} AmpPhaseFDWaveform;
+
+/* QuickCBC.h:27-51 */
+struct Het {
+  int M;
+  int MM;
+  int MN;
+  int ell;
+  int J;
+  int NR;
+  double hh;
+  double hr;
+  double logLb;
+  double*** IP;
+  double*** SL;
+  double** amp;
+  double** phase;
+  double** rc;
+  double** rs;
+  double** aa;
+  double*** lc;
+  double*** ls;
+  double* pref;
+  int* fgrid;
+  RealVector* freq;
+};
+#endif
+
+/* Band of the full likelihood: the reference's compile-time fmin/fmax
+ * (ConstCBC.h:33-34, defaults 16 Hz and 1024 Hz). */
+int qcbc_set_band(double fmin, double fmax);
+
+/* Register caller arrays so later calls with the same pointers skip uploads. */
+int qcbc_bind_data(struct Net* net, double** D, double** SN, int N, double Tobs);
+int qcbc_unbind_all(void);
+
+/* replaces QuickCBC.c:4236 */
+double log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN, double* rho,
+                           int N, double Tobs);
+/* replaces QuickCBC.c:5303; the struct Het tables are uploaded on first use and
+ * re-uploaded when het->IP, het->M or het->logLb change (re-heterodyne). */
+double log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs);
+/* replaces QuickCBC.c:5112; needs het->M, MN, MM, J, NR, fgrid, freq from het_space.
+ * Allocates the table arrays with the reference's row-pointer layout
+ * (Utilities.c:2981-3015) so freehet() (QuickCBC.c:5096) releases them. */
+void heterodyne(struct Net* net, struct Het* het, double** D, double* params, RealVector* freq, double** SN, int N,
+                double Tobs);
+/* replaces QuickCBC.c:3683 */
+void fulltemplates(struct Net* net, double** hwave, RealVector* freq, double* params, int N);
+/* replaces QuickCBC.c:3780 */
+void fullphaseamp(struct Net* net, double** amp, double** phase, RealVector* freq, double* params, int N);
+/* replaces IMRPhenomD.c:186; *h22 is malloc'd like CreateAmpPhaseFDWaveform
+ * (IMRPhenomD_internals.c:130-146) so DestroyAmpPhaseFDWaveform frees it.
+ * Returns 0 (PD_SUCCESS) or 33 (PD_EDOM) instead of exiting on bad input. */
+int IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, const double phi0,
+                                    const double fRef_in, const double m1_SI, const double m2_SI, const double chi1,
+                                    const double chi2, const double distance);
+/* replaces Utilities.c:716 */
+double fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,2 @@
+/* GSL-API shim header (oracle test infrastructure); declarations in ../gsl_shim.h */
+#include "../gsl_shim.h"

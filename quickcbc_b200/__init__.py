@@ -1,0 +1,15 @@
+"""B200-native likelihood hot path for QuickCBC.
+
+IMRPhenomD frequency-domain amplitude/phase, detector projection with time and
+phase shifts, and the PSD-weighted inner products behind the full and
+heterodyned log-likelihoods, as hand-written sm_100a CUDA kernels behind a
+C ABI (include/qcbc_gpu.h, include/qcbc_quickcbc.h).  See ``engine`` for the
+host interface and ``synth`` for the seeded synthetic workloads.
+"""
+from ._lib import FP64, MIXED, QcbcError, launch_count  # noqa: F401
+from .engine import (Event, DeviceBuffer, amp_phase, fourier_nwip, fullphaseamp, fulltemplates,  # noqa: F401
+                     log_likelihood_full, set_band, LegacyHet, time_lnl_full, time_lnl_het)
+
+__all__ = ["FP64", "MIXED", "QcbcError", "Event", "DeviceBuffer", "amp_phase", "fourier_nwip", "fullphaseamp",
+           "fulltemplates", "log_likelihood_full", "set_band", "LegacyHet", "time_lnl_full", "time_lnl_het",
+           "launch_count"]

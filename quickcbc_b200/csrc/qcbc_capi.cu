@@ -1,0 +1,1145 @@
+// C ABI of the QuickCBC likelihood engine: events resident on the device,
+// batched likelihood calls, the reference-signature drop-ins and timing helpers.
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+#include <algorithm>
+
+#include "qcbc_kernels.cuh"
+#include "../../include/qcbc_gpu.h"
+#include "../../include/qcbc_quickcbc.h"
+#include "_gen/qnm_table.h"
+
+using namespace qcbc;
+
+// ------------------------------------------------------------------ errors
+static thread_local std::string tls_err;
+static thread_local long long tls_launches = 0;
+
+static int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  tls_err = buf;
+  return code;
+}
+#define CU(call)                                                                               \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(QCBC_ECUDA, "%s: %s", #call, cudaGetErrorString(e_));   \
+  } while (0)
+
+extern "C" const char* qcbc_last_error(void) { return tls_err.c_str(); }
+extern "C" const char* qcbc_version(void) { return "qcbc-b200 0.1 (sm_100a)"; }
+extern "C" long long qcbc_launch_count(void) { return tls_launches; }
+
+// ------------------------------------------------------------------ device state
+struct DeviceState {
+  bool ready = false;
+  double* d_qnm = nullptr;   // x, yr, mr, yd, md (5 * n)
+  int n = 0;
+  QnmTable qnm{};
+};
+static std::mutex g_mu;
+static DeviceState g_dev[16];
+static std::vector<double> g_qnm_host[3];   // a, fring, fdamp
+
+static void natural_spline_m2(const std::vector<double>& x, const std::vector<double>& y, std::vector<double>& M) {
+  int n = (int)x.size();
+  M.assign(n, 0.0);
+  if (n < 3) return;
+  std::vector<double> diag(n), rhs(n);
+  for (int i = 1; i < n - 1; i++) {
+    double h0 = x[i] - x[i - 1], h1 = x[i + 1] - x[i];
+    diag[i] = 2.0 * (h0 + h1);
+    rhs[i] = 6.0 * ((y[i + 1] - y[i]) / h1 - (y[i] - y[i - 1]) / h0);
+  }
+  for (int i = 2; i < n - 1; i++) {
+    double h = x[i] - x[i - 1], w = h / diag[i - 1];
+    diag[i] -= w * h;
+    rhs[i] -= w * rhs[i - 1];
+  }
+  for (int i = n - 2; i >= 1; i--) M[i] = (rhs[i] - (x[i + 1] - x[i]) * M[i + 1]) / diag[i];
+}
+
+static int upload_qnm(DeviceState& ds) {
+  if (g_qnm_host[0].empty()) {
+    g_qnm_host[0].assign(QCBC_QNM_A, QCBC_QNM_A + QCBC_QNM_N);
+    g_qnm_host[1].assign(QCBC_QNM_FRING, QCBC_QNM_FRING + QCBC_QNM_N);
+    g_qnm_host[2].assign(QCBC_QNM_FDAMP, QCBC_QNM_FDAMP + QCBC_QNM_N);
+  }
+  int n = (int)g_qnm_host[0].size();
+  std::vector<double> mr, md;
+  natural_spline_m2(g_qnm_host[0], g_qnm_host[1], mr);
+  natural_spline_m2(g_qnm_host[0], g_qnm_host[2], md);
+  std::vector<double> all;
+  all.reserve(5 * n);
+  all.insert(all.end(), g_qnm_host[0].begin(), g_qnm_host[0].end());
+  all.insert(all.end(), g_qnm_host[1].begin(), g_qnm_host[1].end());
+  all.insert(all.end(), mr.begin(), mr.end());
+  all.insert(all.end(), g_qnm_host[2].begin(), g_qnm_host[2].end());
+  all.insert(all.end(), md.begin(), md.end());
+  if (ds.d_qnm) cudaFree(ds.d_qnm);
+  CU(cudaMalloc(&ds.d_qnm, all.size() * sizeof(double)));
+  CU(cudaMemcpy(ds.d_qnm, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+  ds.n = n;
+  ds.qnm = QnmTable{ds.d_qnm, ds.d_qnm + n, ds.d_qnm + 2 * n, ds.d_qnm + 3 * n, ds.d_qnm + 4 * n, n};
+  return QCBC_OK;
+}
+
+static int current_device() {
+  int d = 0;
+  cudaGetDevice(&d);
+  return d;
+}
+
+extern "C" int qcbc_init(int device) {
+  if (device < 0 || device >= 16) return fail(QCBC_EINVAL, "device %d out of range", device);
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0)
+    return fail(QCBC_ECUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+  if (device >= ndev) return fail(QCBC_EINVAL, "device %d >= device count %d", device, ndev);
+  CU(cudaSetDevice(device));
+  std::lock_guard<std::mutex> lk(g_mu);
+  DeviceState& ds = g_dev[device];
+  if (!ds.ready) {
+    int rc = upload_qnm(ds);
+    if (rc) return rc;
+    ds.ready = true;
+  }
+  return QCBC_OK;
+}
+
+static int ensure_init() {
+  int d = current_device();
+  if (g_dev[d].ready) return QCBC_OK;
+  return qcbc_init(d);
+}
+
+extern "C" int qcbc_set_qnm_table(const double* a, const double* fring, const double* fdamp, int n) {
+  if (!a || !fring || !fdamp || n < 4) return fail(QCBC_EINVAL, "bad QNM table");
+  for (int i = 1; i < n; i++)
+    if (!(a[i] > a[i - 1])) return fail(QCBC_EINVAL, "QNM spins must increase strictly");
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_qnm_host[0].assign(a, a + n);
+  g_qnm_host[1].assign(fring, fring + n);
+  g_qnm_host[2].assign(fdamp, fdamp + n);
+  for (auto& ds : g_dev)
+    if (ds.ready) {
+      int rc = upload_qnm(ds);
+      if (rc) return rc;
+    }
+  return QCBC_OK;
+}
+
+// ------------------------------------------------------------------ per-thread workspace
+template <typename T>
+static int grow(T*& p, size_t& cap, size_t n) {
+  if (n <= cap && p) return QCBC_OK;
+  if (p) cudaFree(p);
+  p = nullptr;
+  cap = 0;
+  size_t want = std::max(n, (size_t)256);
+  cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+  if (e != cudaSuccess) return fail(QCBC_ENOMEM, "cudaMalloc %zu B: %s", want * sizeof(T), cudaGetErrorString(e));
+  cap = want;
+  return QCBC_OK;
+}
+template <typename T>
+static int grow_host(T*& p, size_t& cap, size_t n) {
+  if (n <= cap && p) return QCBC_OK;
+  if (p) cudaFreeHost(p);
+  p = nullptr;
+  cap = 0;
+  size_t want = std::max(n, (size_t)256);
+  cudaError_t e = cudaMallocHost(&p, want * sizeof(T));
+  if (e != cudaSuccess) return fail(QCBC_ENOMEM, "cudaMallocHost %zu B: %s", want * sizeof(T), cudaGetErrorString(e));
+  cap = want;
+  return QCBC_OK;
+}
+
+struct Workspace {
+  int device = -1;
+  cudaStream_t stream = nullptr;
+  double* d_params = nullptr; size_t c_params = 0;
+  PhdRec* d_recs = nullptr; size_t c_recs = 0;
+  int* d_status = nullptr; size_t c_status = 0;
+  double* d_part = nullptr; size_t c_part = 0;
+  double* d_lnl = nullptr; size_t c_lnl = 0;
+  double* d_rho = nullptr; size_t c_rho = 0;
+  double* h_params = nullptr; size_t ch_params = 0;
+  double* h_lnl = nullptr; size_t ch_lnl = 0;
+  double* h_rho = nullptr; size_t ch_rho = 0;
+  int* h_status = nullptr; size_t ch_status = 0;
+  // generic scratch for the reference-signature entry points
+  double* d_a = nullptr; size_t c_a = 0;
+  double* d_b = nullptr; size_t c_b = 0;
+  double* d_c = nullptr; size_t c_c = 0;
+  double* h_a = nullptr; size_t ch_a = 0;
+  double* h_b = nullptr; size_t ch_b = 0;
+  unsigned char* d_flush = nullptr; size_t c_flush = 0;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+};
+static thread_local Workspace tls_ws;
+
+static int workspace(Workspace*& w) {
+  int rc = ensure_init();
+  if (rc) return rc;
+  w = &tls_ws;
+  int d = current_device();
+  if (w->device != d) {
+    if (w->device >= 0) return fail(QCBC_EINVAL, "thread switched device (%d -> %d)", w->device, d);
+    CU(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    CU(cudaEventCreate(&w->e0));
+    CU(cudaEventCreate(&w->e1));
+    CU(cudaEventCreate(&w->e2));
+    CU(cudaEventCreate(&w->e3));
+    w->device = d;
+  }
+  return QCBC_OK;
+}
+
+// ------------------------------------------------------------------ events
+struct HetDev {
+  int M = 0, J = 0, NR = 0, MN = 0, MM = 0;
+  double logLb = 0.0;
+  double* buf = nullptr;   // freq, amp, phase, IP, SL, lc, ls, aa, rc, rs
+  int* d_fgrid = nullptr;
+  size_t bytes = 0;
+  std::vector<int> fgrid;
+};
+
+struct qcbc_event {
+  int device = 0;
+  NetGeom g{};
+  double fmin = 16.0, fmax = 1024.0;
+  int nh = 0;
+  double* d_w64 = nullptr;
+  float* d_w32 = nullptr;
+  double* d_D = nullptr;     // raw data [nifo][N] (heterodyne setup)
+  double* d_S = nullptr;     // raw PSD [nifo][nh+1]
+  double* d_freq = nullptr;  // canonical frequencies [nh]
+  double inv_sigma[kMaxIfo] = {1, 1, 1};
+  HetDev het;
+  int fixed_tiles = 0, fixed_threads = 0;
+  std::map<long long, FullLaunch> tuned;
+  long long bytes = 0;
+  bool has_data = false;
+};
+
+static EventData event_data(const qcbc_event* ev) {
+  EventData d{};
+  d.w64 = ev->d_w64;
+  d.w32 = ev->d_w32;
+  d.nh = ev->nh;
+  for (int k = 0; k < kMaxIfo; k++) d.inv_sigma[k] = ev->inv_sigma[k];
+  return d;
+}
+
+static HetData het_data(const qcbc_event* ev) {
+  const HetDev& h = ev->het;
+  HetData d{};
+  d.M = h.M; d.J = h.J; d.NR = h.NR; d.MN = h.MN; d.MM = h.MM; d.logLb = h.logLb;
+  int nI = ev->g.nifo, J1 = h.J + 1;
+  double* p = h.buf;
+  d.freq = p; p += h.M;
+  d.amp = p; p += (size_t)nI * h.M;
+  d.phase = p; p += (size_t)nI * h.M;
+  d.IP = p; p += (size_t)h.NR * J1 * J1;
+  d.SL = p; p += (size_t)h.NR * nI * J1;
+  d.lc = p; p += (size_t)h.NR * nI * J1;
+  d.ls = p; p += (size_t)h.NR * nI * J1;
+  d.aa = p; p += (size_t)nI * h.NR;
+  d.rc = p; p += (size_t)nI * h.NR;
+  d.rs = p;
+  return d;
+}
+
+static size_t het_doubles(int nifo, int M, int J) {
+  int NR = (M - 1) / J, J1 = J + 1;
+  return (size_t)M + 2 * (size_t)nifo * M + (size_t)NR * J1 * J1 + 3 * (size_t)NR * nifo * J1 + 3 * (size_t)nifo * NR;
+}
+
+static bool pow2_exact(double Tobs) {
+  int e;
+  double m = frexp(Tobs, &e);
+  return m == 0.5;
+}
+
+static void fill_geom(NetGeom& g, int nifo, const int* labels, double Tobs, double GMST, int N, double fmin,
+                      double fmax) {
+  memset(&g, 0, sizeof(g));
+  g.nifo = nifo;
+  for (int i = 0; i < nifo && i < kMaxIfo; i++) g.labels[i] = labels[i];
+  g.N = N;
+  g.imin = (int)(Tobs * fmin);
+  g.imax = (int)(Tobs * fmax);
+  if (g.imax > N / 2) g.imax = N / 2;
+  g.GMST = GMST;
+  g.Tobs = Tobs;
+  g.df = 1.0 / Tobs;
+  g.div_exact = pow2_exact(Tobs) ? 1 : 0;
+}
+
+static int check_geom(int nifo, const int* labels, double Tobs, int N) {
+  if (nifo < 1 || nifo > kMaxIfo) return fail(QCBC_EINVAL, "nifo=%d (1..3 supported)", nifo);
+  if (!labels) return fail(QCBC_EINVAL, "labels is NULL");
+  for (int i = 0; i < nifo; i++)
+    if (labels[i] < 0 || labels[i] > 2) return fail(QCBC_EINVAL, "detector label %d (0=H,1=L,2=V)", labels[i]);
+  if (!(Tobs > 0.0)) return fail(QCBC_EINVAL, "Tobs must be positive");
+  if (N < 8 || (N & 1)) return fail(QCBC_EINVAL, "N=%d must be even and >= 8", N);
+  return QCBC_OK;
+}
+
+// Data upload: weighted FP64/FP32 copies plus raw D, S (rows gathered on the host).
+static int event_upload(qcbc_event* ev, const double* const* Drows, const double* const* Srows) {
+  const int nI = ev->g.nifo, N = ev->g.N, nh = N / 2;
+  ev->nh = nh;
+  std::vector<double> w64((size_t)nI * 3 * nh, 0.0);
+  std::vector<float> w32((size_t)nI * 3 * nh, 0.0f);
+  std::vector<double> Dall((size_t)nI * N), Sall((size_t)nI * (nh + 1), 0.0);
+  int lo = std::max(ev->g.imin, 1), hi = std::min(ev->g.imax, nh);
+  for (int id = 0; id < nI; id++) {
+    const double* D = Drows[id];
+    const double* S = Srows[id];
+    memcpy(&Dall[(size_t)id * N], D, sizeof(double) * N);
+    for (int i = 0; i < nh; i++) Sall[(size_t)id * (nh + 1) + i] = S[i];
+    // sigma^2 = smallest PSD in band keeps 4 sigma^2/S <= 4 and 4 sigma D/S = O(1)
+    double smin = HUGE_VAL;
+    for (int i = lo; i < hi; i++)
+      if (S[i] > 0.0 && S[i] < smin) smin = S[i];
+    if (!(smin < HUGE_VAL)) smin = 1.0;
+    double sigma = sqrt(smin);
+    ev->inv_sigma[id] = 1.0 / sigma;
+    double* wr = &w64[(size_t)id * 3 * nh];
+    double* wi = wr + nh;
+    double* ws = wi + nh;
+    for (int i = lo; i < hi; i++) {
+      double s = S[i];
+      wr[i] = 4.0 * sigma * D[i] / s;
+      wi[i] = 4.0 * sigma * D[N - i] / s;
+      ws[i] = 4.0 * sigma * sigma / s;
+    }
+    for (int k = 0; k < 3 * nh; k++) w32[(size_t)id * 3 * nh + k] = (float)w64[(size_t)id * 3 * nh + k];
+  }
+  std::vector<double> freq(nh);
+  freq[0] = 1.0 / ev->g.Tobs;
+  for (int i = 1; i < nh; i++) freq[i] = (double)i / ev->g.Tobs;
+  size_t b64 = w64.size() * 8, b32 = w32.size() * 4, bD = Dall.size() * 8, bS = Sall.size() * 8, bf = freq.size() * 8;
+  if (!ev->d_w64) {
+    CU(cudaMalloc(&ev->d_w64, b64));
+    CU(cudaMalloc(&ev->d_w32, b32));
+    CU(cudaMalloc(&ev->d_D, bD));
+    CU(cudaMalloc(&ev->d_S, bS));
+    CU(cudaMalloc(&ev->d_freq, bf));
+  }
+  CU(cudaMemcpy(ev->d_w64, w64.data(), b64, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ev->d_w32, w32.data(), b32, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ev->d_D, Dall.data(), bD, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ev->d_S, Sall.data(), bS, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ev->d_freq, freq.data(), bf, cudaMemcpyHostToDevice));
+  ev->bytes = (long long)(b64 + b32 + bD + bS + bf);
+  ev->has_data = true;
+  return QCBC_OK;
+}
+
+static void event_free_device(qcbc_event* ev) {
+  cudaFree(ev->d_w64); cudaFree(ev->d_w32); cudaFree(ev->d_D); cudaFree(ev->d_S); cudaFree(ev->d_freq);
+  cudaFree(ev->het.buf); cudaFree(ev->het.d_fgrid);
+  ev->d_w64 = nullptr; ev->d_w32 = nullptr; ev->d_D = nullptr; ev->d_S = nullptr; ev->d_freq = nullptr;
+  ev->het.buf = nullptr; ev->het.d_fgrid = nullptr;
+}
+
+extern "C" qcbc_event* qcbc_event_open(int nifo, const int* labels, double Tobs, double GMST, int N, const double* D,
+                                       int d_stride, const double* SN, int sn_stride, double fmin, double fmax) {
+  if (ensure_init()) return nullptr;
+  if (check_geom(nifo, labels, Tobs, N)) return nullptr;
+  if (!D || !SN) { fail(QCBC_EINVAL, "D and SN must not be NULL"); return nullptr; }
+  if (d_stride < N || sn_stride < N / 2) { fail(QCBC_EINVAL, "row strides too small"); return nullptr; }
+  if (!(fmin >= 0.0) || !(fmax > fmin)) { fail(QCBC_EINVAL, "bad band [%g, %g)", fmin, fmax); return nullptr; }
+  qcbc_event* ev = new qcbc_event();
+  ev->device = current_device();
+  ev->fmin = fmin;
+  ev->fmax = fmax;
+  fill_geom(ev->g, nifo, labels, Tobs, GMST, N, fmin, fmax);
+  std::vector<const double*> Dr(nifo), Sr(nifo);
+  for (int i = 0; i < nifo; i++) { Dr[i] = D + (size_t)i * d_stride; Sr[i] = SN + (size_t)i * sn_stride; }
+  if (event_upload(ev, Dr.data(), Sr.data())) { event_free_device(ev); delete ev; return nullptr; }
+  return ev;
+}
+
+extern "C" int qcbc_event_close(qcbc_event* ev) {
+  if (!ev) return QCBC_OK;
+  event_free_device(ev);
+  delete ev;
+  return QCBC_OK;
+}
+
+extern "C" long long qcbc_event_device_bytes(const qcbc_event* ev) {
+  if (!ev) return 0;
+  return ev->bytes + (long long)ev->het.bytes;
+}
+
+// ------------------------------------------------------------------ launch choice
+// Blocks per parameter set: enough blocks to fill 148 SMs several times over,
+// but at least ~512 bins per block.  The measured variant (tune_full) overrides.
+static FullLaunch heuristic_launch(const qcbc_event* ev, int B, int prec) {
+  FullLaunch L;
+  L.threads = 256;
+  int bins = std::max(1, ev->g.imax - ev->g.imin);
+  int want_blocks = 148 * 8;
+  int tiles = (want_blocks + B - 1) / B;
+  int max_tiles = std::max(1, bins / 512);
+  L.tiles = std::max(1, std::min(tiles, max_tiles));
+  (void)prec;
+  return L;
+}
+
+static FullLaunch choose_launch(qcbc_event* ev, int B, int prec) {
+  if (ev->fixed_tiles > 0) return FullLaunch{ev->fixed_tiles, ev->fixed_threads > 0 ? ev->fixed_threads : 256};
+  long long key = ((long long)B << 2) | prec;
+  auto it = ev->tuned.find(key);
+  if (it != ev->tuned.end()) return it->second;
+  return heuristic_launch(ev, B, prec);
+}
+
+extern "C" int qcbc_set_full_launch(qcbc_event* ev, int tiles, int threads) {
+  if (!ev) return fail(QCBC_EINVAL, "event is NULL");
+  if (tiles < 0 || (threads != 0 && (threads < 32 || threads > 256 || threads % 32)))
+    return fail(QCBC_EINVAL, "tiles >= 0, threads in {32..256} multiple of 32");
+  ev->fixed_tiles = tiles;
+  ev->fixed_threads = threads;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_get_full_launch(qcbc_event* ev, int B, int precision, int* tiles, int* threads) {
+  if (!ev || !tiles || !threads) return fail(QCBC_EINVAL, "NULL argument");
+  FullLaunch L = choose_launch(ev, B, precision);
+  *tiles = L.tiles;
+  *threads = L.threads;
+  return QCBC_OK;
+}
+
+// ------------------------------------------------------------------ full likelihood
+static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
+                        int prec, cudaStream_t s, const NetGeom& g, cudaEvent_t k0 = nullptr,
+                        cudaEvent_t k1 = nullptr) {
+  FullLaunch L = choose_launch(ev, B, prec);
+  int rc;
+  if ((rc = grow(w->d_recs, w->c_recs, (size_t)B))) return rc;
+  if ((rc = grow(w->d_status, w->c_status, (size_t)B))) return rc;
+  if ((rc = grow(w->d_part, w->c_part, (size_t)B * L.tiles * 2 * kMaxIfo))) return rc;
+  DeviceState& ds = g_dev[current_device()];
+  EventData ed = event_data(ev);
+  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s);
+  if (k0) cudaEventRecord(k0, s);
+  launch_lnl_full(w->d_recs, B, g, ed, prec == QCBC_MIXED ? kMixed : kFP64, L, w->d_part, s);
+  if (k1) cudaEventRecord(k1, s);
+  launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, d_lnl, d_rho, s);
+  tls_launches += 3;
+  CU(cudaGetLastError());
+  return QCBC_OK;
+}
+
+static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int prec,
+                    const NetGeom& g) {
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_params, w->c_params, (size_t)B * 11))) return rc;
+  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
+  if ((rc = grow(w->d_rho, w->c_rho, (size_t)B * kMaxIfo))) return rc;
+  if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * 11))) return rc;
+  if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
+  if ((rc = grow_host(w->h_rho, w->ch_rho, (size_t)B * kMaxIfo))) return rc;
+  if ((rc = grow_host(w->h_status, w->ch_status, (size_t)B))) return rc;
+  memcpy(w->h_params, params, sizeof(double) * 11 * (size_t)B);
+  cudaStream_t s = w->stream;
+  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_full(w, ev, w->d_params, B, w->d_lnl, rho ? w->d_rho : nullptr, prec, s, g))) return rc;
+  CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+  if (rho) CU(cudaMemcpyAsync(w->h_rho, w->d_rho, sizeof(double) * B * g.nifo, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  memcpy(lnl, w->h_lnl, sizeof(double) * B);
+  if (rho) memcpy(rho, w->h_rho, sizeof(double) * B * g.nifo);
+  int bad = 0;
+  for (int b = 0; b < B; b++) bad += w->h_status[b] != 0;
+  if (bad) return fail(QCBC_EDOM, "%d of %d parameter sets outside the waveform domain (lnL=-1e20)", bad, B);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_lnl_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int precision) {
+  if (!ev || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (B < 0) return fail(QCBC_EINVAL, "B < 0");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B == 0) return QCBC_OK;
+  return run_full(ev, params, B, lnl, rho, precision, ev->g);
+}
+
+extern "C" int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
+                                 int precision, void* stream) {
+  if (!ev || !d_params || !d_lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : w->stream;
+  return enqueue_full(w, ev, d_params, B, d_lnl, d_rho, precision, s, ev->g);
+}
+
+// ------------------------------------------------------------------ heterodyne
+static int het_alloc(qcbc_event* ev, int M, int J, int MN, int MM) {
+  HetDev& h = ev->het;
+  if (M < J + 1 || J < 1 || J > 3) return fail(QCBC_EINVAL, "heterodyne grid M=%d J=%d", M, J);
+  size_t need = het_doubles(ev->g.nifo, M, J);
+  if (h.buf && h.M == M && h.J == J) {
+    // same shape: reuse
+  } else {
+    cudaFree(h.buf);
+    cudaFree(h.d_fgrid);
+    h.buf = nullptr;
+    h.d_fgrid = nullptr;
+    CU(cudaMalloc(&h.buf, need * sizeof(double)));
+    CU(cudaMalloc(&h.d_fgrid, (size_t)M * sizeof(int)));
+  }
+  h.M = M; h.J = J; h.NR = (M - 1) / J; h.MN = MN; h.MM = MM;
+  h.bytes = need * sizeof(double) + (size_t)M * sizeof(int);
+  size_t smem = het_smem_bytes(ev->g, het_data(ev));
+  if (smem > 200 * 1024) return fail(QCBC_EINVAL, "heterodyne grid M=%d too large for one block (%zu B)", M, smem);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_set(qcbc_event* ev, const qcbc_het_tables* t) {
+  if (!ev || !t) return fail(QCBC_EINVAL, "NULL argument");
+  int rc = ensure_init();
+  if (rc) return rc;
+  if ((rc = het_alloc(ev, t->M, t->J, t->MN, t->MM))) return rc;
+  HetDev& h = ev->het;
+  h.logLb = t->logLb;
+  h.fgrid.assign(t->fgrid, t->fgrid + t->M);
+  HetData d = het_data(ev);
+  int nI = ev->g.nifo, M = h.M, NR = h.NR, J1 = h.J + 1;
+  struct { const double* src; const double* dst; size_t n; } parts[] = {
+    {t->freq, d.freq, (size_t)M}, {t->amp, d.amp, (size_t)nI * M}, {t->phase, d.phase, (size_t)nI * M},
+    {t->IP, d.IP, (size_t)NR * J1 * J1}, {t->SL, d.SL, (size_t)NR * nI * J1}, {t->lc, d.lc, (size_t)NR * nI * J1},
+    {t->ls, d.ls, (size_t)NR * nI * J1}, {t->aa, d.aa, (size_t)nI * NR}, {t->rc, d.rc, (size_t)nI * NR},
+    {t->rs, d.rs, (size_t)nI * NR}};
+  for (auto& p : parts) {
+    if (!p.src) return fail(QCBC_EINVAL, "heterodyne table pointer is NULL");
+    CU(cudaMemcpy((void*)p.dst, p.src, p.n * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  CU(cudaMemcpy(h.d_fgrid, t->fgrid, (size_t)M * sizeof(int), cudaMemcpyHostToDevice));
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_sizes(const qcbc_event* ev, int* M, int* J, int* NR, int* MN, int* MM) {
+  if (!ev) return fail(QCBC_EINVAL, "NULL event");
+  if (M) *M = ev->het.M;
+  if (J) *J = ev->het.J;
+  if (NR) *NR = ev->het.NR;
+  if (MN) *MN = ev->het.MN;
+  if (MM) *MM = ev->het.MM;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_export(const qcbc_event* ev, int* fgrid, double* freq, double* amp, double* phase, double* IP,
+                               double* SL, double* lc, double* ls, double* aa, double* rc, double* rs, double* logLb) {
+  if (!ev || !ev->het.buf) return fail(QCBC_EINVAL, "event has no heterodyne tables");
+  HetData d = het_data(ev);
+  const HetDev& h = ev->het;
+  int nI = ev->g.nifo, M = h.M, NR = h.NR, J1 = h.J + 1;
+  struct { double* dst; const double* src; size_t n; } parts[] = {
+    {freq, d.freq, (size_t)M}, {amp, d.amp, (size_t)nI * M}, {phase, d.phase, (size_t)nI * M},
+    {IP, d.IP, (size_t)NR * J1 * J1}, {SL, d.SL, (size_t)NR * nI * J1}, {lc, d.lc, (size_t)NR * nI * J1},
+    {ls, d.ls, (size_t)NR * nI * J1}, {aa, d.aa, (size_t)nI * NR}, {rc, d.rc, (size_t)nI * NR},
+    {rs, d.rs, (size_t)nI * NR}};
+  for (auto& p : parts)
+    if (p.dst) CU(cudaMemcpy(p.dst, p.src, p.n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (fgrid) memcpy(fgrid, h.fgrid.data(), sizeof(int) * M);
+  if (logLb) *logLb = h.logLb;
+  return QCBC_OK;
+}
+
+// Transpose of the inverse of the sampled Legendre basis, per region (QuickCBC.c:5232-5253).
+static void invert_small(const double* A, double* Ainv, int n) {
+  double W[4][8];
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < 2 * n; j++) W[i][j] = j < n ? A[i * n + j] : (j - n == i ? 1.0 : 0.0);
+  for (int col = 0; col < n; col++) {
+    int piv = col;
+    for (int i = col + 1; i < n; i++)
+      if (fabs(W[i][col]) > fabs(W[piv][col])) piv = i;
+    if (piv != col)
+      for (int j = 0; j < 2 * n; j++) std::swap(W[col][j], W[piv][j]);
+    double dd = W[col][col];
+    for (int j = 0; j < 2 * n; j++) W[col][j] /= dd;
+    for (int i = 0; i < n; i++) {
+      if (i == col) continue;
+      double f = W[i][col];
+      for (int j = 0; j < 2 * n; j++) W[i][j] -= f * W[col][j];
+    }
+  }
+  for (int i = 0; i < n; i++)
+    for (int j = 0; j < n; j++) Ainv[i * n + j] = W[i][n + j];
+}
+
+static void gram_values(int J, int U, int n, double* P) {
+  double c0 = 0.0, c1 = (double)(U - 2 * n), c2 = (double)U;
+  double d0 = c2, d1 = c1 + c1, d2 = d0;
+  P[0] = 1.0;
+  if (J >= 1) P[1] = c1 / (double)U;
+  for (int i = 1; i < J; i++) {
+    d0 += 2.0; d2 -= 2.0; c0 += d0; c1 += d1; c2 += d2;
+    P[i + 1] = (c1 * P[i] - c0 * P[i - 1]) / c2;
+  }
+}
+
+extern "C" int qcbc_het_setup(qcbc_event* ev, const double* pref, const int* fgrid, int M, int MN, int MM, int J) {
+  if (!ev || !pref || !fgrid) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->has_data) return fail(QCBC_EINVAL, "event has no data");
+  const int nI = ev->g.nifo, N = ev->g.N, nh = N / 2;
+  for (int i = 0; i < M; i++)
+    if (fgrid[i] < 1 || fgrid[i] >= nh || (i && fgrid[i] <= fgrid[i - 1]))
+      return fail(QCBC_EINVAL, "fgrid must increase strictly inside [1, N/2)");
+  if (MN < 1 || MM > nh || MN > MM) return fail(QCBC_EINVAL, "bad [MN, MM) = [%d, %d)", MN, MM);
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = het_alloc(ev, M, J, MN, MM))) return rc;
+  cudaStream_t s = w->stream;
+  DeviceState& ds = g_dev[current_device()];
+  // scratch: h [nifo][N], amp/phase [nifo][nh], RC/RS/AA [nifo][nh]
+  size_t nA = (size_t)nI * N + 5 * (size_t)nI * nh;
+  if ((rc = grow(w->d_a, w->c_a, nA))) return rc;
+  if ((rc = grow(w->d_params, w->c_params, 11))) return rc;
+  if ((rc = grow(w->d_recs, w->c_recs, 1))) return rc;
+  if ((rc = grow(w->d_status, w->c_status, 1))) return rc;
+  if ((rc = grow(w->d_b, w->c_b, (size_t)2 * kMaxIfo))) return rc;
+  double* d_h = w->d_a;
+  double* d_amp = d_h + (size_t)nI * N;
+  double* d_ph = d_amp + (size_t)nI * nh;
+  double* d_RC = d_ph + (size_t)nI * nh;
+  double* d_RS = d_RC + (size_t)nI * nh;
+  double* d_AA = d_RS + (size_t)nI * nh;
+  CU(cudaMemcpyAsync(w->d_params, pref, 11 * sizeof(double), cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(ev->het.d_fgrid, fgrid, (size_t)M * sizeof(int), cudaMemcpyHostToDevice, s));
+  // fulltemplates uses Tobs = 1/freq[1]; the canonical grid has freq[1] = 1/Tobs
+  NetGeom gt = ev->g;
+  gt.Tobs = 1.0 / (1.0 / ev->g.Tobs);
+  launch_fulltemplates(w->d_params, gt, ds.qnm, ev->d_freq, w->d_recs, w->d_status, d_h, s);
+  launch_fullphaseamp(w->d_params, ev->g, ds.qnm, ev->d_freq, nh, w->d_recs, w->d_status, d_amp, d_ph, s);
+  launch_het_bins(d_h, d_amp, d_ph, ev->d_D, ev->d_S, nh + 1, N, nI, d_RC, d_RS, d_AA, s);
+  HetData hd = het_data(ev);
+  launch_het_region_sums(d_RC, d_RS, d_AA, ev->het.d_fgrid, M, J, nI, nh, (double*)hd.SL, (double*)hd.lc,
+                         (double*)hd.ls, s);
+  launch_nwip_pairs(d_h, ev->d_D, ev->d_S, nh + 1, N, nI, MN, MM, w->d_b, s);
+  tls_launches += 8;
+  CU(cudaGetLastError());
+  // grid gathers and per-region small tables on the host (FP64)
+  std::vector<double> ampb((size_t)nI * nh), phb((size_t)nI * nh), RC((size_t)nI * nh), RS((size_t)nI * nh),
+      AA((size_t)nI * nh);
+  double pairs[2 * kMaxIfo];
+  CU(cudaMemcpyAsync(ampb.data(), d_amp, ampb.size() * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(phb.data(), d_ph, phb.size() * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(RC.data(), d_RC, RC.size() * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(RS.data(), d_RS, RS.size() * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(AA.data(), d_AA, AA.size() * 8, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(pairs, w->d_b, sizeof(double) * 2 * nI, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  HetDev& h = ev->het;
+  int NR = h.NR, J1 = J + 1;
+  std::vector<double> freq(M), amp((size_t)nI * M), ph((size_t)nI * M), IP((size_t)NR * J1 * J1), aa((size_t)nI * NR),
+      rcv((size_t)nI * NR), rsv((size_t)nI * NR);
+  for (int j = 0; j < M; j++) freq[j] = (double)fgrid[j] / ev->g.Tobs;
+  for (int id = 0; id < nI; id++)
+    for (int j = 0; j < M; j++) {
+      amp[(size_t)id * M + j] = ampb[(size_t)id * nh + fgrid[j]];
+      ph[(size_t)id * M + j] = phb[(size_t)id * nh + fgrid[j]];
+    }
+  for (int id = 0; id < nI; id++)
+    for (int r = 0; r < NR; r++) {
+      int k = fgrid[r * J];
+      rcv[(size_t)id * NR + r] = RC[(size_t)id * nh + k];
+      rsv[(size_t)id * NR + r] = RS[(size_t)id * nh + k];
+      aa[(size_t)id * NR + r] = AA[(size_t)id * nh + k];
+    }
+  for (int r = 0; r < NR; r++) {
+    int U = fgrid[(r + 1) * J] - fgrid[r * J];
+    double PP[16], inv[16], P[4];
+    for (int k = 0; k <= J; k++) {
+      gram_values(J, U, fgrid[r * J + k] - fgrid[r * J], P);
+      for (int a = 0; a <= J; a++) PP[a * J1 + k] = P[a];
+    }
+    invert_small(PP, inv, J1);
+    for (int a = 0; a <= J; a++)
+      for (int b = 0; b <= J; b++) IP[((size_t)r * J1 + a) * J1 + b] = inv[b * J1 + a];
+  }
+  double L = 0.0;
+  for (int id = 0; id < nI; id++) L += pairs[2 * id + 1] + 0.5 * pairs[2 * id];
+  h.logLb = L;
+  h.fgrid.assign(fgrid, fgrid + M);
+  CU(cudaMemcpy((void*)hd.freq, freq.data(), M * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.amp, amp.data(), amp.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.phase, ph.data(), ph.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.IP, IP.data(), IP.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.aa, aa.data(), aa.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.rc, rcv.data(), rcv.size() * 8, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy((void*)hd.rs, rsv.data(), rsv.size() * 8, cudaMemcpyHostToDevice));
+  return QCBC_OK;
+}
+
+static int enqueue_het(Workspace* w, qcbc_event* ev, const double* d_params, int B, double* d_lnl, int prec,
+                       cudaStream_t s, const NetGeom& g) {
+  int rc;
+  if ((rc = grow(w->d_recs, w->c_recs, (size_t)B))) return rc;
+  if ((rc = grow(w->d_status, w->c_status, (size_t)B))) return rc;
+  DeviceState& ds = g_dev[current_device()];
+  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s);
+  launch_lnl_het(w->d_recs, w->d_status, B, g, het_data(ev), prec == QCBC_MIXED ? kMixed : kFP64, 128, d_lnl, s);
+  tls_launches += 2;
+  CU(cudaGetLastError());
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double* lnl, int precision) {
+  if (!ev || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->het.buf) return fail(QCBC_EINVAL, "event has no heterodyne tables");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_params, w->c_params, (size_t)B * 11))) return rc;
+  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
+  if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * 11))) return rc;
+  if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
+  if ((rc = grow_host(w->h_status, w->ch_status, (size_t)B))) return rc;
+  memcpy(w->h_params, params, sizeof(double) * 11 * (size_t)B);
+  cudaStream_t s = w->stream;
+  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_het(w, ev, w->d_params, B, w->d_lnl, precision, s, ev->g))) return rc;
+  CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  memcpy(lnl, w->h_lnl, sizeof(double) * B);
+  int bad = 0;
+  for (int b = 0; b < B; b++) bad += w->h_status[b] != 0;
+  if (bad) return fail(QCBC_EDOM, "%d of %d parameter sets outside the waveform domain (lnL=-1e20)", bad, B);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, int precision,
+                                void* stream) {
+  if (!ev || !d_params || !d_lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->het.buf) return fail(QCBC_EINVAL, "event has no heterodyne tables");
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : w->stream;
+  return enqueue_het(w, ev, d_params, B, d_lnl, precision, s, ev->g);
+}
+
+// ------------------------------------------------------------------ device memory helpers
+extern "C" void* qcbc_device_alloc(long long bytes) {
+  if (ensure_init()) return nullptr;
+  void* p = nullptr;
+  if (cudaMalloc(&p, (size_t)bytes) != cudaSuccess) { fail(QCBC_ENOMEM, "cudaMalloc %lld", bytes); return nullptr; }
+  return p;
+}
+extern "C" int qcbc_device_free(void* p) { CU(cudaFree(p)); return QCBC_OK; }
+extern "C" int qcbc_memcpy_h2d(void* dst, const void* src, long long bytes) {
+  CU(cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyHostToDevice));
+  return QCBC_OK;
+}
+extern "C" int qcbc_memcpy_d2h(void* dst, const void* src, long long bytes) {
+  CU(cudaMemcpy(dst, src, (size_t)bytes, cudaMemcpyDeviceToHost));
+  return QCBC_OK;
+}
+extern "C" int qcbc_synchronize(void) { CU(cudaDeviceSynchronize()); return QCBC_OK; }
+
+// ------------------------------------------------------------------ timing helpers
+static int flush_l2(Workspace* w, cudaStream_t s) {
+  const size_t bytes = (size_t)512 << 20;   // 512 MiB > 126 MB L2
+  int rc = grow(w->d_flush, w->c_flush, bytes);
+  if (rc) return rc;
+  CU(cudaMemsetAsync(w->d_flush, 0x5a, bytes, s));
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_time_lnl_full(qcbc_event* ev, const double* d_params, int B, int precision, int iters,
+                                  int flush, float* ms, float* kernel_ms) {
+  if (!ev || !d_params || !ms || iters <= 0) return fail(QCBC_EINVAL, "bad argument");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
+  cudaStream_t s = w->stream;
+  for (int it = 0; it < iters; it++) {
+    if (flush && (rc = flush_l2(w, s))) return rc;
+    CU(cudaEventRecord(w->e0, s));
+    if ((rc = enqueue_full(w, ev, d_params, B, w->d_lnl, nullptr, precision, s, ev->g, w->e2, w->e3))) return rc;
+    CU(cudaEventRecord(w->e1, s));
+    CU(cudaEventSynchronize(w->e1));
+    CU(cudaEventElapsedTime(&ms[it], w->e0, w->e1));
+    if (kernel_ms) CU(cudaEventElapsedTime(&kernel_ms[it], w->e2, w->e3));
+  }
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_time_lnl_het(qcbc_event* ev, const double* d_params, int B, int precision, int iters, int flush,
+                                 float* ms) {
+  if (!ev || !d_params || !ms || iters <= 0) return fail(QCBC_EINVAL, "bad argument");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
+  cudaStream_t s = w->stream;
+  for (int it = 0; it < iters; it++) {
+    if (flush && (rc = flush_l2(w, s))) return rc;
+    CU(cudaEventRecord(w->e0, s));
+    if ((rc = enqueue_het(w, ev, d_params, B, w->d_lnl, precision, s, ev->g))) return rc;
+    CU(cudaEventRecord(w->e1, s));
+    CU(cudaEventSynchronize(w->e1));
+    CU(cudaEventElapsedTime(&ms[it], w->e0, w->e1));
+  }
+  return QCBC_OK;
+}
+
+// ================================================================== reference-signature drop-ins
+static double g_band_fmin = 16.0, g_band_fmax = 1024.0;   // ConstCBC.h:33-34
+
+extern "C" int qcbc_set_band(double fmin, double fmax) {
+  if (!(fmin >= 0.0) || !(fmax > fmin)) return fail(QCBC_EINVAL, "bad band");
+  g_band_fmin = fmin;
+  g_band_fmax = fmax;
+  return QCBC_OK;
+}
+
+struct BindKey {
+  const void *net, *D, *SN;
+  int N;
+  bool operator<(const BindKey& o) const {
+    if (net != o.net) return net < o.net;
+    if (D != o.D) return D < o.D;
+    if (SN != o.SN) return SN < o.SN;
+    return N < o.N;
+  }
+};
+static std::map<BindKey, qcbc_event*> g_bound;
+static std::mutex g_bind_mu;
+
+static qcbc_event* open_from_rows(struct Net* net, double** D, double** SN, int N, double Tobs) {
+  if (check_geom(net->Nifo, net->labels, Tobs, N)) return nullptr;
+  qcbc_event* ev = new qcbc_event();
+  ev->device = current_device();
+  ev->fmin = g_band_fmin;
+  ev->fmax = g_band_fmax;
+  fill_geom(ev->g, net->Nifo, net->labels, Tobs, net->GMST, N, g_band_fmin, g_band_fmax);
+  std::vector<const double*> Dr(net->Nifo), Sr(net->Nifo);
+  for (int i = 0; i < net->Nifo; i++) { Dr[i] = D[i]; Sr[i] = SN[i]; }
+  if (event_upload(ev, Dr.data(), Sr.data())) { event_free_device(ev); delete ev; return nullptr; }
+  return ev;
+}
+
+extern "C" int qcbc_bind_data(struct Net* net, double** D, double** SN, int N, double Tobs) {
+  if (!net || !D || !SN) return fail(QCBC_EINVAL, "NULL argument");
+  int rc = ensure_init();
+  if (rc) return rc;
+  BindKey k{net, D, SN, N};
+  std::lock_guard<std::mutex> lk(g_bind_mu);
+  auto it = g_bound.find(k);
+  if (it != g_bound.end()) { qcbc_event_close(it->second); g_bound.erase(it); }
+  qcbc_event* ev = open_from_rows(net, D, SN, N, Tobs);
+  if (!ev) return QCBC_ENOMEM;
+  g_bound[k] = ev;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_unbind_all(void) {
+  std::lock_guard<std::mutex> lk(g_bind_mu);
+  for (auto& kv : g_bound) qcbc_event_close(kv.second);
+  g_bound.clear();
+  return QCBC_OK;
+}
+
+// Upload a caller frequency vector into thread scratch (legacy paths read freq[i] like the reference).
+static int stage_freq(Workspace* w, const RealVector* freq, size_t n, double** d_out) {
+  if (!freq || !freq->data || freq->length < n) return fail(QCBC_EINVAL, "freq shorter than needed (%zu)", n);
+  int rc = grow(w->d_c, w->c_c, n);
+  if (rc) return rc;
+  CU(cudaMemcpyAsync(w->d_c, freq->data, n * sizeof(double), cudaMemcpyHostToDevice, w->stream));
+  *d_out = w->d_c;
+  return QCBC_OK;
+}
+
+extern "C" double log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
+                                      double* rho, int N, double Tobs) {
+  (void)freq;   // the grid is i/Tobs, exactly what QuickCBC.c:419-420 builds
+  if (!net || !D || !SN || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
+  if (ensure_init()) return -1.0e20;
+  qcbc_event* ev = nullptr;
+  bool temp = false;
+  {
+    std::lock_guard<std::mutex> lk(g_bind_mu);
+    auto it = g_bound.find(BindKey{net, D, SN, N});
+    if (it != g_bound.end()) ev = it->second;
+  }
+  if (!ev) {
+    ev = open_from_rows(net, D, SN, N, Tobs);
+    if (!ev) return -1.0e20;
+    temp = true;
+  }
+  NetGeom g = ev->g;
+  fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, ev->fmin, ev->fmax);
+  double lnl = -1.0e20, r[kMaxIfo];
+  int rc = run_full(ev, params, 1, &lnl, r, QCBC_FP64, g);
+  if (rho && rc == QCBC_OK)
+    for (int i = 0; i < net->Nifo; i++) rho[i] = r[i];
+  if (temp) qcbc_event_close(ev);
+  return rc == QCBC_OK ? lnl : -1.0e20;
+}
+
+struct HetCacheEntry {
+  qcbc_event* ev = nullptr;
+  const void* ip = nullptr;
+  int M = 0;
+  double logLb = 0.0;
+};
+static std::map<const void*, HetCacheEntry> g_het_cache;
+static std::mutex g_het_mu;
+
+static qcbc_event* het_event_for(struct Net* net, struct Het* het) {
+  std::lock_guard<std::mutex> lk(g_het_mu);
+  HetCacheEntry& e = g_het_cache[het];
+  if (e.ev && e.ip == (const void*)het->IP && e.M == het->M && e.logLb == het->logLb) return e.ev;
+  if (!e.ev) {
+    e.ev = new qcbc_event();
+    e.ev->device = current_device();
+  }
+  qcbc_event* ev = e.ev;
+  fill_geom(ev->g, net->Nifo, net->labels, net->Tobs, net->GMST, 2 * het->M, 0.0, 1.0);
+  int nI = net->Nifo, M = het->M, J = het->J, NR = het->NR, J1 = J + 1;
+  if (NR != (M - 1) / J) { fail(QCBC_EINVAL, "het NR inconsistent with M, J"); return nullptr; }
+  std::vector<double> amp((size_t)nI * M), ph((size_t)nI * M), IP((size_t)NR * J1 * J1), SL((size_t)NR * nI * J1),
+      lc(SL.size()), ls(SL.size()), aa((size_t)nI * NR), rcv(aa.size()), rsv(aa.size());
+  for (int id = 0; id < nI; id++)
+    for (int j = 0; j < M; j++) { amp[(size_t)id * M + j] = het->amp[id][j]; ph[(size_t)id * M + j] = het->phase[id][j]; }
+  for (int r = 0; r < NR; r++) {
+    for (int a = 0; a < J1; a++)
+      for (int b = 0; b < J1; b++) IP[((size_t)r * J1 + a) * J1 + b] = het->IP[r][a][b];
+    for (int id = 0; id < nI; id++)
+      for (int a = 0; a < J1; a++) {
+        size_t o = ((size_t)r * nI + id) * J1 + a;
+        SL[o] = het->SL[r][id][a]; lc[o] = het->lc[r][id][a]; ls[o] = het->ls[r][id][a];
+      }
+  }
+  for (int id = 0; id < nI; id++)
+    for (int r = 0; r < NR; r++) {
+      aa[(size_t)id * NR + r] = het->aa[id][r]; rcv[(size_t)id * NR + r] = het->rc[id][r];
+      rsv[(size_t)id * NR + r] = het->rs[id][r];
+    }
+  qcbc_het_tables t{M, het->MN, het->MM, J, NR, het->logLb, het->fgrid, het->freq->data, amp.data(), ph.data(),
+                    IP.data(), SL.data(), lc.data(), ls.data(), aa.data(), rcv.data(), rsv.data()};
+  if (qcbc_het_set(ev, &t) != QCBC_OK) return nullptr;
+  e.ip = het->IP;
+  e.M = het->M;
+  e.logLb = het->logLb;
+  return ev;
+}
+
+extern "C" double log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs) {
+  (void)Tobs;   // fullphaseamp inside the reference's het lnL uses net->Tobs (QuickCBC.c:3797)
+  if (!net || !het || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
+  if (ensure_init()) return -1.0e20;
+  qcbc_event* ev = het_event_for(net, het);
+  if (!ev) return -1.0e20;
+  double lnl = -1.0e20;
+  int rc = qcbc_lnl_het(ev, params, 1, &lnl, QCBC_FP64);
+  return rc == QCBC_OK ? lnl : -1.0e20;
+}
+
+// Allocation helpers with the reference's layout (Utilities.c:2941-3015): N+1 rows of M+1 entries.
+static double** alloc_matrix(int N, int M) {
+  double** m = (double**)malloc((size_t)(N + 1) * sizeof(double*));
+  for (int i = 0; i < N + 1; i++) m[i] = (double*)malloc((size_t)(M + 1) * sizeof(double));
+  return m;
+}
+static double*** alloc_tensor(int N, int M, int L) {
+  double*** t = (double***)malloc((size_t)(N + 1) * sizeof(double**));
+  for (int i = 0; i < N + 1; i++) t[i] = alloc_matrix(M, L);
+  return t;
+}
+
+extern "C" void heterodyne(struct Net* net, struct Het* het, double** D, double* params, RealVector* freq,
+                           double** SN, int N, double Tobs) {
+  (void)freq;
+  if (!net || !het || !D || !SN || !params || !het->fgrid) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  if (ensure_init()) return;
+  qcbc_event* ev = open_from_rows(net, D, SN, N, Tobs);
+  if (!ev) return;
+  int M = het->M, J = het->J, NR = het->NR, nI = net->Nifo, J1 = J + 1;
+  if (qcbc_het_setup(ev, params, het->fgrid, M, het->MN, het->MM, J) != QCBC_OK) { qcbc_event_close(ev); return; }
+  std::vector<double> fr(M), amp((size_t)nI * M), ph((size_t)nI * M), IP((size_t)NR * J1 * J1),
+      SL((size_t)NR * nI * J1), lc(SL.size()), ls(SL.size()), aa((size_t)nI * NR), rcv(aa.size()), rsv(aa.size());
+  double logLb = 0.0;
+  qcbc_het_export(ev, nullptr, fr.data(), amp.data(), ph.data(), IP.data(), SL.data(), lc.data(), ls.data(), aa.data(),
+                  rcv.data(), rsv.data(), &logLb);
+  qcbc_event_close(ev);
+  het->IP = alloc_tensor(NR, J + 1, J + 1);
+  het->SL = alloc_tensor(NR, nI, J + 1);
+  het->amp = alloc_matrix(nI, M);
+  het->phase = alloc_matrix(nI, M);
+  het->rc = alloc_matrix(nI, NR);
+  het->rs = alloc_matrix(nI, NR);
+  het->aa = alloc_matrix(nI, NR);
+  het->lc = alloc_tensor(NR, nI, J + 1);
+  het->ls = alloc_tensor(NR, nI, J + 1);
+  het->pref = (double*)malloc(12 * sizeof(double));
+  for (int k = 0; k < 11; k++) het->pref[k] = params[k];
+  for (int id = 0; id < nI; id++)
+    for (int j = 0; j < M; j++) { het->amp[id][j] = amp[(size_t)id * M + j]; het->phase[id][j] = ph[(size_t)id * M + j]; }
+  for (int r = 0; r < NR; r++) {
+    for (int a = 0; a < J1; a++)
+      for (int b = 0; b < J1; b++) het->IP[r][a][b] = IP[((size_t)r * J1 + a) * J1 + b];
+    for (int id = 0; id < nI; id++)
+      for (int a = 0; a < J1; a++) {
+        size_t o = ((size_t)r * nI + id) * J1 + a;
+        het->SL[r][id][a] = SL[o]; het->lc[r][id][a] = lc[o]; het->ls[r][id][a] = ls[o];
+      }
+  }
+  for (int id = 0; id < nI; id++)
+    for (int r = 0; r < NR; r++) {
+      het->aa[id][r] = aa[(size_t)id * NR + r]; het->rc[id][r] = rcv[(size_t)id * NR + r];
+      het->rs[id][r] = rsv[(size_t)id * NR + r];
+    }
+  het->logLb = logLb;
+}
+
+extern "C" void fulltemplates(struct Net* net, double** hwave, RealVector* freq, double* params, int N) {
+  if (!net || !hwave || !freq || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  Workspace* w;
+  if (workspace(w)) return;
+  if (check_geom(net->Nifo, net->labels, 1.0, N)) return;
+  cudaStream_t s = w->stream;
+  double* d_freq;
+  if (stage_freq(w, freq, (size_t)N / 2, &d_freq)) return;
+  double Tobs = 1.0 / freq->data[1];   // QuickCBC.c:3703
+  NetGeom g;
+  fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, 0.0, 1.0);
+  int nI = net->Nifo;
+  if (grow(w->d_a, w->c_a, (size_t)nI * N) || grow(w->d_params, w->c_params, 11) || grow(w->d_recs, w->c_recs, 1) ||
+      grow(w->d_status, w->c_status, 1) || grow_host(w->h_a, w->ch_a, (size_t)nI * N))
+    return;
+  if (cudaMemcpyAsync(w->d_params, params, 11 * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return;
+  DeviceState& ds = g_dev[current_device()];
+  launch_fulltemplates(w->d_params, g, ds.qnm, d_freq, w->d_recs, w->d_status, w->d_a, s);
+  tls_launches += 2;
+  cudaMemcpyAsync(w->h_a, w->d_a, sizeof(double) * nI * N, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "fulltemplates failed"); return; }
+  for (int id = 0; id < nI; id++) memcpy(hwave[id], w->h_a + (size_t)id * N, sizeof(double) * N);
+}
+
+extern "C" void fullphaseamp(struct Net* net, double** amp, double** phase, RealVector* freq, double* params, int N) {
+  if (!net || !amp || !phase || !freq || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  Workspace* w;
+  if (workspace(w)) return;
+  if (check_geom(net->Nifo, net->labels, net->Tobs, N)) return;
+  cudaStream_t s = w->stream;
+  int n = N / 2, nI = net->Nifo;
+  double* d_freq;
+  if (stage_freq(w, freq, (size_t)n, &d_freq)) return;
+  NetGeom g;
+  fill_geom(g, nI, net->labels, net->Tobs, net->GMST, N, 0.0, 1.0);
+  if (grow(w->d_a, w->c_a, (size_t)2 * nI * n) || grow(w->d_params, w->c_params, 11) || grow(w->d_recs, w->c_recs, 1) ||
+      grow(w->d_status, w->c_status, 1) || grow_host(w->h_a, w->ch_a, (size_t)2 * nI * n))
+    return;
+  cudaMemcpyAsync(w->d_params, params, 11 * sizeof(double), cudaMemcpyHostToDevice, s);
+  DeviceState& ds = g_dev[current_device()];
+  launch_fullphaseamp(w->d_params, g, ds.qnm, d_freq, n, w->d_recs, w->d_status, w->d_a, w->d_a + (size_t)nI * n, s);
+  tls_launches += 2;
+  cudaMemcpyAsync(w->h_a, w->d_a, sizeof(double) * 2 * nI * n, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "fullphaseamp failed"); return; }
+  for (int id = 0; id < nI; id++) {
+    memcpy(amp[id], w->h_a + (size_t)id * n, sizeof(double) * n);
+    memcpy(phase[id], w->h_a + (size_t)(nI + id) * n, sizeof(double) * n);
+  }
+}
+
+extern "C" int IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, const double phi0,
+                                               const double fRef_in, const double m1_SI, const double m2_SI,
+                                               const double chi1, const double chi2, const double distance) {
+  const int PD_EFAULT = 14, PD_EDOM = 33;
+  if (!h22 || *h22 || !freq || !freq->data || freq->length == 0) { fail(QCBC_EINVAL, "bad pointers"); return PD_EFAULT; }
+  double m1 = m1_SI / kMsun, m2 = m2_SI / kMsun;
+  size_t n = freq->length;
+  double fmin_ = freq->data[0];
+  if (fRef_in < 0 || m1 <= 0 || m2 <= 0 || fmin_ <= 0 || distance <= 0 || chi1 > 1.0 || chi1 < -1.0 || chi2 > 1.0 ||
+      chi2 < -1.0) {
+    fail(QCBC_EDOM, "IMRPhenomD input outside its domain");
+    return PD_EDOM;
+  }
+  double fCut = kFcut / ((m1 + m2) * kMtsun);
+  if (fCut <= fmin_) { fail(QCBC_EDOM, "fCut %g <= f_min %g", fCut, fmin_); return PD_EDOM; }
+  double fRef = (fRef_in == 0.0) ? fmin_ : fRef_in;
+  Workspace* w;
+  if (workspace(w)) return PD_EFAULT;
+  cudaStream_t s = w->stream;
+  double* d_freq;
+  if (stage_freq(w, freq, n, &d_freq)) return PD_EFAULT;
+  if (grow(w->d_a, w->c_a, 2 * n) || grow(w->d_recs, w->c_recs, 1) || grow(w->d_status, w->c_status, 1) ||
+      grow_host(w->h_a, w->ch_a, 2 * n) || grow_host(w->h_status, w->ch_status, 1))
+    return PD_EFAULT;
+  DeviceState& ds = g_dev[current_device()];
+  launch_amp_phase(d_freq, (int)n, phi0, fRef, m1, m2, chi1, chi2, distance, ds.qnm, w->d_recs, w->d_a, w->d_a + n,
+                   w->d_status, s);
+  tls_launches += 2;
+  cudaMemcpyAsync(w->h_a, w->d_a, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "amp/phase failed"); return PD_EFAULT; }
+  if (w->h_status[0] != 0) { fail(QCBC_EDOM, "IMRPhenomD input outside its domain"); return PD_EDOM; }
+  AmpPhaseFDWaveform* wf = (AmpPhaseFDWaveform*)malloc(sizeof(AmpPhaseFDWaveform));
+  wf->length = n;
+  wf->freq = (double*)malloc(sizeof(double) * n);
+  wf->amp = (double*)malloc(sizeof(double) * n);
+  wf->phase = (double*)malloc(sizeof(double) * n);
+  memcpy(wf->freq, freq->data, sizeof(double) * n);
+  memcpy(wf->amp, w->h_a, sizeof(double) * n);
+  memcpy(wf->phase, w->h_a + n, sizeof(double) * n);
+  *h22 = wf;
+  return 0;
+}
+
+extern "C" double fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N) {
+  if (!a || !b || !Sn) { fail(QCBC_EINVAL, "NULL argument"); return 0.0; }
+  if (imin >= imax) return 0.0;
+  if (imin < 1 || imax > N / 2 + 1 || N - imax + 1 < 0) { fail(QCBC_EINVAL, "bad band"); return 0.0; }
+  Workspace* w;
+  if (workspace(w)) return 0.0;
+  cudaStream_t s = w->stream;
+  if (grow(w->d_a, w->c_a, (size_t)2 * N + imax + 1) || grow(w->d_b, w->c_b, 2 * kMaxIfo)) return 0.0;
+  double* d_x = w->d_a;
+  double* d_y = d_x + N;
+  double* d_s = d_y + N;
+  cudaMemcpyAsync(d_x, a, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_y, b, sizeof(double) * N, cudaMemcpyHostToDevice, s);
+  cudaMemcpyAsync(d_s, Sn, sizeof(double) * imax, cudaMemcpyHostToDevice, s);
+  launch_nwip(d_x, d_y, d_s, imin, imax, N, w->d_b, s);
+  tls_launches += 1;
+  double out = 0.0;
+  cudaMemcpyAsync(&out, w->d_b, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "fourier_nwip failed"); return 0.0; }
+  return out;
+}

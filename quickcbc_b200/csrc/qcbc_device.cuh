@@ -1,0 +1,225 @@
+// Device-side IMRPhenomD and detector projection for the QuickCBC likelihood.
+//
+// Layout of the work: everything that depends only on one parameter set is
+// computed once, in FP64, by qcbc_setup_record() into a PhdRec (about 80
+// doubles).  The per-bin evaluators then read the record from shared memory.
+//
+// Reference behaviour restated here (QuickCBC, file:line):
+//   parameter mapping and projection        QuickCBC.c:3698-3771 (fulltemplates)
+//                                          QuickCBC.c:3795-3866 (fullphaseamp)
+//   IMRPhenomD setup                        IMRPhenomD.c:413-503
+//   phenomenological fits (Table V)         IMRPhenomD_internals.c:537-1399
+//   amplitude / phase evaluators            IMRPhenomD_internals.c:594-604, 715-726,
+//                                           1107-1134, 1222-1240, 1299-1310, 1399-1425,
+//                                           1590-1617
+//   antenna patterns and geocentre delays   Utilities.c:995-1109
+//   start frequency                         Utilities.c:587-629 (fbegin)
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace qcbc {
+
+// ---- constants (IMRPhenomD_internals.h:106-136, Constants.h, ConstCBC.h) ----
+constexpr double kPi = 3.141592653589793238462643383279502884;
+constexpr double kPi4 = 0.785398163397448309615660845819875721;
+constexpr double kGammaE = 0.577215664901532860606512090082402431;
+constexpr double kMsun = 1.988546954961461467461011951140572744e30;
+constexpr double kMtsun = 4.925491025543575903411922162094833998e-6;
+constexpr double kMrsun = 1.476625061404649406193430731479084713e3;
+constexpr double kTsunCBC = 4.92569043916e-6;       // fbegin uses the QuickCBC value
+constexpr double kTwoPi = 6.2831853071795862319959269370884;
+constexpr double kClight = 299792458.0;
+constexpr double kH22fac = 0.31539156525252;
+constexpr double kFref = 100.0;
+constexpr double kFcut = 0.2;
+constexpr double kAmpJoin = 0.014;
+constexpr double kPhiJoin = 0.018;
+constexpr int kMaxIfo = 3;
+
+// Record flags
+constexpr int kRecValid = 1;
+
+struct PhdRec {
+  // dimensional scales
+  double Msec, fCut, amp_scale, eta, inv_eta;
+  double fRD, fDM, fmax;
+  // amplitude
+  double a0;           // amp0Func(eta)
+  double ai[8];        // inspiral prefactors of Mf^{2/3}, Mf, 4/3, 5/3, 2, 7/3, 8/3, 3
+  double g1, g2, g3;   // merger-ringdown
+  double hx1, hx2, hx3, hc[5];   // intermediate amplitude, Newton form
+  // phase
+  double pq[13];       // inspiral phase prefactors
+  double b1, b2, b3, al1, al2, al3, al4, al5;
+  double C1Int, C2Int, C1MRD, C2MRD, fMRDJoin;
+  double t0, MfRef, phi_pre, pi_third;
+  // projection
+  double fs, ts, sqT;
+  double Fs[kMaxIfo], lam[kMaxIfo], td[kMaxIfo];
+  int i_lo, i_hi;      // bins with f > fbegin and f <= fCut (inclusive), clamped to the band
+  int flags, pad;
+};
+
+// Table V of arXiv:1508.07253: lambda = l00 + l10 eta + (l01 + l11 eta + l21 eta^2) xi
+//   + (l02 + l12 eta + l22 eta^2) xi^2 + (l03 + l13 eta + l23 eta^2) xi^3, xi = chiPN - 1.
+enum FitId { F_RHO1, F_RHO2, F_RHO3, F_GAM1, F_GAM2, F_GAM3, F_V2, F_AL1, F_AL2, F_AL3, F_AL4, F_AL5,
+             F_BE1, F_BE2, F_BE3, F_SI1, F_SI2, F_SI3, F_SI4, F_COUNT };
+
+// antenna monomials: coefficient + exponents of cos psi, sin psi, cos delta, sin delta,
+// cos(alpha-GMST), sin(alpha-GMST); F+ 21 terms, Fx 18 terms per detector.  The tables
+// themselves (and the fit table) live in qcbc_kernels.cu's constant memory.
+struct Mono { double c; unsigned char e[8]; };
+
+// QNM spline table (natural cubic spline over final spin), device global:
+// x[n], fring[n], fring''[n], fdamp[n], fdamp''[n]
+struct QnmTable { const double *x, *yr, *mr, *yd, *md; int n; };
+
+struct Pow6 { double sixth, third, two_thirds, four_thirds, five_thirds, two, seven_thirds, eight_thirds; };
+
+// Powers of x from one x^{1/6} (IMRPhenomD_internals.c:515-533).
+__device__ __forceinline__ Pow6 pow6(double x) {
+  Pow6 p;
+  if (x < 0.0) x = 1.0e-10;
+  p.sixth = pow(x, 1.0 / 6.0);
+  p.third = p.sixth * p.sixth;
+  p.two_thirds = x / p.third;
+  p.four_thirds = x * p.third;
+  p.five_thirds = p.four_thirds * p.third;
+  p.two = x * x;
+  p.seven_thirds = p.third * p.two;
+  p.eight_thirds = p.two_thirds * p.two;
+  return p;
+}
+
+__device__ __forceinline__ double qnm_eval(const QnmTable& t, const double* y, const double* m2, double s) {
+  int lo = 0, hi = t.n - 1;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    if (__ldg(t.x + mid) > s) hi = mid; else lo = mid;
+  }
+  double xl = __ldg(t.x + lo), h = __ldg(t.x + lo + 1) - xl, dx = s - xl;
+  double Ml = __ldg(m2 + lo), Mr = __ldg(m2 + lo + 1), yl = __ldg(y + lo);
+  double b = (__ldg(y + lo + 1) - yl) / h - h * (2.0 * Ml + Mr) / 6.0;
+  return yl + dx * (b + dx * (0.5 * Ml + dx * (Mr - Ml) / (6.0 * h)));
+}
+
+// ------------------------------------------------------------- amplitude
+__device__ __forceinline__ double amp_mrd(const PhdRec& c, double f) {
+  double fg = c.fDM * c.g3, df = f - c.fRD;
+  return exp(-df * c.g2 / fg) * (fg * c.g1) / (df * df + fg * fg);
+}
+__device__ __forceinline__ double amp_ins(const PhdRec& c, double Mf, const Pow6& p) {
+  return 1.0 + p.two_thirds * c.ai[0] + Mf * c.ai[1] + p.four_thirds * c.ai[2] + p.five_thirds * c.ai[3] +
+         p.two * c.ai[4] + p.seven_thirds * c.ai[5] + p.eight_thirds * c.ai[6] + Mf * p.two * c.ai[7];
+}
+__device__ __forceinline__ double amp_int(const PhdRec& c, double Mf) {
+  double x = Mf - c.hx1;
+  return c.hc[0] + x * (c.hc[1] + x * (c.hc[2] + (Mf - c.hx2) * (c.hc[3] + (Mf - c.hx3) * c.hc[4])));
+}
+
+// ------------------------------------------------------------- phase pieces
+__device__ __forceinline__ double phi_ins(const PhdRec& c, double Mf, const Pow6& p) {
+  double v = p.third * c.pi_third, logv = log(v);
+  const double* q = c.pq;
+  double ph = q[0];
+  ph += q[1] * p.two_thirds;
+  ph += q[2] * p.third;
+  ph += q[3] * logv * p.third;
+  ph += q[4] * logv;
+  ph += q[5] / p.third;
+  ph += q[6] / p.two_thirds;
+  ph += q[7] / Mf;
+  ph += q[8] / p.five_thirds;
+  ph += (q[9] * Mf + q[10] * p.four_thirds + q[11] * p.five_thirds + q[12] * p.two) / c.eta;
+  return ph;
+}
+__device__ __forceinline__ double phi_int(const PhdRec& c, double f) {
+  return c.b1 * f - c.b3 / (3. * f * f * f) + c.b2 * log(f);
+}
+__device__ __forceinline__ double dphi_int(const PhdRec& c, double f) {
+  return (c.b1 + c.b3 / (f * f * f * f) + c.b2 / f) / c.eta;
+}
+__device__ __forceinline__ double phi_mrd(const PhdRec& c, double f) {
+  double sq = sqrt(f), f34 = sqrt(f * sq);
+  return -(c.al2 / f) + (4.0 / 3.0) * (c.al3 * f34) + c.al1 * f + c.al4 * atan((f - c.al5 * c.fRD) / c.fDM);
+}
+__device__ __forceinline__ double dphi_mrd(const PhdRec& c, double f) {
+  double x = f - c.al5 * c.fRD;
+  return (c.al1 + c.al2 / (f * f) + c.al3 / pow(f, 0.25) + c.al4 / (c.fDM * (1 + x * x / (c.fDM * c.fDM)))) / c.eta;
+}
+
+// FP64 amplitude (without amp_scale) and phase (with the fRef shift) at geometric frequency Mf.
+__device__ __forceinline__ void phd_eval64(const PhdRec& c, double Mf, double& amp, double& phase) {
+  Pow6 p = pow6(Mf);
+  double pre = c.a0 / (Mf * p.sixth);
+  if (Mf < kAmpJoin) amp = pre * amp_ins(c, Mf, p);
+  else if (Mf >= c.fmax) amp = pre * amp_mrd(c, Mf);
+  else amp = pre * amp_int(c, Mf);
+  double ph;
+  if (Mf < kPhiJoin) ph = phi_ins(c, Mf, p);
+  else if (Mf >= c.fMRDJoin) ph = phi_mrd(c, Mf) * c.inv_eta + c.C1MRD + c.C2MRD * Mf;
+  else ph = phi_int(c, Mf) * c.inv_eta + c.C1Int + c.C2Int * Mf;
+  phase = ph - (c.t0 * (Mf - c.MfRef) + c.phi_pre);
+}
+
+// Mixed precision: phase in FP64 (its magnitude reaches 1e4-1e6 rad), the
+// amplitude in FP32.  Mf^{-1/3} comes from an FP32 seed refined by two FP64
+// Newton steps r <- r (4 - x r^3)/3 (quadratic convergence: 1e-7 -> 1e-14 -> 1e-16).
+__device__ __forceinline__ void phd_eval_mixed(const PhdRec& c, double Mf, float& amp, double& phase) {
+  float mff = (float)Mf;
+  double r = (double)(1.0f / cbrtf(mff));
+  r = r * (4.0 - Mf * r * r * r) * (1.0 / 3.0);
+  r = r * (4.0 - Mf * r * r * r) * (1.0 / 3.0);
+  double r2 = r * r;                       // Mf^{-2/3}
+  double third = Mf * r2;                  // Mf^{1/3}
+  // amplitude, FP32
+  float rf = (float)r, thf = (float)third;
+  float sixth_inv = sqrtf(rf);             // Mf^{-1/6}
+  float pre = (float)c.a0 * rf * rf * rf * sixth_inv;   // a0 Mf^{-7/6}
+  float a;
+  if (Mf < kAmpJoin) {
+    float t2 = thf * thf, m = mff;
+    float p43 = m * thf, p53 = p43 * thf, p2 = m * m, p73 = thf * p2, p83 = t2 * p2;
+    a = 1.0f + t2 * (float)c.ai[0] + m * (float)c.ai[1] + p43 * (float)c.ai[2] + p53 * (float)c.ai[3] +
+        p2 * (float)c.ai[4] + p73 * (float)c.ai[5] + p83 * (float)c.ai[6] + m * p2 * (float)c.ai[7];
+  } else if (Mf >= c.fmax) {
+    float fg = (float)(c.fDM * c.g3), df = (float)(Mf - c.fRD);
+    a = __expf(-df * (float)c.g2 / fg) * (fg * (float)c.g1) / (df * df + fg * fg);
+  } else {
+    float x = (float)(Mf - c.hx1), x2 = (float)(Mf - c.hx2), x3 = (float)(Mf - c.hx3);
+    a = (float)c.hc[0] + x * ((float)c.hc[1] + x * ((float)c.hc[2] + x2 * ((float)c.hc[3] + x3 * (float)c.hc[4])));
+  }
+  amp = pre * a;
+  // phase, FP64
+  double ph;
+  if (Mf < kPhiJoin) {
+    const double* q = c.pq;
+    double logv = log(third * c.pi_third);
+    double r3 = r2 * r, r5 = r3 * r2;
+    ph = q[0] + q[1] * (third * third) + q[2] * third + q[3] * logv * third + q[4] * logv + q[5] * r + q[6] * r2 +
+         q[7] * r3 + q[8] * r5;
+    double p43 = Mf * third, p53 = p43 * third;
+    ph += (q[9] * Mf + q[10] * p43 + q[11] * p53 + q[12] * Mf * Mf) * c.inv_eta;
+  } else if (Mf >= c.fMRDJoin) {
+    double sq = sqrt(Mf), f34 = sqrt(Mf * sq);
+    double at = (double)atanf((float)((Mf - c.al5 * c.fRD) / c.fDM));
+    ph = (-(c.al2 / Mf) + (4.0 / 3.0) * (c.al3 * f34) + c.al1 * Mf + c.al4 * at) * c.inv_eta + c.C1MRD + c.C2MRD * Mf;
+  } else {
+    // b3/(3 Mf^3) with r^9 = Mf^{-3}; the beta2 log term reaches ~1e2 rad, so FP64 log
+    ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r2 * r2 * r2 * r2 * r + c.b2 * log(Mf)) * c.inv_eta + c.C1Int + c.C2Int * Mf;
+  }
+  phase = ph - (c.t0 * (Mf - c.MfRef) + c.phi_pre);
+}
+
+// Reduce x to [-pi, pi] in FP64 with a two-constant 2 pi (|x| < 1e9 keeps it exact to ~1e-15).
+__device__ __forceinline__ double reduce_2pi(double x) {
+  constexpr double kInv2Pi = 0.15915494309189533577;
+  constexpr double kHi = 6.28318530717958623200;      // 2 pi rounded to double
+  constexpr double kLo = 2.4492935982947064e-16;      // 2 pi - kHi
+  double k = rint(x * kInv2Pi);
+  double r = fma(-k, kHi, x);
+  return fma(-k, kLo, r);
+}
+
+}  // namespace qcbc

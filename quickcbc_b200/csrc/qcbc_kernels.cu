@@ -1,0 +1,953 @@
+// CUDA kernels of the QuickCBC likelihood hot path (sm_100a).
+//
+//   k_setup          one thread per parameter set: IMRPhenomD coefficients,
+//                    start/cut-off bins and detector response, all FP64.
+//   k_lnl_full<P>    fused waveform -> projection -> PSD-weighted inner
+//                    products over one tile of bins of one parameter set; no
+//                    h(f) is written to memory.  P = FP64 or mixed.
+//   k_finalize_full  fixed-order sum of the tile partials -> lnL, rho.
+//   k_lnl_het<P>     heterodyned likelihood, one block per parameter set.
+//   waveform kernels for the reference-signature entry points and the FP64
+//   heterodyne setup sums.
+//
+// Reference algorithm: QuickCBC.c:3683-3869 (templates), 4236-4273 (full
+// lnL), 5112-5299 (heterodyne), 5303-5444 (heterodyned lnL); Utilities.c
+// :587-629, 716-736, 995-1109; IMRPhenomD.c:413-563.
+#include "qcbc_kernels.cuh"
+#include <cstdio>
+
+namespace qcbc {
+
+// ---------------------------------------------------------------- tables
+__constant__ double c_fits[F_COUNT][11] = {
+  {3931.8979897196696, -17395.758706812805, 3132.375545898835, 343965.86092361377, -1216256.5819981997, -70698.00600428853, 1383907.177859705, -3966276.1890979446, -60017.52423652596, 803515.1181825735, -2091710.365941658},
+  {-40105.47653771657, 112253.0169706701, 23561.696065836168, -3476180.699403351, 11375936.70849482, 754313.1127166454, -13084760.44625268, 36444584.853928134, 596226.612472288, -7427790.1143564405, 18928977.514040343},
+  {83208.35471266537, -191237.7264145924, -210916.2454782992, 8717975.08352568, -26914942.420669552, -1988980.6527362722, 30888029.960154563, -83908702.79256162, -1453503.1953446497, 17063528.990822166, -42748659.731120914},
+  {0.006927402739328343, 0.03020474290328911, 0.006308024337706171, -0.12074130661131138, 0.26271598905781324, 0.0034151773647198794, -0.10779338611188374, 0.27098966966891747, 0.0007374185938559283, -0.02749621038376281, 0.0733150789135702},
+  {1.010344404799477, 0.0008993122007234548, 0.283949116804459, -4.049752962958005, 13.207828172665366, 0.10396278486805426, -7.025059158961947, 24.784892370130475, 0.03093202475605892, -2.6924023896851663, 9.609374464684983},
+  {1.3081615607036106, -0.005537729694807678, -0.06782917938621007, -0.6689834970767117, 3.403147966134083, -0.05296577374411866, -0.9923793203111362, 4.820681208409587, -0.006134139870393713, -0.38429253308696365, 1.7561754421985984},
+  {0.8149838730507785, 2.5747553517454658, 1.1610198035496786, -2.3627771785551537, 6.771038707057573, 0.7570782938606834, -2.7256896890432474, 7.1140380397149965, 0.1766934149293479, -0.7978690983168183, 2.1162391502005153},
+  {43.31514709695348, 638.6332679188081, -32.85768747216059, 2415.8938269370315, -5766.875169379177, -61.85459307173841, 2953.967762459948, -8986.29057591497, -21.571435779762044, 981.2158224673428, -3239.5664895930286},
+  {-0.07020209449091723, -0.16269798450687084, -0.1872514685185499, 1.138313650449945, -2.8334196304430046, -0.17137955686840617, 1.7197549338119527, -4.539717148261272, -0.049983437357548705, 0.6062072055948309, -1.682769616644546},
+  {9.5988072383479, -397.05438595557433, 16.202126189517813, -1574.8286986717037, 3600.3410843831093, 27.092429659075467, -1786.482357315139, 5152.919378666511, 11.175710130033895, -577.7999423177481, 1808.730762932043},
+  {-0.02989487384493607, 1.4022106448583738, -0.07356049468633846, 0.8337006542278661, 0.2240008282397391, -0.055202870001177226, 0.5667186343606578, 0.7186931973380503, -0.015507437354325743, 0.15750322779277187, 0.21076815715176228},
+  {0.9974408278363099, -0.007884449714907203, -0.059046901195591035, 1.3958712396764088, -4.516631601676276, -0.05585343136869692, 1.7516580039343603, -5.990208965347804, -0.017945336522161195, 0.5965097794825992, -2.0608879367971804},
+  {97.89747327985583, -42.659730877489224, 153.48421037904913, -1417.0620760768954, 2752.8614143665027, 138.7406469558649, -1433.6585075135881, 2857.7418952430758, 41.025109467376126, -423.680737974639, 850.3594335657173},
+  {-3.282701958759534, -9.051384468245866, -12.415449742258042, 55.4716447709787, -106.05109938966335, -11.953044553690658, 76.80704618365418, -155.33172948098394, -3.4129261592393263, 25.572377569952536, -54.408036707740465},
+  {-2.5156429818799565e-05, 1.9750256942201327e-05, -1.8370671469295915e-05, 2.1886317041311973e-05, 8.250240316860033e-05, 7.157371250566708e-06, -5.5780000112270685e-05, 0.00019142082884072178, 5.447166261464217e-06, -3.220610095021982e-05, 7.974016714984341e-05},
+  {2096.551999295543, 1463.7493168261553, 1312.5493286098522, 18307.330017082117, -43534.1440746107, -833.2889543511114, 32047.31997183187, -108609.45037520859, 452.25136398112204, 8353.439546391714, -44531.3250037322},
+  {-10114.056472621156, -44631.01109458185, -6541.308761668722, -266959.23419307504, 686328.3229317984, 3405.6372187679685, -437507.7208209015, 1631817.1307344697, -7462.648563007646, -114585.25177153319, 674402.4689098676},
+  {22933.658273436497, 230960.00814979506, 14961.083974183695, 1194018.1342318142, -3104223.9693052764, -3038.166617199259, 1872032.2849093592, -7309145.012085539, 42738.22871475411, 467502.018616601, -3064853.498512499},
+  {-14621.71522218357, -377812.8579387104, -9608.682631509726, -1710892.5257214056, 4332924.601416521, -22366.683262266528, -2501971.6386377467, 10274495.902259542, -85360.30079034246, -570025.3441737515, 4396844.346849777},
+};
+
+// F+ / Fx of H1, L1, V1 as polynomials with the reference's rounded coefficients
+// (Utilities.c:1004-1076).  Exponents: cos psi, sin psi, cos delta, sin delta,
+// cos(alpha-GMST), sin(alpha-GMST).
+__constant__ Mono c_antp[3][21] = {
+  {{0.3104536562,{2,0,0,0,1,1}},{0.494778091,{0,0,1,1,1,0}},{1.424276331,{2,0,0,2,2,0}},{-0.4559956644,{0,0,1,1,0,1}},
+   {-0.1552268274,{0,0,0,2,1,1}},{0.3104536562,{1,1,0,1,0,0}},{-0.1552268276,{0,0,0,0,1,1}},{-0.4928680677,{2,0,0,2,0,0}},
+   {1.424276334,{2,0,0,0,2,0}},{0.3104536558,{2,0,0,2,1,1}},{-0.9119913289,{1,1,1,0,1,0}},{-0.9314082637,{2,0,0,0,0,0}},
+   {-0.712138166,{0,0,0,0,2,0}},{0.9119913288,{2,0,1,1,0,1}},{-0.6209073089,{1,1,0,1,2,0}},{2.848552667,{1,1,0,1,1,1}},
+   {-0.9895561804,{2,0,1,1,1,0}},{0.2464340337,{0,0,0,2,0,0}},{-0.9895561811,{1,1,1,0,0,1}},{-0.7121381653,{0,0,0,2,2,0}},
+   {0.4657041323,{0,0,0,0,0,0}}},
+  {{-0.5608410611,{2,0,0,0,1,1}},{-0.4945891833,{0,0,1,1,1,0}},{-1.040573095,{2,0,0,2,2,0}},{0.363231261,{0,0,1,1,0,1}},
+   {0.2804205304,{0,0,0,2,1,1}},{-0.5608410611,{1,1,0,1,0,0}},{0.2804205305,{0,0,0,0,1,1}},{-0.3865389475,{2,0,0,2,0,0}},
+   {-1.040573095,{2,0,0,0,2,0}},{-0.5608410611,{2,0,0,2,1,1}},{0.7264625218,{1,1,1,0,1,0}},{-0.7135560209,{0,0,0,0,0,0}},
+   {1.427112041,{2,0,0,0,0,0}},{0.5202865467,{0,0,0,0,2,0}},{-0.7264625224,{2,0,1,1,0,1}},{1.121682123,{1,1,0,1,2,0}},
+   {-2.081146187,{1,1,0,1,1,1}},{0.9891783667,{2,0,1,1,1,0}},{0.1932694762,{0,0,0,2,0,0}},{0.9891783666,{1,1,1,0,0,1}},
+   {0.5202865474,{0,0,0,2,2,0}}},
+  {{0.3963351156,{2,0,0,0,1,1}},{0.465152434,{0,0,1,1,1,0}},{-1.383399753,{2,0,0,2,2,0}},{-0.3756662059,{0,0,1,1,0,1}},
+   {-0.1981675579,{0,0,0,2,1,1}},{0.3963351153,{1,1,0,1,0,0}},{-0.1981675578,{0,0,0,0,1,1}},{1.303555289,{2,0,0,2,0,0}},
+   {-1.383399752,{2,0,0,0,2,0}},{-0.039922232,{0,0,0,0,0,0}},{0.3963351158,{2,0,0,2,1,1}},{-0.7513324118,{1,1,1,0,1,0}},
+   {0.0798444642,{2,0,0,0,0,0}},{0.6916998761,{0,0,0,0,2,0}},{0.7513324118,{2,0,1,1,0,1}},{-0.792670233,{1,1,0,1,2,0}},
+   {-2.766799504,{1,1,0,1,1,1}},{-0.9303048681,{2,0,1,1,1,0}},{-0.6517776444,{0,0,0,2,0,0}},{-0.9303048681,{1,1,1,0,0,1}},
+   {0.6916998765,{0,0,0,2,2,0}}},
+};
+__constant__ Mono c_antx[3][18] = {
+  {{-1.424276332,{1,1,0,2,2,0}},{-0.3104536551,{1,1,0,0,1,1}},{-0.6209073087,{2,0,0,1,2,0}},{-0.989556182,{2,0,1,0,0,1}},
+   {0.3104536561,{0,0,0,1,2,0}},{0.9895561812,{1,1,1,1,1,0}},{-1.424276332,{0,0,0,1,1,1}},{-0.9119913298,{2,0,1,0,1,0}},
+   {2.848552668,{2,0,0,1,1,1}},{-0.911991329,{1,1,1,1,0,1}},{0.9314082638,{1,1,0,0,0,0}},{-1.424276333,{1,1,0,0,2,0}},
+   {-0.1552268276,{0,0,0,1,0,0}},{0.3104536564,{2,0,0,1,0,0}},{0.4947780906,{0,0,1,0,0,1}},{-0.3104536556,{1,1,0,2,1,1}},
+   {0.4928680679,{1,1,0,2,0,0}},{0.4559956636,{0,0,1,0,1,0}}},
+  {{1.040573095,{1,1,0,2,2,0}},{0.5608410611,{1,1,0,0,1,1}},{1.121682122,{2,0,0,1,2,0}},{0.9891783668,{2,0,1,0,0,1}},
+   {-0.5608410611,{0,0,0,1,2,0}},{-0.9891783668,{1,1,1,1,1,0}},{1.040573095,{0,0,0,1,1,1}},{0.7264625222,{2,0,1,0,1,0}},
+   {-2.081146187,{2,0,0,1,1,1}},{0.7264625218,{1,1,1,1,0,1}},{-1.427112042,{1,1,0,0,0,0}},{1.040573094,{1,1,0,0,2,0}},
+   {0.2804205304,{0,0,0,1,0,0}},{-0.560841061,{2,0,0,1,0,0}},{-0.4945891833,{0,0,1,0,0,1}},{0.5608410611,{1,1,0,2,1,1}},
+   {0.3865389466,{1,1,0,2,0,0}},{-0.3632312614,{0,0,1,0,1,0}}},
+  {{1.383399753,{1,1,0,2,2,0}},{-0.396335116,{1,1,0,0,1,1}},{-0.7926702326,{2,0,0,1,2,0}},{-0.9303048681,{2,0,1,0,0,1}},
+   {0.3963351158,{0,0,0,1,2,0}},{0.9303048686,{1,1,1,1,1,0}},{1.383399752,{0,0,0,1,1,1}},{-0.7513324118,{2,0,1,0,1,0}},
+   {-2.766799505,{2,0,0,1,1,1}},{-0.7513324118,{1,1,1,1,0,1}},{-0.0798444646,{1,1,0,0,0,0}},{1.383399752,{1,1,0,0,2,0}},
+   {-0.1981675579,{0,0,0,1,0,0}},{0.3963351158,{2,0,0,1,0,0}},{0.465152434,{0,0,1,0,0,1}},{-0.3963351158,{1,1,0,2,1,1}},
+   {-1.303555288,{1,1,0,2,0,0}},{0.3756662059,{0,0,1,0,1,0}}},
+};
+// detector vertices, metres (Utilities.c:1078-1109)
+__constant__ double c_detpos[3][3] = {
+  {-2.161414928e6, 3.834695183e6, 4.600350224e6},
+  {-74276.04192, 5.496283721e6, 3.224257016e6},
+  {4546374.098, -842989.6972, 4378576.963},
+};
+
+__device__ __forceinline__ double fit_eval(int k, double eta, double chi) {
+  const double* c = c_fits[k];
+  double xi = -1 + chi, xi2 = xi * xi, xi3 = xi2 * xi, eta2 = eta * eta;
+  return c[0] + c[1] * eta + (c[2] + c[3] * eta + c[4] * eta2) * xi + (c[5] + c[6] * eta + c[7] * eta2) * xi2 +
+         (c[8] + c[9] * eta + c[10] * eta2) * xi3;
+}
+
+void upload_tables() {}   // tables are statically initialised __constant__ data
+
+// ---------------------------------------------------------------- setup
+__device__ double mono_sum(const Mono* t, int n, const double* v) {
+  double s = 0.0;
+  for (int k = 0; k < n; k++) {
+    double term = t[k].c;
+    for (int j = 0; j < 6; j++)
+      for (int e = 0; e < t[k].e[j]; e++) term *= v[j];
+    s += term;
+  }
+  return s;
+}
+
+// final spin, eq. 3.6 of arXiv:1508.07250
+__device__ double final_spin(double eta, double chi1, double chi2) {
+  double Seta = sqrt(1.0 - 4.0 * eta), m1 = 0.5 * (1.0 + Seta), m2 = 0.5 * (1.0 - Seta);
+  double s = m1 * m1 * chi1 + m2 * m2 * chi2;
+  double e2 = eta * eta, e3 = e2 * eta, e4 = e3 * eta, s2 = s * s, s3 = s2 * s, s4 = s3 * s;
+  return 3.4641016151377544 * eta - 4.399247300629289 * e2 + 9.397292189321194 * e3 - 13.180949901606242 * e4 +
+         (1 - 0.0850917821418767 * eta - 5.837029316602263 * e2) * s +
+         (0.1014665242971878 * eta - 2.0967746996832157 * e2) * s2 +
+         (-1.3546806617824356 * eta + 4.108962025369336 * e2) * s3 +
+         (-0.8676969352555539 * eta + 2.064046835273906 * e2) * s4;
+}
+// radiated energy, eqs. 3.7-3.8 of arXiv:1508.07250
+__device__ double erad(double eta, double chi1, double chi2) {
+  double Seta = sqrt(1.0 - 4.0 * eta), m1 = 0.5 * (1.0 + Seta), m2 = 0.5 * (1.0 - Seta);
+  double m1s = m1 * m1, m2s = m2 * m2, s = (m1s * chi1 + m2s * chi2) / (m1s + m2s);
+  double e2 = eta * eta, e3 = e2 * eta, e4 = e3 * eta;
+  return ((0.055974469826360077 * eta + 0.5809510763115132 * e2 - 0.9606726679372312 * e3 + 3.352411249771192 * e4) *
+          (1. + (-0.0030302335878845507 - 2.0066110851351073 * eta + 7.7050567802399215 * e2) * s)) /
+         (1. + (-0.6714403054720589 - 1.4756929437702908 * eta + 7.304676214885011 * e2) * s);
+}
+
+__device__ double damp_ins(const PhdRec& c, double Mf) {
+  Pow6 p = pow6(Mf);
+  return (2.0 / 3.0) * c.ai[0] / p.third + c.ai[1] + (4.0 / 3.0) * c.ai[2] * p.third +
+         (5.0 / 3.0) * c.ai[3] * p.two_thirds + 2.0 * c.ai[4] * Mf + (7.0 / 3.0) * c.ai[5] * p.four_thirds +
+         (8.0 / 3.0) * c.ai[6] * p.five_thirds + 3.0 * c.ai[7] * p.two;
+}
+__device__ double damp_mrd(const PhdRec& c, double f) {
+  double fg = c.fDM * c.g3, df = f - c.fRD, den = df * df + fg * fg;
+  return amp_mrd(c, f) * (-c.g2 / fg - 2.0 * df / den);
+}
+// d(phi_ins)/dMf (IMRPhenomD_internals.c:1455-1493); pv/pvl are the TaylorF2 series
+__device__ double dphi_ins(const PhdRec& c, const double* pv, const double* pvl, double s1, double s2, double s3,
+                           double s4, double pi_third, double pi_two_thirds, double Mf) {
+  double v = cbrt(kPi * Mf), logv = log(v);
+  double v2 = v * v, v3 = v * v2, v4 = v * v3, v5 = v * v4, v6 = v * v5, v7 = v * v6, v8 = v * v7;
+  double D = 0.0;
+  D += 2.0 * pv[7] * v7;
+  D += (pv[6] + pvl[6] * (1.0 + logv)) * v6;
+  D += pvl[5] * v5;
+  D += -1.0 * pv[4] * v4;
+  D += -2.0 * pv[3] * v3;
+  D += -3.0 * pv[2] * v2;
+  D += -4.0 * pv[1] * v;
+  D += -5.0 * pv[0];
+  D /= v8 * 3.0 / kPi;
+  D += (s1 + s2 * v / pi_third + s3 * v2 / pi_two_thirds + (s4 / kPi) * v3) / c.eta;
+  return D;
+}
+
+// IMRPhenomD coefficient setup for one system (IMRPhenomD.c:413-503). Masses in Msun.
+__device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, double m2_in, double chi1_in,
+                         double chi2_in, double dist, const QnmTable& q) {
+  int st = kStOK;
+  if (!(m1_in > 0.0) || !(m2_in > 0.0)) st |= kStBadMass;
+  if (!(dist > 0.0)) st |= kStBadDist;
+  if (!(chi1_in <= 1.0 && chi1_in >= -1.0 && chi2_in <= 1.0 && chi2_in >= -1.0)) st |= kStBadSpin;
+  double m1 = m1_in, m2 = m2_in, chi1 = chi1_in, chi2 = chi2_in;
+  if (!(m1_in > m2_in)) { m1 = m2_in; m2 = m1_in; chi1 = chi2_in; chi2 = chi1_in; }
+  Pow6 pip = pow6(kPi);
+  c.pi_third = pip.third;
+  double M = m1 + m2, eta = m1 * m2 / (M * M);
+  c.eta = eta; c.inv_eta = 1.0 / eta;
+  c.Msec = M * kMtsun;
+  c.amp_scale = M * kMrsun * M * kMtsun / dist;
+  c.fCut = kFcut / c.Msec;
+  double Seta = sqrt(1.0 - 4.0 * eta);
+  double chi = (chi1 + chi2) / 2.0 * (1.0 - eta * 76.0 / 113.0) + Seta * ((chi1 - chi2) / 2.0);
+  double fsp = final_spin(eta, chi1, chi2);
+  if (!(fsp <= 1.0)) { st |= kStBadSpinFinal; fsp = 1.0; }
+  if (!(fsp >= -1.0)) fsp = -1.0;
+  double er = erad(eta, chi1, chi2);
+  c.fRD = qnm_eval(q, q.yr, q.mr, fsp) / (1.0 - er);
+  c.fDM = qnm_eval(q, q.yd, q.md, fsp) / (1.0 - er);
+  // amplitude
+  c.g1 = fit_eval(F_GAM1, eta, chi); c.g2 = fit_eval(F_GAM2, eta, chi); c.g3 = fit_eval(F_GAM3, eta, chi);
+  if (c.g2 <= 1)
+    c.fmax = fabs(c.fRD + (c.fDM * (-1 + sqrt(1 - c.g2 * c.g2)) * c.g3) / c.g2);
+  else
+    c.fmax = fabs(c.fRD + (c.fDM * (-1) * c.g3) / c.g2);
+  c.a0 = (sqrt(2.0 / 3.0) * sqrt(eta)) / pip.sixth;
+  {
+    // inspiral amplitude prefactors, Appendix B of arXiv:1508.07253
+    double x1 = chi1, x2 = chi2, x1s = x1 * x1, x2s = x2 * x2, e2 = eta * eta, e3 = eta * e2, Pi = kPi;
+    double Pi2 = pip.two;
+    c.ai[0] = ((-969 + 1804 * eta) * pip.two_thirds) / 672.;
+    c.ai[1] = ((x1 * (81 * (1 + Seta) - 44 * eta) + x2 * (81 - 81 * Seta - 44 * eta)) * Pi) / 48.;
+    c.ai[2] = ((-27312085.0 - 10287648 * x2s - 10287648 * x1s * (1 + Seta) + 10287648 * x2s * Seta +
+                24 * (-1975055 + 857304 * x1s - 994896 * x1 * x2 + 857304 * x2s) * eta + 35371056 * e2) *
+               pip.four_thirds) / 8.128512e6;
+    c.ai[3] = (pip.five_thirds * (x2 * (-285197 * (-1 + Seta) + 4 * (-91902 + 1579 * Seta) * eta - 35632 * e2) +
+                                  x1 * (285197 * (1 + Seta) - 4 * (91902 + 1579 * Seta) * eta - 35632 * e2) +
+                                  42840 * (-1.0 + 4 * eta) * Pi)) / 32256.;
+    c.ai[4] = -(Pi2 * (-336 * (-3248849057.0 + 2943675504 * x1s - 3339284256 * x1 * x2 + 2943675504 * x2s) * e2 -
+                       324322727232 * e3 -
+                       7 * (-177520268561 + 107414046432 * x2s + 107414046432 * x1s * (1 + Seta) -
+                            107414046432 * x2s * Seta + 11087290368 * (x1 + x2 + x1 * Seta - x2 * Seta) * Pi) +
+                       12 * eta * (-545384828789 - 176491177632 * x1 * x2 + 202603761360 * x2s +
+                                   77616 * x1s * (2610335 + 995766 * Seta) - 77287373856 * x2s * Seta +
+                                   5841690624 * (x1 + x2) * Pi + 21384760320 * Pi2))) / 6.0085960704e10;
+    c.ai[5] = fit_eval(F_RHO1, eta, chi);
+    c.ai[6] = fit_eval(F_RHO2, eta, chi);
+    c.ai[7] = fit_eval(F_RHO3, eta, chi);
+  }
+  {
+    // intermediate amplitude: quartic with value and slope at f1, value at f2, value and
+    // slope at f3 (eqs. 21-26 of arXiv:1508.07253), kept in Newton form on nodes f1,f1,f2,f3,f3
+    double f1 = kAmpJoin, f3 = c.fmax, f2 = f1 + (f3 - f1) / 2.0;
+    Pow6 p1 = pow6(f1);
+    double v1 = amp_ins(c, f1, p1), d1 = damp_ins(c, f1);
+    double v3 = amp_mrd(c, f3), d2 = damp_mrd(c, f3);
+    double v2 = fit_eval(F_V2, eta, chi);
+    double q01 = d1, q12 = (v2 - v1) / (f2 - f1), q23 = (v3 - v2) / (f3 - f2), q34 = d2;
+    double q012 = (q12 - q01) / (f2 - f1), q123 = (q23 - q12) / (f3 - f1), q234 = (q34 - q23) / (f3 - f2);
+    double q0123 = (q123 - q012) / (f3 - f1), q1234 = (q234 - q123) / (f3 - f1);
+    c.hx1 = f1; c.hx2 = f2; c.hx3 = f3;
+    c.hc[0] = v1; c.hc[1] = q01; c.hc[2] = q012; c.hc[3] = q0123; c.hc[4] = (q1234 - q0123) / (f3 - f1);
+  }
+  // phase
+  double s1 = fit_eval(F_SI1, eta, chi), s2 = fit_eval(F_SI2, eta, chi), s3 = fit_eval(F_SI3, eta, chi),
+         s4 = fit_eval(F_SI4, eta, chi);
+  c.b1 = fit_eval(F_BE1, eta, chi); c.b2 = fit_eval(F_BE2, eta, chi); c.b3 = fit_eval(F_BE3, eta, chi);
+  c.al1 = fit_eval(F_AL1, eta, chi); c.al2 = fit_eval(F_AL2, eta, chi); c.al3 = fit_eval(F_AL3, eta, chi);
+  c.al4 = fit_eval(F_AL4, eta, chi); c.al5 = fit_eval(F_AL5, eta, chi);
+  double pv[8], pvl[8];
+  {
+    // TaylorF2 phasing incl. aligned-spin terms (IMRPhenomD_internals.c:244-365), then minus the
+    // 3PN spin-spin term PhenomD was not tuned with (IMRPhenomD.c:478)
+    double mt = m1 + m2, d = (m1 - m2) / mt, et = m1 * m2 / mt / mt, m1M = m1 / mt, m2M = m2 / mt;
+    double SL = m1M * m1M * chi1 + m2M * m2M * chi2, dSigmaL = d * (m2M * chi2 - m1M * chi1);
+    double pfaN = 3.0 / (128.0 * et);
+    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vl[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    v[0] = 1.0;
+    v[2] = 5.0 * (743.0 / 84.0 + 11.0 * et) / 9.0;
+    v[3] = -16.0 * kPi;
+    v[4] = 5.0 * (3058.673 / 7.056 + 5429.0 / 7.0 * et + 617.0 * et * et) / 72.0;
+    v[5] = 5.0 / 9.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
+    vl[5] = 5.0 / 3.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
+    v[6] = (11583.231236531 / 4.694215680 - 640.0 / 3.0 * kPi * kPi - 6848.0 / 21.0 * kGammaE) +
+           et * (-15737.765635 / 3.048192 + 2255. / 12. * kPi * kPi) + et * et * 76055.0 / 1728.0 -
+           et * et * et * 127825.0 / 1296.0;
+    v[6] += (-6848.0 / 21.0) * log(4.);
+    vl[6] = -6848.0 / 21.0;
+    v[7] = kPi * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * et - 74045.0 / 756.0 * et * et);
+    double sig = et * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
+    sig += (720.0 - 1.0) / 96.0 * m1M * m1M * chi1 * chi1;
+    sig += (720.0 - 1.0) / 96.0 * m2M * m2M * chi2 * chi2;
+    sig -= (240.0 - 7.0) / 96.0 * m1M * m1M * chi1 * chi1;
+    sig -= (240.0 - 7.0) / 96.0 * m2M * m2M * chi2 * chi2;
+    double ss3 = (326.75 / 1.12 + 557.5 / 1.8 * et) * et * chi1 * chi2;
+    ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m1M - 120.0 * m1M * m1M) +
+            (-4108.25 / 6.72 - 108.5 / 1.2 * m1M + 125.5 / 3.6 * m1M * m1M)) * m1M * m1M * chi1 * chi1;
+    ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m2M - 120.0 * m2M * m2M) +
+            (-4108.25 / 6.72 - 108.5 / 1.2 * m2M + 125.5 / 3.6 * m2M * m2M)) * m2M * m2M * chi2 * chi2;
+    double gam = (554345.0 / 1134.0 + 110.0 * et / 9.0) * SL + (13915.0 / 84.0 - 10.0 * et / 3.0) * dSigmaL;
+    v[7] += (-8980424995.0 / 762048.0 + 6586595.0 * et / 756.0 - 305.0 * et * et / 36.0) * SL -
+            (170978035.0 / 48384.0 - 2876425.0 * et / 672.0 - 4735.0 * et * et / 144.0) * dSigmaL;
+    v[6] += kPi * (3760.0 * SL + 1490.0 * dSigmaL) / 3.0 + ss3;
+    v[5] += -1.0 * gam;
+    vl[5] += -3.0 * gam;
+    v[4] += -10.0 * sig;
+    v[3] += 188.0 * SL / 3.0 + 25.0 * dSigmaL;
+    for (int k = 0; k < 8; k++) { pv[k] = v[k] * pfaN; pvl[k] = vl[k] * pfaN; }
+    pv[6] -= ss3 * pv[0];
+  }
+  c.pq[0] = pv[5] - kPi4;
+  c.pq[1] = pv[7] * pip.two_thirds;
+  c.pq[2] = pv[6] * pip.third;
+  c.pq[3] = pvl[6] * pip.third;
+  c.pq[4] = pvl[5];
+  c.pq[5] = pv[4] / pip.third;
+  c.pq[6] = pv[3] / pip.two_thirds;
+  c.pq[7] = pv[2] / kPi;
+  c.pq[8] = pv[0] / pip.five_thirds;
+  c.pq[9] = s1;
+  c.pq[10] = s2 * 3.0 / 4.0;
+  c.pq[11] = s3 * 3.0 / 5.0;
+  c.pq[12] = s4 / 2.0;
+  {
+    // C^1 joins (IMRPhenomD_internals.c:1547-1584)
+    double fj = kPhiJoin;
+    c.C2Int = dphi_ins(c, pv, pvl, s1, s2, s3, s4, pip.third, pip.two_thirds, fj) - dphi_int(c, fj);
+    Pow6 pj = pow6(fj);
+    c.C1Int = phi_ins(c, fj, pj) - 1.0 / eta * phi_int(c, fj) - c.C2Int * fj;
+    c.fMRDJoin = 0.5 * c.fRD;
+    double fm = c.fMRDJoin;
+    double phiT = 1.0 / eta * phi_int(c, fm) + c.C1Int + c.C2Int * fm;
+    double dphiT = c.C2Int + dphi_int(c, fm);
+    c.C2MRD = dphiT - dphi_mrd(c, fm);
+    c.C1MRD = phiT - 1.0 / eta * phi_mrd(c, fm) - c.C2MRD * fm;
+  }
+  c.t0 = dphi_mrd(c, c.fmax);
+  c.MfRef = c.Msec * fRef;
+  {
+    // phase at the reference frequency (IMRPhenomD.c:497-503)
+    double Mf = c.MfRef, phr;
+    Pow6 pr = pow6(Mf);
+    if (Mf < kPhiJoin) phr = phi_ins(c, Mf, pr);
+    else if (Mf >= c.fMRDJoin) phr = 1.0 / c.eta * phi_mrd(c, Mf) + c.C1MRD + c.C2MRD * Mf;
+    else phr = 1.0 / c.eta * phi_int(c, Mf) + c.C1Int + c.C2Int * Mf;
+    c.phi_pre = 2. * phi0 + phr;
+  }
+  c.flags = (st == kStOK) ? kRecValid : 0;
+  return st;
+}
+
+// start frequency: 3PN inversion of t(f) for time params[5] before merger (Utilities.c:587-629)
+__device__ double fbegin_dev(const double* p) {
+  const double gE = 0.5772156649;
+  double Mc = exp(p[0]) / kMsun * kTsunCBC, M = exp(p[1]) / kMsun * kTsunCBC;
+  double eta = pow(Mc / M, 5.0 / 3.0);
+  if (eta > 0.25) eta = 0.25;
+  double dm = sqrt(1.0 - 4.0 * eta), m1 = M * (1.0 + dm) / 2.0, m2 = M * (1.0 - dm) / 2.0;
+  double c1 = p[2], c2 = p[3], chi = (m1 * c1 + m2 * c2) / M, tc = p[5];
+  double th = pow(eta * tc / (5.0 * M), -1.0 / 8.0);
+  double t2 = th * th, t3 = t2 * th, t4 = t2 * t2, t5 = t2 * t3, t6 = t3 * t3;
+  double PN1 = (11.0 / 32.0 * eta + 743.0 / 2688.0) * t2;
+  double PN15 = -3.0 * kPi / 10.0 * t3 + (1.0 / 160.0) * (113.0 * chi - 38.0 * eta * (c1 + c2)) * t3;
+  double PN2 = (1855099.0 / 14450688.0 + 56975.0 / 258048.0 * eta + 371.0 / 2048.0 * eta * eta) * t4 +
+               (1.0 / 14450688.0) * (-3386880.0 * chi * chi + 1512.0 * c1 * c2) * t4;
+  double PN25 = -(7729.0 / 21504.0 - 13.0 / 256.0 * eta) * kPi * t5;
+  double PN3 = (-720817631400877.0 / 288412611379200.0 + 53.0 / 200.0 * kPi * kPi + 107.0 / 280.0 * gE +
+                (25302017977.0 / 4161798144.0 - 451.0 / 2048.0 * kPi * kPi) * eta - 30913.0 / 1835008.0 * eta * eta +
+                235925.0 / 1769472.0 * eta * eta * eta + 107.0 / 280.0 * log(2.0 * th)) * t6;
+  return t3 / (8.0 * M * kPi) * (1.0 + PN1 + PN15 + PN2 + PN25 + PN3);
+}
+
+__device__ __forceinline__ double bin_freq(const NetGeom& g, int i) {
+  return g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
+}
+
+// Full parameter set -> record: waveform coefficients + per-detector projection
+// (QuickCBC.c:3698-3755 / 3795-3850).  Returns status bits.
+__device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, const QnmTable& q) {
+  double fs = fbegin_dev(p);
+  double mc = exp(p[0]), mt = exp(p[1]);
+  double eta = pow((mc / mt), (5.0 / 3.0));
+  double dm = eta > 0.25 ? 0.0 : sqrt(1.0 - 4.0 * eta);
+  double m1 = mt * (1.0 + dm) / 2.0, m2 = mt * (1.0 - dm) / 2.0;
+  int st = phd_setup(c, 0.5 * p[4], kFref, m1 / kMsun, m2 / kMsun, p[2], p[3], exp(p[6]), q);
+  c.fs = fs;
+  c.ts = g.Tobs - p[5];
+  c.sqT = sqrt(g.Tobs);
+  double Ap = (1.0 + p[10] * p[10]) / 2.0, Ac = -p[10];
+  double cd = sqrt(1.0 - p[8] * p[8]);
+  double ca = cos(g.GMST - p[7]), sa = sin(g.GMST - p[7]);
+  double v[6] = {cos(p[9]), sin(p[9]), cd, p[8], cos(p[7] - g.GMST), sin(p[7] - g.GMST)};
+  for (int id = 0; id < g.nifo; id++) {
+    int l = g.labels[id];
+    double fp = mono_sum(c_antp[l], 21, v), fx = mono_sum(c_antx[l], 18, v);
+    c.Fs[id] = sqrt(Ap * Ap * fp * fp + Ac * Ac * fx * fx);
+    double lam = atan2(Ac * fx, Ap * fp);
+    if (lam < 0.0) lam += kTwoPi;
+    c.lam[id] = lam;
+    double r = c_detpos[l][0] * cd * ca + c_detpos[l][1] * cd * sa + c_detpos[l][2] * p[8];
+    c.td[id] = -r / kClight;
+  }
+  // bins that carry signal: f > fbegin (QuickCBC.c:3758) and f <= fCut (IMRPhenomD.c:530),
+  // inside the band and inside [1, N/2) (bin N/2 of the template is zero, QuickCBC.c:3754)
+  int lo = g.imin > 1 ? g.imin : 1;
+  int hi = g.imax - 1;
+  if (hi > g.N / 2 - 1) hi = g.N / 2 - 1;
+  if (fs == fs) {
+    double x = fs * g.Tobs;
+    if (x >= (double)hi + 1.0) lo = hi + 1;
+    else if (x >= (double)lo) {
+      int c0 = (int)floor(x) + 1;
+      for (int k = 0; k < 3 && c0 - 1 >= lo && bin_freq(g, c0 - 1) > fs; k++) c0--;
+      for (int k = 0; k < 3 && c0 <= hi && !(bin_freq(g, c0) > fs); k++) c0++;
+      if (c0 > lo) lo = c0;
+    }
+  } else {
+    lo = hi + 1;                                   // NaN start frequency: template is zero
+  }
+  {
+    double x = c.fCut * g.Tobs;
+    if (x < (double)hi) {
+      int c1 = x < 0.0 ? -1 : (int)floor(x);
+      for (int k = 0; k < 3 && c1 + 1 <= hi && bin_freq(g, c1 + 1) <= c.fCut; k++) c1++;
+      for (int k = 0; k < 3 && c1 >= 0 && bin_freq(g, c1) > c.fCut; k++) c1--;
+      if (c1 < hi) hi = c1;
+    }
+  }
+  c.i_lo = lo;
+  c.i_hi = hi;
+  return st;
+}
+
+__global__ void k_setup(const double* __restrict__ params, int B, NetGeom g, QnmTable q, PhdRec* __restrict__ recs,
+                        int* __restrict__ status) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  double p[11];
+#pragma unroll
+  for (int k = 0; k < 11; k++) p[k] = params[(size_t)b * 11 + k];
+  PhdRec c;
+  int st = record_from_params(c, p, g, q);
+  recs[b] = c;
+  status[b] = st;
+}
+
+void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
+                  int* d_status, cudaStream_t s) {
+  if (B <= 0) return;
+  int th = 64;
+  k_setup<<<(B + th - 1) / th, th, 0, s>>>(d_params, B, g, q, d_recs, d_status);
+}
+
+// ---------------------------------------------------------------- reductions
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double* smem /* [32][NV] */) {
+#pragma unroll
+  for (int k = 0; k < NV; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+  if (lane == 0)
+    for (int k = 0; k < NV; k++) smem[w * NV + k] = v[k];
+  __syncthreads();
+  if (w == 0) {
+    for (int k = 0; k < NV; k++) {
+      double x = lane < nw ? smem[lane * NV + k] : 0.0;
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+      v[k] = x;
+    }
+  }
+}
+
+__device__ __forceinline__ void kahan_add(float& s, float& comp, float x) {
+  float y = x - comp;
+  float t = s + y;
+  comp = (t - s) - y;
+  s = t;
+}
+
+// ---------------------------------------------------------------- full lnL
+// One block = one tile of bins of one parameter set.  Per detector the block
+// accumulates  SD = sum amp (wr cos x + wi sin x)  and  SH = sum amp^2 ws
+// (wr/wi/ws carry 4/S and the event scale sigma); the finaliser applies the
+// per-detector factor K = Fs h22fac amp_scale / sqrt(T) / sigma:
+//   <d|h> = K SD,  <h|h> = K^2 SH   (QuickCBC.c:4258-4266, Utilities.c:716-736).
+template <int PREC, int NIFO>
+__global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ recs, NetGeom g, EventData ev, int tiles,
+                                                  double* __restrict__ partials) {
+  __shared__ PhdRec rec;
+  __shared__ double red[32 * 2 * kMaxIfo];
+  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  {
+    const int nw = sizeof(PhdRec) / 8;
+    const double* src = reinterpret_cast<const double*>(recs + b);
+    double* dst = reinterpret_cast<double*>(&rec);
+    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  const PhdRec& c = rec;
+  double acc[2 * NIFO];
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
+  if (c.flags & kRecValid) {
+    int n = c.i_hi - c.i_lo + 1;
+    if (n > 0) {
+      int chunk = (n + tiles - 1) / tiles;
+      int i0 = c.i_lo + t * chunk;
+      int i1 = min(i0 + chunk - 1, c.i_hi);
+      const size_t nh = (size_t)ev.nh;
+      if (PREC == kFP64) {
+        for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
+          double f = bin_freq(g, i);
+          double Mf = c.Msec * f;
+          double amp, ph;
+          phd_eval64(c, Mf, amp, ph);
+#pragma unroll
+          for (int id = 0; id < NIFO; id++) {
+            // x = 2 pi f (ts - td) + lambda - phi, evaluated in the reference's order
+            double x = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+            double sx, cx;
+            sincos(reduce_2pi(x), &sx, &cx);
+            const double* w = ev.w64 + (size_t)id * 3 * nh;
+            double wr = __ldg(w + i), wi = __ldg(w + nh + i), ws = __ldg(w + 2 * nh + i);
+            acc[2 * id] += amp * (wr * cx + wi * sx);
+            acc[2 * id + 1] += amp * amp * ws;
+          }
+        }
+      } else {
+        float sd[NIFO], cd[NIFO], sh[NIFO], ch[NIFO];
+#pragma unroll
+        for (int id = 0; id < NIFO; id++) { sd[id] = cd[id] = sh[id] = ch[id] = 0.f; }
+        constexpr double kInv2Pi = 0.15915494309189533577;
+        double tsd[NIFO], lamc[NIFO];
+#pragma unroll
+        for (int id = 0; id < NIFO; id++) { tsd[id] = c.ts - c.td[id]; lamc[id] = c.lam[id] * kInv2Pi; }
+        for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
+          double f = bin_freq(g, i);
+          double Mf = c.Msec * f;
+          float amp;
+          double ph;
+          phd_eval_mixed(c, Mf, amp, ph);
+          double phc = ph * kInv2Pi;
+#pragma unroll
+          for (int id = 0; id < NIFO; id++) {
+            double cyc = fma(f, tsd[id], lamc[id] - phc);      // x / (2 pi)
+            float r = (float)(cyc - rint(cyc));
+            float sx, cx;
+            sincospif(2.0f * r, &sx, &cx);
+            const float* w = ev.w32 + (size_t)id * 3 * nh;
+            float wr = __ldg(w + i), wi = __ldg(w + nh + i), ws = __ldg(w + 2 * nh + i);
+            kahan_add(sd[id], cd[id], amp * fmaf(wr, cx, wi * sx));
+            kahan_add(sh[id], ch[id], amp * amp * ws);
+          }
+        }
+#pragma unroll
+        for (int id = 0; id < NIFO; id++) {
+          acc[2 * id] = (double)sd[id] - (double)cd[id];
+          acc[2 * id + 1] = (double)sh[id] - (double)ch[id];
+        }
+      }
+    }
+  }
+  block_sum<2 * NIFO>(acc, red);
+  if (threadIdx.x == 0) {
+    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+#pragma unroll
+    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  }
+}
+
+template <int PREC>
+static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
+                             double* part, cudaStream_t s) {
+  dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
+  switch (g.nifo) {
+    case 1: k_lnl_full<PREC, 1><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
+    case 2: k_lnl_full<PREC, 2><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
+    default: k_lnl_full<PREC, 3><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
+  }
+}
+
+void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
+                     const FullLaunch& L, double* d_partials, cudaStream_t s) {
+  if (B <= 0) return;
+  if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, s);
+  else launch_full_prec<kMixed>(d_recs, B, g, ev, L, d_partials, s);
+}
+
+__global__ void k_finalize_full(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
+                                const int* __restrict__ status, int B, int tiles, NetGeom g, EventData ev,
+                                double* __restrict__ lnl, double* __restrict__ rho) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const PhdRec& c = recs[b];
+  if (status[b] != kStOK) {
+    lnl[b] = -1.0e20;                      // the reference's rejected-sample value (QuickCBC.c:2366)
+    if (rho) for (int id = 0; id < g.nifo; id++) rho[(size_t)b * g.nifo + id] = 0.0;
+    return;
+  }
+  double L = 0.0;
+  for (int id = 0; id < g.nifo; id++) {
+    double sd = 0.0, sh = 0.0;
+    for (int t = 0; t < tiles; t++) {
+      const double* p = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+      sd += p[2 * id];
+      sh += p[2 * id + 1];
+    }
+    double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * ev.inv_sigma[id];
+    double HD = K * sd, HH = K * K * sh;
+    if (rho) rho[(size_t)b * g.nifo + id] = HD / sqrt(HH);
+    L += HD - 0.5 * HH;
+  }
+  lnl[b] = L;
+}
+
+void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
+                          const NetGeom& g, const EventData& ev, double* d_lnl, double* d_rho, cudaStream_t s) {
+  if (B <= 0) return;
+  k_finalize_full<<<(B + 127) / 128, 128, 0, s>>>(d_partials, d_recs, d_status, B, tiles, g, ev, d_lnl, d_rho);
+}
+
+// ---------------------------------------------------------------- heterodyned lnL
+// One block per parameter set.  Phase 1: waveform at the M grid points and the
+// per-detector ratios hc, hs, cc to the reference (QuickCBC.c:5332-5345) into
+// shared memory.  Phase 2: per region r, uu = IP[r] v for v in {cc, hc, hs},
+// contracted with SL / lc / ls and the edge over-count correction
+// (QuickCBC.c:5347-5425); block sum; lnL = logLb - sum (HR + HH/2).
+template <int PREC>
+__global__ void __launch_bounds__(256) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+                                                 NetGeom g, HetData h, double* __restrict__ lnl) {
+  extern __shared__ double sm[];
+  __shared__ PhdRec rec;
+  __shared__ double red[32 * 4 * kMaxIfo];
+  int b = blockIdx.x;
+  {
+    const int nw = sizeof(PhdRec) / 8;
+    const double* src = reinterpret_cast<const double*>(recs + b);
+    double* dst = reinterpret_cast<double*>(&rec);
+    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
+  }
+  __syncthreads();
+  const PhdRec& c = rec;
+  if (status[b] != kStOK) {
+    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+    return;
+  }
+  const int M = h.M, nifo = g.nifo;
+  double* s_hc = sm;                 // [nifo][M]
+  double* s_hs = sm + nifo * M;
+  double* s_cc = sm + 2 * nifo * M;
+  constexpr double kInv2Pi = 0.15915494309189533577;
+  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+    double f = __ldg(h.freq + j);
+    double y = 1.0;
+    if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);          // taper below fbegin (QuickCBC.c:3859)
+    if (PREC == kFP64) {
+      double amp = 0.0, ph = 0.0;
+      if (!(f > c.fCut)) { phd_eval64(c, c.Msec * f, amp, ph); amp *= c.amp_scale; }
+      for (int id = 0; id < nifo; id++) {
+        double A = c.Fs[id] * kH22fac * amp / c.sqT * y;
+        double x = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+        double aref = __ldg(h.amp + id * M + j), pref = __ldg(h.phase + id * M + j);
+        double sx, cx;
+        sincos(reduce_2pi(pref - x), &sx, &cx);
+        double cc = 2.0 * (aref - A * cx), ss = 2.0 * A * sx;
+        double hc = cc / aref, hs = ss / aref;
+        s_hc[id * M + j] = hc;
+        s_hs[id * M + j] = hs;
+        s_cc[id * M + j] = hc * hc + hs * hs;
+      }
+    } else {
+      float amp = 0.f;
+      double ph = 0.0;
+      if (!(f > c.fCut)) phd_eval_mixed(c, c.Msec * f, amp, ph);
+      double phc = ph * kInv2Pi;
+      for (int id = 0; id < nifo; id++) {
+        double aref = __ldg(h.amp + id * M + j), pref = __ldg(h.phase + id * M + j);
+        float ratio = amp * (float)(c.Fs[id] * kH22fac * c.amp_scale / c.sqT * y / aref);
+        double cyc = pref * kInv2Pi - fma(f, c.ts - c.td[id], c.lam[id] * kInv2Pi - phc);
+        float r = (float)(cyc - rint(cyc));
+        float sx, cx;
+        sincospif(2.0f * r, &sx, &cx);
+        float hc = 2.0f * (1.0f - ratio * cx), hs = 2.0f * ratio * sx;
+        s_hc[id * M + j] = (double)hc;
+        s_hs[id * M + j] = (double)hs;
+        s_cc[id * M + j] = (double)hc * (double)hc + (double)hs * (double)hs;
+      }
+    }
+  }
+  __syncthreads();
+  const int J = h.J, J1 = J + 1, NR = h.NR;
+  double acc[4 * kMaxIfo];           // per detector: HH, HR, x, y
+#pragma unroll
+  for (int k = 0; k < 4 * kMaxIfo; k++) acc[k] = 0.0;
+  for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+    const double* ip = h.IP + (size_t)r * J1 * J1;
+    for (int id = 0; id < nifo; id++) {
+      const double* sl = h.SL + ((size_t)r * nifo + id) * J1;
+      const double* lc = h.lc + ((size_t)r * nifo + id) * J1;
+      const double* ls = h.ls + ((size_t)r * nifo + id) * J1;
+      const double* vc = s_cc + id * M + r * J;
+      const double* vh = s_hc + id * M + r * J;
+      const double* vs = s_hs + id * M + r * J;
+      double HH = 0.0, HR = 0.0;
+      for (int a = 0; a < J1; a++) {
+        double u1 = 0.0, u2 = 0.0, u3 = 0.0;
+        for (int k = 0; k < J1; k++) {
+          double w = __ldg(ip + a * J1 + k);
+          u1 += w * vc[k];
+          u2 += w * vh[k];
+          u3 += w * vs[k];
+        }
+        HH += u1 * __ldg(sl + a);
+        HR += u2 * __ldg(lc + a) + u3 * __ldg(ls + a);
+      }
+      acc[4 * id] += HH;
+      acc[4 * id + 1] += HR;
+      if (r < NR - 2) {
+        acc[4 * id + 2] += __ldg(h.aa + id * NR + r + 1) * vc[J];
+        acc[4 * id + 3] += __ldg(h.rc + id * NR + r + 1) * vh[J] + __ldg(h.rs + id * NR + r + 1) * vs[J];
+      }
+    }
+  }
+  block_sum<4 * kMaxIfo>(acc, red);
+  if (threadIdx.x == 0) {
+    double L = h.logLb;
+    for (int id = 0; id < nifo; id++) {
+      double HH = acc[4 * id] - acc[4 * id + 2], HR = acc[4 * id + 1] - acc[4 * id + 3];
+      L -= (HR + 0.5 * HH);
+    }
+    lnl[b] = L;
+  }
+}
+
+size_t het_smem_bytes(const NetGeom& g, const HetData& h) { return (size_t)3 * g.nifo * h.M * sizeof(double); }
+
+void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
+                    Precision prec, int threads, double* d_lnl, cudaStream_t s) {
+  if (B <= 0) return;
+  size_t smem = het_smem_bytes(g, h);
+  if (prec == kFP64) {
+    cudaFuncSetAttribute(k_lnl_het<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lnl_het<kFP64><<<B, threads, smem, s>>>(d_recs, d_status, g, h, d_lnl);
+  } else {
+    cudaFuncSetAttribute(k_lnl_het<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lnl_het<kMixed><<<B, threads, smem, s>>>(d_recs, d_status, g, h, d_lnl);
+  }
+}
+
+// ---------------------------------------------------------------- waveform outputs
+__global__ void k_setup_phys(double phi0, double fRef, double m1, double m2, double chi1, double chi2, double dist,
+                             QnmTable q, PhdRec* rec, int* status) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    PhdRec c;
+    status[0] = phd_setup(c, phi0, fRef, m1, m2, chi1, chi2, dist, q);
+    *rec = c;
+  }
+}
+
+// IMRPhenomDGenerateh22FDAmpPhase on an arbitrary frequency list (IMRPhenomD.c:527-556)
+__global__ void k_amp_phase(const PhdRec* __restrict__ recp, const double* __restrict__ freq, int n,
+                            double* __restrict__ amp, double* __restrict__ phase) {
+  __shared__ PhdRec c;
+  if (threadIdx.x == 0) c = *recp;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double f = freq[i];
+    if (f > c.fCut) { amp[i] = 0.0; phase[i] = 0.0; continue; }
+    double a, p;
+    phd_eval64(c, c.Msec * f, a, p);
+    amp[i] = c.amp_scale * a;
+    phase[i] = p;
+  }
+}
+
+void launch_amp_phase(const double* d_freq, int n, double phi0, double fRef, double m1, double m2, double chi1,
+                      double chi2, double dist, const QnmTable& q, PhdRec* d_rec, double* d_amp, double* d_phase,
+                      int* d_status, cudaStream_t s) {
+  k_setup_phys<<<1, 32, 0, s>>>(phi0, fRef, m1, m2, chi1, chi2, dist, q, d_rec, d_status);
+  int blocks = (n + 255) / 256;
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) blocks = 1;
+  k_amp_phase<<<blocks, 256, 0, s>>>(d_rec, d_freq, n, d_amp, d_phase);
+}
+
+__global__ void k_setup_one(const double* __restrict__ params, NetGeom g, QnmTable q, PhdRec* rec, int* status) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    double p[11];
+    for (int k = 0; k < 11; k++) p[k] = params[k];
+    PhdRec c;
+    status[0] = record_from_params(c, p, g, q);
+    *rec = c;
+  }
+}
+
+// fulltemplates: h[id][i] = A cos x, h[id][N-i] = A sin x for f > fbegin, else 0 (QuickCBC.c:3752-3772)
+__global__ void k_fulltemplates(const PhdRec* __restrict__ recp, NetGeom g, const double* __restrict__ freq,
+                                double* __restrict__ h) {
+  __shared__ PhdRec c;
+  if (threadIdx.x == 0) c = *recp;
+  __syncthreads();
+  const int N = g.N, half = N / 2;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i <= half; i += gridDim.x * blockDim.x) {
+    if (i == 0 || i == half) {
+      for (int id = 0; id < g.nifo; id++) h[(size_t)id * N + i] = 0.0;
+      continue;
+    }
+    double f = freq[i];
+    if (!(f > c.fs)) {
+      for (int id = 0; id < g.nifo; id++) { h[(size_t)id * N + i] = 0.0; h[(size_t)id * N + N - i] = 0.0; }
+      continue;
+    }
+    double amp = 0.0, ph = 0.0;
+    if (!(f > c.fCut)) { phd_eval64(c, c.Msec * f, amp, ph); amp *= c.amp_scale; }
+    for (int id = 0; id < g.nifo; id++) {
+      double A = c.Fs[id] * kH22fac * amp / c.sqT;
+      double x = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+      double sx, cx;
+      sincos(reduce_2pi(x), &sx, &cx);
+      h[(size_t)id * N + i] = A * cx;
+      h[(size_t)id * N + N - i] = A * sx;
+    }
+  }
+}
+
+void launch_fulltemplates(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq,
+                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s) {
+  k_setup_one<<<1, 32, 0, s>>>(d_params, g, q, d_rec, d_status);
+  int blocks = (g.N / 2 + 256) / 256;
+  if (blocks > 2368) blocks = 2368;
+  k_fulltemplates<<<blocks, 256, 0, s>>>(d_rec, g, d_freq, d_h);
+}
+
+// fullphaseamp: amp = A * taper, phase = x on freq[0..n) (QuickCBC.c:3850-3866)
+__global__ void k_fullphaseamp(const PhdRec* __restrict__ recp, NetGeom g, const double* __restrict__ freq, int n,
+                               double* __restrict__ amp_out, double* __restrict__ ph_out) {
+  __shared__ PhdRec c;
+  if (threadIdx.x == 0) c = *recp;
+  __syncthreads();
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double f = freq[i];
+    double amp = 0.0, ph = 0.0;
+    if (!(f > c.fCut)) { phd_eval64(c, c.Msec * f, amp, ph); amp *= c.amp_scale; }
+    double y = 1.0;
+    if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);
+    for (int id = 0; id < g.nifo; id++) {
+      double A = c.Fs[id] * kH22fac * amp / c.sqT;
+      amp_out[(size_t)id * n + i] = A * y;
+      ph_out[(size_t)id * n + i] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+    }
+  }
+}
+
+void launch_fullphaseamp(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq, int n,
+                         PhdRec* d_rec, int* d_status, double* d_amp, double* d_phase, cudaStream_t s) {
+  k_setup_one<<<1, 32, 0, s>>>(d_params, g, q, d_rec, d_status);
+  int blocks = (n + 255) / 256;
+  if (blocks > 2368) blocks = 2368;
+  if (blocks < 1) blocks = 1;
+  k_fullphaseamp<<<blocks, 256, 0, s>>>(d_rec, g, d_freq, n, d_amp, d_phase);
+}
+
+// ---------------------------------------------------------------- heterodyne setup (FP64)
+// Per bin j in [1, N/2): residual r = D - h, RC = 2 (r_re cos p + r_im sin p) A / S,
+// RS = 2 (-r_re sin p + r_im cos p) A / S, AA = A^2 / S  (QuickCBC.c:5190-5203).
+__global__ void k_het_bins(const double* __restrict__ h, const double* __restrict__ amp,
+                           const double* __restrict__ phase, const double* __restrict__ D,
+                           const double* __restrict__ S, int sn_stride, int N, int nifo, double* __restrict__ RC,
+                           double* __restrict__ RS, double* __restrict__ AA) {
+  const int half = N / 2;
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < nifo * half; idx += gridDim.x * blockDim.x) {
+    int id = idx / half, j = idx - id * half;
+    size_t o = (size_t)id * half + j;
+    if (j == 0) { RC[o] = 0.0; RS[o] = 0.0; AA[o] = 0.0; continue; }
+    const double* hr = h + (size_t)id * N;
+    const double* dr = D + (size_t)id * N;
+    double rre = dr[j] - hr[j], rim = dr[N - j] - hr[N - j];
+    double a = amp[o], s = S[(size_t)id * sn_stride + j];
+    double sp, cp;
+    sincos(phase[o], &sp, &cp);
+    double x = a / s;
+    RC[o] = 2.0 * (rre * cp + rim * sp) * x;
+    RS[o] = 2.0 * (-rre * sp + rim * cp) * x;
+    AA[o] = a * a / s;
+  }
+}
+
+void launch_het_bins(const double* d_h, const double* d_amp, const double* d_phase, const double* d_D,
+                     const double* d_S, int sn_stride, int N, int nifo, double* d_RC, double* d_RS, double* d_AA,
+                     cudaStream_t s) {
+  int total = nifo * (N / 2);
+  int blocks = (total + 255) / 256;
+  if (blocks > 4736) blocks = 4736;
+  k_het_bins<<<blocks, 256, 0, s>>>(d_h, d_amp, d_phase, d_D, d_S, sn_stride, N, nifo, d_RC, d_RS, d_AA);
+}
+
+// One block per (region, detector): sums over the region's U+1 bins of AA, RC, RS times the
+// discrete Legendre polynomials P_a(n) (QuickCBC.c:5265-5281, recurrence of 5055-5094).
+__global__ void k_het_region_sums(const double* __restrict__ RC, const double* __restrict__ RS,
+                                  const double* __restrict__ AA, const int* __restrict__ fgrid, int M, int J,
+                                  int nifo, int nh, double* __restrict__ SL, double* __restrict__ lc,
+                                  double* __restrict__ ls) {
+  __shared__ double red[32 * 12];
+  int r = blockIdx.x / nifo, id = blockIdx.x - r * nifo;
+  int J1 = J + 1;
+  int k0 = fgrid[r * J], U = fgrid[(r + 1) * J] - k0;
+  double acc[12];
+#pragma unroll
+  for (int a = 0; a < 12; a++) acc[a] = 0.0;
+  for (int n = threadIdx.x; n <= U; n += blockDim.x) {
+    double P[4];
+    double c0 = 0.0, c1 = (double)(U - 2 * n), c2 = (double)U;
+    double d0 = c2, d1 = c1 + c1, d2 = d0;
+    P[0] = 1.0;
+    if (J >= 1) P[1] = c1 / (double)U;
+    for (int i = 1; i < J && i < 3; i++) {
+      d0 += 2.0; d2 -= 2.0; c0 += d0; c1 += d1; c2 += d2;
+      P[i + 1] = (c1 * P[i] - c0 * P[i - 1]) / c2;
+    }
+    size_t k = (size_t)id * nh + k0 + n;
+    double aa = AA[k], rc = RC[k], rs = RS[k];
+    for (int a = 0; a < J1 && a < 4; a++) {
+      acc[3 * a] += aa * P[a];
+      acc[3 * a + 1] += rc * P[a];
+      acc[3 * a + 2] += rs * P[a];
+    }
+  }
+  block_sum<12>(acc, red);
+  if (threadIdx.x == 0) {
+    for (int a = 0; a < J1 && a < 4; a++) {
+      size_t o = ((size_t)r * nifo + id) * J1 + a;
+      SL[o] = acc[3 * a];
+      lc[o] = acc[3 * a + 1];
+      ls[o] = acc[3 * a + 2];
+    }
+  }
+}
+
+void launch_het_region_sums(const double* d_RC, const double* d_RS, const double* d_AA, const int* d_fgrid, int M,
+                            int J, int nifo, int nh, double* d_SL, double* d_lc, double* d_ls, cudaStream_t s) {
+  int NR = (M - 1) / J;
+  if (NR <= 0) return;
+  k_het_region_sums<<<NR * nifo, 256, 0, s>>>(d_RC, d_RS, d_AA, d_fgrid, M, J, nifo, nh, d_SL, d_lc, d_ls);
+}
+
+// <h|h> and <D-h|h> over [imin, imax) per detector, one block per detector (Utilities.c:716-736)
+__global__ void k_nwip_pairs(const double* __restrict__ h, const double* __restrict__ D, const double* __restrict__ S,
+                             int sn_stride, int N, int imin, int imax, double* __restrict__ out) {
+  __shared__ double red[32 * 2];
+  int id = blockIdx.x;
+  const double* hr = h + (size_t)id * N;
+  const double* dr = D + (size_t)id * N;
+  const double* sr = S + (size_t)id * sn_stride;
+  double acc[2] = {0.0, 0.0};
+  for (int i = imin + threadIdx.x; i < imax; i += blockDim.x) {
+    int k = N - i;
+    double s = sr[i];
+    acc[0] += (hr[i] * hr[i] + hr[k] * hr[k]) / s;
+    acc[1] += ((dr[i] - hr[i]) * hr[i] + (dr[k] - hr[k]) * hr[k]) / s;
+  }
+  block_sum<2>(acc, red);
+  if (threadIdx.x == 0) { out[2 * id] = 4.0 * acc[0]; out[2 * id + 1] = 4.0 * acc[1]; }
+}
+
+void launch_nwip_pairs(const double* d_h, const double* d_D, const double* d_S, int sn_stride, int N, int nifo,
+                       int imin, int imax, double* d_out, cudaStream_t s) {
+  k_nwip_pairs<<<nifo, 1024, 0, s>>>(d_h, d_D, d_S, sn_stride, N, imin, imax, d_out);
+}
+
+__global__ void k_nwip(const double* __restrict__ a, const double* __restrict__ b, const double* __restrict__ S,
+                       int imin, int imax, int N, double* __restrict__ out) {
+  __shared__ double red[32];
+  double acc[1] = {0.0};
+  for (int i = imin + threadIdx.x; i < imax; i += blockDim.x) {
+    int k = N - i;
+    acc[0] += (a[i] * b[i] + a[k] * b[k]) / S[i];
+  }
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) out[0] = 4.0 * acc[0];
+}
+
+void launch_nwip(const double* d_a, const double* d_b, const double* d_S, int imin, int imax, int N, double* d_out,
+                 cudaStream_t s) {
+  k_nwip<<<1, 1024, 0, s>>>(d_a, d_b, d_S, imin, imax, N, d_out);
+}
+
+}  // namespace qcbc

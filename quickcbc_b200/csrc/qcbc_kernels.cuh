@@ -1,0 +1,81 @@
+// Kernel launch interface shared by the C ABI (qcbc_capi.cu) and the kernels (qcbc_kernels.cu).
+#pragma once
+#include "qcbc_device.cuh"
+
+namespace qcbc {
+
+// Network geometry and band of one analysis (by value into every kernel).
+struct NetGeom {
+  int nifo;
+  int labels[kMaxIfo];
+  int N;                 // samples; bins are 0..N/2
+  int imin, imax;        // analysis band [imin, imax) (QuickCBC.c:4250-4252)
+  double GMST;
+  double Tobs;           // used for ts = Tobs - tc and sqrt(Tobs)
+  double df;             // 1/Tobs
+  int div_exact;         // 1: f_i = i*df equals i/Tobs bit for bit (power-of-two Tobs)
+  int pad;
+};
+
+// Device-resident data of one analysis, pre-weighted by the PSD and scaled by
+// sigma[id] so that the FP32 copy stays in range:
+//   wr = 4 sigma Re(D)/S,  wi = 4 sigma Im(D)/S,  ws = 4 sigma^2 / S  per bin.
+struct EventData {
+  const double* w64;     // [nifo][3][nh]
+  const float* w32;      // [nifo][3][nh]
+  int nh;                // row length (N/2)
+  double inv_sigma[kMaxIfo];
+};
+
+// Heterodyne summary tables on the device (layouts as the reference's struct Het, flattened):
+//   freq[M], amp/phase[nifo][M], IP[NR][J+1][J+1], SL/lc/ls[NR][nifo][J+1], aa/rc/rs[nifo][NR].
+struct HetData {
+  int M, J, NR, MN, MM;
+  double logLb;
+  const double *freq, *amp, *phase, *IP, *SL, *lc, *ls, *aa, *rc, *rs;
+};
+
+enum Precision { kFP64 = 0, kMixed = 1 };
+
+// status bits written by the setup kernel per parameter set
+enum RecStatus { kStOK = 0, kStBadMass = 1, kStBadSpin = 2, kStBadDist = 4, kStBadSpinFinal = 8, kStFcut = 16 };
+
+struct FullLaunch {
+  int tiles;             // blocks per parameter set
+  int threads;           // threads per block
+};
+
+void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
+                  int* d_status, cudaStream_t s);
+void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
+                     const FullLaunch& L, double* d_partials, cudaStream_t s);
+void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
+                          const NetGeom& g, const EventData& ev, double* d_lnl, double* d_rho, cudaStream_t s);
+void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
+                    Precision prec, int threads, double* d_lnl, cudaStream_t s);
+size_t het_smem_bytes(const NetGeom& g, const HetData& h);
+
+// waveform outputs for the reference-signature entry points
+void launch_amp_phase(const double* d_freq, int n, double phi0, double fRef, double m1_Msun, double m2_Msun,
+                      double chi1, double chi2, double dist, const QnmTable& q, PhdRec* d_rec, double* d_amp,
+                      double* d_phase, int* d_status, cudaStream_t s);
+// 4 sum_{i in [imin,imax)} (a_i b_i + a_{N-i} b_{N-i}) / S_i  (Utilities.c:716-736) into d_out[0]
+void launch_nwip(const double* d_a, const double* d_b, const double* d_S, int imin, int imax, int N, double* d_out,
+                 cudaStream_t s);
+void launch_fulltemplates(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq,
+                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s);
+void launch_fullphaseamp(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq, int n,
+                         PhdRec* d_rec, int* d_status, double* d_amp, double* d_phase, cudaStream_t s);
+
+// heterodyne setup pieces (FP64)
+void launch_het_bins(const double* d_h, const double* d_amp, const double* d_phase, const double* d_D,
+                     const double* d_S, int sn_stride, int N, int nifo, double* d_RC, double* d_RS, double* d_AA,
+                     cudaStream_t s);
+void launch_het_region_sums(const double* d_RC, const double* d_RS, const double* d_AA, const int* d_fgrid, int M,
+                            int J, int nifo, int nh, double* d_SL, double* d_lc, double* d_ls, cudaStream_t s);
+void launch_nwip_pairs(const double* d_h, const double* d_D, const double* d_S, int sn_stride, int N, int nifo,
+                       int imin, int imax, double* d_out /* nifo x 2: HH, HR */, cudaStream_t s);
+
+void upload_tables();    // constant-memory tables; call once per device
+
+}  // namespace qcbc

@@ -1,0 +1,206 @@
+"""Seeded synthetic events for the likelihood hot path.
+
+No public data set is used: every event is coloured Gaussian noise plus one
+injected IMRPhenomD signal, in the normalisation of the QuickCBC reference:
+
+* data ``D`` is the half-complex FFT scaled by sqrt(Tobs)/N
+  (QuickCBC.c:254-313), so the noise in bin i has Re, Im ~ N(0, S_i/4) and
+  <n|n> = 2 per bin under the inner product of Utilities.c:716-736;
+* ``SN`` is the analytic one-sided PSD
+  S(f) = 1e-49 [ x^-4.14 - 5 x^-2 + 111 (1 - x^2 + x^4/2) / (1 + x^2/2) ],
+  x = f / 215 Hz, stored per bin with row length N/2 + 1 (the reference's
+  ``double_matrix(Nifo, N/2)`` allocates N/2 + 1 entries, Utilities.c:2981);
+* ``freq`` is the reference's frequency vector: freq[0] = 1/Tobs and
+  freq[i] = i/Tobs (QuickCBC.c:419-420);
+* parameters use the reference's 11-entry layout (QuickCBC.c:1867):
+  [0] ln(Mc kg) [1] ln(Mt kg) [2] chi1 [3] chi2 [4] phi0 [5] t_c
+  [6] ln(D_L m) [7] alpha [8] sin(delta) [9] psi [10] cos(iota).
+
+The injected waveform comes from a caller-supplied template function
+(``template(params) -> h[Nifo, N]``), so a test can inject with the oracle and
+the benchmark can inject with the product; the distance is scaled so that the
+network optimal SNR over the analysis band equals the requested value.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+import numpy as np
+
+MSUN_SI = 1.988546954961461467461011951140572744e30
+PC_SI = 3.085677581491367278913937957796471611e16
+FMAX = 1024.0           # reference analysis band upper edge (ConstCBC.h:33)
+NP = 11
+
+
+def psd(f):
+    """Analytic PSD of the synthetic configs (one-sided, strain^2/Hz)."""
+    x = np.asarray(f, dtype=np.float64) / 215.0
+    x2 = x * x
+    return 1e-49 * (x ** -4.14 - 5.0 / x2 + 111.0 * (1.0 - x2 + 0.5 * x2 * x2) / (1.0 + 0.5 * x2))
+
+
+def masses_to_params(m1, m2):
+    """(m1, m2) in Msun -> (ln Mc_kg, ln Mt_kg)."""
+    mt = m1 + m2
+    eta = m1 * m2 / (mt * mt)
+    mc = mt * eta ** 0.6
+    return np.log(mc * MSUN_SI), np.log(mt * MSUN_SI)
+
+
+@dataclass
+class Event:
+    """One analysis: detector network, data, PSD, frequency grid, injection."""
+    labels: np.ndarray           # int32 [Nifo], 0=H1 1=L1 2=V1
+    Tobs: float
+    fs: float
+    N: int
+    fmin: float
+    GMST: float
+    D: np.ndarray                # [Nifo, N] half-complex
+    SN: np.ndarray               # [Nifo, N/2+1]
+    freq: np.ndarray             # [N/2]
+    inj: np.ndarray              # [11]
+    snr: float
+    seed: int
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def nifo(self):
+        return len(self.labels)
+
+    @property
+    def imin(self):
+        return int(self.Tobs * self.fmin)
+
+    @property
+    def imax(self):
+        return min(int(self.Tobs * FMAX), self.N // 2)
+
+
+def make_grid(Tobs, fs):
+    N = int(round(Tobs * fs))
+    freq = np.arange(N // 2, dtype=np.float64) / Tobs
+    freq[0] = 1.0 / Tobs
+    return N, freq
+
+
+def make_psd_rows(nifo, N, Tobs):
+    f = np.arange(N // 2 + 1, dtype=np.float64) / Tobs
+    f[0] = 1.0 / Tobs
+    S = psd(f)
+    return np.ascontiguousarray(np.broadcast_to(S, (nifo, N // 2 + 1)))
+
+
+def inner(a, b, S, imin, imax, N):
+    """4 sum_{i in [imin,imax)} (Re a Re b + Im a Im b)/S_i  (Utilities.c:716-736)."""
+    i = np.arange(imin, imax)
+    k = N - i
+    return 4.0 * np.sum((a[i] * b[i] + a[k] * b[k]) / S[i])
+
+
+def random_extrinsic(rng, p):
+    p[4] = rng.uniform(0.0, 2.0 * np.pi)
+    p[7] = rng.uniform(0.0, 2.0 * np.pi)
+    p[8] = rng.uniform(-1.0, 1.0)
+    p[9] = rng.uniform(0.0, np.pi)
+    p[10] = rng.uniform(-1.0, 1.0)
+    return p
+
+
+def make_event(template, *, labels, Tobs, fs, fmin, m1, m2, chi1, chi2, snr, seed, tc=None):
+    """Coloured Gaussian noise + one injection scaled to network SNR ``snr``.
+
+    ``template(net_info, params) -> h[Nifo, N]`` where ``net_info`` is a dict
+    with labels/Tobs/GMST/N/freq.
+    """
+    rng = np.random.default_rng(seed)
+    labels = np.asarray(labels, dtype=np.int32)
+    nifo = len(labels)
+    N, freq = make_grid(Tobs, fs)
+    SN = make_psd_rows(nifo, N, Tobs)
+    GMST = rng.uniform(0.0, 2.0 * np.pi)
+    p = np.zeros(NP)
+    p[0], p[1] = masses_to_params(m1, m2)
+    p[2], p[3] = chi1, chi2
+    p[5] = Tobs - 2.0 if tc is None else tc
+    p[6] = np.log(400e6 * PC_SI)
+    random_extrinsic(rng, p)
+    info = dict(labels=labels, Tobs=Tobs, GMST=GMST, N=N, freq=freq, fmin=fmin)
+    imin, imax = int(Tobs * fmin), min(int(Tobs * FMAX), N // 2)
+    h = template(info, p)
+    s2 = sum(inner(h[i], h[i], SN[i], imin, imax, N) for i in range(nifo))
+    if s2 > 0:
+        p[6] += np.log(np.sqrt(s2) / snr)
+        h = template(info, p)
+    D = np.zeros((nifo, N))
+    half = N // 2
+    for i in range(nifo):
+        sig = np.sqrt(SN[i, 1:half] / 4.0)
+        D[i, 1:half] = rng.normal(size=half - 1) * sig
+        D[i, N - 1:half:-1] = rng.normal(size=half - 1) * sig
+    D += h
+    D[:, 0] = 0.0
+    D[:, half] = 0.0
+    return Event(labels=labels, Tobs=float(Tobs), fs=float(fs), N=N, fmin=float(fmin), GMST=GMST,
+                 D=np.ascontiguousarray(D), SN=SN, freq=freq, inj=p, snr=float(snr), seed=seed)
+
+
+def draw_params(rng, B, inj, *, mc=(10.0, 30.0), q=(0.25, 1.0), chi=(-0.9, 0.9), dtc=0.05,
+                dl_factor=(0.5, 2.0)):
+    """Parameter sets drawn around an injection (chirp mass, mass ratio and
+    spins uniform, t_c jitter, uniform phase/polarisation, isotropic sky)."""
+    P = np.zeros((B, NP))
+    Mc = rng.uniform(*mc, size=B)
+    qq = rng.uniform(*q, size=B)
+    m1 = Mc * (1.0 + qq) ** 0.2 / qq ** 0.6
+    m2 = m1 * qq
+    P[:, 0], P[:, 1] = masses_to_params(m1, m2)
+    P[:, 2] = rng.uniform(*chi, size=B)
+    P[:, 3] = rng.uniform(*chi, size=B)
+    P[:, 4] = rng.uniform(0.0, 2.0 * np.pi, size=B)
+    P[:, 5] = inj[5] + rng.uniform(-dtc, dtc, size=B)
+    P[:, 6] = inj[6] + np.log(rng.uniform(*dl_factor, size=B))
+    P[:, 7] = rng.uniform(0.0, 2.0 * np.pi, size=B)
+    P[:, 8] = rng.uniform(-1.0, 1.0, size=B)
+    P[:, 9] = rng.uniform(0.0, np.pi, size=B)
+    P[:, 10] = rng.uniform(-1.0, 1.0, size=B)
+    return P
+
+
+def jitter_params(rng, B, center, scale=1e-3):
+    """Parameter sets in a small neighbourhood of ``center`` (chains near the
+    posterior peak); angular entries stay in range."""
+    P = np.tile(np.asarray(center, dtype=np.float64), (B, 1))
+    P[:, 0] += scale * 0.1 * rng.normal(size=B)
+    P[:, 1] += scale * rng.normal(size=B)
+    P[:, 2] = np.clip(P[:, 2] + 10 * scale * rng.normal(size=B), -0.95, 0.95)
+    P[:, 3] = np.clip(P[:, 3] + 10 * scale * rng.normal(size=B), -0.95, 0.95)
+    P[:, 4] = np.mod(P[:, 4] + 50 * scale * rng.normal(size=B), 2 * np.pi)
+    P[:, 5] += scale * 1e-2 * rng.normal(size=B)
+    P[:, 6] += 10 * scale * rng.normal(size=B)
+    P[:, 7] = np.mod(P[:, 7] + 10 * scale * rng.normal(size=B), 2 * np.pi)
+    P[:, 8] = np.clip(P[:, 8] + 10 * scale * rng.normal(size=B), -1, 1)
+    P[:, 9] = np.mod(P[:, 9] + 10 * scale * rng.normal(size=B), np.pi)
+    P[:, 10] = np.clip(P[:, 10] + 10 * scale * rng.normal(size=B), -1, 1)
+    # keep eta <= 0.25: Mc <= Mt * 0.25^(3/5)
+    lim = P[:, 1] + 0.6 * np.log(0.25)
+    P[:, 0] = np.minimum(P[:, 0], lim - 1e-9)
+    return P
+
+
+# --- the synthetic workloads (sizes from the reference's usage) -------------
+CONFIGS = {
+    1: dict(labels=[0, 1], Tobs=4.0, fs=2048.0, fmin=16.0, m1=36.0, m2=29.0, chi1=0.3, chi2=-0.1,
+            snr=24.0, seed=1000, batch=16),
+    2: dict(labels=[0, 1, 2], Tobs=16.0, fs=4096.0, fmin=20.0, m1=30.0, m2=25.0, chi1=0.2, chi2=0.1,
+            snr=20.0, seed=2000, batch=2048),
+    3: dict(labels=[0, 1, 2], Tobs=128.0, fs=4096.0, fmin=20.0, m1=1.45, m2=1.30, chi1=0.03, chi2=-0.02,
+            snr=30.0, seed=3000, batch=4096),
+}
+
+
+def config_event(c, template, **over):
+    kw = dict(CONFIGS[c])
+    kw.update(over)
+    kw.pop("batch", None)
+    return make_event(template, **kw)

@@ -1,0 +1,235 @@
+"""Parity of the CUDA path (called through the C ABI) with the reference's
+outputs (golden fixtures) and with the CPU oracle on the same seeded inputs.
+
+Tolerances:
+  FP64 plain form   lnL within 1e-8 absolute (reference arithmetic is FP64;
+                    differences come from libm vs CUDA transcendental rounding)
+  mixed precision   |lnL - lnL_FP64 oracle| <= 1e-3 (the stated target)
+"""
+import numpy as np
+import pytest
+
+import quickcbc_b200 as q
+from quickcbc_b200 import synth
+from conftest import GoldenEvent, oracle_template, load_golden
+
+pytestmark = pytest.mark.gpu
+
+LNL_ATOL_FP64 = 1e-8
+LNL_ATOL_MIXED = 1e-3
+
+
+@pytest.fixture(scope="module")
+def ev1(cfg1_event):
+    ev, z = cfg1_event
+    e = q.Event.from_synthetic(ev)
+    yield ev, z, e
+    e.close()
+
+
+@pytest.fixture(scope="module")
+def cfg2(ora):
+    ev = synth.config_event(2, oracle_template(ora))
+    e = q.Event.from_synthetic(ev)
+    yield ev, e
+    e.close()
+
+
+def test_amp_phase_vs_reference(golden, ora):
+    z = golden("wave.npz")
+    for k, m in enumerate(z["meta"]):
+        st, a, p = q.amp_phase(z["freq"], *m)
+        assert st == 0
+        ar, pr = z["amp"][k], z["phase"][k]
+        assert np.array_equal(ar != 0, a != 0)
+        nz = ar != 0
+        np.testing.assert_allclose(a[nz], ar[nz], rtol=1e-12)
+        np.testing.assert_allclose(p, pr, rtol=0, atol=1e-9 * max(1.0, np.abs(pr).max()))
+
+
+def test_amp_phase_domain_errors():
+    f = np.geomspace(10, 1000, 50)
+    st, _, _ = q.amp_phase(f, 0.0, 100.0, 30 * synth.MSUN_SI, 20 * synth.MSUN_SI, 1.2, 0.0, 1e25)
+    assert st == 33
+    st, _, _ = q.amp_phase(f, 0.0, 100.0, -1.0, 20 * synth.MSUN_SI, 0.1, 0.0, 1e25)
+    assert st == 33
+    # fCut below the first frequency (IMRPhenomD.c:228-233)
+    st, _, _ = q.amp_phase(np.array([500.0, 600.0]), 0.0, 100.0, 2e3 * synth.MSUN_SI, 1e3 * synth.MSUN_SI, 0, 0, 1e25)
+    assert st == 33
+
+
+def test_fulltemplates_vs_reference(ev1):
+    ev, z, _ = ev1
+    for H, k in zip(z["h"], z["h_idx"]):
+        h = q.fulltemplates(ev.labels, ev.GMST, ev.freq, z["params"][k], ev.N)
+        np.testing.assert_allclose(h, H, rtol=0, atol=1e-11 * np.abs(H).max())
+
+
+def test_fullphaseamp_vs_reference(ev1):
+    ev, z, _ = ev1
+    a, p = q.fullphaseamp(ev.labels, ev.GMST, ev.Tobs, ev.freq, z["params"][0], ev.N)
+    np.testing.assert_allclose(a, z["pa_amp"], rtol=1e-12, atol=1e-40)
+    np.testing.assert_allclose(p, z["pa_phase"], rtol=0, atol=1e-9 * np.abs(z["pa_phase"]).max())
+
+
+def test_lnl_full_fp64_vs_reference(ev1):
+    ev, z, e = ev1
+    L, rho = e.lnl_full(z["params"], q.FP64, rho=True)
+    np.testing.assert_allclose(L, z["lnl"], rtol=0, atol=LNL_ATOL_FP64)
+    np.testing.assert_allclose(rho, z["rho"], rtol=1e-9)
+
+
+def test_lnl_full_mixed_vs_fp64_oracle(ev1, ora):
+    ev, z, e = ev1
+    L = e.lnl_full(z["params"], q.MIXED)
+    Lo, _ = ora.lnl_full_batch(ev, z["params"])
+    assert np.max(np.abs(L - Lo)) <= LNL_ATOL_MIXED
+
+
+def test_lnl_full_cfg2_fp64_and_mixed(cfg2, ora):
+    ev, e = cfg2
+    rng = np.random.default_rng(2501)
+    P = np.vstack([synth.jitter_params(rng, 16, ev.inj), synth.draw_params(rng, 48, ev.inj)])
+    Lo, _ = ora.lnl_full_batch(ev, P)
+    L64 = e.lnl_full(P, q.FP64)
+    np.testing.assert_allclose(L64, Lo, rtol=0, atol=LNL_ATOL_FP64 * max(1.0, np.abs(Lo).max() / 100))
+    Lm = e.lnl_full(P, q.MIXED)
+    assert np.max(np.abs(Lm - Lo)) <= LNL_ATOL_MIXED
+
+
+def test_batch_equals_single_and_deterministic(cfg2):
+    ev, e = cfg2
+    rng = np.random.default_rng(2502)
+    P = synth.draw_params(rng, 24, ev.inj)
+    for prec in (q.FP64, q.MIXED):
+        Lb = e.lnl_full(P, prec)
+        Ls = np.array([e.lnl_full(p, prec)[0] for p in P[:6]])
+        # a single set gets more blocks per set than a batch, so the block sums differ in order
+        np.testing.assert_allclose(Ls, Lb[:6], rtol=0, atol=1e-9 if prec == q.FP64 else 2e-4)
+        assert np.array_equal(Lb, e.lnl_full(P, prec)), "repeat calls must be bit-identical"
+
+
+def test_launch_shapes_agree(cfg2):
+    """Tile count and block size are tuning knobs only: results agree across them."""
+    ev, e = cfg2
+    P = synth.draw_params(np.random.default_rng(2503), 8, ev.inj)
+    ref_L = e.lnl_full(P, q.FP64)
+    for tiles, threads in ((1, 256), (3, 128), (17, 64), (64, 256)):
+        e.set_launch(tiles, threads)
+        np.testing.assert_allclose(e.lnl_full(P, q.FP64), ref_L, rtol=0, atol=1e-9)
+        np.testing.assert_allclose(e.lnl_full(P, q.MIXED), ref_L, rtol=0, atol=LNL_ATOL_MIXED)
+    e.set_launch(0, 0)
+
+
+def test_invalid_parameter_sets_flagged(ev1):
+    ev, z, e = ev1
+    P = z["params"][:4].copy()
+    P[1, 2] = 1.5                      # spin outside [-1, 1]
+    P[3, 6] = -np.inf                  # zero distance
+    L = e.lnl_full(P, q.FP64, allow_invalid=True)
+    assert L[1] == -1e20 and L[3] == -1e20
+    np.testing.assert_allclose(L[[0, 2]], z["lnl"][[0, 2]], rtol=0, atol=LNL_ATOL_FP64)
+    with pytest.raises(q.QcbcError) as ei:
+        e.lnl_full(P, q.FP64)
+    assert ei.value.code == 33
+
+
+def test_empty_batch_and_empty_band(ev1, ora):
+    ev, z, e = ev1
+    assert e.lnl_full(np.zeros((0, 11)), q.FP64).shape == (0,)
+    # very heavy system: fCut = 0.2/(M Msun_s) below fmin, template is zero everywhere
+    p = z["params"][0].copy()
+    p[0], p[1] = synth.masses_to_params(1500.0, 1400.0)
+    Lo, _ = ora.lnl_full(ev, p)
+    assert Lo == 0.0
+    assert e.lnl_full(p, q.FP64)[0] == 0.0 and e.lnl_full(p, q.MIXED)[0] == 0.0
+    # merger time 0: fbegin is NaN in the reference, every bin is zeroed
+    p = z["params"][0].copy()
+    p[5] = -1.0
+    Lo, _ = ora.lnl_full(ev, p)
+    assert e.lnl_full(p, q.FP64)[0] == Lo
+
+
+@pytest.mark.parametrize("labels,Tobs,fs", [([1], 6.0, 2048.0), ([2, 1, 0], 5.0, 1024.0), ([0, 2], 4.0, 4096.0)])
+def test_networks_and_non_power_of_two_durations(ora, labels, Tobs, fs):
+    ev = synth.make_event(oracle_template(ora), labels=labels, Tobs=Tobs, fs=fs, fmin=16.0, m1=20.0, m2=15.0,
+                          chi1=0.2, chi2=-0.3, snr=14.0, seed=int(Tobs * 100 + fs))
+    e = q.Event.from_synthetic(ev)
+    P = synth.draw_params(np.random.default_rng(7), 12, ev.inj, mc=(6.0, 30.0))
+    Lo, _ = ora.lnl_full_batch(ev, P)
+    np.testing.assert_allclose(e.lnl_full(P, q.FP64), Lo, rtol=0, atol=1e-8)
+    assert np.max(np.abs(e.lnl_full(P, q.MIXED) - Lo)) <= LNL_ATOL_MIXED
+    e.close()
+
+
+def test_reference_signature_full_likelihood(ev1):
+    ev, z, _ = ev1
+    q.set_band(16.0, 1024.0)
+    for bind in (False, True):
+        for k in (0, 5, 12):
+            L, rho = q.log_likelihood_full(ev.labels, ev.GMST, ev.D, z["params"][k], ev.freq, ev.SN, ev.N, ev.Tobs,
+                                           bind=bind)
+            assert abs(L - z["lnl"][k]) < LNL_ATOL_FP64
+            np.testing.assert_allclose(rho, z["rho"][k], rtol=1e-9)
+
+
+def test_fourier_nwip(ev1):
+    ev, z, _ = ev1
+    a, b, S = ev.D[0], z["h"][0][0], ev.SN[0]
+    i = np.arange(64, 4096)
+    want = 4.0 * np.sum((a[i] * b[i] + a[ev.N - i] * b[ev.N - i]) / S[i])
+    got = q.fourier_nwip(a, b, S, 64, 4096, ev.N)
+    assert abs(got - want) <= 1e-12 * max(1.0, abs(want))
+
+
+# ---------------------------------------------------------------- heterodyne
+def test_het_setup_tables_vs_reference(ev1, golden):
+    ev, _, e = ev1
+    h = golden("het1.npz")
+    e.het_setup(h["pref"], h["fgrid"], int(h["MN"]), int(h["MM"]), int(h["J"]))
+    t = e.het_export()
+    assert abs(t["logLb"] - float(h["logLb"])) < 1e-8
+    for k in ("amp", "phase", "IP", "SL", "lc", "ls", "aa", "rc", "rs"):
+        np.testing.assert_allclose(t[k], h[k], rtol=0, atol=1e-10 * np.abs(h[k]).max(), err_msg=k)
+
+
+def test_lnl_het_vs_reference(ev1, golden):
+    ev, _, e = ev1
+    h = golden("het1.npz")
+    e.het_set(h)
+    L = e.lnl_het(h["params"], q.FP64)
+    np.testing.assert_allclose(L, h["lnl"], rtol=0, atol=LNL_ATOL_FP64)
+    Lm = e.lnl_het(h["params"], q.MIXED)
+    assert np.max(np.abs(Lm - h["lnl"])) <= LNL_ATOL_MIXED
+
+
+def test_reference_signature_heterodyne(ev1, golden):
+    ev, _, _ = ev1
+    h = golden("het1.npz")
+    H = q.LegacyHet(ev.labels, ev.GMST, ev.Tobs, h["fgrid"], int(h["MN"]), int(h["MM"]), int(h["J"]))
+    H.heterodyne(ev.D, h["pref"], ev.freq, ev.SN, ev.N)
+    t = H.tables()
+    assert abs(t["logLb"] - float(h["logLb"])) < 1e-8
+    np.testing.assert_allclose(t["SL"], h["SL"], rtol=0, atol=1e-10 * np.abs(h["SL"]).max())
+    for k in range(len(h["params"])):
+        assert abs(H.lnl(h["params"][k]) - h["lnl"][k]) < LNL_ATOL_FP64
+
+
+def test_cfg3_heterodyne_long_signal(ora):
+    """Config 3 (3 det, 128 s, 4096 Hz, BNS): reference het grid, tables set up on
+    the GPU in FP64, het lnL against the reference's value and the oracle."""
+    g = load_golden("grid3.npz")
+    ev = synth.config_event(3, oracle_template(ora))
+    assert abs(ev.GMST - float(g["GMST"])) == 0.0
+    e = q.Event.from_synthetic(ev)
+    e.het_setup(ev.inj, g["fgrid"], int(g["MN"]), int(g["MM"]), int(g["J"]))
+    t = e.het_export()
+    assert abs(t["logLb"] - float(g["logLb"])) < 1e-6
+    L = e.lnl_het(g["params"], q.FP64)
+    np.testing.assert_allclose(L, g["lnl"], rtol=0, atol=1e-6)
+    Lm = e.lnl_het(g["params"], q.MIXED)
+    assert np.max(np.abs(Lm - g["lnl"])) <= LNL_ATOL_MIXED
+    to = ora.heterodyne(ev, ev.inj, g["fgrid"], int(g["MN"]), int(g["MM"]), int(g["J"]))
+    Lo, _ = ora.lnl_het_batch(ev, to, g["params"])
+    np.testing.assert_allclose(L, Lo, rtol=0, atol=1e-7)
+    e.close()
