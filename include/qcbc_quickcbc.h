@@ -115,6 +115,20 @@ int IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, 
 /* replaces Utilities.c:716 */
 double fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N);
 
+/* The same seven functions under prefixed names, for a forwarding object that
+ * gives an unchanged QuickCBC build strong definitions. */
+double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
+                                    double* rho, int N, double Tobs);
+double qcbc_gpu_log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs);
+void qcbc_gpu_heterodyne(struct Net* net, struct Het* het, double** D, double* params, RealVector* freq,
+                         double** SN, int N, double Tobs);
+void qcbc_gpu_fulltemplates(struct Net* net, double** hwave, RealVector* freq, double* params, int N);
+void qcbc_gpu_fullphaseamp(struct Net* net, double** amp, double** phase, RealVector* freq, double* params, int N);
+int qcbc_gpu_IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, const double phi0,
+                                             const double fRef_in, const double m1_SI, const double m2_SI,
+                                             const double chi1, const double chi2, const double distance);
+double qcbc_gpu_fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N);
+
 #ifdef __cplusplus
 }
 #endif

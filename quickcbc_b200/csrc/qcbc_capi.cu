@@ -1143,3 +1143,31 @@ extern "C" double fourier_nwip(double* a, double* b, double* Sn, int imin, int i
   if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "fourier_nwip failed"); return 0.0; }
   return out;
 }
+
+// ------------------------------------------------------------------ prefixed aliases
+extern "C" double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq,
+                                               double** SN, double* rho, int N, double Tobs) {
+  return log_likelihood_full(net, D, params, freq, SN, rho, N, Tobs);
+}
+extern "C" double qcbc_gpu_log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs) {
+  return log_likelihood_het(net, het, params, Tobs);
+}
+extern "C" void qcbc_gpu_heterodyne(struct Net* net, struct Het* het, double** D, double* params, RealVector* freq,
+                                    double** SN, int N, double Tobs) {
+  heterodyne(net, het, D, params, freq, SN, N, Tobs);
+}
+extern "C" void qcbc_gpu_fulltemplates(struct Net* net, double** hwave, RealVector* freq, double* params, int N) {
+  fulltemplates(net, hwave, freq, params, N);
+}
+extern "C" void qcbc_gpu_fullphaseamp(struct Net* net, double** amp, double** phase, RealVector* freq, double* params,
+                                      int N) {
+  fullphaseamp(net, amp, phase, freq, params, N);
+}
+extern "C" int qcbc_gpu_IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, const double phi0,
+                                                        const double fRef_in, const double m1_SI, const double m2_SI,
+                                                        const double chi1, const double chi2, const double distance) {
+  return IMRPhenomDGenerateh22FDAmpPhase(h22, freq, phi0, fRef_in, m1_SI, m2_SI, chi1, chi2, distance);
+}
+extern "C" double qcbc_gpu_fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N) {
+  return fourier_nwip(a, b, Sn, imin, imax, N);
+}
