@@ -93,6 +93,32 @@ int qcbc_het_export(const qcbc_event* ev, int* fgrid, double* freq, double* amp,
 int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double* lnl, int precision);
 int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, int precision, void* stream);
 
+/* ---- allocation-free form (no counterpart in the reference) ---- */
+/* Some callers cannot allocate device memory at call time: code that runs inside
+ * another framework's runtime, which owns all device memory and hands the
+ * operation pre-allocated buffers, and long-running services that keep a fixed
+ * device-memory budget (cudaMalloc can fail under fragmentation, and cudaFree
+ * synchronises the whole device, stalling every other stream).  For them this
+ * entry point runs the full likelihood on device pointers they own (d_params
+ * [B][11], d_lnl [B], d_rho [B][nifo] or NULL) and allocates nothing: its
+ * scratch (records, status, tile partials) is a fixed array of
+ * QCBC_NOALLOC_SCRATCH_BYTES in device memory, part of the library, held by
+ * every GPU that loads the library until the process exits.
+ *  - B is limited to QCBC_NOALLOC_MAX_SETS; larger B returns QCBC_EINVAL.
+ *  - The event must have been opened (that allocates, once) on the current device.
+ *  - The first call on a device looks up the array's device address; make that
+ *    first call before any stream capture.
+ *  - All calls share the one array: calls whose GPU work overlaps (different
+ *    streams, or host threads without ordering) race and corrupt each other's
+ *    results.  Serialise them, e.g. on one stream.
+ *  - stream is a cudaStream_t passed as void* (NULL = the default stream);
+ *    results are ready when the work on that stream completes. */
+#define QCBC_NOALLOC_MAX_SETS 4096
+#define QCBC_NOALLOC_MAX_TILE_SLOTS 16384
+#define QCBC_NOALLOC_SCRATCH_BYTES 3162112
+int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
+                          int precision, void* stream);
+
 /* ---- launch tuning ---- */
 /* Blocks per parameter set and threads per block for the full likelihood
  * (0 = automatic: measured once per (bins, nifo, B, precision) and cached). */

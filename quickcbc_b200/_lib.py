@@ -80,6 +80,8 @@ def lib():
         L.qcbc_event_device_bytes.argtypes = [vp]
         L.qcbc_lnl_full.argtypes = [vp, _PD, i, _PD, _PD, i]
         L.qcbc_lnl_full_dev.argtypes = [vp, vp, i, vp, vp, i, vp]
+        L.qcbc_lnl_full_noalloc.argtypes = [vp, vp, i, vp, vp, i, vp]
+        L.qcbc_synchronize.argtypes = []
         L.qcbc_het_set.argtypes = [vp, C.POINTER(HetTables)]
         L.qcbc_het_setup.argtypes = [vp, _PD, pi, i, i, i, i]
         L.qcbc_het_sizes.argtypes = [vp, pi, pi, pi, pi, pi]

@@ -1171,3 +1171,67 @@ extern "C" int qcbc_gpu_IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22
 extern "C" double qcbc_gpu_fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N) {
   return fourier_nwip(a, b, Sn, imin, imax, N);
 }
+
+// ------------------------------------------------------------------ allocation-free entry point
+// Scratch of qcbc_lnl_full_noalloc in a file-scope device array: per-set records,
+// per-set status and per-(set, tile) partial sums for up to QCBC_NOALLOC_MAX_SETS
+// sets and QCBC_NOALLOC_MAX_TILE_SLOTS (set, tile) pairs.  Every GPU that loads
+// this library holds it until the process exits.  Nothing in it needs to start at
+// zero: each launch writes every record, status and partial it later reads.
+constexpr size_t kNaRecBytes = (size_t)QCBC_NOALLOC_MAX_SETS * sizeof(PhdRec);
+constexpr size_t kNaStatusOff = (kNaRecBytes + 255) / 256 * 256;
+constexpr size_t kNaPartOff = (kNaStatusOff + (size_t)QCBC_NOALLOC_MAX_SETS * sizeof(int) + 255) / 256 * 256;
+constexpr size_t kNaBytes = kNaPartOff + (size_t)QCBC_NOALLOC_MAX_TILE_SLOTS * 2 * kMaxIfo * sizeof(double);
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+static_assert(kNaBytes == QCBC_NOALLOC_SCRATCH_BYTES, "header size constant out of date");
+
+// Device address of g_noalloc_scratch per device.  In host code the array's name
+// only stands in for the symbol; the address comes from cudaGetSymbolAddress,
+// taken once per device with that device current.
+static void* g_noalloc_addr[16] = {nullptr};
+static std::mutex g_noalloc_mu;
+
+extern "C" int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
+                                     int precision, void* stream) {
+  if (!ev || !d_params || !d_lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B < 0) return fail(QCBC_EINVAL, "B < 0");
+  if (B == 0) return QCBC_OK;
+  if (B > QCBC_NOALLOC_MAX_SETS)
+    return fail(QCBC_EINVAL, "qcbc_lnl_full_noalloc: B=%d exceeds QCBC_NOALLOC_MAX_SETS=%d", B,
+                QCBC_NOALLOC_MAX_SETS);
+  int dev = 0;
+  CU(cudaGetDevice(&dev));
+  if (dev != ev->device)
+    return fail(QCBC_EINVAL, "event lives on device %d but device %d is current", ev->device, dev);
+  if (!g_dev[dev].ready) return fail(QCBC_EINVAL, "device %d not initialised (open an event first)", dev);
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess)
+        return fail(QCBC_ECUDA, "cudaGetSymbolAddress(g_noalloc_scratch): %s", cudaGetErrorString(e));
+      g_noalloc_addr[dev] = p;
+    }
+    base = g_noalloc_addr[dev];
+  }
+  FullLaunch L = choose_launch(ev, B, precision);
+  int max_tiles = QCBC_NOALLOC_MAX_TILE_SLOTS / B;
+  if (L.tiles > max_tiles) L.tiles = max_tiles;
+  if (L.tiles < 1) L.tiles = 1;
+  unsigned char* b = static_cast<unsigned char*>(base);
+  PhdRec* recs = reinterpret_cast<PhdRec*>(b);
+  int* status = reinterpret_cast<int*>(b + kNaStatusOff);
+  double* part = reinterpret_cast<double*>(b + kNaPartOff);
+  cudaStream_t s = (cudaStream_t)stream;
+  DeviceState& ds = g_dev[dev];
+  EventData ed = event_data(ev);
+  launch_setup(d_params, B, ev->g, ds.qnm, recs, status, s);
+  launch_lnl_full(recs, B, ev->g, ed, precision == QCBC_MIXED ? kMixed : kFP64, L, part, s);
+  launch_finalize_full(part, recs, status, B, L.tiles, ev->g, ed, d_lnl, d_rho, s);
+  tls_launches += 3;
+  CU(cudaGetLastError());
+  return QCBC_OK;
+}
