@@ -187,6 +187,24 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def run_profile(args):
+    """Warm-up then timed steps of the benchmark workload in one precision; three
+    kernel launches per step (k_setup, k_lnl_full, k_finalize_full)."""
+    import quickcbc_b200 as q
+    from quickcbc_b200 import _lib
+    _lib.check(_lib.lib().qcbc_init(0))
+    ev, P = make_workload()
+    e = q.Event.from_synthetic(ev)
+    dbuf = q.DeviceBuffer(P.nbytes)
+    dbuf.upload(P)
+    prec = q.MIXED if args.prec == "mixed" else q.FP64
+    q.time_lnl_full(e, dbuf, len(P), prec, args.warmup, flush_l2=False)
+    ms, kms = q.time_lnl_full(e, dbuf, len(P), prec, args.steps, flush_l2=True)
+    print(json.dumps({"profile": args.prec, "B": len(P), "step_ms": [float(x) for x in ms],
+                      "kernel_ms": [float(x) for x in kms], "tiles_threads": e.get_launch(len(P), prec)}))
+    e.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -194,11 +212,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--extra", action="store_true", help="also time the per-call drop-in and the het path")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling run: warm-up and timed steps of one precision only (for ncu)")
+    ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.profile:
+        return run_profile(args)
 
     rank, world, local = env_rank()
     dist = None
