@@ -7,7 +7,7 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libqcbc_gpu.so")
+LIB_PATH = os.environ.get("QCBC_LIB_PATH") or os.path.join(HERE, "libqcbc_gpu.so")
 
 QCBC_OK = 0
 QCBC_EDOM = 33

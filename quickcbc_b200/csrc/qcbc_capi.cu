@@ -48,6 +48,11 @@ struct DeviceState {
   double* d_qnm = nullptr;   // x, yr, mr, yd, md (5 * n)
   int n = 0;
   QnmTable qnm{};
+  // per-bin constants for the mixed kernel: (i^{1/3}, i^{-1/3}) and (log i, i^{3/4})
+  double2* d_tabA = nullptr;
+  double2* d_tabB = nullptr;
+  int tab_n = 0;
+  int* d_bucket = nullptr;   // QNM interval index per 0.001 of final spin
 };
 static std::mutex g_mu;
 static DeviceState g_dev[16];
@@ -91,8 +96,41 @@ static int upload_qnm(DeviceState& ds) {
   if (ds.d_qnm) cudaFree(ds.d_qnm);
   CU(cudaMalloc(&ds.d_qnm, all.size() * sizeof(double)));
   CU(cudaMemcpy(ds.d_qnm, all.data(), all.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // interval index for spins -1 + k/1000 (the table spacing is >= 0.001)
+  const std::vector<double>& x = g_qnm_host[0];
+  int nb = 2001;
+  std::vector<int> bucket(nb);
+  for (int k = 0, j = 0; k < nb; k++) {
+    double sk = -1.0 + k / 1000.0;
+    while (j < n - 2 && x[j + 1] <= sk) j++;
+    bucket[k] = j;
+  }
+  if (ds.d_bucket) cudaFree(ds.d_bucket);
+  CU(cudaMalloc(&ds.d_bucket, nb * sizeof(int)));
+  CU(cudaMemcpy(ds.d_bucket, bucket.data(), nb * sizeof(int), cudaMemcpyHostToDevice));
+  bool uniform_ok = x.front() >= -1.0 && x.back() <= 1.0;
+  for (int i = 1; i < n && uniform_ok; i++) uniform_ok = (x[i] - x[i - 1]) >= 0.999e-3;
   ds.n = n;
-  ds.qnm = QnmTable{ds.d_qnm, ds.d_qnm + n, ds.d_qnm + 2 * n, ds.d_qnm + 3 * n, ds.d_qnm + 4 * n, n};
+  ds.qnm = QnmTable{ds.d_qnm, ds.d_qnm + n, ds.d_qnm + 2 * n, ds.d_qnm + 3 * n, ds.d_qnm + 4 * n,
+                    uniform_ok ? ds.d_bucket : nullptr, n, nb};
+  return QCBC_OK;
+}
+
+// Bin tables cover bins [0, n); grown (never shrunk) under g_mu when an event needs more.
+static int ensure_bin_tables(DeviceState& ds, int n) {
+  if (ds.tab_n >= n) return QCBC_OK;
+  int want = std::max(n, 1 << 20);
+  double2 *a = nullptr, *b = nullptr;
+  CU(cudaMalloc(&a, (size_t)want * sizeof(double2)));
+  CU(cudaMalloc(&b, (size_t)want * sizeof(double2)));
+  launch_fill_bin_tables(a, b, want, 0);
+  tls_launches += 1;
+  CU(cudaDeviceSynchronize());
+  cudaFree(ds.d_tabA);
+  cudaFree(ds.d_tabB);
+  ds.d_tabA = a;
+  ds.d_tabB = b;
+  ds.tab_n = want;
   return QCBC_OK;
 }
 
@@ -113,7 +151,10 @@ extern "C" int qcbc_init(int device) {
   std::lock_guard<std::mutex> lk(g_mu);
   DeviceState& ds = g_dev[device];
   if (!ds.ready) {
+    upload_tables();
     int rc = upload_qnm(ds);
+    if (rc) return rc;
+    rc = ensure_bin_tables(ds, 1 << 20);
     if (rc) return rc;
     ds.ready = true;
   }
@@ -225,7 +266,7 @@ struct qcbc_event {
   double fmin = 16.0, fmax = 1024.0;
   int nh = 0;
   double* d_w64 = nullptr;
-  float* d_w32 = nullptr;
+  float4* d_w4 = nullptr;
   double* d_D = nullptr;     // raw data [nifo][N] (heterodyne setup)
   double* d_S = nullptr;     // raw PSD [nifo][nh+1]
   double* d_freq = nullptr;  // canonical frequencies [nh]
@@ -240,9 +281,13 @@ struct qcbc_event {
 static EventData event_data(const qcbc_event* ev) {
   EventData d{};
   d.w64 = ev->d_w64;
-  d.w32 = ev->d_w32;
+  d.w4 = ev->d_w4;
   d.nh = ev->nh;
   for (int k = 0; k < kMaxIfo; k++) d.inv_sigma[k] = ev->inv_sigma[k];
+  const DeviceState& ds = g_dev[ev->device];
+  d.tab_n = ds.tab_n;
+  d.tabA = ds.d_tabA;
+  d.tabB = ds.d_tabB;
   return d;
 }
 
@@ -304,9 +349,14 @@ static int check_geom(int nifo, const int* labels, double Tobs, int N) {
 // Data upload: weighted FP64/FP32 copies plus raw D, S (rows gathered on the host).
 static int event_upload(qcbc_event* ev, const double* const* Drows, const double* const* Srows) {
   const int nI = ev->g.nifo, N = ev->g.N, nh = N / 2;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int rc = ensure_bin_tables(g_dev[ev->device], nh + 1);
+    if (rc) return rc;
+  }
   ev->nh = nh;
   std::vector<double> w64((size_t)nI * 3 * nh, 0.0);
-  std::vector<float> w32((size_t)nI * 3 * nh, 0.0f);
+  std::vector<float4> w4((size_t)nI * nh, make_float4(0.f, 0.f, 0.f, 0.f));
   std::vector<double> Dall((size_t)nI * N), Sall((size_t)nI * (nh + 1), 0.0);
   int lo = std::max(ev->g.imin, 1), hi = std::min(ev->g.imax, nh);
   for (int id = 0; id < nI; id++) {
@@ -330,21 +380,27 @@ static int event_upload(qcbc_event* ev, const double* const* Drows, const double
       wi[i] = 4.0 * sigma * D[N - i] / s;
       ws[i] = 4.0 * sigma * sigma / s;
     }
-    for (int k = 0; k < 3 * nh; k++) w32[(size_t)id * 3 * nh + k] = (float)w64[(size_t)id * 3 * nh + k];
+    for (int i = 0; i < nh; i++) {
+      float4& v = w4[(size_t)id * nh + i];
+      v.x = (float)wr[i];
+      v.y = (float)wi[i];
+      v.z = (float)ws[i];
+      v.w = id == 0 ? (float)std::pow((double)(i > 0 ? i : 1), -7.0 / 6.0) : 0.0f;
+    }
   }
   std::vector<double> freq(nh);
   freq[0] = 1.0 / ev->g.Tobs;
   for (int i = 1; i < nh; i++) freq[i] = (double)i / ev->g.Tobs;
-  size_t b64 = w64.size() * 8, b32 = w32.size() * 4, bD = Dall.size() * 8, bS = Sall.size() * 8, bf = freq.size() * 8;
+  size_t b64 = w64.size() * 8, b32 = w4.size() * sizeof(float4), bD = Dall.size() * 8, bS = Sall.size() * 8, bf = freq.size() * 8;
   if (!ev->d_w64) {
     CU(cudaMalloc(&ev->d_w64, b64));
-    CU(cudaMalloc(&ev->d_w32, b32));
+    CU(cudaMalloc(&ev->d_w4, b32));
     CU(cudaMalloc(&ev->d_D, bD));
     CU(cudaMalloc(&ev->d_S, bS));
     CU(cudaMalloc(&ev->d_freq, bf));
   }
   CU(cudaMemcpy(ev->d_w64, w64.data(), b64, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ev->d_w32, w32.data(), b32, cudaMemcpyHostToDevice));
+  CU(cudaMemcpy(ev->d_w4, w4.data(), b32, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(ev->d_D, Dall.data(), bD, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(ev->d_S, Sall.data(), bS, cudaMemcpyHostToDevice));
   CU(cudaMemcpy(ev->d_freq, freq.data(), bf, cudaMemcpyHostToDevice));
@@ -354,9 +410,9 @@ static int event_upload(qcbc_event* ev, const double* const* Drows, const double
 }
 
 static void event_free_device(qcbc_event* ev) {
-  cudaFree(ev->d_w64); cudaFree(ev->d_w32); cudaFree(ev->d_D); cudaFree(ev->d_S); cudaFree(ev->d_freq);
+  cudaFree(ev->d_w64); cudaFree(ev->d_w4); cudaFree(ev->d_D); cudaFree(ev->d_S); cudaFree(ev->d_freq);
   cudaFree(ev->het.buf); cudaFree(ev->het.d_fgrid);
-  ev->d_w64 = nullptr; ev->d_w32 = nullptr; ev->d_D = nullptr; ev->d_S = nullptr; ev->d_freq = nullptr;
+  ev->d_w64 = nullptr; ev->d_w4 = nullptr; ev->d_D = nullptr; ev->d_S = nullptr; ev->d_freq = nullptr;
   ev->het.buf = nullptr; ev->het.d_fgrid = nullptr;
 }
 
@@ -445,7 +501,8 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   if (k0) cudaEventRecord(k0, s);
   launch_lnl_full(w->d_recs, B, g, ed, prec == QCBC_MIXED ? kMixed : kFP64, L, w->d_part, s);
   if (k1) cudaEventRecord(k1, s);
-  launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, d_lnl, d_rho, s);
+  launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, prec == QCBC_MIXED ? kMixed : kFP64,
+                       d_lnl, d_rho, s);
   tls_launches += 3;
   CU(cudaGetLastError());
   return QCBC_OK;
@@ -1230,7 +1287,8 @@ extern "C" int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int
   EventData ed = event_data(ev);
   launch_setup(d_params, B, ev->g, ds.qnm, recs, status, s);
   launch_lnl_full(recs, B, ev->g, ed, precision == QCBC_MIXED ? kMixed : kFP64, L, part, s);
-  launch_finalize_full(part, recs, status, B, L.tiles, ev->g, ed, d_lnl, d_rho, s);
+  launch_finalize_full(part, recs, status, B, L.tiles, ev->g, ed, precision == QCBC_MIXED ? kMixed : kFP64, d_lnl,
+                       d_rho, s);
   tls_launches += 3;
   CU(cudaGetLastError());
   return QCBC_OK;

@@ -57,6 +57,8 @@ struct PhdRec {
   // projection
   double fs, ts, sqT;
   double Fs[kMaxIfo], lam[kMaxIfo], td[kMaxIfo];
+  // scales of Mf = (Msec df) i for the per-bin tables of the mixed kernel
+  double mdf, mdf_third, mdf_rthird, mdf_log, mdf_m76, mdf_34;
   int i_lo, i_hi;      // bins with f > fbegin and f <= fCut (inclusive), clamped to the band
   int flags, pad;
 };
@@ -66,14 +68,13 @@ struct PhdRec {
 enum FitId { F_RHO1, F_RHO2, F_RHO3, F_GAM1, F_GAM2, F_GAM3, F_V2, F_AL1, F_AL2, F_AL3, F_AL4, F_AL5,
              F_BE1, F_BE2, F_BE3, F_SI1, F_SI2, F_SI3, F_SI4, F_COUNT };
 
-// antenna monomials: coefficient + exponents of cos psi, sin psi, cos delta, sin delta,
-// cos(alpha-GMST), sin(alpha-GMST); F+ 21 terms, Fx 18 terms per detector.  The tables
-// themselves (and the fit table) live in qcbc_kernels.cu's constant memory.
-struct Mono { double c; unsigned char e[8]; };
+// The fit and antenna tables live in qcbc_kernels.cu's constant memory.
 
 // QNM spline table (natural cubic spline over final spin), device global:
 // x[n], fring[n], fring''[n], fdamp[n], fdamp''[n]
-struct QnmTable { const double *x, *yr, *mr, *yd, *md; int n; };
+// bucket[k] = index of the interval holding spin -1 + k/1000 (k = 0..2000), so one or two
+// comparisons find the interval instead of a binary search over the table.
+struct QnmTable { const double *x, *yr, *mr, *yd, *md; const int* bucket; int n, nbucket; };
 
 struct Pow6 { double sixth, third, two_thirds, four_thirds, five_thirds, two, seven_thirds, eight_thirds; };
 
@@ -92,12 +93,26 @@ __device__ __forceinline__ Pow6 pow6(double x) {
   return p;
 }
 
-__device__ __forceinline__ double qnm_eval(const QnmTable& t, const double* y, const double* m2, double s) {
-  int lo = 0, hi = t.n - 1;
-  while (hi - lo > 1) {
-    int mid = (lo + hi) >> 1;
-    if (__ldg(t.x + mid) > s) hi = mid; else lo = mid;
+__device__ __forceinline__ int qnm_interval(const QnmTable& t, double s) {
+  int lo;
+  if (t.bucket) {
+    int k = (int)floor((s + 1.0) * 1000.0);
+    k = k < 0 ? 0 : (k >= t.nbucket ? t.nbucket - 1 : k);
+    lo = __ldg(t.bucket + k);
+    for (int it = 0; it < 4 && lo > 0 && __ldg(t.x + lo) > s; it++) lo--;
+    for (int it = 0; it < 4 && lo < t.n - 2 && __ldg(t.x + lo + 1) <= s; it++) lo++;
+  } else {
+    lo = 0;
+    int hi = t.n - 1;
+    while (hi - lo > 1) {
+      int mid = (lo + hi) >> 1;
+      if (__ldg(t.x + mid) > s) hi = mid; else lo = mid;
+    }
   }
+  return lo;
+}
+
+__device__ __forceinline__ double qnm_eval_at(const QnmTable& t, const double* y, const double* m2, int lo, double s) {
   double xl = __ldg(t.x + lo), h = __ldg(t.x + lo + 1) - xl, dx = s - xl;
   double Ml = __ldg(m2 + lo), Mr = __ldg(m2 + lo + 1), yl = __ldg(y + lo);
   double b = (__ldg(y + lo + 1) - yl) / h - h * (2.0 * Ml + Mr) / 6.0;

@@ -14,6 +14,7 @@
 // lnL), 5112-5299 (heterodyne), 5303-5444 (heterodyned lnL); Utilities.c
 // :587-629, 716-736, 995-1109; IMRPhenomD.c:413-563.
 #include "qcbc_kernels.cuh"
+#include <cmath>
 #include <cstdio>
 
 namespace qcbc {
@@ -41,46 +42,20 @@ __constant__ double c_fits[F_COUNT][11] = {
   {-14621.71522218357, -377812.8579387104, -9608.682631509726, -1710892.5257214056, 4332924.601416521, -22366.683262266528, -2501971.6386377467, 10274495.902259542, -85360.30079034246, -570025.3441737515, 4396844.346849777},
 };
 
-// F+ / Fx of H1, L1, V1 as polynomials with the reference's rounded coefficients
-// (Utilities.c:1004-1076).  Exponents: cos psi, sin psi, cos delta, sin delta,
-// cos(alpha-GMST), sin(alpha-GMST).
-__constant__ Mono c_antp[3][21] = {
-  {{0.3104536562,{2,0,0,0,1,1}},{0.494778091,{0,0,1,1,1,0}},{1.424276331,{2,0,0,2,2,0}},{-0.4559956644,{0,0,1,1,0,1}},
-   {-0.1552268274,{0,0,0,2,1,1}},{0.3104536562,{1,1,0,1,0,0}},{-0.1552268276,{0,0,0,0,1,1}},{-0.4928680677,{2,0,0,2,0,0}},
-   {1.424276334,{2,0,0,0,2,0}},{0.3104536558,{2,0,0,2,1,1}},{-0.9119913289,{1,1,1,0,1,0}},{-0.9314082637,{2,0,0,0,0,0}},
-   {-0.712138166,{0,0,0,0,2,0}},{0.9119913288,{2,0,1,1,0,1}},{-0.6209073089,{1,1,0,1,2,0}},{2.848552667,{1,1,0,1,1,1}},
-   {-0.9895561804,{2,0,1,1,1,0}},{0.2464340337,{0,0,0,2,0,0}},{-0.9895561811,{1,1,1,0,0,1}},{-0.7121381653,{0,0,0,2,2,0}},
-   {0.4657041323,{0,0,0,0,0,0}}},
-  {{-0.5608410611,{2,0,0,0,1,1}},{-0.4945891833,{0,0,1,1,1,0}},{-1.040573095,{2,0,0,2,2,0}},{0.363231261,{0,0,1,1,0,1}},
-   {0.2804205304,{0,0,0,2,1,1}},{-0.5608410611,{1,1,0,1,0,0}},{0.2804205305,{0,0,0,0,1,1}},{-0.3865389475,{2,0,0,2,0,0}},
-   {-1.040573095,{2,0,0,0,2,0}},{-0.5608410611,{2,0,0,2,1,1}},{0.7264625218,{1,1,1,0,1,0}},{-0.7135560209,{0,0,0,0,0,0}},
-   {1.427112041,{2,0,0,0,0,0}},{0.5202865467,{0,0,0,0,2,0}},{-0.7264625224,{2,0,1,1,0,1}},{1.121682123,{1,1,0,1,2,0}},
-   {-2.081146187,{1,1,0,1,1,1}},{0.9891783667,{2,0,1,1,1,0}},{0.1932694762,{0,0,0,2,0,0}},{0.9891783666,{1,1,1,0,0,1}},
-   {0.5202865474,{0,0,0,2,2,0}}},
-  {{0.3963351156,{2,0,0,0,1,1}},{0.465152434,{0,0,1,1,1,0}},{-1.383399753,{2,0,0,2,2,0}},{-0.3756662059,{0,0,1,1,0,1}},
-   {-0.1981675579,{0,0,0,2,1,1}},{0.3963351153,{1,1,0,1,0,0}},{-0.1981675578,{0,0,0,0,1,1}},{1.303555289,{2,0,0,2,0,0}},
-   {-1.383399752,{2,0,0,0,2,0}},{-0.039922232,{0,0,0,0,0,0}},{0.3963351158,{2,0,0,2,1,1}},{-0.7513324118,{1,1,1,0,1,0}},
-   {0.0798444642,{2,0,0,0,0,0}},{0.6916998761,{0,0,0,0,2,0}},{0.7513324118,{2,0,1,1,0,1}},{-0.792670233,{1,1,0,1,2,0}},
-   {-2.766799504,{1,1,0,1,1,1}},{-0.9303048681,{2,0,1,1,1,0}},{-0.6517776444,{0,0,0,2,0,0}},{-0.9303048681,{1,1,1,0,0,1}},
-   {0.6916998765,{0,0,0,2,2,0}}},
+// F+ / Fx of H1, L1, V1: the reference's polynomials in cos/sin of psi, delta and
+// (alpha - GMST) with its rounded coefficients (Utilities.c:1004-1076), rearranged as dense
+// rows over one basis of 21 (F+) and 18 (Fx) monomials shared by the three detectors.
+__constant__ double c_antP[3][21] = {
+  {0.3104536562, 0.494778091, 1.424276331, -0.4559956644, -0.1552268274, 0.3104536562, -0.1552268276, -0.4928680677, 1.424276334, 0.3104536558, -0.9119913289, -0.9314082637, -0.712138166, 0.9119913288, -0.6209073089, 2.848552667, -0.9895561804, 0.2464340337, -0.9895561811, -0.7121381653, 0.4657041323},
+  {-0.5608410611, -0.4945891833, -1.040573095, 0.363231261, 0.2804205304, -0.5608410611, 0.2804205305, -0.3865389475, -1.040573095, -0.5608410611, 0.7264625218, 1.427112041, 0.5202865467, -0.7264625224, 1.121682123, -2.081146187, 0.9891783667, 0.1932694762, 0.9891783666, 0.5202865474, -0.7135560209},
+  {0.3963351156, 0.465152434, -1.383399753, -0.3756662059, -0.1981675579, 0.3963351153, -0.1981675578, 1.303555289, -1.383399752, 0.3963351158, -0.7513324118, 0.0798444642, 0.6916998761, 0.7513324118, -0.792670233, -2.766799504, -0.9303048681, -0.6517776444, -0.9303048681, 0.6916998765, -0.039922232}
 };
-__constant__ Mono c_antx[3][18] = {
-  {{-1.424276332,{1,1,0,2,2,0}},{-0.3104536551,{1,1,0,0,1,1}},{-0.6209073087,{2,0,0,1,2,0}},{-0.989556182,{2,0,1,0,0,1}},
-   {0.3104536561,{0,0,0,1,2,0}},{0.9895561812,{1,1,1,1,1,0}},{-1.424276332,{0,0,0,1,1,1}},{-0.9119913298,{2,0,1,0,1,0}},
-   {2.848552668,{2,0,0,1,1,1}},{-0.911991329,{1,1,1,1,0,1}},{0.9314082638,{1,1,0,0,0,0}},{-1.424276333,{1,1,0,0,2,0}},
-   {-0.1552268276,{0,0,0,1,0,0}},{0.3104536564,{2,0,0,1,0,0}},{0.4947780906,{0,0,1,0,0,1}},{-0.3104536556,{1,1,0,2,1,1}},
-   {0.4928680679,{1,1,0,2,0,0}},{0.4559956636,{0,0,1,0,1,0}}},
-  {{1.040573095,{1,1,0,2,2,0}},{0.5608410611,{1,1,0,0,1,1}},{1.121682122,{2,0,0,1,2,0}},{0.9891783668,{2,0,1,0,0,1}},
-   {-0.5608410611,{0,0,0,1,2,0}},{-0.9891783668,{1,1,1,1,1,0}},{1.040573095,{0,0,0,1,1,1}},{0.7264625222,{2,0,1,0,1,0}},
-   {-2.081146187,{2,0,0,1,1,1}},{0.7264625218,{1,1,1,1,0,1}},{-1.427112042,{1,1,0,0,0,0}},{1.040573094,{1,1,0,0,2,0}},
-   {0.2804205304,{0,0,0,1,0,0}},{-0.560841061,{2,0,0,1,0,0}},{-0.4945891833,{0,0,1,0,0,1}},{0.5608410611,{1,1,0,2,1,1}},
-   {0.3865389466,{1,1,0,2,0,0}},{-0.3632312614,{0,0,1,0,1,0}}},
-  {{1.383399753,{1,1,0,2,2,0}},{-0.396335116,{1,1,0,0,1,1}},{-0.7926702326,{2,0,0,1,2,0}},{-0.9303048681,{2,0,1,0,0,1}},
-   {0.3963351158,{0,0,0,1,2,0}},{0.9303048686,{1,1,1,1,1,0}},{1.383399752,{0,0,0,1,1,1}},{-0.7513324118,{2,0,1,0,1,0}},
-   {-2.766799505,{2,0,0,1,1,1}},{-0.7513324118,{1,1,1,1,0,1}},{-0.0798444646,{1,1,0,0,0,0}},{1.383399752,{1,1,0,0,2,0}},
-   {-0.1981675579,{0,0,0,1,0,0}},{0.3963351158,{2,0,0,1,0,0}},{0.465152434,{0,0,1,0,0,1}},{-0.3963351158,{1,1,0,2,1,1}},
-   {-1.303555288,{1,1,0,2,0,0}},{0.3756662059,{0,0,1,0,1,0}}},
+__constant__ double c_antX[3][18] = {
+  {-1.424276332, -0.3104536551, -0.6209073087, -0.989556182, 0.3104536561, 0.9895561812, -1.424276332, -0.9119913298, 2.848552668, -0.911991329, 0.9314082638, -1.424276333, -0.1552268276, 0.3104536564, 0.4947780906, -0.3104536556, 0.4928680679, 0.4559956636},
+  {1.040573095, 0.5608410611, 1.121682122, 0.9891783668, -0.5608410611, -0.9891783668, 1.040573095, 0.7264625222, -2.081146187, 0.7264625218, -1.427112042, 1.040573094, 0.2804205304, -0.560841061, -0.4945891833, 0.5608410611, 0.3865389466, -0.3632312614},
+  {1.383399753, -0.396335116, -0.7926702326, -0.9303048681, 0.3963351158, 0.9303048686, 1.383399752, -0.7513324118, -2.766799505, -0.7513324118, -0.0798444646, 1.383399752, -0.1981675579, 0.3963351158, 0.465152434, -0.3963351158, -1.303555288, 0.3756662059}
 };
+
 // detector vertices, metres (Utilities.c:1078-1109)
 __constant__ double c_detpos[3][3] = {
   {-2.161414928e6, 3.834695183e6, 4.600350224e6},
@@ -95,18 +70,87 @@ __device__ __forceinline__ double fit_eval(int k, double eta, double chi) {
          (c[8] + c[9] * eta + c[10] * eta2) * xi3;
 }
 
-void upload_tables() {}   // tables are statically initialised __constant__ data
+// Frequency-independent constants of the setup: x^{1/6}-powers of pi and of the two fixed join
+// frequencies, and the PN quantities at the phase join, computed once on the host with the C
+// library exactly as the reference computes them (IMRPhenomD_internals.c:515-533, 1455-1493).
+struct SetupConst {
+  Pow6 pi6, f1p, fjp;
+  double vj[9];        // v^k at v = cbrt(pi * 0.018), k = 0..8
+  double logvj;        // log v there
+  double log_fj;       // log 0.018
+};
+__constant__ SetupConst c_setup;
+
+static Pow6 host_pow6(double x) {
+  Pow6 p;
+  p.sixth = std::pow(x, 1.0 / 6.0);
+  p.third = p.sixth * p.sixth;
+  p.two_thirds = x / p.third;
+  p.four_thirds = x * p.third;
+  p.five_thirds = p.four_thirds * p.third;
+  p.two = x * x;
+  p.seven_thirds = p.third * p.two;
+  p.eight_thirds = p.two_thirds * p.two;
+  return p;
+}
+
+void upload_tables() {
+  SetupConst h;
+  h.pi6 = host_pow6(kPi);
+  h.f1p = host_pow6(kAmpJoin);
+  h.fjp = host_pow6(kPhiJoin);
+  double v = std::cbrt(kPi * kPhiJoin);
+  h.vj[0] = 1.0;
+  for (int k = 1; k < 9; k++) h.vj[k] = v * h.vj[k - 1];
+  h.logvj = std::log(v);
+  h.log_fj = std::log(kPhiJoin);
+  cudaMemcpyToSymbol(c_setup, &h, sizeof(h));
+}   // tables are statically initialised __constant__ data
 
 // ---------------------------------------------------------------- setup
-__device__ double mono_sum(const Mono* t, int n, const double* v) {
-  double s = 0.0;
-  for (int k = 0; k < n; k++) {
-    double term = t[k].c;
-    for (int j = 0; j < 6; j++)
-      for (int e = 0; e < t[k].e[j]; e++) term *= v[j];
-    s += term;
-  }
-  return s;
+// The 39 antenna monomials for one sky position / polarisation (straight-line code).
+__device__ __forceinline__ void antenna_basis(double cp, double sp, double cd, double sd, double ca, double sa,
+                                              double* mp, double* mx) {
+  const double cp2 = cp * cp, sd2 = sd * sd, ca2 = ca * ca;
+  mp[0] = cp2*ca*sa;
+  mp[1] = cd*sd*ca;
+  mp[2] = cp2*sd2*ca2;
+  mp[3] = cd*sd*sa;
+  mp[4] = sd2*ca*sa;
+  mp[5] = cp*sp*sd;
+  mp[6] = ca*sa;
+  mp[7] = cp2*sd2;
+  mp[8] = cp2*ca2;
+  mp[9] = cp2*sd2*ca*sa;
+  mp[10] = cp*sp*cd*ca;
+  mp[11] = cp2;
+  mp[12] = ca2;
+  mp[13] = cp2*cd*sd*sa;
+  mp[14] = cp*sp*sd*ca2;
+  mp[15] = cp*sp*sd*ca*sa;
+  mp[16] = cp2*cd*sd*ca;
+  mp[17] = sd2;
+  mp[18] = cp*sp*cd*sa;
+  mp[19] = sd2*ca2;
+  mp[20] = 1.0;
+  mx[0] = cp*sp*sd2*ca2;
+  mx[1] = cp*sp*ca*sa;
+  mx[2] = cp2*sd*ca2;
+  mx[3] = cp2*cd*sa;
+  mx[4] = sd*ca2;
+  mx[5] = cp*sp*cd*sd*ca;
+  mx[6] = sd*ca*sa;
+  mx[7] = cp2*cd*ca;
+  mx[8] = cp2*sd*ca*sa;
+  mx[9] = cp*sp*cd*sd*sa;
+  mx[10] = cp*sp;
+  mx[11] = cp*sp*ca2;
+  mx[12] = sd;
+  mx[13] = cp2*sd;
+  mx[14] = cd*sa;
+  mx[15] = cp*sp*sd2*ca*sa;
+  mx[16] = cp*sp*sd2;
+  mx[17] = cd*ca;
 }
 
 // final spin, eq. 3.6 of arXiv:1508.07250
@@ -140,6 +184,45 @@ __device__ double damp_mrd(const PhdRec& c, double f) {
   double fg = c.fDM * c.g3, df = f - c.fRD, den = df * df + fg * fg;
   return amp_mrd(c, f) * (-c.g2 / fg - 2.0 * df / den);
 }
+__device__ double damp_ins_p(const PhdRec& c, double Mf, const Pow6& p) {
+  return (2.0 / 3.0) * c.ai[0] / p.third + c.ai[1] + (4.0 / 3.0) * c.ai[2] * p.third +
+         (5.0 / 3.0) * c.ai[3] * p.two_thirds + 2.0 * c.ai[4] * Mf + (7.0 / 3.0) * c.ai[5] * p.four_thirds +
+         (8.0 / 3.0) * c.ai[6] * p.five_thirds + 3.0 * c.ai[7] * p.two;
+}
+// d(phi_ins)/dMf at the join Mf = 0.018 from the host-computed powers of v there
+__device__ double dphi_ins_join(const PhdRec& c, const double* pv, const double* pvl, double s1, double s2, double s3,
+                                double s4, double pi_third, double pi_two_thirds) {
+  const double* v = c_setup.vj;
+  double logv = c_setup.logvj;
+  double D = 0.0;
+  D += 2.0 * pv[7] * v[7];
+  D += (pv[6] + pvl[6] * (1.0 + logv)) * v[6];
+  D += pvl[5] * v[5];
+  D += -1.0 * pv[4] * v[4];
+  D += -2.0 * pv[3] * v[3];
+  D += -3.0 * pv[2] * v[2];
+  D += -4.0 * pv[1] * v[1];
+  D += -5.0 * pv[0];
+  D /= v[8] * 3.0 / kPi;
+  D += (s1 + s2 * v[1] / pi_third + s3 * v[2] / pi_two_thirds + (s4 / kPi) * v[3]) / c.eta;
+  return D;
+}
+// phi_ins with log v supplied
+__device__ double phi_ins_logv(const PhdRec& c, double Mf, const Pow6& p, double logv) {
+  const double* q = c.pq;
+  double ph = q[0];
+  ph += q[1] * p.two_thirds;
+  ph += q[2] * p.third;
+  ph += q[3] * logv * p.third;
+  ph += q[4] * logv;
+  ph += q[5] / p.third;
+  ph += q[6] / p.two_thirds;
+  ph += q[7] / Mf;
+  ph += q[8] / p.five_thirds;
+  ph += (q[9] * Mf + q[10] * p.four_thirds + q[11] * p.five_thirds + q[12] * p.two) / c.eta;
+  return ph;
+}
+
 // d(phi_ins)/dMf (IMRPhenomD_internals.c:1455-1493); pv/pvl are the TaylorF2 series
 __device__ double dphi_ins(const PhdRec& c, const double* pv, const double* pvl, double s1, double s2, double s3,
                            double s4, double pi_third, double pi_two_thirds, double Mf) {
@@ -168,7 +251,7 @@ __device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, doub
   if (!(chi1_in <= 1.0 && chi1_in >= -1.0 && chi2_in <= 1.0 && chi2_in >= -1.0)) st |= kStBadSpin;
   double m1 = m1_in, m2 = m2_in, chi1 = chi1_in, chi2 = chi2_in;
   if (!(m1_in > m2_in)) { m1 = m2_in; m2 = m1_in; chi1 = chi2_in; chi2 = chi1_in; }
-  Pow6 pip = pow6(kPi);
+  const Pow6 pip = c_setup.pi6;
   c.pi_third = pip.third;
   double M = m1 + m2, eta = m1 * m2 / (M * M);
   c.eta = eta; c.inv_eta = 1.0 / eta;
@@ -181,8 +264,9 @@ __device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, doub
   if (!(fsp <= 1.0)) { st |= kStBadSpinFinal; fsp = 1.0; }
   if (!(fsp >= -1.0)) fsp = -1.0;
   double er = erad(eta, chi1, chi2);
-  c.fRD = qnm_eval(q, q.yr, q.mr, fsp) / (1.0 - er);
-  c.fDM = qnm_eval(q, q.yd, q.md, fsp) / (1.0 - er);
+  int qi = qnm_interval(q, fsp);
+  c.fRD = qnm_eval_at(q, q.yr, q.mr, qi, fsp) / (1.0 - er);
+  c.fDM = qnm_eval_at(q, q.yd, q.md, qi, fsp) / (1.0 - er);
   // amplitude
   c.g1 = fit_eval(F_GAM1, eta, chi); c.g2 = fit_eval(F_GAM2, eta, chi); c.g3 = fit_eval(F_GAM3, eta, chi);
   if (c.g2 <= 1)
@@ -217,9 +301,11 @@ __device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, doub
     // intermediate amplitude: quartic with value and slope at f1, value at f2, value and
     // slope at f3 (eqs. 21-26 of arXiv:1508.07253), kept in Newton form on nodes f1,f1,f2,f3,f3
     double f1 = kAmpJoin, f3 = c.fmax, f2 = f1 + (f3 - f1) / 2.0;
-    Pow6 p1 = pow6(f1);
-    double v1 = amp_ins(c, f1, p1), d1 = damp_ins(c, f1);
-    double v3 = amp_mrd(c, f3), d2 = damp_mrd(c, f3);
+    const Pow6 p1 = c_setup.f1p;
+    double v1 = amp_ins(c, f1, p1), d1 = damp_ins_p(c, f1, p1);
+    double v3 = amp_mrd(c, f3);
+    double fg3 = c.fDM * c.g3, df3 = f3 - c.fRD;
+    double d2 = v3 * (-c.g2 / fg3 - 2.0 * df3 / (df3 * df3 + fg3 * fg3));
     double v2 = fit_eval(F_V2, eta, chi);
     double q01 = d1, q12 = (v2 - v1) / (f2 - f1), q23 = (v3 - v2) / (f3 - f2), q34 = d2;
     double q012 = (q12 - q01) / (f2 - f1), q123 = (q23 - q12) / (f3 - f1), q234 = (q34 - q23) / (f3 - f2);
@@ -290,9 +376,10 @@ __device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, doub
   {
     // C^1 joins (IMRPhenomD_internals.c:1547-1584)
     double fj = kPhiJoin;
-    c.C2Int = dphi_ins(c, pv, pvl, s1, s2, s3, s4, pip.third, pip.two_thirds, fj) - dphi_int(c, fj);
-    Pow6 pj = pow6(fj);
-    c.C1Int = phi_ins(c, fj, pj) - 1.0 / eta * phi_int(c, fj) - c.C2Int * fj;
+    c.C2Int = dphi_ins_join(c, pv, pvl, s1, s2, s3, s4, pip.third, pip.two_thirds) - dphi_int(c, fj);
+    const Pow6 pj = c_setup.fjp;
+    double phi_int_fj = c.b1 * fj - c.b3 / (3. * fj * fj * fj) + c.b2 * c_setup.log_fj;
+    c.C1Int = phi_ins_logv(c, fj, pj, c_setup.logvj) - 1.0 / eta * phi_int_fj - c.C2Int * fj;
     c.fMRDJoin = 0.5 * c.fRD;
     double fm = c.fMRDJoin;
     double phiT = 1.0 / eta * phi_int(c, fm) + c.C1Int + c.C2Int * fm;
@@ -354,11 +441,18 @@ __device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, 
   c.sqT = sqrt(g.Tobs);
   double Ap = (1.0 + p[10] * p[10]) / 2.0, Ac = -p[10];
   double cd = sqrt(1.0 - p[8] * p[8]);
-  double ca = cos(g.GMST - p[7]), sa = sin(g.GMST - p[7]);
-  double v[6] = {cos(p[9]), sin(p[9]), cd, p[8], cos(p[7] - g.GMST), sin(p[7] - g.GMST)};
+  double sa, ca, sps, cps;
+  sincos(g.GMST - p[7], &sa, &ca);      // Times() angle; F_ant uses alpha - GMST = -(GMST - alpha)
+  sincos(p[9], &sps, &cps);
+  double mp[21], mx[18];
+  antenna_basis(cps, sps, cd, p[8], ca, -sa, mp, mx);
   for (int id = 0; id < g.nifo; id++) {
     int l = g.labels[id];
-    double fp = mono_sum(c_antp[l], 21, v), fx = mono_sum(c_antx[l], 18, v);
+    double fp = 0.0, fx = 0.0;
+#pragma unroll
+    for (int k = 0; k < 21; k++) fp += c_antP[l][k] * mp[k];
+#pragma unroll
+    for (int k = 0; k < 18; k++) fx += c_antX[l][k] * mx[k];
     c.Fs[id] = sqrt(Ap * Ap * fp * fp + Ac * Ac * fx * fx);
     double lam = atan2(Ac * fx, Ap * fp);
     if (lam < 0.0) lam += kTwoPi;
@@ -394,6 +488,15 @@ __device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, 
   }
   c.i_lo = lo;
   c.i_hi = hi;
+  c.mdf = c.Msec * g.df;
+  c.mdf_third = cbrt(c.mdf);
+  c.mdf_rthird = 1.0 / c.mdf_third;
+  c.mdf_log = log(c.mdf);
+  {
+    double sixth = sqrt(c.mdf_third), sq = sqrt(c.mdf);
+    c.mdf_m76 = 1.0 / (c.mdf * sixth);
+    c.mdf_34 = sqrt(c.mdf * sq);
+  }
   return st;
 }
 
@@ -413,7 +516,7 @@ __global__ void k_setup(const double* __restrict__ params, int B, NetGeom g, Qnm
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                   int* d_status, cudaStream_t s) {
   if (B <= 0) return;
-  int th = 64;
+  int th = 32;
   k_setup<<<(B + th - 1) / th, th, 0, s>>>(d_params, B, g, q, d_recs, d_status);
 }
 
@@ -491,38 +594,6 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
             acc[2 * id + 1] += amp * amp * ws;
           }
         }
-      } else {
-        float sd[NIFO], cd[NIFO], sh[NIFO], ch[NIFO];
-#pragma unroll
-        for (int id = 0; id < NIFO; id++) { sd[id] = cd[id] = sh[id] = ch[id] = 0.f; }
-        constexpr double kInv2Pi = 0.15915494309189533577;
-        double tsd[NIFO], lamc[NIFO];
-#pragma unroll
-        for (int id = 0; id < NIFO; id++) { tsd[id] = c.ts - c.td[id]; lamc[id] = c.lam[id] * kInv2Pi; }
-        for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
-          double f = bin_freq(g, i);
-          double Mf = c.Msec * f;
-          float amp;
-          double ph;
-          phd_eval_mixed(c, Mf, amp, ph);
-          double phc = ph * kInv2Pi;
-#pragma unroll
-          for (int id = 0; id < NIFO; id++) {
-            double cyc = fma(f, tsd[id], lamc[id] - phc);      // x / (2 pi)
-            float r = (float)(cyc - rint(cyc));
-            float sx, cx;
-            sincospif(2.0f * r, &sx, &cx);
-            const float* w = ev.w32 + (size_t)id * 3 * nh;
-            float wr = __ldg(w + i), wi = __ldg(w + nh + i), ws = __ldg(w + 2 * nh + i);
-            kahan_add(sd[id], cd[id], amp * fmaf(wr, cx, wi * sx));
-            kahan_add(sh[id], ch[id], amp * amp * ws);
-          }
-        }
-#pragma unroll
-        for (int id = 0; id < NIFO; id++) {
-          acc[2 * id] = (double)sd[id] - (double)cd[id];
-          acc[2 * id + 1] = (double)sh[id] - (double)ch[id];
-        }
       }
     }
   }
@@ -531,6 +602,196 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
     double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
 #pragma unroll
     for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  }
+}
+
+// ---------------------------------------------------------------- full lnL, mixed precision
+// Per bin i (f = i df, Mf = Msec f):
+//  * phase in FP64 from per-bin tables: Mf^{1/3} = (Msec df)^{1/3} i^{1/3}, Mf^{-1/3} likewise,
+//    log Mf = log(Msec df) + log i; reduced to one cycle in FP64, then one FP32 sincospi gives
+//    e^{-i phi(f)};
+//  * detector rotation e^{2 pi i (f (ts - td) + lambda/2pi)} = base(thread) x R[k] with a per-block
+//    FP32 table R[k] = e^{2 pi i k (blockDim df)(ts - td)} built in FP64;
+//  * amplitude in FP32 without the constant a0 (Msec df)^{-7/6} (applied in FP64 by the finaliser);
+//  * FP32 partial sums over 8 bins, accumulated in FP64.
+struct MixCoef {
+  float ai[8];
+  float hcf[5], h21, h31;            // intermediate: Newton coefficients, node offsets from hx1
+  float fg, g2_over_fg, fg_g1;       // merger-ringdown
+  float inv_fdm;                     // 1/fDM for the ringdown phase's atan
+};
+
+#ifndef QCBC_MIXED_MINBLOCKS
+#define QCBC_MIXED_MINBLOCKS 4
+#endif
+template <int NIFO>
+__global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g, EventData ev,
+                                                        int tiles, double* __restrict__ partials) {
+  __shared__ PhdRec rec;
+  __shared__ MixCoef mc;
+  __shared__ double red[32 * 2 * kMaxIfo];
+  extern __shared__ float2 s_rot[];   // [NIFO][nk]
+  const int bs = blockDim.x, tid = threadIdx.x;
+  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  {
+    const int nw = sizeof(PhdRec) / 8;
+    const double* src = reinterpret_cast<const double*>(recs + b);
+    double* dst = reinterpret_cast<double*>(&rec);
+    for (int k = tid; k < nw; k += bs) dst[k] = src[k];
+  }
+  __syncthreads();
+  const PhdRec& c = rec;
+  int i0 = 0, i1 = -1;
+  if (c.flags & kRecValid) {
+    int n = c.i_hi - c.i_lo + 1;
+    if (n > 0) {
+      int chunk = (n + tiles - 1) / tiles;
+      i0 = c.i_lo + t * chunk;
+      i1 = min(i0 + chunk - 1, c.i_hi);
+    }
+  }
+  const int nk = i1 >= i0 ? (i1 - i0 + bs) / bs : 0;
+  constexpr double kInv2Pi = 0.15915494309189533577;
+  const double Dstep = (double)bs * g.df;
+  for (int k = tid; k < nk; k += bs) {
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) {
+      double cyc = (double)k * (Dstep * (c.ts - c.td[id]));
+      double sv, cv;
+      sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
+      s_rot[id * nk + k] = make_float2((float)cv, (float)sv);
+    }
+  }
+  if (tid == 0) {
+    for (int k = 0; k < 8; k++) mc.ai[k] = (float)c.ai[k];
+    for (int k = 0; k < 5; k++) mc.hcf[k] = (float)c.hc[k];
+    mc.h21 = (float)(c.hx2 - c.hx1);
+    mc.h31 = (float)(c.hx3 - c.hx1);
+    double fg = c.fDM * c.g3;
+    mc.fg = (float)fg;
+    mc.g2_over_fg = (float)(c.g2 / fg);
+    mc.fg_g1 = (float)(fg * c.g1);
+    mc.inv_fdm = (float)(1.0 / c.fDM);
+  }
+  __syncthreads();
+  double acc[2 * NIFO];
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
+  int i = i0 + tid;
+  if (i <= i1) {
+    double f = g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
+    float2 base[NIFO];
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) {
+      double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi;
+      double sv, cv;
+      sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
+      base[id] = make_float2((float)cv, (float)sv);
+    }
+    const size_t nh = (size_t)ev.nh;
+    const float4* w4 = ev.w4;
+    const double Dmf = c.Msec * Dstep;
+    double Mf = c.Msec * f;
+    const double lnpi = 1.1447298858494002;     // log(pi)
+    int k = 0;
+    while (k < nk && i <= i1) {
+      float sd[NIFO], sh[NIFO];
+#pragma unroll
+      for (int id = 0; id < NIFO; id++) { sd[id] = 0.f; sh[id] = 0.f; }
+      for (int kk = 0; kk < 8 && k < nk && i <= i1; kk++, k++, i += bs, Mf += Dmf) {
+        const double2 tA = __ldg(ev.tabA + i), tB = __ldg(ev.tabB + i);
+        float4 wv[NIFO];
+#pragma unroll
+        for (int id = 0; id < NIFO; id++) wv[id] = __ldg(w4 + (size_t)id * nh + i);
+        double third = tA.x * c.mdf_third;
+        double r = tA.y * c.mdf_rthird;
+        double logMf = tB.x + c.mdf_log;
+        float m76 = wv[0].w;
+        // amplitude (relative to a0 (Msec df)^{-7/6}), FP32
+        float a;
+        if (Mf < kAmpJoin) {
+          float th = (float)third, m = (float)Mf;
+          float t2 = th * th, p43 = m * th, p53 = p43 * th, p2 = m * m;
+          a = 1.0f + t2 * mc.ai[0] + m * mc.ai[1] + p43 * mc.ai[2] + p53 * mc.ai[3] + p2 * mc.ai[4] +
+              (p2 * th) * mc.ai[5] + (p2 * t2) * mc.ai[6] + (m * p2) * mc.ai[7];
+        } else if (Mf >= c.fmax) {
+          float dfr = (float)(Mf - c.fRD);
+          a = __expf(-dfr * mc.g2_over_fg) * mc.fg_g1 / (dfr * dfr + mc.fg * mc.fg);
+        } else {
+          float x = (float)(Mf - c.hx1), x2 = x - mc.h21, x3 = x - mc.h31;
+          a = mc.hcf[0] + x * (mc.hcf[1] + x * (mc.hcf[2] + x2 * (mc.hcf[3] + x3 * mc.hcf[4])));
+        }
+        float amp = m76 * a;
+        // phase, FP64
+        double ph;
+        if (Mf < kPhiJoin) {
+          const double* q = c.pq;
+          double logv = (logMf + lnpi) * (1.0 / 3.0);
+          double r2 = r * r, r3 = r2 * r;
+          ph = q[0] + third * (q[2] + q[1] * third) + (q[3] * third + q[4]) * logv + r * q[5] + r2 * q[6] +
+               r3 * (q[7] + r2 * q[8]) + c.inv_eta * (Mf * (q[9] + third * (q[10] + third * q[11]) + q[12] * Mf));
+        } else if (Mf >= c.fMRDJoin) {
+          double f34 = tB.y * c.mdf_34;
+          double at = (double)atanf((float)(Mf - c.al5 * c.fRD) * mc.inv_fdm);
+          ph = (c.al1 * Mf - c.al2 * (r * r * r) + (4.0 / 3.0) * c.al3 * f34 + c.al4 * at) * c.inv_eta + c.C1MRD +
+               c.C2MRD * Mf;
+        } else {
+          double r3 = r * r * r;
+          ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r3 * r3 * r3 + c.b2 * logMf) * c.inv_eta + c.C1Int + c.C2Int * Mf;
+        }
+        ph -= c.t0 * (Mf - c.MfRef) + c.phi_pre;
+        double phc = ph * kInv2Pi;
+        float u = (float)(phc - rint(phc));
+        float sw, cw;
+        sincospif(2.0f * u, &sw, &cw);
+        float amp2 = amp * amp;
+#pragma unroll
+        for (int id = 0; id < NIFO; id++) {
+          float2 R = s_rot[id * nk + k];
+          float rc = base[id].x * R.x - base[id].y * R.y;
+          float rs = base[id].x * R.y + base[id].y * R.x;
+          float cx = rc * cw + rs * sw;            // e^{ix} = rot * e^{-i phi}
+          float sx = rs * cw - rc * sw;
+          sd[id] = fmaf(amp, fmaf(wv[id].x, cx, wv[id].y * sx), sd[id]);
+          sh[id] = fmaf(amp2, wv[id].z, sh[id]);
+        }
+      }
+#pragma unroll
+      for (int id = 0; id < NIFO; id++) { acc[2 * id] += (double)sd[id]; acc[2 * id + 1] += (double)sh[id]; }
+    }
+  }
+  block_sum<2 * NIFO>(acc, red);
+  if (tid == 0) {
+    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+#pragma unroll
+    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  }
+}
+
+// rotation-table length per block for a launch: ceil(max bins per tile / threads)
+static int mixed_nk(const NetGeom& g, const FullLaunch& L) {
+  int bins = max(1, g.imax - g.imin);
+  int chunk = (bins + L.tiles - 1) / L.tiles;
+  return (chunk + L.threads - 1) / L.threads + 1;
+}
+
+static void launch_full_mixed(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
+                              double* part, cudaStream_t s) {
+  dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
+  size_t smem = (size_t)mixed_nk(g, L) * g.nifo * sizeof(float2);
+  switch (g.nifo) {
+    case 1:
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_lnl_full_mixed<1><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
+      break;
+    case 2:
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_lnl_full_mixed<2><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
+      break;
+    default:
+      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      k_lnl_full_mixed<3><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
+      break;
   }
 }
 
@@ -549,12 +810,12 @@ void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventD
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, s);
-  else launch_full_prec<kMixed>(d_recs, B, g, ev, L, d_partials, s);
+  else launch_full_mixed(d_recs, B, g, ev, L, d_partials, s);
 }
 
 __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
                                 const int* __restrict__ status, int B, int tiles, NetGeom g, EventData ev,
-                                double* __restrict__ lnl, double* __restrict__ rho) {
+                                int mixed, double* __restrict__ lnl, double* __restrict__ rho) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   const PhdRec& c = recs[b];
@@ -572,6 +833,7 @@ __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRe
       sh += p[2 * id + 1];
     }
     double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * ev.inv_sigma[id];
+    if (mixed) K *= c.a0 * c.mdf_m76;       // the mixed kernel sums the amplitude without this factor
     double HD = K * sd, HH = K * K * sh;
     if (rho) rho[(size_t)b * g.nifo + id] = HD / sqrt(HH);
     L += HD - 0.5 * HH;
@@ -580,9 +842,24 @@ __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRe
 }
 
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
-                          const NetGeom& g, const EventData& ev, double* d_lnl, double* d_rho, cudaStream_t s) {
+                          const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
+                          cudaStream_t s) {
   if (B <= 0) return;
-  k_finalize_full<<<(B + 127) / 128, 128, 0, s>>>(d_partials, d_recs, d_status, B, tiles, g, ev, d_lnl, d_rho);
+  k_finalize_full<<<(B + 127) / 128, 128, 0, s>>>(d_partials, d_recs, d_status, B, tiles, g, ev,
+                                                  prec == kMixed ? 1 : 0, d_lnl, d_rho);
+}
+
+__global__ void k_fill_bin_tables(double2* __restrict__ A, double2* __restrict__ Bt, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double x = (double)(i > 0 ? i : 1);
+    double c3 = cbrt(x);
+    A[i] = make_double2(c3, 1.0 / c3);
+    Bt[i] = make_double2(log(x), pow(x, 0.75));
+  }
+}
+
+void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s) {
+  k_fill_bin_tables<<<(n + 255) / 256, 256, 0, s>>>(d_tabA, d_tabB, n);
 }
 
 // ---------------------------------------------------------------- heterodyned lnL

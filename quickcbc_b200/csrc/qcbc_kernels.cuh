@@ -21,10 +21,15 @@ struct NetGeom {
 // sigma[id] so that the FP32 copy stays in range:
 //   wr = 4 sigma Re(D)/S,  wi = 4 sigma Im(D)/S,  ws = 4 sigma^2 / S  per bin.
 struct EventData {
-  const double* w64;     // [nifo][3][nh]
-  const float* w32;      // [nifo][3][nh]
+  const double* w64;     // [nifo][3][nh]: wr, wi, ws rows (FP64 kernels)
+  const float4* w4;      // [nifo][nh]: (wr, wi, ws, x) with x = i^{-7/6} in detector 0 (mixed kernel)
   int nh;                // row length (N/2)
   double inv_sigma[kMaxIfo];
+  // per-bin constants shared by all events on a device (index = bin number i >= 1):
+  // tabA = (i^{1/3}, i^{-1/3}), tabB = (log i, i^{3/4})
+  const double2* tabA;
+  const double2* tabB;
+  int tab_n;
 };
 
 // Heterodyne summary tables on the device (layouts as the reference's struct Het, flattened):
@@ -50,7 +55,10 @@ void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTabl
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s);
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
-                          const NetGeom& g, const EventData& ev, double* d_lnl, double* d_rho, cudaStream_t s);
+                          const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
+                          cudaStream_t s);
+// fill the per-bin tables for bins [0, n)
+void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, int threads, double* d_lnl, cudaStream_t s);
 size_t het_smem_bytes(const NetGeom& g, const HetData& h);
