@@ -79,6 +79,30 @@ int qcbc_lnl_full(qcbc_event* ev, const double* params, int B, double* lnl, doub
 int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho, int precision,
                       void* stream);
 
+/* ---- many events in one launch ---- */
+/* A batch groups open events (same device) so that parameter sets of different
+ * analyses -- differing networks, durations, sample rates and bands -- are
+ * evaluated together.  Each set's signal band is cut into tiles of tile_bins
+ * bins; a persistent kernel takes (set, tile) work items from a device queue;
+ * the sequence (copies, setup, work list, kernel, finalise) is one captured CUDA
+ * graph per (batch-size bucket, precision), launched once per call.  A set's
+ * lnL depends only on its own inputs and the tiling, not on the other sets in
+ * the call.  Calls on one batch are serialised internally. */
+typedef struct qcbc_batch qcbc_batch;
+qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events);
+int qcbc_batch_destroy(qcbc_batch* batch);
+/* tile_bins > 0 and threads in {64,128,256}; 0 keeps the current/automatic value */
+int qcbc_batch_set_tiling(qcbc_batch* batch, int tile_bins, int threads);
+int qcbc_batch_get_tiling(qcbc_batch* batch, int* tile_bins, int* threads);
+/* Times each candidate tiling on the given call and keeps the fastest. */
+int qcbc_batch_autotune(qcbc_batch* batch, const int* event_of, const double* params, int B, int precision);
+/* event_of[B] indexes the batch's events; rho is [B][3] (unused detectors 0) or NULL. */
+int qcbc_lnl_multi(qcbc_batch* batch, const int* event_of, const double* params, int B, double* lnl, double* rho,
+                   int precision);
+/* Device time of `iters` graph launches on inputs already uploaded by a previous
+ * qcbc_lnl_multi call with the same B (no host copies inside the timed span). */
+int qcbc_time_lnl_multi(qcbc_batch* batch, int B, int precision, int iters, int flush_l2, float* ms);
+
 /* ---- heterodyned likelihood ---- */
 /* Upload tables computed elsewhere (e.g. by the reference's heterodyne()). */
 int qcbc_het_set(qcbc_event* ev, const qcbc_het_tables* t);

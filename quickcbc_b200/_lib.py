@@ -82,6 +82,14 @@ def lib():
         L.qcbc_lnl_full_dev.argtypes = [vp, vp, i, vp, vp, i, vp]
         L.qcbc_lnl_full_noalloc.argtypes = [vp, vp, i, vp, vp, i, vp]
         L.qcbc_synchronize.argtypes = []
+        L.qcbc_batch_create.restype = vp
+        L.qcbc_batch_create.argtypes = [C.POINTER(vp), i]
+        L.qcbc_batch_destroy.argtypes = [vp]
+        L.qcbc_batch_set_tiling.argtypes = [vp, i, i]
+        L.qcbc_batch_get_tiling.argtypes = [vp, pi, pi]
+        L.qcbc_batch_autotune.argtypes = [vp, pi, _PD, i, i]
+        L.qcbc_lnl_multi.argtypes = [vp, pi, _PD, i, _PD, _PD, i]
+        L.qcbc_time_lnl_multi.argtypes = [vp, i, i, i, i, C.POINTER(C.c_float)]
         L.qcbc_het_set.argtypes = [vp, C.POINTER(HetTables)]
         L.qcbc_het_setup.argtypes = [vp, _PD, pi, i, i, i, i]
         L.qcbc_het_sizes.argtypes = [vp, pi, pi, pi, pi, pi]

@@ -875,6 +875,256 @@ extern "C" int qcbc_time_lnl_het(qcbc_event* ev, const double* d_params, int B, 
   return QCBC_OK;
 }
 
+// ================================================================== multi-event batches
+struct MultiGraph {
+  int Bcap = 0, items_cap = 0, tile_bins = 0, threads = 0, blocks = 0;
+  int prec = 0;
+  double* d_params = nullptr; int* d_eof = nullptr; PhdRec* d_recs = nullptr; int* d_status = nullptr;
+  int* d_ntile = nullptr; int* d_off = nullptr; int* d_items = nullptr; int* d_counter = nullptr;
+  double* d_part = nullptr; double* d_lnl = nullptr; double* d_rho = nullptr;
+  double* h_params = nullptr; int* h_eof = nullptr; double* h_lnl = nullptr; double* h_rho = nullptr;
+  int* h_status = nullptr;
+  cudaGraphExec_t exec_full = nullptr, exec_dev = nullptr;
+};
+
+struct qcbc_batch {
+  int device = 0;
+  std::vector<qcbc_event*> events;
+  EventDesc* d_events = nullptr;
+  int nh_max = 0;
+  int tile_bins = 2048, threads = 256;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  unsigned char* d_flush = nullptr;
+  std::mutex mu;
+  std::map<long long, MultiGraph*> graphs;
+};
+
+static void free_graph(MultiGraph* m) {
+  if (!m) return;
+  if (m->exec_full) cudaGraphExecDestroy(m->exec_full);
+  if (m->exec_dev) cudaGraphExecDestroy(m->exec_dev);
+  cudaFree(m->d_params); cudaFree(m->d_eof); cudaFree(m->d_recs); cudaFree(m->d_status); cudaFree(m->d_ntile);
+  cudaFree(m->d_off); cudaFree(m->d_items); cudaFree(m->d_counter); cudaFree(m->d_part); cudaFree(m->d_lnl);
+  cudaFree(m->d_rho);
+  cudaFreeHost(m->h_params); cudaFreeHost(m->h_eof); cudaFreeHost(m->h_lnl); cudaFreeHost(m->h_rho);
+  cudaFreeHost(m->h_status);
+  delete m;
+}
+
+extern "C" qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events) {
+  if (!events || n_events <= 0) { fail(QCBC_EINVAL, "no events"); return nullptr; }
+  if (ensure_init()) return nullptr;
+  int dev = current_device();
+  std::vector<EventDesc> h(n_events);
+  qcbc_batch* bt = new qcbc_batch();
+  bt->device = dev;
+  for (int i = 0; i < n_events; i++) {
+    qcbc_event* ev = events[i];
+    if (!ev || !ev->has_data || ev->device != dev) {
+      fail(QCBC_EINVAL, "event %d is NULL, has no data or lives on another device", i);
+      delete bt;
+      return nullptr;
+    }
+    h[i].g = ev->g;
+    h[i].ev = event_data(ev);
+    bt->events.push_back(ev);
+    bt->nh_max = std::max(bt->nh_max, ev->nh);
+  }
+  if (cudaMalloc(&bt->d_events, sizeof(EventDesc) * n_events) != cudaSuccess ||
+      cudaMemcpy(bt->d_events, h.data(), sizeof(EventDesc) * n_events, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&bt->e0) != cudaSuccess || cudaEventCreate(&bt->e1) != cudaSuccess) {
+    fail(QCBC_ECUDA, "batch allocation failed");
+    cudaFree(bt->d_events);
+    delete bt;
+    return nullptr;
+  }
+  return bt;
+}
+
+extern "C" int qcbc_batch_destroy(qcbc_batch* bt) {
+  if (!bt) return QCBC_OK;
+  {
+    std::lock_guard<std::mutex> lk(bt->mu);
+    cudaStreamSynchronize(bt->stream);
+    for (auto& kv : bt->graphs) free_graph(kv.second);
+    bt->graphs.clear();
+  }
+  cudaFree(bt->d_events);
+  cudaFree(bt->d_flush);
+  cudaEventDestroy(bt->e0);
+  cudaEventDestroy(bt->e1);
+  cudaStreamDestroy(bt->stream);
+  delete bt;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_batch_set_tiling(qcbc_batch* bt, int tile_bins, int threads) {
+  if (!bt) return fail(QCBC_EINVAL, "NULL batch");
+  if (tile_bins < 0 || (threads != 0 && threads != 64 && threads != 128 && threads != 256))
+    return fail(QCBC_EINVAL, "tile_bins >= 0, threads in {64, 128, 256}");
+  std::lock_guard<std::mutex> lk(bt->mu);
+  if (tile_bins > 0) bt->tile_bins = tile_bins;
+  if (threads > 0) bt->threads = threads;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_batch_get_tiling(qcbc_batch* bt, int* tile_bins, int* threads) {
+  if (!bt || !tile_bins || !threads) return fail(QCBC_EINVAL, "NULL argument");
+  *tile_bins = bt->tile_bins;
+  *threads = bt->threads;
+  return QCBC_OK;
+}
+
+// Buffers + captured graphs for (Bcap, precision, tiling); caller holds bt->mu.
+static int multi_graph(qcbc_batch* bt, int Bcap, int prec, MultiGraph** out) {
+  long long key = ((long long)Bcap << 24) ^ ((long long)bt->tile_bins << 4) ^ ((long long)bt->threads << 1) ^ prec;
+  auto it = bt->graphs.find(key);
+  if (it != bt->graphs.end()) { *out = it->second; return QCBC_OK; }
+  MultiGraph* m = new MultiGraph();
+  m->Bcap = Bcap;
+  m->prec = prec;
+  m->tile_bins = bt->tile_bins;
+  m->threads = bt->threads;
+  long long tiles_per_set = (bt->nh_max + m->tile_bins - 1) / m->tile_bins;
+  long long cap = (long long)Bcap * tiles_per_set;
+  if (cap > (1LL << 30)) { delete m; return fail(QCBC_EINVAL, "work list too large"); }
+  m->items_cap = (int)cap;
+  cudaDeviceProp prop;
+  CU(cudaGetDeviceProperties(&prop, bt->device));
+  Precision P = prec == QCBC_MIXED ? kMixed : kFP64;
+  m->blocks = prop.multiProcessorCount * multi_blocks_per_sm(P, m->threads, m->tile_bins);
+  bool ok = cudaMalloc(&m->d_params, sizeof(double) * 11 * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_eof, sizeof(int) * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_recs, sizeof(PhdRec) * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_status, sizeof(int) * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_ntile, sizeof(int) * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_off, sizeof(int) * (Bcap + 1)) == cudaSuccess &&
+            cudaMalloc(&m->d_items, sizeof(int) * cap) == cudaSuccess &&
+            cudaMalloc(&m->d_counter, sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&m->d_part, sizeof(double) * 2 * kMaxIfo * cap) == cudaSuccess &&
+            cudaMalloc(&m->d_lnl, sizeof(double) * Bcap) == cudaSuccess &&
+            cudaMalloc(&m->d_rho, sizeof(double) * kMaxIfo * Bcap) == cudaSuccess &&
+            cudaMallocHost(&m->h_params, sizeof(double) * 11 * Bcap) == cudaSuccess &&
+            cudaMallocHost(&m->h_eof, sizeof(int) * Bcap) == cudaSuccess &&
+            cudaMallocHost(&m->h_lnl, sizeof(double) * Bcap) == cudaSuccess &&
+            cudaMallocHost(&m->h_rho, sizeof(double) * kMaxIfo * Bcap) == cudaSuccess &&
+            cudaMallocHost(&m->h_status, sizeof(int) * Bcap) == cudaSuccess;
+  if (!ok) { free_graph(m); return fail(QCBC_ENOMEM, "multi-event buffers for B=%d", Bcap); }
+  DeviceState& ds = g_dev[bt->device];
+  cudaStream_t s = bt->stream;
+  for (int with_copies = 1; with_copies >= 0; with_copies--) {
+    cudaGraph_t graph = nullptr;
+    CU(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    if (with_copies) {
+      cudaMemcpyAsync(m->d_params, m->h_params, sizeof(double) * 11 * Bcap, cudaMemcpyHostToDevice, s);
+      cudaMemcpyAsync(m->d_eof, m->h_eof, sizeof(int) * Bcap, cudaMemcpyHostToDevice, s);
+    }
+    cudaMemsetAsync(m->d_counter, 0, sizeof(int), s);
+    launch_setup_multi(m->d_params, m->d_eof, Bcap, bt->d_events, (int)bt->events.size(), ds.qnm, m->tile_bins,
+                       m->d_recs, m->d_status, m->d_ntile, s);
+    launch_scan_expand(m->d_ntile, Bcap, m->d_off, m->d_items, m->items_cap, s);
+    launch_lnl_multi(m->d_recs, bt->d_events, m->d_off, m->d_items, Bcap, m->tile_bins, m->items_cap, P, m->threads,
+                     m->blocks, m->d_counter, m->d_part, s);
+    launch_finalize_multi(m->d_part, m->d_recs, m->d_status, m->d_off, bt->d_events, Bcap, m->items_cap, P, m->d_lnl,
+                          m->d_rho, s);
+    if (with_copies) {
+      cudaMemcpyAsync(m->h_lnl, m->d_lnl, sizeof(double) * Bcap, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(m->h_rho, m->d_rho, sizeof(double) * kMaxIfo * Bcap, cudaMemcpyDeviceToHost, s);
+      cudaMemcpyAsync(m->h_status, m->d_status, sizeof(int) * Bcap, cudaMemcpyDeviceToHost, s);
+    }
+    cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (e != cudaSuccess) { free_graph(m); return fail(QCBC_ECUDA, "graph capture: %s", cudaGetErrorString(e)); }
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) { free_graph(m); return fail(QCBC_ECUDA, "graph instantiate: %s", cudaGetErrorString(e)); }
+    if (with_copies) m->exec_full = exec; else m->exec_dev = exec;
+  }
+  bt->graphs[key] = m;
+  *out = m;
+  return QCBC_OK;
+}
+
+static int bucket_of(int B) { return std::max(256, (B + 255) / 256 * 256); }
+
+static int run_multi(qcbc_batch* bt, const int* event_of, const double* params, int B, double* lnl, double* rho,
+                     int precision) {
+  MultiGraph* m = nullptr;
+  int rc = multi_graph(bt, bucket_of(B), precision, &m);
+  if (rc) return rc;
+  memcpy(m->h_params, params, sizeof(double) * 11 * (size_t)B);
+  memcpy(m->h_eof, event_of, sizeof(int) * (size_t)B);
+  for (int b = B; b < m->Bcap; b++) m->h_eof[b] = -1;      // padding sets: no event, no work
+  CU(cudaGraphLaunch(m->exec_full, bt->stream));
+  tls_launches += 4;
+  CU(cudaStreamSynchronize(bt->stream));
+  memcpy(lnl, m->h_lnl, sizeof(double) * (size_t)B);
+  if (rho) memcpy(rho, m->h_rho, sizeof(double) * kMaxIfo * (size_t)B);
+  int bad = 0;
+  for (int b = 0; b < B; b++) bad += m->h_status[b] != 0;
+  if (bad) return fail(QCBC_EDOM, "%d of %d parameter sets invalid (bad input or event index; lnL=-1e20)", bad, B);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_lnl_multi(qcbc_batch* bt, const int* event_of, const double* params, int B, double* lnl,
+                              double* rho, int precision) {
+  if (!bt || !event_of || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  int dev = current_device();
+  if (dev != bt->device) return fail(QCBC_EINVAL, "batch lives on device %d, %d is current", bt->device, dev);
+  std::lock_guard<std::mutex> lk(bt->mu);
+  return run_multi(bt, event_of, params, B, lnl, rho, precision);
+}
+
+extern "C" int qcbc_time_lnl_multi(qcbc_batch* bt, int B, int precision, int iters, int flush, float* ms) {
+  if (!bt || !ms || iters <= 0 || B <= 0) return fail(QCBC_EINVAL, "bad argument");
+  std::lock_guard<std::mutex> lk(bt->mu);
+  MultiGraph* m = nullptr;
+  int rc = multi_graph(bt, bucket_of(B), precision, &m);
+  if (rc) return rc;
+  size_t fb = (size_t)512 << 20;
+  if (flush && !bt->d_flush) CU(cudaMalloc(&bt->d_flush, fb));
+  for (int it = 0; it < iters; it++) {
+    if (flush) CU(cudaMemsetAsync(bt->d_flush, 0x5a, fb, bt->stream));
+    CU(cudaEventRecord(bt->e0, bt->stream));
+    CU(cudaGraphLaunch(m->exec_dev, bt->stream));
+    tls_launches += 4;
+    CU(cudaEventRecord(bt->e1, bt->stream));
+    CU(cudaEventSynchronize(bt->e1));
+    CU(cudaEventElapsedTime(&ms[it], bt->e0, bt->e1));
+  }
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_batch_autotune(qcbc_batch* bt, const int* event_of, const double* params, int B, int precision) {
+  if (!bt || !event_of || !params || B <= 0) return fail(QCBC_EINVAL, "bad argument");
+  static const int cand[][2] = {{1024, 128}, {2048, 256}, {4096, 256}, {8192, 256}, {2048, 128}, {1024, 256}};
+  std::vector<double> lnl(B);
+  float best = 1e30f;
+  int bt_tiles = bt->tile_bins, bt_threads = bt->threads;
+  for (auto& c : cand) {
+    {
+      std::lock_guard<std::mutex> lk(bt->mu);
+      bt->tile_bins = c[0];
+      bt->threads = c[1];
+      int rc = run_multi(bt, event_of, params, B, lnl.data(), nullptr, precision);
+      if (rc && rc != QCBC_EDOM) return rc;
+    }
+    float ms[5];
+    int rc = qcbc_time_lnl_multi(bt, B, precision, 5, 0, ms);
+    if (rc) return rc;
+    std::sort(ms, ms + 5);
+    if (ms[2] < best) { best = ms[2]; bt_tiles = c[0]; bt_threads = c[1]; }
+  }
+  std::lock_guard<std::mutex> lk(bt->mu);
+  bt->tile_bins = bt_tiles;
+  bt->threads = bt_threads;
+  return QCBC_OK;
+}
+
 // ================================================================== reference-signature drop-ins
 static double g_band_fmin = 16.0, g_band_fmax = 1024.0;   // ConstCBC.h:33-34
 

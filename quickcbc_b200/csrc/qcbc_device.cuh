@@ -60,7 +60,7 @@ struct PhdRec {
   // scales of Mf = (Msec df) i for the per-bin tables of the mixed kernel
   double mdf, mdf_third, mdf_rthird, mdf_log, mdf_m76, mdf_34;
   int i_lo, i_hi;      // bins with f > fbegin and f <= fCut (inclusive), clamped to the band
-  int flags, pad;
+  int flags, event;    // event: index into the event table (multi-event launches)
 };
 
 // Table V of arXiv:1508.07253: lambda = l00 + l10 eta + (l01 + l11 eta + l21 eta^2) xi

@@ -546,71 +546,42 @@ __device__ __forceinline__ void kahan_add(float& s, float& comp, float x) {
   s = t;
 }
 
-// ---------------------------------------------------------------- full lnL
-// One block = one tile of bins of one parameter set.  Per detector the block
-// accumulates  SD = sum amp (wr cos x + wi sin x)  and  SH = sum amp^2 ws
-// (wr/wi/ws carry 4/S and the event scale sigma); the finaliser applies the
-// per-detector factor K = Fs h22fac amp_scale / sqrt(T) / sigma:
+// ---------------------------------------------------------------- full lnL: one tile of bins
+// A block accumulates, per detector, SD = sum amp (wr cos x + wi sin x) and SH = sum amp^2 ws over
+// bins [i0, i1] of one parameter set (wr/wi/ws carry 4/S and the event scale sigma); the finaliser
+// applies the per-detector factor K = Fs h22fac amp_scale / sqrt(T) / sigma:
 //   <d|h> = K SD,  <h|h> = K^2 SH   (QuickCBC.c:4258-4266, Utilities.c:716-736).
-template <int PREC, int NIFO>
-__global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ recs, NetGeom g, EventData ev, int tiles,
-                                                  double* __restrict__ partials) {
-  __shared__ PhdRec rec;
-  __shared__ double red[32 * 2 * kMaxIfo];
-  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
-  {
-    const int nw = sizeof(PhdRec) / 8;
-    const double* src = reinterpret_cast<const double*>(recs + b);
-    double* dst = reinterpret_cast<double*>(&rec);
-    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
-  }
-  __syncthreads();
-  const PhdRec& c = rec;
-  double acc[2 * NIFO];
+// Results land in acc[2*NIFO] of every thread (summed over the block by the caller).
+
+// FP64 form: IMRPhenomD evaluated bin by bin as the reference does.
+template <int NIFO>
+__device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
+                                          double* acc) {
+  const size_t nh = (size_t)ev.nh;
+  for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
+    double f = bin_freq(g, i);
+    double Mf = c.Msec * f;
+    double amp, ph;
+    phd_eval64(c, Mf, amp, ph);
 #pragma unroll
-  for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
-  if (c.flags & kRecValid) {
-    int n = c.i_hi - c.i_lo + 1;
-    if (n > 0) {
-      int chunk = (n + tiles - 1) / tiles;
-      int i0 = c.i_lo + t * chunk;
-      int i1 = min(i0 + chunk - 1, c.i_hi);
-      const size_t nh = (size_t)ev.nh;
-      if (PREC == kFP64) {
-        for (int i = i0 + threadIdx.x; i <= i1; i += blockDim.x) {
-          double f = bin_freq(g, i);
-          double Mf = c.Msec * f;
-          double amp, ph;
-          phd_eval64(c, Mf, amp, ph);
-#pragma unroll
-          for (int id = 0; id < NIFO; id++) {
-            // x = 2 pi f (ts - td) + lambda - phi, evaluated in the reference's order
-            double x = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
-            double sx, cx;
-            sincos(reduce_2pi(x), &sx, &cx);
-            const double* w = ev.w64 + (size_t)id * 3 * nh;
-            double wr = __ldg(w + i), wi = __ldg(w + nh + i), ws = __ldg(w + 2 * nh + i);
-            acc[2 * id] += amp * (wr * cx + wi * sx);
-            acc[2 * id + 1] += amp * amp * ws;
-          }
-        }
-      }
+    for (int id = 0; id < NIFO; id++) {
+      // x = 2 pi f (ts - td) + lambda - phi, evaluated in the reference's order
+      double x = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+      double sx, cx;
+      sincos(reduce_2pi(x), &sx, &cx);
+      const double* w = ev.w64 + (size_t)id * 3 * nh;
+      double wr = __ldg(w + i), wi = __ldg(w + nh + i), ws = __ldg(w + 2 * nh + i);
+      acc[2 * id] += amp * (wr * cx + wi * sx);
+      acc[2 * id + 1] += amp * amp * ws;
     }
-  }
-  block_sum<2 * NIFO>(acc, red);
-  if (threadIdx.x == 0) {
-    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
-#pragma unroll
-    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
   }
 }
 
-// ---------------------------------------------------------------- full lnL, mixed precision
-// Per bin i (f = i df, Mf = Msec f):
+// Mixed form.  Per bin i (f = i df, Mf = Msec f):
 //  * phase in FP64 from per-bin tables: Mf^{1/3} = (Msec df)^{1/3} i^{1/3}, Mf^{-1/3} likewise,
-//    log Mf = log(Msec df) + log i; reduced to one cycle in FP64, then one FP32 sincospi gives
-//    e^{-i phi(f)};
-//  * detector rotation e^{2 pi i (f (ts - td) + lambda/2pi)} = base(thread) x R[k] with a per-block
+//    log Mf = log(Msec df) + log i, Mf^{3/4} likewise; reduced to one cycle in FP64, then one FP32
+//    sincospi gives e^{-i phi(f)};
+//  * detector rotation e^{2 pi i (f (ts - td) + lambda/2pi)} = base(thread) x R[k] with a per-tile
 //    FP32 table R[k] = e^{2 pi i k (blockDim df)(ts - td)} built in FP64;
 //  * amplitude in FP32 without the constant a0 (Msec df)^{-7/6} (applied in FP64 by the finaliser);
 //  * FP32 partial sums over 8 bins, accumulated in FP64.
@@ -621,36 +592,17 @@ struct MixCoef {
   float inv_fdm;                     // 1/fDM for the ringdown phase's atan
 };
 
-#ifndef QCBC_MIXED_MINBLOCKS
-#define QCBC_MIXED_MINBLOCKS 4
-#endif
+__device__ __forceinline__ int mixed_table_len(int i0, int i1) {
+  return i1 >= i0 ? (i1 - i0 + (int)blockDim.x) / (int)blockDim.x : 0;
+}
+
+// Builds the rotation table and FP32 coefficients (shared), then runs the bin loop.  Contains
+// __syncthreads(): every thread of the block must call it.
 template <int NIFO>
-__global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g, EventData ev,
-                                                        int tiles, double* __restrict__ partials) {
-  __shared__ PhdRec rec;
-  __shared__ MixCoef mc;
-  __shared__ double red[32 * 2 * kMaxIfo];
-  extern __shared__ float2 s_rot[];   // [NIFO][nk]
+__device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
+                                           MixCoef& mc, float2* s_rot, double* acc) {
   const int bs = blockDim.x, tid = threadIdx.x;
-  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
-  {
-    const int nw = sizeof(PhdRec) / 8;
-    const double* src = reinterpret_cast<const double*>(recs + b);
-    double* dst = reinterpret_cast<double*>(&rec);
-    for (int k = tid; k < nw; k += bs) dst[k] = src[k];
-  }
-  __syncthreads();
-  const PhdRec& c = rec;
-  int i0 = 0, i1 = -1;
-  if (c.flags & kRecValid) {
-    int n = c.i_hi - c.i_lo + 1;
-    if (n > 0) {
-      int chunk = (n + tiles - 1) / tiles;
-      i0 = c.i_lo + t * chunk;
-      i1 = min(i0 + chunk - 1, c.i_hi);
-    }
-  }
-  const int nk = i1 >= i0 ? (i1 - i0 + bs) / bs : 0;
+  const int nk = mixed_table_len(i0, i1);
   constexpr double kInv2Pi = 0.15915494309189533577;
   const double Dstep = (double)bs * g.df;
   for (int k = tid; k < nk; k += bs) {
@@ -674,94 +626,154 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
     mc.inv_fdm = (float)(1.0 / c.fDM);
   }
   __syncthreads();
+  int i = i0 + tid;
+  if (i > i1) return;
+  double f = g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
+  float2 base[NIFO];
+#pragma unroll
+  for (int id = 0; id < NIFO; id++) {
+    double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi;
+    double sv, cv;
+    sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
+    base[id] = make_float2((float)cv, (float)sv);
+  }
+  const size_t nh = (size_t)ev.nh;
+  const float4* w4 = ev.w4;
+  const double Dmf = c.Msec * Dstep;
+  double Mf = c.Msec * f;
+  const double lnpi = 1.1447298858494002;     // log(pi)
+  int k = 0;
+  while (k < nk && i <= i1) {
+    float sd[NIFO], sh[NIFO];
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) { sd[id] = 0.f; sh[id] = 0.f; }
+    for (int kk = 0; kk < 8 && k < nk && i <= i1; kk++, k++, i += bs, Mf += Dmf) {
+      const double2 tA = __ldg(ev.tabA + i), tB = __ldg(ev.tabB + i);
+      float4 wv[NIFO];
+#pragma unroll
+      for (int id = 0; id < NIFO; id++) wv[id] = __ldg(w4 + (size_t)id * nh + i);
+      double third = tA.x * c.mdf_third;
+      double r = tA.y * c.mdf_rthird;
+      double logMf = tB.x + c.mdf_log;
+      float m76 = wv[0].w;
+      // amplitude (relative to a0 (Msec df)^{-7/6}), FP32
+      float a;
+      if (Mf < kAmpJoin) {
+        float th = (float)third, m = (float)Mf;
+        float t2 = th * th, p43 = m * th, p53 = p43 * th, p2 = m * m;
+        a = 1.0f + t2 * mc.ai[0] + m * mc.ai[1] + p43 * mc.ai[2] + p53 * mc.ai[3] + p2 * mc.ai[4] +
+            (p2 * th) * mc.ai[5] + (p2 * t2) * mc.ai[6] + (m * p2) * mc.ai[7];
+      } else if (Mf >= c.fmax) {
+        float dfr = (float)(Mf - c.fRD);
+        a = __expf(-dfr * mc.g2_over_fg) * mc.fg_g1 / (dfr * dfr + mc.fg * mc.fg);
+      } else {
+        float x = (float)(Mf - c.hx1), x2 = x - mc.h21, x3 = x - mc.h31;
+        a = mc.hcf[0] + x * (mc.hcf[1] + x * (mc.hcf[2] + x2 * (mc.hcf[3] + x3 * mc.hcf[4])));
+      }
+      float amp = m76 * a;
+      // phase, FP64
+      double ph;
+      if (Mf < kPhiJoin) {
+        const double* q = c.pq;
+        double logv = (logMf + lnpi) * (1.0 / 3.0);
+        double r2 = r * r, r3 = r2 * r;
+        ph = q[0] + third * (q[2] + q[1] * third) + (q[3] * third + q[4]) * logv + r * q[5] + r2 * q[6] +
+             r3 * (q[7] + r2 * q[8]) + c.inv_eta * (Mf * (q[9] + third * (q[10] + third * q[11]) + q[12] * Mf));
+      } else if (Mf >= c.fMRDJoin) {
+        double f34 = tB.y * c.mdf_34;
+        double at = (double)atanf((float)(Mf - c.al5 * c.fRD) * mc.inv_fdm);
+        ph = (c.al1 * Mf - c.al2 * (r * r * r) + (4.0 / 3.0) * c.al3 * f34 + c.al4 * at) * c.inv_eta + c.C1MRD +
+             c.C2MRD * Mf;
+      } else {
+        double r3 = r * r * r;
+        ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r3 * r3 * r3 + c.b2 * logMf) * c.inv_eta + c.C1Int + c.C2Int * Mf;
+      }
+      ph -= c.t0 * (Mf - c.MfRef) + c.phi_pre;
+      double phc = ph * kInv2Pi;
+      float u = (float)(phc - rint(phc));
+      float sw, cw;
+      sincospif(2.0f * u, &sw, &cw);
+      float amp2 = amp * amp;
+#pragma unroll
+      for (int id = 0; id < NIFO; id++) {
+        float2 R = s_rot[id * nk + k];
+        float rc = base[id].x * R.x - base[id].y * R.y;
+        float rs = base[id].x * R.y + base[id].y * R.x;
+        float cx = rc * cw + rs * sw;            // e^{ix} = rot * e^{-i phi}
+        float sx = rs * cw - rc * sw;
+        sd[id] = fmaf(amp, fmaf(wv[id].x, cx, wv[id].y * sx), sd[id]);
+        sh[id] = fmaf(amp2, wv[id].z, sh[id]);
+      }
+    }
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) { acc[2 * id] += (double)sd[id]; acc[2 * id + 1] += (double)sh[id]; }
+  }
+}
+
+__device__ __forceinline__ void load_record(PhdRec& dst, const PhdRec* src) {
+  const int nw = sizeof(PhdRec) / 8;
+  const double* s = reinterpret_cast<const double*>(src);
+  double* d = reinterpret_cast<double*>(&dst);
+  for (int k = threadIdx.x; k < nw; k += blockDim.x) d[k] = s[k];
+}
+
+__device__ __forceinline__ void tile_range(const PhdRec& c, int tiles, int t, int& i0, int& i1) {
+  i0 = 0;
+  i1 = -1;
+  if (c.flags & kRecValid) {
+    int n = c.i_hi - c.i_lo + 1;
+    if (n > 0) {
+      int chunk = (n + tiles - 1) / tiles;
+      i0 = c.i_lo + t * chunk;
+      i1 = min(i0 + chunk - 1, c.i_hi);
+    }
+  }
+}
+
+template <int PREC, int NIFO>
+__global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ recs, NetGeom g, EventData ev, int tiles,
+                                                  double* __restrict__ partials) {
+  __shared__ PhdRec rec;
+  __shared__ double red[32 * 2 * kMaxIfo];
+  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  load_record(rec, recs + b);
+  __syncthreads();
+  int i0, i1;
+  tile_range(rec, tiles, t, i0, i1);
   double acc[2 * NIFO];
 #pragma unroll
   for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
-  int i = i0 + tid;
-  if (i <= i1) {
-    double f = g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
-    float2 base[NIFO];
-#pragma unroll
-    for (int id = 0; id < NIFO; id++) {
-      double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi;
-      double sv, cv;
-      sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
-      base[id] = make_float2((float)cv, (float)sv);
-    }
-    const size_t nh = (size_t)ev.nh;
-    const float4* w4 = ev.w4;
-    const double Dmf = c.Msec * Dstep;
-    double Mf = c.Msec * f;
-    const double lnpi = 1.1447298858494002;     // log(pi)
-    int k = 0;
-    while (k < nk && i <= i1) {
-      float sd[NIFO], sh[NIFO];
-#pragma unroll
-      for (int id = 0; id < NIFO; id++) { sd[id] = 0.f; sh[id] = 0.f; }
-      for (int kk = 0; kk < 8 && k < nk && i <= i1; kk++, k++, i += bs, Mf += Dmf) {
-        const double2 tA = __ldg(ev.tabA + i), tB = __ldg(ev.tabB + i);
-        float4 wv[NIFO];
-#pragma unroll
-        for (int id = 0; id < NIFO; id++) wv[id] = __ldg(w4 + (size_t)id * nh + i);
-        double third = tA.x * c.mdf_third;
-        double r = tA.y * c.mdf_rthird;
-        double logMf = tB.x + c.mdf_log;
-        float m76 = wv[0].w;
-        // amplitude (relative to a0 (Msec df)^{-7/6}), FP32
-        float a;
-        if (Mf < kAmpJoin) {
-          float th = (float)third, m = (float)Mf;
-          float t2 = th * th, p43 = m * th, p53 = p43 * th, p2 = m * m;
-          a = 1.0f + t2 * mc.ai[0] + m * mc.ai[1] + p43 * mc.ai[2] + p53 * mc.ai[3] + p2 * mc.ai[4] +
-              (p2 * th) * mc.ai[5] + (p2 * t2) * mc.ai[6] + (m * p2) * mc.ai[7];
-        } else if (Mf >= c.fmax) {
-          float dfr = (float)(Mf - c.fRD);
-          a = __expf(-dfr * mc.g2_over_fg) * mc.fg_g1 / (dfr * dfr + mc.fg * mc.fg);
-        } else {
-          float x = (float)(Mf - c.hx1), x2 = x - mc.h21, x3 = x - mc.h31;
-          a = mc.hcf[0] + x * (mc.hcf[1] + x * (mc.hcf[2] + x2 * (mc.hcf[3] + x3 * mc.hcf[4])));
-        }
-        float amp = m76 * a;
-        // phase, FP64
-        double ph;
-        if (Mf < kPhiJoin) {
-          const double* q = c.pq;
-          double logv = (logMf + lnpi) * (1.0 / 3.0);
-          double r2 = r * r, r3 = r2 * r;
-          ph = q[0] + third * (q[2] + q[1] * third) + (q[3] * third + q[4]) * logv + r * q[5] + r2 * q[6] +
-               r3 * (q[7] + r2 * q[8]) + c.inv_eta * (Mf * (q[9] + third * (q[10] + third * q[11]) + q[12] * Mf));
-        } else if (Mf >= c.fMRDJoin) {
-          double f34 = tB.y * c.mdf_34;
-          double at = (double)atanf((float)(Mf - c.al5 * c.fRD) * mc.inv_fdm);
-          ph = (c.al1 * Mf - c.al2 * (r * r * r) + (4.0 / 3.0) * c.al3 * f34 + c.al4 * at) * c.inv_eta + c.C1MRD +
-               c.C2MRD * Mf;
-        } else {
-          double r3 = r * r * r;
-          ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r3 * r3 * r3 + c.b2 * logMf) * c.inv_eta + c.C1Int + c.C2Int * Mf;
-        }
-        ph -= c.t0 * (Mf - c.MfRef) + c.phi_pre;
-        double phc = ph * kInv2Pi;
-        float u = (float)(phc - rint(phc));
-        float sw, cw;
-        sincospif(2.0f * u, &sw, &cw);
-        float amp2 = amp * amp;
-#pragma unroll
-        for (int id = 0; id < NIFO; id++) {
-          float2 R = s_rot[id * nk + k];
-          float rc = base[id].x * R.x - base[id].y * R.y;
-          float rs = base[id].x * R.y + base[id].y * R.x;
-          float cx = rc * cw + rs * sw;            // e^{ix} = rot * e^{-i phi}
-          float sx = rs * cw - rc * sw;
-          sd[id] = fmaf(amp, fmaf(wv[id].x, cx, wv[id].y * sx), sd[id]);
-          sh[id] = fmaf(amp2, wv[id].z, sh[id]);
-        }
-      }
-#pragma unroll
-      for (int id = 0; id < NIFO; id++) { acc[2 * id] += (double)sd[id]; acc[2 * id + 1] += (double)sh[id]; }
-    }
-  }
+  tile_fp64<NIFO>(rec, g, ev, i0, i1, acc);
   block_sum<2 * NIFO>(acc, red);
-  if (tid == 0) {
+  if (threadIdx.x == 0) {
+    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+#pragma unroll
+    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  }
+}
+
+#ifndef QCBC_MIXED_MINBLOCKS
+#define QCBC_MIXED_MINBLOCKS 4
+#endif
+template <int NIFO>
+__global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
+                                                                               EventData ev, int tiles,
+                                                                               double* __restrict__ partials) {
+  __shared__ PhdRec rec;
+  __shared__ MixCoef mc;
+  __shared__ double red[32 * 2 * kMaxIfo];
+  extern __shared__ float2 s_rot[];   // [NIFO][nk]
+  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  load_record(rec, recs + b);
+  __syncthreads();
+  int i0, i1;
+  tile_range(rec, tiles, t, i0, i1);
+  double acc[2 * NIFO];
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
+  tile_mixed<NIFO>(rec, g, ev, i0, i1, mc, s_rot, acc);
+  block_sum<2 * NIFO>(acc, red);
+  if (threadIdx.x == 0) {
     double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
 #pragma unroll
     for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
@@ -775,23 +787,22 @@ static int mixed_nk(const NetGeom& g, const FullLaunch& L) {
   return (chunk + L.threads - 1) / L.threads + 1;
 }
 
+template <int NIFO>
+static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
+                           double* part, cudaStream_t s) {
+  dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
+  size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_lnl_full_mixed<NIFO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
+}
+
 static void launch_full_mixed(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
                               double* part, cudaStream_t s) {
-  dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
-  size_t smem = (size_t)mixed_nk(g, L) * g.nifo * sizeof(float2);
   switch (g.nifo) {
-    case 1:
-      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_lnl_full_mixed<1><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
-      break;
-    case 2:
-      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_lnl_full_mixed<2><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
-      break;
-    default:
-      if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_full_mixed<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      k_lnl_full_mixed<3><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
-      break;
+    case 1: launch_mixed_n<1>(r, B, g, ev, L, part, s); break;
+    case 2: launch_mixed_n<2>(r, B, g, ev, L, part, s); break;
+    default: launch_mixed_n<3>(r, B, g, ev, L, part, s); break;
   }
 }
 
@@ -860,6 +871,210 @@ __global__ void k_fill_bin_tables(double2* __restrict__ A, double2* __restrict__
 
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s) {
   k_fill_bin_tables<<<(n + 255) / 256, 256, 0, s>>>(d_tabA, d_tabB, n);
+}
+
+// ---------------------------------------------------------------- multi-event launches
+__global__ void k_setup_multi(const double* __restrict__ params, const int* __restrict__ event_of, int B,
+                              const EventDesc* __restrict__ events, int n_events, QnmTable q, int tile_bins,
+                              PhdRec* __restrict__ recs, int* __restrict__ status, int* __restrict__ ntile) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  int e = event_of[b];
+  PhdRec c;
+  if (e < 0 || e >= n_events) {
+    c.flags = 0;
+    c.event = -1;
+    c.i_lo = 1;
+    c.i_hi = 0;
+    recs[b] = c;
+    status[b] = kStNoEvent;
+    ntile[b] = 0;
+    return;
+  }
+  double p[11];
+#pragma unroll
+  for (int k = 0; k < 11; k++) p[k] = params[(size_t)b * 11 + k];
+  NetGeom g = events[e].g;
+  int st = record_from_params(c, p, g, q);
+  c.event = e;
+  recs[b] = c;
+  status[b] = st;
+  int bins = (st == kStOK) ? c.i_hi - c.i_lo + 1 : 0;
+  ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+}
+
+void launch_setup_multi(const double* d_params, const int* d_event_of, int B, const EventDesc* d_events, int n_events,
+                        const QnmTable& q, int tile_bins, PhdRec* d_recs, int* d_status, int* d_ntile, cudaStream_t s) {
+  if (B <= 0) return;
+  k_setup_multi<<<(B + 31) / 32, 32, 0, s>>>(d_params, d_event_of, B, d_events, n_events, q, tile_bins, d_recs,
+                                             d_status, d_ntile);
+}
+
+// One block: exclusive scan of ntile into off[0..B], then expansion into items (bounded by items_cap).
+__global__ void k_scan_expand(const int* __restrict__ ntile, int B, int* __restrict__ off, int* __restrict__ items,
+                              int items_cap) {
+  __shared__ int wsum[32];
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int per = (B + nt - 1) / nt;
+  const int lo = tid * per, hi = min(lo + per, B);
+  int local = 0;
+  for (int b = lo; b < hi; b++) local += ntile[b];
+  // inclusive scan of thread totals
+  int lane = tid & 31, w = tid >> 5;
+  int x = local;
+  for (int o = 1; o < 32; o <<= 1) {
+    int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[w] = x;
+  __syncthreads();
+  if (w == 0) {
+    int v = lane < (nt >> 5) ? wsum[lane] : 0;
+    for (int o = 1; o < 32; o <<= 1) {
+      int y = __shfl_up_sync(0xffffffffu, v, o);
+      if (lane >= o) v += y;
+    }
+    wsum[lane] = v;
+  }
+  __syncthreads();
+  int run = x - local + (w > 0 ? wsum[w - 1] : 0);
+  if (tid == 0) off[0] = 0;
+  for (int b = lo; b < hi; b++) {
+    int n = ntile[b];
+    for (int t = 0; t < n; t++)
+      if (run + t < items_cap) items[run + t] = b;
+    run += n;
+    off[b + 1] = run;
+  }
+}
+
+void launch_scan_expand(const int* d_ntile, int B, int* d_off, int* d_items, int items_cap, cudaStream_t s) {
+  k_scan_expand<<<1, 1024, 0, s>>>(d_ntile, B, d_off, d_items, items_cap);
+}
+
+template <int PREC>
+__global__ void __launch_bounds__(256, 4) k_lnl_multi(const PhdRec* __restrict__ recs,
+                                                      const EventDesc* __restrict__ events,
+                                                      const int* __restrict__ off, const int* __restrict__ items,
+                                                      int B, int tile_bins, int items_cap, int* __restrict__ counter,
+                                                      double* __restrict__ partials) {
+  __shared__ PhdRec rec;
+  __shared__ MixCoef mc;
+  __shared__ EventDesc evd;
+  __shared__ int s_item, s_b;
+  __shared__ double red[32 * 2 * kMaxIfo];
+  extern __shared__ float2 s_rot[];   // [3][nk]
+  int total = off[B];
+  if (total > items_cap) total = items_cap;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      int it = atomicAdd(counter, 1);
+      s_item = it;
+      s_b = it < total ? items[it] : -1;
+    }
+    __syncthreads();
+    const int item = s_item, b = s_b;
+    if (item >= total) break;
+    load_record(rec, recs + b);
+    __syncthreads();
+    if (threadIdx.x == 0) evd = events[rec.event];
+    __syncthreads();
+    const int t = item - off[b];
+    const int i0 = rec.i_lo + t * tile_bins;
+    const int i1 = min(i0 + tile_bins - 1, rec.i_hi);
+    double acc[2 * kMaxIfo];
+#pragma unroll
+    for (int k = 0; k < 2 * kMaxIfo; k++) acc[k] = 0.0;
+    const int nifo = evd.g.nifo;
+    if (PREC == kFP64) {
+      if (nifo == 1) tile_fp64<1>(rec, evd.g, evd.ev, i0, i1, acc);
+      else if (nifo == 2) tile_fp64<2>(rec, evd.g, evd.ev, i0, i1, acc);
+      else tile_fp64<3>(rec, evd.g, evd.ev, i0, i1, acc);
+    } else {
+      if (nifo == 1) tile_mixed<1>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
+      else if (nifo == 2) tile_mixed<2>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
+      else tile_mixed<3>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
+    }
+    block_sum<2 * kMaxIfo>(acc, red);
+    if (threadIdx.x == 0) {
+      double* out = partials + (size_t)item * (2 * kMaxIfo);
+#pragma unroll
+      for (int k = 0; k < 2 * kMaxIfo; k++) out[k] = acc[k];
+    }
+    __syncthreads();
+  }
+}
+
+static size_t multi_smem(int threads, int tile_bins) {
+  int nk = (tile_bins + threads - 1) / threads + 1;
+  return (size_t)nk * kMaxIfo * sizeof(float2);
+}
+
+int multi_blocks_per_sm(Precision prec, int threads, int tile_bins) {
+  int n = 0;
+  size_t smem = multi_smem(threads, tile_bins);
+  if (prec == kFP64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lnl_multi<kFP64>, threads, smem);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lnl_multi<kMixed>, threads, smem);
+  return n > 0 ? n : 1;
+}
+
+void launch_lnl_multi(const PhdRec* d_recs, const EventDesc* d_events, const int* d_off, const int* d_items, int B,
+                      int tile_bins, int items_cap, Precision prec, int threads, int blocks, int* d_counter,
+                      double* d_partials, cudaStream_t s) {
+  if (B <= 0) return;
+  size_t smem = multi_smem(threads, tile_bins);
+  const int cap = items_cap;
+  if (prec == kFP64) {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_multi<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lnl_multi<kFP64><<<blocks, threads, smem, s>>>(d_recs, d_events, d_off, d_items, B, tile_bins, cap, d_counter,
+                                                     d_partials);
+  } else {
+    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_multi<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_lnl_multi<kMixed><<<blocks, threads, smem, s>>>(d_recs, d_events, d_off, d_items, B, tile_bins, cap, d_counter,
+                                                      d_partials);
+  }
+}
+
+__global__ void k_finalize_multi(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
+                                 const int* __restrict__ status, const int* __restrict__ off,
+                                 const EventDesc* __restrict__ events, int B, int items_cap, int mixed,
+                                 double* __restrict__ lnl, double* __restrict__ rho) {
+  int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const PhdRec& c = recs[b];
+  if (status[b] != kStOK) {
+    lnl[b] = -1.0e20;
+    if (rho) for (int id = 0; id < kMaxIfo; id++) rho[(size_t)b * kMaxIfo + id] = 0.0;
+    return;
+  }
+  const EventDesc& e = events[c.event];
+  double L = 0.0;
+  for (int id = 0; id < kMaxIfo; id++) {
+    if (id >= e.g.nifo) {
+      if (rho) rho[(size_t)b * kMaxIfo + id] = 0.0;
+      continue;
+    }
+    double sd = 0.0, sh = 0.0;
+    const int it_end = min(off[b + 1], items_cap);
+    for (int it = off[b]; it < it_end; it++) {
+      sd += partials[(size_t)it * (2 * kMaxIfo) + 2 * id];
+      sh += partials[(size_t)it * (2 * kMaxIfo) + 2 * id + 1];
+    }
+    double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * e.ev.inv_sigma[id];
+    if (mixed) K *= c.a0 * c.mdf_m76;
+    double HD = K * sd, HH = K * K * sh;
+    if (rho) rho[(size_t)b * kMaxIfo + id] = HD / sqrt(HH);
+    L += HD - 0.5 * HH;
+  }
+  lnl[b] = L;
+}
+
+void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const int* d_status, const int* d_off,
+                           const EventDesc* d_events, int B, int items_cap, Precision prec, double* d_lnl,
+                           double* d_rho, cudaStream_t s) {
+  if (B <= 0) return;
+  k_finalize_multi<<<(B + 127) / 128, 128, 0, s>>>(d_partials, d_recs, d_status, d_off, d_events, B, items_cap,
+                                                   prec == kMixed ? 1 : 0, d_lnl, d_rho);
 }
 
 // ---------------------------------------------------------------- heterodyned lnL

@@ -42,8 +42,15 @@ struct HetData {
 
 enum Precision { kFP64 = 0, kMixed = 1 };
 
+// One entry of the device-resident event table of a multi-event launch.
+struct EventDesc {
+  NetGeom g;
+  EventData ev;
+};
+
 // status bits written by the setup kernel per parameter set
-enum RecStatus { kStOK = 0, kStBadMass = 1, kStBadSpin = 2, kStBadDist = 4, kStBadSpinFinal = 8, kStFcut = 16 };
+enum RecStatus { kStOK = 0, kStBadMass = 1, kStBadSpin = 2, kStBadDist = 4, kStBadSpinFinal = 8, kStFcut = 16,
+                 kStNoEvent = 32 };
 
 struct FullLaunch {
   int tiles;             // blocks per parameter set
@@ -83,6 +90,22 @@ void launch_het_region_sums(const double* d_RC, const double* d_RS, const double
                             int J, int nifo, int nh, double* d_SL, double* d_lc, double* d_ls, cudaStream_t s);
 void launch_nwip_pairs(const double* d_h, const double* d_D, const double* d_S, int sn_stride, int N, int nifo,
                        int imin, int imax, double* d_out /* nifo x 2: HH, HR */, cudaStream_t s);
+
+// ---- multi-event launches: parameter set b belongs to event event_of[b]; its signal bins are cut
+// into tiles of tile_bins bins; the (set, tile) work items are processed by a persistent kernel.
+// A set's tiling depends only on its own bins, so its lnL is the same in any mix of events.
+void launch_setup_multi(const double* d_params, const int* d_event_of, int B, const EventDesc* d_events, int n_events,
+                        const QnmTable& q, int tile_bins, PhdRec* d_recs, int* d_status, int* d_ntile, cudaStream_t s);
+// d_off[0] = 0, d_off[b+1] = d_off[b] + ntile[b]; then d_items[d_off[b] + t] = b
+void launch_scan_expand(const int* d_ntile, int B, int* d_off, int* d_items, int items_cap, cudaStream_t s);
+// persistent kernel: `blocks` blocks pull work items from *d_counter (zeroed by the caller)
+void launch_lnl_multi(const PhdRec* d_recs, const EventDesc* d_events, const int* d_off, const int* d_items, int B,
+                      int tile_bins, int items_cap, Precision prec, int threads, int blocks, int* d_counter,
+                      double* d_partials, cudaStream_t s);
+void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const int* d_status, const int* d_off,
+                           const EventDesc* d_events, int B, int items_cap, Precision prec, double* d_lnl,
+                           double* d_rho, cudaStream_t s);
+int multi_blocks_per_sm(Precision prec, int threads, int tile_bins);
 
 void upload_tables();    // constant-memory tables; call once per device
 

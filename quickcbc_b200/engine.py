@@ -137,6 +137,66 @@ class Event:
         return out
 
 
+class Batch:
+    """Several open events evaluated together (qcbc_batch_create / qcbc_lnl_multi).
+
+    Parameter set b belongs to events[event_of[b]]; networks, durations, sample
+    rates and bands may differ between events.  One persistent kernel serves all
+    sets, launched as one captured CUDA graph per call.
+    """
+
+    def __init__(self, events):
+        self.events = list(events)
+        arr = (C.c_void_p * len(self.events))(*[e.handle for e in self.events])
+        self._h = lib().qcbc_batch_create(arr, len(self.events))
+        if not self._h:
+            raise QcbcError(-1, _lib.last_error())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().qcbc_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tiling(self, tile_bins=0, threads=0):
+        check(lib().qcbc_batch_set_tiling(self._h, int(tile_bins), int(threads)))
+
+    def tiling(self):
+        t, th = C.c_int(), C.c_int()
+        check(lib().qcbc_batch_get_tiling(self._h, C.byref(t), C.byref(th)))
+        return t.value, th.value
+
+    def autotune(self, event_of, params, precision=MIXED):
+        eo = np.ascontiguousarray(event_of, dtype=np.int32)
+        P = _f64(np.atleast_2d(params))
+        check(lib().qcbc_batch_autotune(self._h, eo.ctypes.data_as(C.POINTER(C.c_int)), _ptr(P), P.shape[0],
+                                        precision_code(precision)))
+        return self.tiling()
+
+    def lnl(self, event_of, params, precision=MIXED, rho=False, allow_invalid=False):
+        eo = np.ascontiguousarray(event_of, dtype=np.int32)
+        P = _f64(np.atleast_2d(params))
+        B = P.shape[0]
+        assert eo.shape == (B,)
+        out = np.zeros(B)
+        r = np.zeros((B, 3)) if rho else None
+        rc = lib().qcbc_lnl_multi(self._h, eo.ctypes.data_as(C.POINTER(C.c_int)), _ptr(P), B, _ptr(out),
+                                  _ptr(r) if rho else None, precision_code(precision))
+        if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
+            check(rc)
+        return (out, r) if rho else out
+
+    def time(self, B, precision=MIXED, iters=10, flush_l2=True):
+        ms = (C.c_float * iters)()
+        check(lib().qcbc_time_lnl_multi(self._h, int(B), precision_code(precision), iters, int(flush_l2), ms))
+        return np.array(ms[:])
+
+
 class DeviceBuffer:
     """Raw device allocation owned by the engine (for device-resident inputs)."""
 

@@ -204,3 +204,46 @@ def config_event(c, template, **over):
     kw.update(over)
     kw.pop("batch", None)
     return make_event(template, **kw)
+
+
+# --- config 4: many uneven events in one launch -----------------------------
+TOBS_CHOICES = (4.0, 8.0, 16.0, 32.0, 64.0)
+
+
+def chirp_time(mc_msun, f):
+    """Newtonian time to merger from frequency f (s)."""
+    return 2.18 * (1.21 / mc_msun) ** (5.0 / 3.0) * (100.0 / f) ** (8.0 / 3.0)
+
+
+def uneven_event_specs(n_events=256, seed=4000, fmin=20.0):
+    """Per-event settings of the uneven batch: total mass log-uniform 2.5-150 Msun,
+    mass ratio U[0.25, 1], aligned spins U[-0.5, 0.5], the shortest Tobs in
+    {4, 8, 16, 32, 64} s holding the chirp from fmin plus 2 s, fs 4096 Hz below
+    20 Msun total mass else 2048 Hz, 1-3 detectors in random order, SNR U[10, 40].
+    Event e uses seed `seed + e`."""
+    specs = []
+    for e in range(n_events):
+        rng = np.random.default_rng(seed + e)
+        mt = float(np.exp(rng.uniform(np.log(2.5), np.log(150.0))))
+        q = float(rng.uniform(0.25, 1.0))
+        m1, m2 = mt / (1.0 + q), mt * q / (1.0 + q)
+        mc = mt * (m1 * m2 / mt ** 2) ** 0.6
+        need = chirp_time(mc, fmin) + 2.5
+        Tobs = next((t for t in TOBS_CHOICES if t >= need), TOBS_CHOICES[-1])
+        fs = 4096.0 if mt < 20.0 else 2048.0
+        nifo = int(rng.integers(1, 4))
+        labels = [int(x) for x in rng.permutation(3)[:nifo]]
+        specs.append(dict(labels=labels, Tobs=Tobs, fs=fs, fmin=fmin, m1=m1, m2=m2,
+                          chi1=float(rng.uniform(-0.5, 0.5)), chi2=float(rng.uniform(-0.5, 0.5)),
+                          snr=float(rng.uniform(10.0, 40.0)), seed=seed + e))
+    return specs
+
+
+def uneven_params(events, chains=32, proposals=8, seed=4000 + 500000, scale=1e-3):
+    """chains x proposals parameter sets around each event's injection; returns
+    (event_of [B] int32, params [B, 11]) with sets grouped by event."""
+    rng = np.random.default_rng(seed)
+    n = chains * proposals
+    P = np.vstack([jitter_params(rng, n, ev.inj, scale=scale) for ev in events])
+    eo = np.repeat(np.arange(len(events), dtype=np.int32), n)
+    return eo, P
