@@ -187,6 +187,105 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def bench_cfg1_percall(q, eng, _lib):
+    """Config 1: plain FP64 drop-in, one log_likelihood_full call per chain (16 temperatures)."""
+    import ctypes as C
+    from quickcbc_b200 import synth
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    ev = synth.config_event(1, tmpl)
+    P = synth.jitter_params(np.random.default_rng(1000 + 500000), 16, ev.inj)
+    q.set_band(ev.fmin, 1024.0)
+    nh = eng._NetHolder(ev.labels, ev.Tobs, ev.GMST)
+    Dr, Sr = eng._rows(ev.D), eng._rows(ev.SN)
+    fr, rv = eng._rv(ev.freq)
+    _lib.check(_lib.lib().qcbc_bind_data(nh.ref, Dr, Sr, ev.N, ev.Tobs))
+    rho = np.zeros(4)
+    fn = _lib.lib().log_likelihood_full
+    Pc = [np.ascontiguousarray(p) for p in P]
+    for p in Pc:
+        fn(nh.ref, Dr, eng._ptr(p), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+    steps = 64
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        for p in Pc:
+            fn(nh.ref, Dr, eng._ptr(p), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+    dt = time.perf_counter() - t0
+    _lib.lib().qcbc_unbind_all()
+    q.set_band(16.0, 1024.0)
+    return {"workload": "config 1: H1/L1, 4 s, 2048 Hz, 16 temperatures x 1 call, FP64 drop-in",
+            "value": steps * 16 / dt, "unit": "lnL evals/s", "us_per_call": 1e6 * dt / (steps * 16)}
+
+
+def bench_cfg3_het(q):
+    """Config 3: 3 det, 128 s, 4096 Hz BNS; heterodyned lnL on the reference's het_space grid
+    (tests/golden/grid3.npz) for 4096 sets, and the full lnL for 512 sets."""
+    from quickcbc_b200 import synth
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    g = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
+    ev = synth.config_event(3, tmpl)
+    e = q.Event.from_synthetic(ev)
+    e.het_setup(ev.inj, g["fgrid"], int(g["MN"]), int(g["MM"]), int(g["J"]))
+    P = synth.jitter_params(np.random.default_rng(3000 + 500000), 4096, ev.inj, scale=1e-6)
+    dP = q.DeviceBuffer(P.nbytes)
+    dP.upload(P)
+    out = {"workload": "config 3: 3 det, 128 s, 4096 Hz, BNS 1.45+1.30, het grid M=%d" % len(g["fgrid"])}
+    Lh64 = e.lnl_het(P, q.FP64)
+    Lhm = e.lnl_het(P, q.MIXED)
+    for prec, name in ((q.MIXED, "het_mixed"), (q.FP64, "het_fp64")):
+        q.time_lnl_het(e, dP, len(P), prec, 3, flush_l2=True)
+        ms = q.time_lnl_het(e, dP, len(P), prec, 10, flush_l2=True)
+        out[name] = {"value": len(P) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
+    out["het_max_abs_dlnL_mixed_vs_fp64"] = float(np.max(np.abs(Lh64 - Lhm)))
+    Pf = P[:512]
+    dPf = q.DeviceBuffer(Pf.nbytes)
+    dPf.upload(Pf)
+    Lf64 = e.lnl_full(Pf, q.FP64)
+    Lfm = e.lnl_full(Pf, q.MIXED)
+    for prec, name in ((q.MIXED, "full_mixed"), (q.FP64, "full_fp64")):
+        q.time_lnl_full(e, dPf, len(Pf), prec, 2, flush_l2=True)
+        ms, _ = q.time_lnl_full(e, dPf, len(Pf), prec, 5, flush_l2=True)
+        out[name] = {"value": len(Pf) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
+    out["full_max_abs_dlnL_mixed_vs_fp64"] = float(np.max(np.abs(Lf64 - Lfm)))
+    out["het_vs_full_fp64_max_abs"] = float(np.max(np.abs(Lh64[:512] - Lf64)))
+    e.close()
+    return out
+
+
+def bench_cfg4_uneven(q):
+    """Config 4: 256 uneven events x (32 chains x 8 proposals) in one graph-captured
+    persistent launch, autotuned tiling, mixed and FP64."""
+    from quickcbc_b200 import synth
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    evs = [synth.make_event(tmpl, **s) for s in synth.uneven_event_specs(256)]
+    hs = [q.Event.from_synthetic(x) for x in evs]
+    b = q.Batch(hs)
+    eo, P = synth.uneven_params(evs)
+    tiling = b.autotune(eo, P, q.MIXED)
+    Lm = b.lnl(eo, P, q.MIXED)
+    L64 = b.lnl(eo, P, q.FP64)
+    out = {"workload": "config 4: 256 events (Tobs 4-64 s, fs 2048/4096 Hz, 1-3 det), 65536 sets per launch",
+           "tiling": list(tiling), "device_bytes": int(sum(h.device_bytes() for h in hs)),
+           "max_abs_dlnL_mixed_vs_fp64": float(np.max(np.abs(Lm - L64)))}
+    for prec, name, it in ((q.MIXED, "mixed", 8), (q.FP64, "fp64", 3)):
+        ms = b.time(len(P), prec, iters=it, flush_l2=True)
+        out[name] = {"value": len(P) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
+    t0 = time.perf_counter()
+    for _ in range(3):
+        b.lnl(eo, P, q.MIXED)
+    out["e2e_mixed"] = {"value": 3 * len(P) / (time.perf_counter() - t0), "unit": "lnL evals/s",
+                        "h2d_bytes_per_step": int(P.nbytes + eo.nbytes), "d2h_bytes_per_step": int(len(P) * 44)}
+    b.close()
+    for h in hs:
+        h.close()
+    return out
+
+
 def run_profile(args):
     """Warm-up then timed steps of the benchmark workload in one precision; three
     kernel launches per step (k_setup, k_lnl_full, k_finalize_full)."""
@@ -212,6 +311,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip configs 1, 3 and 4")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
@@ -319,8 +419,9 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_lnl_full<mixed,3>",
                      "kernel_ms": kmean * 1e3, "bytes_per_launch": alg_bytes,
-                     "note": "one event's 0.58 MB of weighted data serves all 2048 sets from L2; the kernel "
-                             "is FP64-pipe bound (phase), see profiles/"},
+                     "note": "algorithmic bytes = 2048 sets x 3 det x 16064 bins x 12 B (FP32 weighted data); "
+                             "one event's data serves all sets from L2, so DRAM traffic is the records plus one "
+                             "pass of the data and the kernel is instruction-issue bound (see profiles/)"},
         "clocks": clk.summary(),
         "fp64_batched": {"value": fp64_rate, "unit": "lnL evals/s", "ms_per_step": float(np.mean(ms64))},
         "fp64_per_call_dropin": {"value": percall_rate, "unit": "lnL evals/s",
@@ -329,6 +430,11 @@ def main():
         "mixed_vs_fp64_batched": value / fp64_rate / world,
         "max_abs_dlnL_mixed_vs_fp64": dmax,
     }
+    if rank == 0 and world == 1 and not args.no_extra:
+        from quickcbc_b200 import engine as eng
+        out["config1_per_call"] = bench_cfg1_percall(q, eng, _lib)
+        out["config3"] = bench_cfg3_het(q)
+        out["config4_uneven"] = bench_cfg4_uneven(q)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_reference(ev, P)
     if rank == 0:

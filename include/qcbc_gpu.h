@@ -90,6 +90,11 @@ int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_l
  * the call.  Calls on one batch are serialised internally. */
 typedef struct qcbc_batch qcbc_batch;
 qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events);
+/* A batch of `capacity` event slots, initially empty, for events of at most max_bins
+ * frequency bins (N/2); slots are (re)filled with qcbc_batch_set_slot (NULL empties a
+ * slot; sets naming an empty slot get lnL = -1e20).  The batch does not own events. */
+qcbc_batch* qcbc_batch_create_slots(int capacity, int max_bins);
+int qcbc_batch_set_slot(qcbc_batch* batch, int slot, qcbc_event* ev);
 int qcbc_batch_destroy(qcbc_batch* batch);
 /* tile_bins > 0 and threads in {64,128,256}; 0 keeps the current/automatic value */
 int qcbc_batch_set_tiling(qcbc_batch* batch, int tile_bins, int threads);

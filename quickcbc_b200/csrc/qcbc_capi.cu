@@ -39,6 +39,11 @@ static int fail(int code, const char* fmt, ...) {
   } while (0)
 
 extern "C" const char* qcbc_last_error(void) { return tls_err.c_str(); }
+// error reporting for the library's other host files (the service)
+extern "C" int qcbc_internal_fail(int code, const char* msg) {
+  tls_err = msg;
+  return code;
+}
 extern "C" const char* qcbc_version(void) { return "qcbc-b200 0.1 (sm_100a)"; }
 extern "C" long long qcbc_launch_count(void) { return tls_launches; }
 
@@ -900,6 +905,8 @@ struct qcbc_batch {
   std::map<long long, MultiGraph*> graphs;
 };
 
+extern "C" int qcbc_batch_destroy(qcbc_batch* bt);
+
 static void free_graph(MultiGraph* m) {
   if (!m) return;
   if (m->exec_full) cudaGraphExecDestroy(m->exec_full);
@@ -912,27 +919,17 @@ static void free_graph(MultiGraph* m) {
   delete m;
 }
 
-extern "C" qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events) {
-  if (!events || n_events <= 0) { fail(QCBC_EINVAL, "no events"); return nullptr; }
+extern "C" qcbc_batch* qcbc_batch_create_slots(int capacity, int max_bins) {
+  if (capacity <= 0 || max_bins <= 0) { fail(QCBC_EINVAL, "capacity and max_bins must be positive"); return nullptr; }
   if (ensure_init()) return nullptr;
-  int dev = current_device();
-  std::vector<EventDesc> h(n_events);
   qcbc_batch* bt = new qcbc_batch();
-  bt->device = dev;
-  for (int i = 0; i < n_events; i++) {
-    qcbc_event* ev = events[i];
-    if (!ev || !ev->has_data || ev->device != dev) {
-      fail(QCBC_EINVAL, "event %d is NULL, has no data or lives on another device", i);
-      delete bt;
-      return nullptr;
-    }
-    h[i].g = ev->g;
-    h[i].ev = event_data(ev);
-    bt->events.push_back(ev);
-    bt->nh_max = std::max(bt->nh_max, ev->nh);
-  }
-  if (cudaMalloc(&bt->d_events, sizeof(EventDesc) * n_events) != cudaSuccess ||
-      cudaMemcpy(bt->d_events, h.data(), sizeof(EventDesc) * n_events, cudaMemcpyHostToDevice) != cudaSuccess ||
+  bt->device = current_device();
+  bt->nh_max = max_bins;
+  bt->events.assign(capacity, nullptr);
+  std::vector<EventDesc> h(capacity);
+  memset(h.data(), 0, sizeof(EventDesc) * capacity);   // nifo = 0 marks an empty slot
+  if (cudaMalloc(&bt->d_events, sizeof(EventDesc) * capacity) != cudaSuccess ||
+      cudaMemcpy(bt->d_events, h.data(), sizeof(EventDesc) * capacity, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&bt->e0) != cudaSuccess || cudaEventCreate(&bt->e1) != cudaSuccess) {
     fail(QCBC_ECUDA, "batch allocation failed");
@@ -940,6 +937,46 @@ extern "C" qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events
     delete bt;
     return nullptr;
   }
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (ensure_bin_tables(g_dev[bt->device], max_bins + 1)) { qcbc_batch_destroy(bt); return nullptr; }
+  }
+  return bt;
+}
+
+extern "C" int qcbc_batch_set_slot(qcbc_batch* bt, int slot, qcbc_event* ev) {
+  if (!bt || slot < 0 || slot >= (int)bt->events.size()) return fail(QCBC_EINVAL, "bad batch or slot");
+  EventDesc d;
+  memset(&d, 0, sizeof(d));
+  if (ev) {
+    if (!ev->has_data || ev->device != bt->device) return fail(QCBC_EINVAL, "event has no data or another device");
+    if (ev->nh > bt->nh_max) return fail(QCBC_EINVAL, "event has %d bins, batch holds at most %d", ev->nh, bt->nh_max);
+    d.g = ev->g;
+    d.ev = event_data(ev);
+  }
+  std::lock_guard<std::mutex> lk(bt->mu);
+  CU(cudaMemcpyAsync(bt->d_events + slot, &d, sizeof(d), cudaMemcpyHostToDevice, bt->stream));
+  CU(cudaStreamSynchronize(bt->stream));
+  bt->events[slot] = ev;
+  return QCBC_OK;
+}
+
+extern "C" qcbc_batch* qcbc_batch_create(qcbc_event* const* events, int n_events) {
+  if (!events || n_events <= 0) { fail(QCBC_EINVAL, "no events"); return nullptr; }
+  if (ensure_init()) return nullptr;
+  int dev = current_device(), nh = 1;
+  for (int i = 0; i < n_events; i++) {
+    qcbc_event* ev = events[i];
+    if (!ev || !ev->has_data || ev->device != dev) {
+      fail(QCBC_EINVAL, "event %d is NULL, has no data or lives on another device", i);
+      return nullptr;
+    }
+    nh = std::max(nh, ev->nh);
+  }
+  qcbc_batch* bt = qcbc_batch_create_slots(n_events, nh);
+  if (!bt) return nullptr;
+  for (int i = 0; i < n_events; i++)
+    if (qcbc_batch_set_slot(bt, i, events[i])) { qcbc_batch_destroy(bt); return nullptr; }
   return bt;
 }
 

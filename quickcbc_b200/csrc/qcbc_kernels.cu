@@ -881,7 +881,7 @@ __global__ void k_setup_multi(const double* __restrict__ params, const int* __re
   if (b >= B) return;
   int e = event_of[b];
   PhdRec c;
-  if (e < 0 || e >= n_events) {
+  if (e < 0 || e >= n_events || events[e].g.nifo == 0) {     // out of range or an empty slot
     c.flags = 0;
     c.event = -1;
     c.i_lo = 1;

@@ -1,0 +1,456 @@
+// Continuous-batching PT-MCMC service over the multi-event likelihood
+// (declared in include/qcbc_serve.h).  Host code only: every likelihood goes
+// through the public C ABI (qcbc_event_open, qcbc_batch_*, qcbc_lnl_multi).
+//
+// The sampler follows the reference's parallel-tempered scheme in outline
+// (QuickCBC.c:1781-2236 MCMC_all, 2238-2405 update): Metropolis updates at
+// temperatures T_t = ladder^t, swaps between adjacent temperatures, prior box
+// of MCMC_all (QuickCBC.c:1871-1896, ConstCBC.h:48-57), angle wrapping as in
+// het_space (QuickCBC.c:4650-4665).  Its proposal is a plain Gaussian with
+// adapted scales; the reference's Fisher, differential-evolution and sky-ring
+// moves are host logic outside the likelihood path.
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <vector>
+
+#include "../../include/qcbc_gpu.h"
+#include "../../include/qcbc_serve.h"
+
+extern "C" int qcbc_internal_fail(int code, const char* msg);
+
+namespace {
+
+int sfail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return qcbc_internal_fail(code, buf);
+}
+
+// xoshiro256** seeded by splitmix64: one independent stream per run
+struct Rng {
+  uint64_t s[4];
+  static uint64_t splitmix(uint64_t& x) {
+    uint64_t z = (x += 0x9e3779b97f4a7c15ULL);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    return z ^ (z >> 31);
+  }
+  void seed(uint64_t v) {
+    for (auto& w : s) w = splitmix(v);
+  }
+  static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  uint64_t next() {
+    uint64_t r = rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+    s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+    s[2] ^= t; s[3] = rotl(s[3], 45);
+    return r;
+  }
+  double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+  double gauss() {   // Box-Muller
+    double u1 = uniform(), u2 = uniform();
+    if (u1 < 1e-300) u1 = 1e-300;
+    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  }
+};
+
+constexpr double kMsun = 1.988546954961461467461011951140572744e30;
+constexpr double kPc = 3.085677581491367278913937957796471611e16;
+constexpr double kTwoPi = 6.2831853071795862319959269370884;
+constexpr double kPi = 3.1415926535897931159979634685442;
+
+struct Run {
+  long long id = 0;
+  int state = QCBC_RUN_QUEUED;
+  // copied submission
+  int nifo = 0, N = 0, sn_stride = 0;
+  int labels[3] = {0, 0, 0};
+  double Tobs = 0, GMST = 0, fmin = 0, fmax = 0;
+  std::vector<double> D, SN;
+  double start[11], sigma[11], pmin[11], pmax[11];
+  int n_temps = 1, n_chains = 1, n_steps = 0, burn_in = 0, thin = 1;
+  double ladder = 1.15;
+  // live state
+  qcbc_event* ev = nullptr;
+  int slot = -1;
+  long long bytes = 0;
+  bool initialised = false;
+  int steps_done = 0;
+  std::vector<double> x, lnl, temp, scale;   // per chain; scale per temperature
+  std::vector<int> acc, prop;                // per temperature, reset each adaptation window
+  long long cold_acc = 0, cold_prop = 0, swaps = 0, swap_tries = 0, evals = 0;
+  std::vector<double> samples;               // rows of 12
+  double t_arrival = 0, t_admit = -1, t_done = -1;
+  Rng rng;
+};
+
+long long estimate_bytes(const Run& r) {
+  long long nh = r.N / 2;
+  return (long long)r.nifo * (3 * nh * 8 + nh * 16 + (long long)r.N * 8 + (nh + 1) * 8) + nh * 8;
+}
+
+}  // namespace
+
+struct qcbc_server {
+  long long budget = 0, bytes_live = 0, evals = 0, launches = 0;
+  int max_live = 0, max_bins = 0, precision = QCBC_MIXED;
+  qcbc_batch* batch = nullptr;
+  std::vector<long long> slot_run;             // run id per slot or -1
+  std::map<long long, Run*> runs;
+  std::deque<long long> queue;
+  std::vector<long long> live;
+  long long next_id = 0;
+  std::chrono::steady_clock::time_point t0;
+  std::mutex mu;
+  // launch staging
+  std::vector<int> eo;
+  std::vector<double> params, out;
+  std::vector<std::pair<long long, int>> owner;  // (run, chain) per set
+};
+
+static double now_s(const qcbc_server* s) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
+}
+
+extern "C" qcbc_server* qcbc_server_create(long long budget, int max_live, int max_bins, int precision) {
+  if (budget <= 0 || max_live <= 0 || max_bins <= 0 || (precision != QCBC_FP64 && precision != QCBC_MIXED)) {
+    sfail(QCBC_EINVAL, "bad server settings");
+    return nullptr;
+  }
+  qcbc_batch* b = qcbc_batch_create_slots(max_live, max_bins);
+  if (!b) return nullptr;
+  qcbc_server* s = new qcbc_server();
+  s->budget = budget;
+  s->max_live = max_live;
+  s->max_bins = max_bins;
+  s->precision = precision;
+  s->batch = b;
+  s->slot_run.assign(max_live, -1);
+  s->t0 = std::chrono::steady_clock::now();
+  return s;
+}
+
+static void retire(qcbc_server* s, Run* r, int state) {
+  if (r->slot >= 0) {
+    qcbc_batch_set_slot(s->batch, r->slot, nullptr);
+    s->slot_run[r->slot] = -1;
+    r->slot = -1;
+  }
+  if (r->ev) {
+    qcbc_event_close(r->ev);
+    r->ev = nullptr;
+    s->bytes_live -= r->bytes;
+  }
+  r->state = state;
+  r->t_done = now_s(s);
+  r->D.clear();
+  r->D.shrink_to_fit();
+  r->SN.clear();
+  r->SN.shrink_to_fit();
+}
+
+extern "C" int qcbc_server_destroy(qcbc_server* s) {
+  if (!s) return QCBC_OK;
+  std::lock_guard<std::mutex> lk(s->mu);
+  for (auto& kv : s->runs) {
+    if (kv.second->state == QCBC_RUN_LIVE) retire(s, kv.second, QCBC_RUN_CANCELLED);
+    delete kv.second;
+  }
+  qcbc_batch_destroy(s->batch);
+  delete s;
+  return QCBC_OK;
+}
+
+extern "C" double qcbc_server_clock(const qcbc_server* s) { return s ? now_s(s) : 0.0; }
+
+extern "C" int qcbc_server_set_tiling(qcbc_server* s, int tile_bins, int threads) {
+  if (!s) return sfail(QCBC_EINVAL, "NULL server");
+  return qcbc_batch_set_tiling(s->batch, tile_bins, threads);
+}
+
+extern "C" long long qcbc_server_submit(qcbc_server* s, const qcbc_run_spec* sp) {
+  if (!s || !sp || !sp->labels || !sp->D || !sp->SN || !sp->start) return sfail(QCBC_EINVAL, "NULL argument");
+  if (sp->nifo < 1 || sp->nifo > 3 || sp->N < 8 || sp->sn_stride < sp->N / 2 || sp->n_temps < 1 ||
+      sp->n_chains < 1 || sp->n_steps < 1 || sp->thin < 1 || sp->burn_in < 0 || !(sp->ladder >= 1.0))
+    return sfail(QCBC_EINVAL, "bad run specification");
+  if (sp->N / 2 > s->max_bins) return sfail(QCBC_EINVAL, "run has %d bins, server holds %d", sp->N / 2, s->max_bins);
+  Run* r = new Run();
+  r->nifo = sp->nifo;
+  r->N = sp->N;
+  r->sn_stride = sp->sn_stride;
+  for (int i = 0; i < sp->nifo; i++) r->labels[i] = sp->labels[i];
+  r->Tobs = sp->Tobs;
+  r->GMST = sp->GMST;
+  r->fmin = sp->fmin;
+  r->fmax = sp->fmax;
+  r->D.assign(sp->D, sp->D + (size_t)sp->nifo * sp->N);
+  r->SN.assign(sp->SN, sp->SN + (size_t)sp->nifo * sp->sn_stride);
+  static const double kSig[11] = {1e-4, 1e-3, 0.02, 0.02, 0.1, 1e-4, 0.02, 0.01, 0.01, 0.02, 0.02};
+  double tmin = std::max(sp->Tobs - 3.5, 1.5), tmax = sp->Tobs - 0.5;   // QuickCBC.c:178-183
+  const double dmin[11] = {std::log(0.5 * kMsun), std::log(0.5 * kMsun), -0.85, -0.85, 0.0, tmin,
+                           std::log(1e6 * kPc), 0.0, -1.0, 0.0, -1.0};
+  const double dmax[11] = {std::log(160.0 * kMsun), std::log(300.0 * kMsun), 0.85, 0.85, kTwoPi, tmax,
+                           std::log(1e10 * kPc), kTwoPi, 1.0, kPi, 1.0};
+  for (int j = 0; j < 11; j++) {
+    r->start[j] = sp->start[j];
+    r->sigma[j] = sp->scales ? sp->scales[j] : kSig[j];
+    r->pmin[j] = sp->prior_min ? sp->prior_min[j] : dmin[j];
+    r->pmax[j] = sp->prior_max ? sp->prior_max[j] : dmax[j];
+  }
+  r->n_temps = sp->n_temps;
+  r->n_chains = sp->n_chains;
+  r->n_steps = sp->n_steps;
+  r->burn_in = sp->burn_in;
+  r->thin = sp->thin;
+  r->ladder = sp->ladder;
+  r->rng.seed(sp->seed);
+  r->bytes = estimate_bytes(*r);
+  std::lock_guard<std::mutex> lk(s->mu);
+  r->id = s->next_id++;
+  r->t_arrival = now_s(s);
+  if (r->bytes > s->budget) {
+    long long need = r->bytes;
+    delete r;
+    return sfail(QCBC_EBUDGET, "run needs %lld B of device memory, budget is %lld B", need, s->budget);
+  }
+  s->runs[r->id] = r;
+  s->queue.push_back(r->id);
+  return r->id;
+}
+
+extern "C" int qcbc_server_cancel(qcbc_server* s, long long id) {
+  if (!s) return sfail(QCBC_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->runs.find(id);
+  if (it == s->runs.end()) return sfail(QCBC_EINVAL, "no run %lld", id);
+  Run* r = it->second;
+  if (r->state == QCBC_RUN_QUEUED) {
+    for (auto q = s->queue.begin(); q != s->queue.end(); ++q)
+      if (*q == id) { s->queue.erase(q); break; }
+    r->state = QCBC_RUN_CANCELLED;
+    r->t_done = now_s(s);
+  } else if (r->state == QCBC_RUN_LIVE) {
+    retire(s, r, QCBC_RUN_CANCELLED);
+    for (size_t k = 0; k < s->live.size(); k++)
+      if (s->live[k] == id) { s->live.erase(s->live.begin() + k); break; }
+  }
+  return QCBC_OK;
+}
+
+// Admit queued runs in arrival order while a slot and the budget allow.
+static void admit(qcbc_server* s) {
+  while (!s->queue.empty()) {
+    Run* r = s->runs[s->queue.front()];
+    if (s->bytes_live + r->bytes > s->budget) break;
+    int slot = -1;
+    for (int k = 0; k < s->max_live; k++)
+      if (s->slot_run[k] < 0) { slot = k; break; }
+    if (slot < 0) break;
+    s->queue.pop_front();
+    r->ev = qcbc_event_open(r->nifo, r->labels, r->Tobs, r->GMST, r->N, r->D.data(), r->N, r->SN.data(),
+                            r->sn_stride, r->fmin, r->fmax);
+    if (!r->ev || qcbc_batch_set_slot(s->batch, slot, r->ev) != QCBC_OK) {
+      if (r->ev) qcbc_event_close(r->ev);
+      r->ev = nullptr;
+      r->state = QCBC_RUN_FAILED;
+      r->t_done = now_s(s);
+      continue;
+    }
+    r->bytes = qcbc_event_device_bytes(r->ev);
+    s->bytes_live += r->bytes;
+    r->slot = slot;
+    s->slot_run[slot] = r->id;
+    r->state = QCBC_RUN_LIVE;
+    r->t_admit = now_s(s);
+    int nc = r->n_temps * r->n_chains;
+    r->x.assign((size_t)nc * 11, 0.0);
+    r->lnl.assign(nc, -1e20);
+    r->temp.assign(nc, 1.0);
+    r->scale.assign(r->n_temps, 1.0);
+    r->acc.assign(r->n_temps, 0);
+    r->prop.assign(r->n_temps, 0);
+    for (int c = 0; c < nc; c++) {
+      int t = c % r->n_temps;
+      r->temp[c] = std::pow(r->ladder, t);
+      for (int j = 0; j < 11; j++) r->x[(size_t)c * 11 + j] = r->start[j];
+    }
+    for (int t = 0; t < r->n_temps; t++) r->scale[t] = std::sqrt(std::pow(r->ladder, t));
+    s->live.push_back(r->id);
+  }
+}
+
+static bool in_prior(const Run* r, const double* y) {
+  for (int j = 0; j < 11; j++)
+    if (y[j] < r->pmin[j] || y[j] > r->pmax[j]) return false;
+  double leta = (5.0 / 3.0) * (y[0] - y[1]);          // symmetric mass ratio (QuickCBC.c:2341-2364)
+  return leta <= std::log(0.25) && leta >= std::log(0.05);
+}
+
+static void wrap(double* y) {
+  y[4] = std::fmod(y[4], kTwoPi);
+  if (y[4] < 0) y[4] += kTwoPi;
+  y[7] = std::fmod(y[7], kTwoPi);
+  if (y[7] < 0) y[7] += kTwoPi;
+  y[9] = std::fmod(y[9], kPi);
+  if (y[9] < 0) y[9] += kPi;
+  for (int j : {8, 10}) {
+    if (y[j] > 1.0) y[j] = 2.0 - y[j];
+    if (y[j] < -1.0) y[j] = -2.0 - y[j];
+  }
+}
+
+extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int* n_done) {
+  if (!s) return sfail(QCBC_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  admit(s);
+  s->eo.clear();
+  s->params.clear();
+  s->owner.clear();
+  // proposals (or the starting points of newly admitted runs)
+  for (long long id : s->live) {
+    Run* r = s->runs[id];
+    int nc = r->n_temps * r->n_chains;
+    for (int c = 0; c < nc; c++) {
+      double y[11];
+      const double* x = &r->x[(size_t)c * 11];
+      if (r->initialised) {
+        int t = c % r->n_temps;
+        for (int j = 0; j < 11; j++) y[j] = x[j] + r->scale[t] * r->sigma[j] * r->rng.gauss();
+        wrap(y);
+      } else {
+        for (int j = 0; j < 11; j++) y[j] = x[j];
+      }
+      bool ok = in_prior(r, y);
+      s->eo.push_back(ok ? r->slot : -1);
+      s->params.insert(s->params.end(), y, y + 11);
+      s->owner.push_back({id, c});
+    }
+  }
+  int B = (int)s->eo.size();
+  if (B > 0) {
+    s->out.assign(B, -1e20);
+    int rc = qcbc_lnl_multi(s->batch, s->eo.data(), s->params.data(), B, s->out.data(), nullptr, s->precision);
+    if (rc != QCBC_OK && rc != QCBC_EDOM) return rc;   // EDOM: out-of-prior or invalid sets, lnL = -1e20
+    s->launches++;
+    s->evals += B;
+  }
+  // accept / reject, swaps, adaptation, samples
+  size_t k = 0;
+  std::vector<long long> finished;
+  for (long long id : s->live) {
+    Run* r = s->runs[id];
+    int nc = r->n_temps * r->n_chains;
+    r->evals += nc;
+    if (!r->initialised) {
+      for (int c = 0; c < nc; c++, k++) r->lnl[c] = s->out[k];
+      r->initialised = true;
+      continue;
+    }
+    for (int c = 0; c < nc; c++, k++) {
+      int t = c % r->n_temps;
+      double Ly = s->out[k];
+      r->prop[t]++;
+      if (t == 0) r->cold_prop++;
+      if (Ly > -1e19) {
+        double la = (Ly - r->lnl[c]) / r->temp[c];
+        if (la >= 0.0 || std::log(r->rng.uniform()) < la) {
+          std::memcpy(&r->x[(size_t)c * 11], &s->params[k * 11], 11 * sizeof(double));
+          r->lnl[c] = Ly;
+          r->acc[t]++;
+          if (t == 0) r->cold_acc++;
+        }
+      }
+    }
+    if (r->n_temps > 1) {
+      for (int ch = 0; ch < r->n_chains; ch++) {
+        int t = (int)(r->rng.uniform() * (r->n_temps - 1));
+        int a = ch * r->n_temps + t, b = a + 1;
+        double la = (r->lnl[b] - r->lnl[a]) * (1.0 / r->temp[a] - 1.0 / r->temp[b]);
+        r->swap_tries++;
+        if (la >= 0.0 || std::log(r->rng.uniform()) < la) {
+          for (int j = 0; j < 11; j++) std::swap(r->x[(size_t)a * 11 + j], r->x[(size_t)b * 11 + j]);
+          std::swap(r->lnl[a], r->lnl[b]);
+          r->swaps++;
+        }
+      }
+    }
+    r->steps_done++;
+    if (r->steps_done <= r->burn_in && r->steps_done % 50 == 0) {
+      for (int t = 0; t < r->n_temps; t++) {
+        double rate = r->prop[t] ? (double)r->acc[t] / r->prop[t] : 0.25;
+        double f = std::exp(rate - 0.25);
+        r->scale[t] = std::min(std::max(r->scale[t] * f, 1e-3), 1e3);
+        r->acc[t] = r->prop[t] = 0;
+      }
+    }
+    if (r->steps_done > r->burn_in && (r->steps_done - r->burn_in) % r->thin == 0) {
+      for (int ch = 0; ch < r->n_chains; ch++) {
+        int c = ch * r->n_temps;   // T = 1
+        r->samples.insert(r->samples.end(), &r->x[(size_t)c * 11], &r->x[(size_t)c * 11] + 11);
+        r->samples.push_back(r->lnl[c]);
+      }
+    }
+    if (r->steps_done >= r->n_steps) finished.push_back(id);
+  }
+  for (long long id : finished) {
+    retire(s, s->runs[id], QCBC_RUN_DONE);
+    for (size_t q = 0; q < s->live.size(); q++)
+      if (s->live[q] == id) { s->live.erase(s->live.begin() + q); break; }
+  }
+  if (n_live) *n_live = (int)s->live.size();
+  if (n_queued) *n_queued = (int)s->queue.size();
+  if (n_done) {
+    int d = 0;
+    for (auto& kv : s->runs) d += kv.second->state >= QCBC_RUN_DONE;
+    *n_done = d;
+  }
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_server_run_info(qcbc_server* s, long long id, qcbc_run_info* o) {
+  if (!s || !o) return sfail(QCBC_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->runs.find(id);
+  if (it == s->runs.end()) return sfail(QCBC_EINVAL, "no run %lld", id);
+  const Run* r = it->second;
+  o->state = r->state;
+  o->steps_done = r->steps_done;
+  o->t_arrival = r->t_arrival;
+  o->t_admit = r->t_admit;
+  o->t_done = r->t_done;
+  o->accept_cold = r->cold_prop ? (double)r->cold_acc / r->cold_prop : 0.0;
+  o->swap_rate = r->swap_tries ? (double)r->swaps / r->swap_tries : 0.0;
+  o->device_bytes = r->bytes;
+  o->lnl_evals = r->evals;
+  o->n_samples = (int)(r->samples.size() / 12);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_server_run_samples(qcbc_server* s, long long id, double* out, int max_rows, int* n_rows) {
+  if (!s || !out || !n_rows) return sfail(QCBC_EINVAL, "NULL argument");
+  std::lock_guard<std::mutex> lk(s->mu);
+  auto it = s->runs.find(id);
+  if (it == s->runs.end()) return sfail(QCBC_EINVAL, "no run %lld", id);
+  int n = (int)std::min<size_t>(it->second->samples.size() / 12, (size_t)std::max(max_rows, 0));
+  std::memcpy(out, it->second->samples.data(), sizeof(double) * 12 * (size_t)n);
+  *n_rows = n;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_server_stats(qcbc_server* s, long long* evals, long long* launches, long long* bytes) {
+  if (!s) return sfail(QCBC_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (evals) *evals = s->evals;
+  if (launches) *launches = s->launches;
+  if (bytes) *bytes = s->bytes_live;
+  return QCBC_OK;
+}

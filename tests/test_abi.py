@@ -11,7 +11,7 @@ from conftest import ROOT
 
 def declared_functions():
     names = set()
-    for h in ("qcbc_gpu.h", "qcbc_quickcbc.h"):
+    for h in ("qcbc_gpu.h", "qcbc_quickcbc.h", "qcbc_serve.h"):
         text = open(os.path.join(ROOT, "include", h)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\(", text, flags=re.M):
