@@ -286,6 +286,32 @@ def bench_cfg4_uneven(q):
     return out
 
 
+def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64"), rate_hz=2.0):
+    """Config 5: Poisson arrivals (mean rate_hz) of PT-MCMC analyses of config-4-like events
+    (16 temperatures x 8 chains x n_steps), device-resident runs admitted by a 150 GB budget,
+    every step of every live run merged into one multi-event launch."""
+    from quickcbc_b200 import serving, synth
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    evs = [synth.make_event(tmpl, **s) for s in synth.uneven_event_specs(n_runs, seed=5000)]
+    out = {"workload": "config 5: %d runs, Poisson %.1f/s, 16 temps x 8 chains x %d steps, config-4 events, "
+                       "HBM budget 150 GB" % (n_runs, rate_hz, n_steps)}
+    for name in precisions:
+        prec = q.MIXED if name == "mixed" else q.FP64
+        srv = serving.Server(hbm_budget_bytes=150 * 10**9, max_live=256, max_bins=1 << 17, precision=prec)
+        srv.set_tiling(8192, 256)
+        res = serving.serve_stream(srv, evs, rate_hz=rate_hz, seed=5,
+                                   sampler=dict(n_temps=16, n_chains=8, n_steps=n_steps, burn_in=n_steps // 4,
+                                                thin=max(1, n_steps // 200)))
+        st = srv.stats()
+        res.pop("ttp_s")
+        res["launches"] = st["launches"]
+        out[name] = res
+        srv.close()
+    return out
+
+
 def run_profile(args):
     """Warm-up then timed steps of the benchmark workload in one precision; three
     kernel launches per step (k_setup, k_lnl_full, k_finalize_full)."""
@@ -311,7 +337,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-extra", action="store_true", help="skip configs 1, 3 and 4")
+    ap.add_argument("--no-extra", action="store_true", help="skip configs 1, 3, 4 and the reduced config 5")
+    ap.add_argument("--serve", action="store_true", help="config 5 serving stream only")
+    ap.add_argument("--serve-runs", type=int, default=32)
+    ap.add_argument("--serve-steps", type=int, default=20000)
+    ap.add_argument("--serve-prec", default="mixed,fp64")
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
@@ -321,6 +351,14 @@ def main():
         return run_reference_arm(args)
     if args.profile:
         return run_profile(args)
+    if args.serve:
+        import quickcbc_b200 as q
+        from quickcbc_b200 import _lib
+        _lib.check(_lib.lib().qcbc_init(0))
+        res = bench_cfg5_serving(q, n_runs=args.serve_runs, n_steps=args.serve_steps,
+                                 precisions=tuple(args.serve_prec.split(",")))
+        print(json.dumps({"metric": "time-to-posterior p50/p99 and aggregate lnL evals/s (config 5)", **res}))
+        return
 
     rank, world, local = env_rank()
     dist = None
@@ -435,6 +473,9 @@ def main():
         out["config1_per_call"] = bench_cfg1_percall(q, eng, _lib)
         out["config3"] = bench_cfg3_het(q)
         out["config4_uneven"] = bench_cfg4_uneven(q)
+        out["config5_serving_reduced"] = bench_cfg5_serving(q, n_runs=16, n_steps=1000, rate_hz=2.0)
+        out["config5_serving_reduced"]["note"] = ("reduced: 16 runs x 1000 steps per run (config 5 specifies "
+                                                  "20000 steps; full run: bench.py --serve)")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_reference(ev, P)
     if rank == 0:
