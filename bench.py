@@ -360,11 +360,9 @@ def main():
         print(json.dumps({"metric": "time-to-posterior p50/p99 and aggregate lnL evals/s (config 5)", **res}))
         return
 
-    rank, world, local = env_rank()
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        dist.init_process_group("gloo", init_method="env://")
+    from quickcbc_b200.replicas import Replicas
+    rep = Replicas()
+    rank, world, local = rep.rank, rep.world, rep.local_rank
     import quickcbc_b200 as q
     from quickcbc_b200 import _lib
     _lib.check(_lib.lib().qcbc_init(local))
@@ -381,8 +379,7 @@ def main():
     dmax = float(np.max(np.abs(L64 - Lmx)))
 
     q.time_lnl_full(e, dbuf, B, q.MIXED, args.warmup, flush_l2=True)
-    if dist:
-        dist.barrier()
+    rep.barrier()
     with ClockSampler(local) as clk:
         # the same workload keeps the GPU loaded around the timed steps so the
         # 200 ms clock samples are taken under this load
@@ -395,13 +392,8 @@ def main():
         t_load = time.perf_counter() + 0.6
         while time.perf_counter() < t_load:
             q.time_lnl_full(e, dbuf, B, q.MIXED, 20, flush_l2=False)
-    t_ms = float(np.sum(ms))
-    if dist:
-        import torch
-        t = torch.tensor([t_ms], dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_ms = float(t.item())
-        dist.barrier()
+    t_ms = rep.max_over_ranks(float(np.sum(ms)))      # device time of the timed steps, max over ranks
+    rep.barrier()
     value = world * B * args.steps / (t_ms * 1e-3)
 
     # FP64 batched on the same inputs (the plain form, batched)
@@ -481,8 +473,7 @@ def main():
     if rank == 0:
         print(json.dumps(out), flush=True)
     e.close()
-    if dist:
-        dist.destroy_process_group()
+    rep.close()
 
 
 if __name__ == "__main__":

@@ -81,6 +81,9 @@ int qcbc_server_run_info(qcbc_server* s, long long run, qcbc_run_info* out);
 /* Rows of 12 doubles (11 parameters, lnL) of the run's T = 1 samples. */
 int qcbc_server_run_samples(qcbc_server* s, long long run, double* out, int max_rows, int* n_rows);
 int qcbc_server_stats(qcbc_server* s, long long* lnl_evals, long long* launches, long long* device_bytes_live);
+/* Seconds spent so far in the three phases of the steps: building proposals, the
+ * merged likelihood launch (including its copies), and the Metropolis/swap updates. */
+int qcbc_server_timing(qcbc_server* s, double* propose_s, double* lnl_s, double* update_s);
 /* Tiling of the merged launches (see qcbc_batch_set_tiling). */
 int qcbc_server_set_tiling(qcbc_server* s, int tile_bins, int threads);
 

@@ -56,10 +56,14 @@ struct Rng {
     return r;
   }
   double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
-  double gauss() {   // Box-Muller
-    double u1 = uniform(), u2 = uniform();
-    if (u1 < 1e-300) u1 = 1e-300;
-    return std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2);
+  // Symmetric, zero-mean, unit-variance step: (u1 + u2 + u3 + u4 - 2) sqrt(3) from four 32-bit
+  // uniforms (two generator calls).  Metropolis-Hastings needs only a symmetric proposal, not
+  // an exact Gaussian, and this one costs a few ns instead of a log, a sqrt and a cos.
+  double step() {
+    uint64_t a = next(), b = next();
+    constexpr double k = 1.0 / 4294967296.0;
+    double s4 = ((double)(uint32_t)a + (double)(a >> 32) + (double)(uint32_t)b + (double)(b >> 32)) * k;
+    return (s4 - 2.0) * 1.7320508075688772;
   }
 };
 
@@ -102,6 +106,7 @@ long long estimate_bytes(const Run& r) {
 
 struct qcbc_server {
   long long budget = 0, bytes_live = 0, evals = 0, launches = 0;
+  double t_propose = 0.0, t_lnl = 0.0, t_update = 0.0;   // seconds spent in each phase of a step
   int max_live = 0, max_bins = 0, precision = QCBC_MIXED;
   qcbc_batch* batch = nullptr;
   std::vector<long long> slot_run;             // run id per slot or -1
@@ -312,6 +317,7 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
   if (!s) return sfail(QCBC_EINVAL, "NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   admit(s);
+  double t0 = now_s(s);
   s->eo.clear();
   s->params.clear();
   s->owner.clear();
@@ -324,7 +330,7 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
       const double* x = &r->x[(size_t)c * 11];
       if (r->initialised) {
         int t = c % r->n_temps;
-        for (int j = 0; j < 11; j++) y[j] = x[j] + r->scale[t] * r->sigma[j] * r->rng.gauss();
+        for (int j = 0; j < 11; j++) y[j] = x[j] + r->scale[t] * r->sigma[j] * r->rng.step();
         wrap(y);
       } else {
         for (int j = 0; j < 11; j++) y[j] = x[j];
@@ -336,6 +342,7 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
     }
   }
   int B = (int)s->eo.size();
+  double t1 = now_s(s);
   if (B > 0) {
     s->out.assign(B, -1e20);
     int rc = qcbc_lnl_multi(s->batch, s->eo.data(), s->params.data(), B, s->out.data(), nullptr, s->precision);
@@ -343,6 +350,7 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
     s->launches++;
     s->evals += B;
   }
+  double t2 = now_s(s);
   // accept / reject, swaps, adaptation, samples
   size_t k = 0;
   std::vector<long long> finished;
@@ -401,6 +409,10 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
     }
     if (r->steps_done >= r->n_steps) finished.push_back(id);
   }
+  double t3 = now_s(s);
+  s->t_propose += t1 - t0;
+  s->t_lnl += t2 - t1;
+  s->t_update += t3 - t2;
   for (long long id : finished) {
     retire(s, s->runs[id], QCBC_RUN_DONE);
     for (size_t q = 0; q < s->live.size(); q++)
@@ -452,5 +464,14 @@ extern "C" int qcbc_server_stats(qcbc_server* s, long long* evals, long long* la
   if (evals) *evals = s->evals;
   if (launches) *launches = s->launches;
   if (bytes) *bytes = s->bytes_live;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_server_timing(qcbc_server* s, double* propose_s, double* lnl_s, double* update_s) {
+  if (!s) return sfail(QCBC_EINVAL, "NULL server");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (propose_s) *propose_s = s->t_propose;
+  if (lnl_s) *lnl_s = s->t_lnl;
+  if (update_s) *update_s = s->t_update;
   return QCBC_OK;
 }

@@ -52,6 +52,7 @@ def _bind():
     L.qcbc_server_run_samples.argtypes = [vp, ll, _PD, i, _PI]
     L.qcbc_server_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
     L.qcbc_server_set_tiling.argtypes = [vp, i, i]
+    L.qcbc_server_timing.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d)]
     L._serve_bound = True
     return L
 
@@ -127,6 +128,11 @@ class Server:
         check(_bind().qcbc_server_stats(self._h, C.byref(e), C.byref(l), C.byref(b)))
         return dict(lnl_evals=e.value, launches=l.value, device_bytes_live=b.value)
 
+    def timing(self):
+        a, b, c = C.c_double(), C.c_double(), C.c_double()
+        check(_bind().qcbc_server_timing(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return dict(propose_s=a.value, lnl_s=b.value, update_s=c.value)
+
     def run_until_idle(self, max_steps=10**9):
         for _ in range(max_steps):
             nl, nq, _ = self.step()
@@ -161,7 +167,8 @@ def serve_stream(server, events, rate_hz, seed=0, sampler=None, log=None):
     infos = [server.info(r) for r in ids]
     ttp = np.array([i["t_done"] - i["t_arrival"] for i in infos if i["state"] == RUN_DONE])
     evals = server.stats()["lnl_evals"] - e0
-    return dict(n_runs=len(ids), n_done=int(len(ttp)), ttp_s=ttp.tolist(),
+    phases = server.timing()
+    return dict(phase_s=phases, n_runs=len(ids), n_done=int(len(ttp)), ttp_s=ttp.tolist(),
                 p50_s=float(np.percentile(ttp, 50)) if len(ttp) else None,
                 p99_s=float(np.percentile(ttp, 99)) if len(ttp) else None,
                 wall_s=wall, lnl_evals=int(evals), evals_per_s=evals / wall if wall > 0 else None,
