@@ -53,7 +53,7 @@ def test_admission_by_budget_and_refusal(events):
     ia, ib = srv.info(a), srv.info(b)
     assert ia["state"] == ib["state"] == serving.RUN_DONE
     assert ib["t_admit"] >= ia["t_done"], "the queued run is admitted when memory is released"
-    tiny = serving.Server(hbm_budget_bytes=1 << 20, max_live=8, max_bins=1 << 15)
+    tiny = serving.Server(hbm_budget_bytes=1 << 10, max_live=8, max_bins=1 << 15)
     with pytest.raises(q.QcbcError) as ei:
         tiny.submit(events[0], **SAMPLER)
     assert ei.value.code == -4
