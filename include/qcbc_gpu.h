@@ -144,7 +144,7 @@ int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_ln
  *    results are ready when the work on that stream completes. */
 #define QCBC_NOALLOC_MAX_SETS 4096
 #define QCBC_NOALLOC_MAX_TILE_SLOTS 16384
-#define QCBC_NOALLOC_SCRATCH_BYTES 3358720
+#define QCBC_NOALLOC_SCRATCH_BYTES 4669440
 int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
                           int precision, void* stream);
 

@@ -157,6 +157,7 @@ extern "C" int qcbc_init(int device) {
   DeviceState& ds = g_dev[device];
   if (!ds.ready) {
     upload_tables();
+    allow_dynamic_smem();
     int rc = upload_qnm(ds);
     if (rc) return rc;
     rc = ensure_bin_tables(ds, 1 << 20);

@@ -40,6 +40,38 @@ constexpr int kMaxIfo = 3;
 // Record flags
 constexpr int kRecValid = 1;
 
+// The waveform of one parameter set as the mixed-precision kernel evaluates it at bin i,
+// Mf = m i with m = Msec df: every power of m and the factor 1/(2 pi) are folded into
+// per-set coefficients (computed in FP64 by the setup), so a bin needs only i, t = i^{1/3},
+// u = i^{-1/3}, L = log i and s = i^{3/4} (per-device tables) and no Mf at all.
+//   phase in cycles (FP64), the three pieces of IMRPhenomD.c:169-186 / internals.c:1540-1584,
+//   each minus t0 (Mf - MfRef) + phi_pre:
+//     inspiral      A0 + t (At + t Att) + L (AL + t AtL) + u (Au + u (Auu + u (Au3 + u^2 Au5)))
+//                   + i (Ai + t (Ait + t Aitt) + i Aii)
+//     intermediate  B0 + i Bi + u^9 Bu9 + L BL
+//     ringdown      R0 + i Ri + u^3 Ru3 + s Rs + Rat atan(i D1 - D0)
+//   amplitude (FP32) relative to a0 (Msec df)^{-7/6} i^{-7/6}, IMRPhenomD_internals.c:576-707:
+//     inspiral      1 + t^2 al0 + i (al1 + t (al2 + t al3) + i (al4 + t (al5 + t al6) + i al7))
+//     intermediate  Newton form in x = m i - hx1 (nodes hx1, hx1, hx2, hx3, hx3), x in FP64
+//     ringdown      exp(-dfr g2/fg) fg g1 / (dfr^2 + fg^2), dfr = m i - fRD in FP64
+//   iA, iF, iP, iM: first bins of the intermediate amplitude, ringdown amplitude, intermediate
+//   phase and ringdown phase (Msec f_i compared with 0.014, fmax, 0.018, fRD/2 in FP64).
+struct MixPhIns { double A0, At, Att, AtL, AL, Au, Auu, Au3, Au5, Ai, Ait, Aitt, Aii; };
+struct MixPhInt { double B0, Bi, Bu9, BL; };
+struct MixPhMrd { double R0, Ri, Ru3, Rs, Rat, D1, D0; };
+struct MixAmpIns { float al[8]; };
+struct MixAmpInt { double m, hx1; float hc[5], h21, h31; };
+struct MixAmpMrd { double m, fRD; float g2_over_fg, fg_g1, fg2; };
+struct MixPoly {
+  MixPhIns pins;
+  MixPhInt pint;
+  MixPhMrd pmrd;
+  MixAmpIns ains;
+  MixAmpInt aint;
+  MixAmpMrd amrd;
+  int iA, iF, iP, iM;
+};
+
 struct PhdRec {
   // dimensional scales
   double Msec, fCut, amp_scale, eta, inv_eta;
@@ -59,9 +91,11 @@ struct PhdRec {
   double Fs[kMaxIfo], lam[kMaxIfo], td[kMaxIfo];
   // scales of Mf = (Msec df) i for the per-bin tables of the mixed kernel
   double mdf, mdf_third, mdf_rthird, mdf_log, mdf_m76, mdf_34;
+  MixPoly mix;
   int i_lo, i_hi;      // bins with f > fbegin and f <= fCut (inclusive), clamped to the band
   int flags, event;    // event: index into the event table (multi-event launches)
 };
+static_assert(sizeof(PhdRec) % 16 == 0, "records are copied in 16-byte words");
 
 // Table V of arXiv:1508.07253: lambda = l00 + l10 eta + (l01 + l11 eta + l21 eta^2) xi
 //   + (l02 + l12 eta + l22 eta^2) xi^2 + (l03 + l13 eta + l23 eta^2) xi^3, xi = chiPN - 1.
@@ -78,11 +112,22 @@ struct QnmTable { const double *x, *yr, *mr, *yd, *md; const int* bucket; int n,
 
 struct Pow6 { double sixth, third, two_thirds, four_thirds, five_thirds, two, seven_thirds, eight_thirds; };
 
+// Math routines of the waveform pieces.  The per-bin kernels inline CUDA's routines; the
+// setup, which evaluates each piece a few times per record in several warps, calls one
+// out-of-line copy of each (MathOutline in qcbc_kernels.cu) to keep its code footprint small.
+struct MathInline {
+  static __device__ __forceinline__ double pow(double x, double y) { return ::pow(x, y); }
+  static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+  static __device__ __forceinline__ double log(double x) { return ::log(x); }
+  static __device__ __forceinline__ double atan(double x) { return ::atan(x); }
+};
+
 // Powers of x from one x^{1/6} (IMRPhenomD_internals.c:515-533).
+template <class M = MathInline>
 __device__ __forceinline__ Pow6 pow6(double x) {
   Pow6 p;
   if (x < 0.0) x = 1.0e-10;
-  p.sixth = pow(x, 1.0 / 6.0);
+  p.sixth = M::pow(x, 1.0 / 6.0);
   p.third = p.sixth * p.sixth;
   p.two_thirds = x / p.third;
   p.four_thirds = x * p.third;
@@ -120,9 +165,10 @@ __device__ __forceinline__ double qnm_eval_at(const QnmTable& t, const double* y
 }
 
 // ------------------------------------------------------------- amplitude
+template <class M = MathInline>
 __device__ __forceinline__ double amp_mrd(const PhdRec& c, double f) {
   double fg = c.fDM * c.g3, df = f - c.fRD;
-  return exp(-df * c.g2 / fg) * (fg * c.g1) / (df * df + fg * fg);
+  return M::exp(-df * c.g2 / fg) * (fg * c.g1) / (df * df + fg * fg);
 }
 __device__ __forceinline__ double amp_ins(const PhdRec& c, double Mf, const Pow6& p) {
   return 1.0 + p.two_thirds * c.ai[0] + Mf * c.ai[1] + p.four_thirds * c.ai[2] + p.five_thirds * c.ai[3] +
@@ -134,8 +180,9 @@ __device__ __forceinline__ double amp_int(const PhdRec& c, double Mf) {
 }
 
 // ------------------------------------------------------------- phase pieces
+template <class M = MathInline>
 __device__ __forceinline__ double phi_ins(const PhdRec& c, double Mf, const Pow6& p) {
-  double v = p.third * c.pi_third, logv = log(v);
+  double v = p.third * c.pi_third, logv = M::log(v);
   const double* q = c.pq;
   double ph = q[0];
   ph += q[1] * p.two_thirds;
@@ -149,19 +196,22 @@ __device__ __forceinline__ double phi_ins(const PhdRec& c, double Mf, const Pow6
   ph += (q[9] * Mf + q[10] * p.four_thirds + q[11] * p.five_thirds + q[12] * p.two) / c.eta;
   return ph;
 }
+template <class M = MathInline>
 __device__ __forceinline__ double phi_int(const PhdRec& c, double f) {
-  return c.b1 * f - c.b3 / (3. * f * f * f) + c.b2 * log(f);
+  return c.b1 * f - c.b3 / (3. * f * f * f) + c.b2 * M::log(f);
 }
 __device__ __forceinline__ double dphi_int(const PhdRec& c, double f) {
   return (c.b1 + c.b3 / (f * f * f * f) + c.b2 / f) / c.eta;
 }
+template <class M = MathInline>
 __device__ __forceinline__ double phi_mrd(const PhdRec& c, double f) {
   double sq = sqrt(f), f34 = sqrt(f * sq);
-  return -(c.al2 / f) + (4.0 / 3.0) * (c.al3 * f34) + c.al1 * f + c.al4 * atan((f - c.al5 * c.fRD) / c.fDM);
+  return -(c.al2 / f) + (4.0 / 3.0) * (c.al3 * f34) + c.al1 * f + c.al4 * M::atan((f - c.al5 * c.fRD) / c.fDM);
 }
+template <class M = MathInline>
 __device__ __forceinline__ double dphi_mrd(const PhdRec& c, double f) {
   double x = f - c.al5 * c.fRD;
-  return (c.al1 + c.al2 / (f * f) + c.al3 / pow(f, 0.25) + c.al4 / (c.fDM * (1 + x * x / (c.fDM * c.fDM)))) / c.eta;
+  return (c.al1 + c.al2 / (f * f) + c.al3 / M::pow(f, 0.25) + c.al4 / (c.fDM * (1 + x * x / (c.fDM * c.fDM)))) / c.eta;
 }
 
 // FP64 amplitude (without amp_scale) and phase (with the fRef shift) at geometric frequency Mf.

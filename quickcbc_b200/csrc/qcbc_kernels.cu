@@ -1,7 +1,8 @@
 // CUDA kernels of the QuickCBC likelihood hot path (sm_100a).
 //
-//   k_setup          one thread per parameter set: IMRPhenomD coefficients,
-//                    start/cut-off bins and detector response, all FP64.
+//   k_setup          one block of 4 warps per 32 parameter sets: IMRPhenomD
+//                    coefficients, start/cut-off bins and detector response,
+//                    all FP64, the warps working on independent pieces.
 //   k_lnl_full<P>    fused waveform -> projection -> PSD-weighted inner
 //                    products over one tile of bins of one parameter set; no
 //                    h(f) is written to memory.  P = FP64 or mixed.
@@ -174,16 +175,6 @@ __device__ double erad(double eta, double chi1, double chi2) {
          (1. + (-0.6714403054720589 - 1.4756929437702908 * eta + 7.304676214885011 * e2) * s);
 }
 
-__device__ double damp_ins(const PhdRec& c, double Mf) {
-  Pow6 p = pow6(Mf);
-  return (2.0 / 3.0) * c.ai[0] / p.third + c.ai[1] + (4.0 / 3.0) * c.ai[2] * p.third +
-         (5.0 / 3.0) * c.ai[3] * p.two_thirds + 2.0 * c.ai[4] * Mf + (7.0 / 3.0) * c.ai[5] * p.four_thirds +
-         (8.0 / 3.0) * c.ai[6] * p.five_thirds + 3.0 * c.ai[7] * p.two;
-}
-__device__ double damp_mrd(const PhdRec& c, double f) {
-  double fg = c.fDM * c.g3, df = f - c.fRD, den = df * df + fg * fg;
-  return amp_mrd(c, f) * (-c.g2 / fg - 2.0 * df / den);
-}
 __device__ double damp_ins_p(const PhdRec& c, double Mf, const Pow6& p) {
   return (2.0 / 3.0) * c.ai[0] / p.third + c.ai[1] + (4.0 / 3.0) * c.ai[2] * p.third +
          (5.0 / 3.0) * c.ai[3] * p.two_thirds + 2.0 * c.ai[4] * Mf + (7.0 / 3.0) * c.ai[5] * p.four_thirds +
@@ -223,143 +214,139 @@ __device__ double phi_ins_logv(const PhdRec& c, double Mf, const Pow6& p, double
   return ph;
 }
 
-// d(phi_ins)/dMf (IMRPhenomD_internals.c:1455-1493); pv/pvl are the TaylorF2 series
-__device__ double dphi_ins(const PhdRec& c, const double* pv, const double* pvl, double s1, double s2, double s3,
-                           double s4, double pi_third, double pi_two_thirds, double Mf) {
-  double v = cbrt(kPi * Mf), logv = log(v);
-  double v2 = v * v, v3 = v * v2, v4 = v * v3, v5 = v * v4, v6 = v * v5, v7 = v * v6, v8 = v * v7;
-  double D = 0.0;
-  D += 2.0 * pv[7] * v7;
-  D += (pv[6] + pvl[6] * (1.0 + logv)) * v6;
-  D += pvl[5] * v5;
-  D += -1.0 * pv[4] * v4;
-  D += -2.0 * pv[3] * v3;
-  D += -3.0 * pv[2] * v2;
-  D += -4.0 * pv[1] * v;
-  D += -5.0 * pv[0];
-  D /= v8 * 3.0 / kPi;
-  D += (s1 + s2 * v / pi_third + s3 * v2 / pi_two_thirds + (s4 / kPi) * v3) / c.eta;
-  return D;
-}
+// One out-of-line copy of each math routine for the setup code (see MathInline).
+struct MathOutline {
+  static __device__ __noinline__ double pow(double x, double y) { return ::pow(x, y); }
+  static __device__ __noinline__ double exp(double x) { return ::exp(x); }
+  static __device__ __noinline__ double log(double x) { return ::log(x); }
+  static __device__ __noinline__ double atan(double x) { return ::atan(x); }
+  static __device__ __noinline__ double atan2(double y, double x) { return ::atan2(y, x); }
+  static __device__ __noinline__ double cbrt(double x) { return ::cbrt(x); }
+  static __device__ __noinline__ void sincos(double x, double* sv, double* cv) { ::sincos(x, sv, cv); }
+};
+using MO = MathOutline;
 
-// IMRPhenomD coefficient setup for one system (IMRPhenomD.c:413-503). Masses in Msun.
-__device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, double m2_in, double chi1_in,
-                         double chi2_in, double dist, const QnmTable& q) {
-  int st = kStOK;
-  if (!(m1_in > 0.0) || !(m2_in > 0.0)) st |= kStBadMass;
-  if (!(dist > 0.0)) st |= kStBadDist;
-  if (!(chi1_in <= 1.0 && chi1_in >= -1.0 && chi2_in <= 1.0 && chi2_in >= -1.0)) st |= kStBadSpin;
-  double m1 = m1_in, m2 = m2_in, chi1 = chi1_in, chi2 = chi2_in;
-  if (!(m1_in > m2_in)) { m1 = m2_in; m2 = m1_in; chi1 = chi2_in; chi2 = chi1_in; }
-  const Pow6 pip = c_setup.pi6;
-  c.pi_third = pip.third;
-  double M = m1 + m2, eta = m1 * m2 / (M * M);
+// ---- IMRPhenomD coefficient setup (IMRPhenomD.c:413-503), in pieces.  The serial
+// phd_setup below and the cooperative k_setup (four warps per 32 parameter sets) evaluate
+// the same expressions; only the compiler's contraction of them may differ (last-bit).
+
+// Validity bits, mass ordering (m1 >= m2), scales.  Masses in Msun.
+struct PhdMass { double m1, m2, chi1, chi2, eta, Seta, chi; int st; };
+__device__ __forceinline__ PhdMass phd_masses(PhdRec& c, double m1_in, double m2_in, double chi1_in, double chi2_in,
+                                              double dist) {
+  PhdMass m;
+  m.st = kStOK;
+  if (!(m1_in > 0.0) || !(m2_in > 0.0)) m.st |= kStBadMass;
+  if (!(dist > 0.0)) m.st |= kStBadDist;
+  if (!(chi1_in <= 1.0 && chi1_in >= -1.0 && chi2_in <= 1.0 && chi2_in >= -1.0)) m.st |= kStBadSpin;
+  m.m1 = m1_in; m.m2 = m2_in; m.chi1 = chi1_in; m.chi2 = chi2_in;
+  if (!(m1_in > m2_in)) { m.m1 = m2_in; m.m2 = m1_in; m.chi1 = chi2_in; m.chi2 = chi1_in; }
+  c.pi_third = c_setup.pi6.third;
+  double M = m.m1 + m.m2, eta = m.m1 * m.m2 / (M * M);
   c.eta = eta; c.inv_eta = 1.0 / eta;
   c.Msec = M * kMtsun;
   c.amp_scale = M * kMrsun * M * kMtsun / dist;
   c.fCut = kFcut / c.Msec;
-  double Seta = sqrt(1.0 - 4.0 * eta);
-  double chi = (chi1 + chi2) / 2.0 * (1.0 - eta * 76.0 / 113.0) + Seta * ((chi1 - chi2) / 2.0);
-  double fsp = final_spin(eta, chi1, chi2);
+  m.eta = eta;
+  m.Seta = sqrt(1.0 - 4.0 * eta);
+  m.chi = (m.chi1 + m.chi2) / 2.0 * (1.0 - eta * 76.0 / 113.0) + m.Seta * ((m.chi1 - m.chi2) / 2.0);
+  return m;
+}
+
+// Ringdown and damping frequencies from the final spin and radiated energy; returns status bits.
+__device__ __forceinline__ int phd_ringdown(PhdRec& c, const PhdMass& m, const QnmTable& q) {
+  int st = 0;
+  double fsp = final_spin(m.eta, m.chi1, m.chi2);
   if (!(fsp <= 1.0)) { st |= kStBadSpinFinal; fsp = 1.0; }
   if (!(fsp >= -1.0)) fsp = -1.0;
-  double er = erad(eta, chi1, chi2);
+  double er = erad(m.eta, m.chi1, m.chi2);
   int qi = qnm_interval(q, fsp);
   c.fRD = qnm_eval_at(q, q.yr, q.mr, qi, fsp) / (1.0 - er);
   c.fDM = qnm_eval_at(q, q.yd, q.md, qi, fsp) / (1.0 - er);
-  // amplitude
+  return st;
+}
+
+// The Table V fits: merger-ringdown amplitude, inspiral amplitude rho_1..3, phase alpha/beta
+// into the record; the collocation value v2 and the sigma_1..4 into the outputs.
+__device__ __forceinline__ void phd_fits(PhdRec& c, double eta, double chi, double& v2, double* s) {
   c.g1 = fit_eval(F_GAM1, eta, chi); c.g2 = fit_eval(F_GAM2, eta, chi); c.g3 = fit_eval(F_GAM3, eta, chi);
-  if (c.g2 <= 1)
-    c.fmax = fabs(c.fRD + (c.fDM * (-1 + sqrt(1 - c.g2 * c.g2)) * c.g3) / c.g2);
-  else
-    c.fmax = fabs(c.fRD + (c.fDM * (-1) * c.g3) / c.g2);
-  c.a0 = (sqrt(2.0 / 3.0) * sqrt(eta)) / pip.sixth;
-  {
-    // inspiral amplitude prefactors, Appendix B of arXiv:1508.07253
-    double x1 = chi1, x2 = chi2, x1s = x1 * x1, x2s = x2 * x2, e2 = eta * eta, e3 = eta * e2, Pi = kPi;
-    double Pi2 = pip.two;
-    c.ai[0] = ((-969 + 1804 * eta) * pip.two_thirds) / 672.;
-    c.ai[1] = ((x1 * (81 * (1 + Seta) - 44 * eta) + x2 * (81 - 81 * Seta - 44 * eta)) * Pi) / 48.;
-    c.ai[2] = ((-27312085.0 - 10287648 * x2s - 10287648 * x1s * (1 + Seta) + 10287648 * x2s * Seta +
-                24 * (-1975055 + 857304 * x1s - 994896 * x1 * x2 + 857304 * x2s) * eta + 35371056 * e2) *
-               pip.four_thirds) / 8.128512e6;
-    c.ai[3] = (pip.five_thirds * (x2 * (-285197 * (-1 + Seta) + 4 * (-91902 + 1579 * Seta) * eta - 35632 * e2) +
-                                  x1 * (285197 * (1 + Seta) - 4 * (91902 + 1579 * Seta) * eta - 35632 * e2) +
-                                  42840 * (-1.0 + 4 * eta) * Pi)) / 32256.;
-    c.ai[4] = -(Pi2 * (-336 * (-3248849057.0 + 2943675504 * x1s - 3339284256 * x1 * x2 + 2943675504 * x2s) * e2 -
-                       324322727232 * e3 -
-                       7 * (-177520268561 + 107414046432 * x2s + 107414046432 * x1s * (1 + Seta) -
-                            107414046432 * x2s * Seta + 11087290368 * (x1 + x2 + x1 * Seta - x2 * Seta) * Pi) +
-                       12 * eta * (-545384828789 - 176491177632 * x1 * x2 + 202603761360 * x2s +
-                                   77616 * x1s * (2610335 + 995766 * Seta) - 77287373856 * x2s * Seta +
-                                   5841690624 * (x1 + x2) * Pi + 21384760320 * Pi2))) / 6.0085960704e10;
-    c.ai[5] = fit_eval(F_RHO1, eta, chi);
-    c.ai[6] = fit_eval(F_RHO2, eta, chi);
-    c.ai[7] = fit_eval(F_RHO3, eta, chi);
-  }
-  {
-    // intermediate amplitude: quartic with value and slope at f1, value at f2, value and
-    // slope at f3 (eqs. 21-26 of arXiv:1508.07253), kept in Newton form on nodes f1,f1,f2,f3,f3
-    double f1 = kAmpJoin, f3 = c.fmax, f2 = f1 + (f3 - f1) / 2.0;
-    const Pow6 p1 = c_setup.f1p;
-    double v1 = amp_ins(c, f1, p1), d1 = damp_ins_p(c, f1, p1);
-    double v3 = amp_mrd(c, f3);
-    double fg3 = c.fDM * c.g3, df3 = f3 - c.fRD;
-    double d2 = v3 * (-c.g2 / fg3 - 2.0 * df3 / (df3 * df3 + fg3 * fg3));
-    double v2 = fit_eval(F_V2, eta, chi);
-    double q01 = d1, q12 = (v2 - v1) / (f2 - f1), q23 = (v3 - v2) / (f3 - f2), q34 = d2;
-    double q012 = (q12 - q01) / (f2 - f1), q123 = (q23 - q12) / (f3 - f1), q234 = (q34 - q23) / (f3 - f2);
-    double q0123 = (q123 - q012) / (f3 - f1), q1234 = (q234 - q123) / (f3 - f1);
-    c.hx1 = f1; c.hx2 = f2; c.hx3 = f3;
-    c.hc[0] = v1; c.hc[1] = q01; c.hc[2] = q012; c.hc[3] = q0123; c.hc[4] = (q1234 - q0123) / (f3 - f1);
-  }
-  // phase
-  double s1 = fit_eval(F_SI1, eta, chi), s2 = fit_eval(F_SI2, eta, chi), s3 = fit_eval(F_SI3, eta, chi),
-         s4 = fit_eval(F_SI4, eta, chi);
+  c.ai[5] = fit_eval(F_RHO1, eta, chi);
+  c.ai[6] = fit_eval(F_RHO2, eta, chi);
+  c.ai[7] = fit_eval(F_RHO3, eta, chi);
+  v2 = fit_eval(F_V2, eta, chi);
+  s[0] = fit_eval(F_SI1, eta, chi); s[1] = fit_eval(F_SI2, eta, chi); s[2] = fit_eval(F_SI3, eta, chi);
+  s[3] = fit_eval(F_SI4, eta, chi);
   c.b1 = fit_eval(F_BE1, eta, chi); c.b2 = fit_eval(F_BE2, eta, chi); c.b3 = fit_eval(F_BE3, eta, chi);
   c.al1 = fit_eval(F_AL1, eta, chi); c.al2 = fit_eval(F_AL2, eta, chi); c.al3 = fit_eval(F_AL3, eta, chi);
   c.al4 = fit_eval(F_AL4, eta, chi); c.al5 = fit_eval(F_AL5, eta, chi);
-  double pv[8], pvl[8];
-  {
-    // TaylorF2 phasing incl. aligned-spin terms (IMRPhenomD_internals.c:244-365), then minus the
-    // 3PN spin-spin term PhenomD was not tuned with (IMRPhenomD.c:478)
-    double mt = m1 + m2, d = (m1 - m2) / mt, et = m1 * m2 / mt / mt, m1M = m1 / mt, m2M = m2 / mt;
-    double SL = m1M * m1M * chi1 + m2M * m2M * chi2, dSigmaL = d * (m2M * chi2 - m1M * chi1);
-    double pfaN = 3.0 / (128.0 * et);
-    double v[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vl[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    v[0] = 1.0;
-    v[2] = 5.0 * (743.0 / 84.0 + 11.0 * et) / 9.0;
-    v[3] = -16.0 * kPi;
-    v[4] = 5.0 * (3058.673 / 7.056 + 5429.0 / 7.0 * et + 617.0 * et * et) / 72.0;
-    v[5] = 5.0 / 9.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
-    vl[5] = 5.0 / 3.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
-    v[6] = (11583.231236531 / 4.694215680 - 640.0 / 3.0 * kPi * kPi - 6848.0 / 21.0 * kGammaE) +
-           et * (-15737.765635 / 3.048192 + 2255. / 12. * kPi * kPi) + et * et * 76055.0 / 1728.0 -
-           et * et * et * 127825.0 / 1296.0;
-    v[6] += (-6848.0 / 21.0) * log(4.);
-    vl[6] = -6848.0 / 21.0;
-    v[7] = kPi * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * et - 74045.0 / 756.0 * et * et);
-    double sig = et * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
-    sig += (720.0 - 1.0) / 96.0 * m1M * m1M * chi1 * chi1;
-    sig += (720.0 - 1.0) / 96.0 * m2M * m2M * chi2 * chi2;
-    sig -= (240.0 - 7.0) / 96.0 * m1M * m1M * chi1 * chi1;
-    sig -= (240.0 - 7.0) / 96.0 * m2M * m2M * chi2 * chi2;
-    double ss3 = (326.75 / 1.12 + 557.5 / 1.8 * et) * et * chi1 * chi2;
-    ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m1M - 120.0 * m1M * m1M) +
-            (-4108.25 / 6.72 - 108.5 / 1.2 * m1M + 125.5 / 3.6 * m1M * m1M)) * m1M * m1M * chi1 * chi1;
-    ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m2M - 120.0 * m2M * m2M) +
-            (-4108.25 / 6.72 - 108.5 / 1.2 * m2M + 125.5 / 3.6 * m2M * m2M)) * m2M * m2M * chi2 * chi2;
-    double gam = (554345.0 / 1134.0 + 110.0 * et / 9.0) * SL + (13915.0 / 84.0 - 10.0 * et / 3.0) * dSigmaL;
-    v[7] += (-8980424995.0 / 762048.0 + 6586595.0 * et / 756.0 - 305.0 * et * et / 36.0) * SL -
-            (170978035.0 / 48384.0 - 2876425.0 * et / 672.0 - 4735.0 * et * et / 144.0) * dSigmaL;
-    v[6] += kPi * (3760.0 * SL + 1490.0 * dSigmaL) / 3.0 + ss3;
-    v[5] += -1.0 * gam;
-    vl[5] += -3.0 * gam;
-    v[4] += -10.0 * sig;
-    v[3] += 188.0 * SL / 3.0 + 25.0 * dSigmaL;
-    for (int k = 0; k < 8; k++) { pv[k] = v[k] * pfaN; pvl[k] = vl[k] * pfaN; }
-    pv[6] -= ss3 * pv[0];
-  }
+}
+
+// a0 and the analytic inspiral amplitude prefactors, Appendix B of arXiv:1508.07253.
+__device__ __forceinline__ void phd_amp_prefactors(PhdRec& c, const PhdMass& m) {
+  const Pow6 pip = c_setup.pi6;
+  double eta = m.eta, Seta = m.Seta;
+  c.a0 = (sqrt(2.0 / 3.0) * sqrt(eta)) / pip.sixth;
+  double x1 = m.chi1, x2 = m.chi2, x1s = x1 * x1, x2s = x2 * x2, e2 = eta * eta, e3 = eta * e2, Pi = kPi;
+  double Pi2 = pip.two;
+  c.ai[0] = ((-969 + 1804 * eta) * pip.two_thirds) / 672.;
+  c.ai[1] = ((x1 * (81 * (1 + Seta) - 44 * eta) + x2 * (81 - 81 * Seta - 44 * eta)) * Pi) / 48.;
+  c.ai[2] = ((-27312085.0 - 10287648 * x2s - 10287648 * x1s * (1 + Seta) + 10287648 * x2s * Seta +
+              24 * (-1975055 + 857304 * x1s - 994896 * x1 * x2 + 857304 * x2s) * eta + 35371056 * e2) *
+             pip.four_thirds) / 8.128512e6;
+  c.ai[3] = (pip.five_thirds * (x2 * (-285197 * (-1 + Seta) + 4 * (-91902 + 1579 * Seta) * eta - 35632 * e2) +
+                                x1 * (285197 * (1 + Seta) - 4 * (91902 + 1579 * Seta) * eta - 35632 * e2) +
+                                42840 * (-1.0 + 4 * eta) * Pi)) / 32256.;
+  c.ai[4] = -(Pi2 * (-336 * (-3248849057.0 + 2943675504 * x1s - 3339284256 * x1 * x2 + 2943675504 * x2s) * e2 -
+                     324322727232 * e3 -
+                     7 * (-177520268561 + 107414046432 * x2s + 107414046432 * x1s * (1 + Seta) -
+                          107414046432 * x2s * Seta + 11087290368 * (x1 + x2 + x1 * Seta - x2 * Seta) * Pi) +
+                     12 * eta * (-545384828789 - 176491177632 * x1 * x2 + 202603761360 * x2s +
+                                 77616 * x1s * (2610335 + 995766 * Seta) - 77287373856 * x2s * Seta +
+                                 5841690624 * (x1 + x2) * Pi + 21384760320 * Pi2))) / 6.0085960704e10;
+}
+
+// TaylorF2 phasing incl. aligned-spin terms (IMRPhenomD_internals.c:244-365), minus the 3PN
+// spin-spin term PhenomD was not tuned with (IMRPhenomD.c:478); the inspiral phase prefactors
+// pq[0..8] follow from it.
+__device__ __forceinline__ void phd_taylorf2(PhdRec& c, const PhdMass& m, double* pv, double* pvl) {
+  const Pow6 pip = c_setup.pi6;
+  double m1 = m.m1, m2 = m.m2, chi1 = m.chi1, chi2 = m.chi2;
+  double mt = m1 + m2, d = (m1 - m2) / mt, et = m1 * m2 / mt / mt, m1M = m1 / mt, m2M = m2 / mt;
+  double SL = m1M * m1M * chi1 + m2M * m2M * chi2, dSigmaL = d * (m2M * chi2 - m1M * chi1);
+  double pfaN = 3.0 / (128.0 * et);
+  double v[8] = {0, 0, 0, 0, 0, 0, 0, 0}, vl[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  v[0] = 1.0;
+  v[2] = 5.0 * (743.0 / 84.0 + 11.0 * et) / 9.0;
+  v[3] = -16.0 * kPi;
+  v[4] = 5.0 * (3058.673 / 7.056 + 5429.0 / 7.0 * et + 617.0 * et * et) / 72.0;
+  v[5] = 5.0 / 9.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
+  vl[5] = 5.0 / 3.0 * (7729.0 / 84.0 - 13.0 * et) * kPi;
+  v[6] = (11583.231236531 / 4.694215680 - 640.0 / 3.0 * kPi * kPi - 6848.0 / 21.0 * kGammaE) +
+         et * (-15737.765635 / 3.048192 + 2255. / 12. * kPi * kPi) + et * et * 76055.0 / 1728.0 -
+         et * et * et * 127825.0 / 1296.0;
+  v[6] += (-6848.0 / 21.0) * MO::log(4.);
+  vl[6] = -6848.0 / 21.0;
+  v[7] = kPi * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * et - 74045.0 / 756.0 * et * et);
+  double sig = et * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
+  sig += (720.0 - 1.0) / 96.0 * m1M * m1M * chi1 * chi1;
+  sig += (720.0 - 1.0) / 96.0 * m2M * m2M * chi2 * chi2;
+  sig -= (240.0 - 7.0) / 96.0 * m1M * m1M * chi1 * chi1;
+  sig -= (240.0 - 7.0) / 96.0 * m2M * m2M * chi2 * chi2;
+  double ss3 = (326.75 / 1.12 + 557.5 / 1.8 * et) * et * chi1 * chi2;
+  ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m1M - 120.0 * m1M * m1M) +
+          (-4108.25 / 6.72 - 108.5 / 1.2 * m1M + 125.5 / 3.6 * m1M * m1M)) * m1M * m1M * chi1 * chi1;
+  ss3 += ((4703.5 / 8.4 + 2935.0 / 6.0 * m2M - 120.0 * m2M * m2M) +
+          (-4108.25 / 6.72 - 108.5 / 1.2 * m2M + 125.5 / 3.6 * m2M * m2M)) * m2M * m2M * chi2 * chi2;
+  double gam = (554345.0 / 1134.0 + 110.0 * et / 9.0) * SL + (13915.0 / 84.0 - 10.0 * et / 3.0) * dSigmaL;
+  v[7] += (-8980424995.0 / 762048.0 + 6586595.0 * et / 756.0 - 305.0 * et * et / 36.0) * SL -
+          (170978035.0 / 48384.0 - 2876425.0 * et / 672.0 - 4735.0 * et * et / 144.0) * dSigmaL;
+  v[6] += kPi * (3760.0 * SL + 1490.0 * dSigmaL) / 3.0 + ss3;
+  v[5] += -1.0 * gam;
+  vl[5] += -3.0 * gam;
+  v[4] += -10.0 * sig;
+  v[3] += 188.0 * SL / 3.0 + 25.0 * dSigmaL;
+  for (int k = 0; k < 8; k++) { pv[k] = v[k] * pfaN; pvl[k] = vl[k] * pfaN; }
+  pv[6] -= ss3 * pv[0];
   c.pq[0] = pv[5] - kPi4;
   c.pq[1] = pv[7] * pip.two_thirds;
   c.pq[2] = pv[6] * pip.third;
@@ -369,48 +356,128 @@ __device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, doub
   c.pq[6] = pv[3] / pip.two_thirds;
   c.pq[7] = pv[2] / kPi;
   c.pq[8] = pv[0] / pip.five_thirds;
-  c.pq[9] = s1;
-  c.pq[10] = s2 * 3.0 / 4.0;
-  c.pq[11] = s3 * 3.0 / 5.0;
-  c.pq[12] = s4 / 2.0;
-  {
-    // C^1 joins (IMRPhenomD_internals.c:1547-1584)
-    double fj = kPhiJoin;
-    c.C2Int = dphi_ins_join(c, pv, pvl, s1, s2, s3, s4, pip.third, pip.two_thirds) - dphi_int(c, fj);
-    const Pow6 pj = c_setup.fjp;
-    double phi_int_fj = c.b1 * fj - c.b3 / (3. * fj * fj * fj) + c.b2 * c_setup.log_fj;
-    c.C1Int = phi_ins_logv(c, fj, pj, c_setup.logvj) - 1.0 / eta * phi_int_fj - c.C2Int * fj;
-    c.fMRDJoin = 0.5 * c.fRD;
-    double fm = c.fMRDJoin;
-    double phiT = 1.0 / eta * phi_int(c, fm) + c.C1Int + c.C2Int * fm;
-    double dphiT = c.C2Int + dphi_int(c, fm);
-    c.C2MRD = dphiT - dphi_mrd(c, fm);
-    c.C1MRD = phiT - 1.0 / eta * phi_mrd(c, fm) - c.C2MRD * fm;
-  }
-  c.t0 = dphi_mrd(c, c.fmax);
+}
+__device__ __forceinline__ void phd_pq_sigma(PhdRec& c, const double* s) {
+  c.pq[9] = s[0];
+  c.pq[10] = s[1] * 3.0 / 4.0;
+  c.pq[11] = s[2] * 3.0 / 5.0;
+  c.pq[12] = s[3] / 2.0;
+}
+
+// Peak frequency of the merger-ringdown amplitude (needs g1..g3, fRD, fDM).
+__device__ __forceinline__ double phd_fmax(const PhdRec& c) {
+  if (c.g2 <= 1) return fabs(c.fRD + (c.fDM * (-1 + sqrt(1 - c.g2 * c.g2)) * c.g3) / c.g2);
+  return fabs(c.fRD + (c.fDM * (-1) * c.g3) / c.g2);
+}
+
+// Intermediate amplitude: quartic with value and slope at f1, value at f2, value and slope at
+// f3 (eqs. 21-26 of arXiv:1508.07253), kept in Newton form on nodes f1,f1,f2,f3,f3.
+__device__ __forceinline__ void phd_amp_int(PhdRec& c, double v2) {
+  double f1 = kAmpJoin, f3 = c.fmax, f2 = f1 + (f3 - f1) / 2.0;
+  const Pow6 p1 = c_setup.f1p;
+  double v1 = amp_ins(c, f1, p1), d1 = damp_ins_p(c, f1, p1);
+  double v3 = amp_mrd<MO>(c, f3);
+  double fg3 = c.fDM * c.g3, df3 = f3 - c.fRD;
+  double d2 = v3 * (-c.g2 / fg3 - 2.0 * df3 / (df3 * df3 + fg3 * fg3));
+  double q01 = d1, q12 = (v2 - v1) / (f2 - f1), q23 = (v3 - v2) / (f3 - f2), q34 = d2;
+  double q012 = (q12 - q01) / (f2 - f1), q123 = (q23 - q12) / (f3 - f1), q234 = (q34 - q23) / (f3 - f2);
+  double q0123 = (q123 - q012) / (f3 - f1), q1234 = (q234 - q123) / (f3 - f1);
+  c.hx1 = f1; c.hx2 = f2; c.hx3 = f3;
+  c.hc[0] = v1; c.hc[1] = q01; c.hc[2] = q012; c.hc[3] = q0123; c.hc[4] = (q1234 - q0123) / (f3 - f1);
+}
+
+// C^1 join inspiral -> intermediate at Mf = 0.018 (IMRPhenomD_internals.c:1547-1566).
+__device__ __forceinline__ void phd_join_int(PhdRec& c, const double* pv, const double* pvl, const double* s) {
+  const Pow6 pip = c_setup.pi6;
+  double fj = kPhiJoin;
+  c.C2Int = dphi_ins_join(c, pv, pvl, s[0], s[1], s[2], s[3], pip.third, pip.two_thirds) - dphi_int(c, fj);
+  const Pow6 pj = c_setup.fjp;
+  double phi_int_fj = c.b1 * fj - c.b3 / (3. * fj * fj * fj) + c.b2 * c_setup.log_fj;
+  c.C1Int = phi_ins_logv(c, fj, pj, c_setup.logvj) - 1.0 / c.eta * phi_int_fj - c.C2Int * fj;
+}
+
+// The four phase pieces at the intermediate -> merger-ringdown join Mf = fRD/2.
+struct MrdJoin { double phi_int, dphi_int, phi_mrd, dphi_mrd; };
+__device__ __forceinline__ MrdJoin phd_mrd_pieces(const PhdRec& c) {
+  double fm = 0.5 * c.fRD;
+  MrdJoin j;
+  j.phi_int = phi_int<MO>(c, fm);
+  j.dphi_int = dphi_int(c, fm);
+  j.phi_mrd = phi_mrd<MO>(c, fm);
+  j.dphi_mrd = dphi_mrd<MO>(c, fm);
+  return j;
+}
+// C^1 join intermediate -> merger-ringdown (IMRPhenomD_internals.c:1568-1584).
+__device__ __forceinline__ void phd_join_mrd(PhdRec& c, const MrdJoin& j) {
+  double eta = c.eta;
+  c.fMRDJoin = 0.5 * c.fRD;
+  double fm = c.fMRDJoin;
+  double phiT = 1.0 / eta * j.phi_int + c.C1Int + c.C2Int * fm;
+  double dphiT = c.C2Int + j.dphi_int;
+  c.C2MRD = dphiT - j.dphi_mrd;
+  c.C1MRD = phiT - 1.0 / eta * j.phi_mrd - c.C2MRD * fm;
+}
+
+// Phase at the reference frequency (IMRPhenomD.c:497-503): the piece that depends on the
+// coefficients alone (needs pq, alpha/beta, fRD, fDM), then the join constants added.
+__device__ __forceinline__ double phd_phi_ref_raw(const PhdRec& c, int& branch) {
+  double Mf = c.MfRef;
+  if (Mf < kPhiJoin) { branch = 0; Pow6 pr = pow6<MO>(Mf); return phi_ins<MO>(c, Mf, pr); }
+  if (Mf >= 0.5 * c.fRD) { branch = 1; return phi_mrd<MO>(c, Mf); }
+  branch = 2;
+  return phi_int<MO>(c, Mf);
+}
+__device__ __forceinline__ void phd_phi_ref(PhdRec& c, double phi0, double raw, int branch) {
+  double Mf = c.MfRef, phr;
+  if (branch == 0) phr = raw;
+  else if (branch == 1) phr = 1.0 / c.eta * raw + c.C1MRD + c.C2MRD * Mf;
+  else phr = 1.0 / c.eta * raw + c.C1Int + c.C2Int * Mf;
+  c.phi_pre = 2. * phi0 + phr;
+}
+
+// Serial setup of one system (used by the amplitude/phase entry point).
+__device__ int phd_setup(PhdRec& c, double phi0, double fRef, double m1_in, double m2_in, double chi1_in,
+                         double chi2_in, double dist, const QnmTable& q) {
+  PhdMass m = phd_masses(c, m1_in, m2_in, chi1_in, chi2_in, dist);
+  int st = m.st | phd_ringdown(c, m, q);
+  double v2, s[4], pv[8], pvl[8];
+  phd_fits(c, m.eta, m.chi, v2, s);
+  c.fmax = phd_fmax(c);
+  phd_amp_prefactors(c, m);
+  phd_amp_int(c, v2);
+  phd_taylorf2(c, m, pv, pvl);
+  phd_pq_sigma(c, s);
+  phd_join_int(c, pv, pvl, s);
+  phd_join_mrd(c, phd_mrd_pieces(c));
+  c.t0 = dphi_mrd<MO>(c, c.fmax);
   c.MfRef = c.Msec * fRef;
-  {
-    // phase at the reference frequency (IMRPhenomD.c:497-503)
-    double Mf = c.MfRef, phr;
-    Pow6 pr = pow6(Mf);
-    if (Mf < kPhiJoin) phr = phi_ins(c, Mf, pr);
-    else if (Mf >= c.fMRDJoin) phr = 1.0 / c.eta * phi_mrd(c, Mf) + c.C1MRD + c.C2MRD * Mf;
-    else phr = 1.0 / c.eta * phi_int(c, Mf) + c.C1Int + c.C2Int * Mf;
-    c.phi_pre = 2. * phi0 + phr;
-  }
+  int br;
+  double raw = phd_phi_ref_raw(c, br);
+  phd_phi_ref(c, phi0, raw, br);
   c.flags = (st == kStOK) ? kRecValid : 0;
   return st;
 }
 
-// start frequency: 3PN inversion of t(f) for time params[5] before merger (Utilities.c:587-629)
-__device__ double fbegin_dev(const double* p) {
-  const double gE = 0.5772156649;
-  double Mc = exp(p[0]) / kMsun * kTsunCBC, M = exp(p[1]) / kMsun * kTsunCBC;
-  double eta = pow(Mc / M, 5.0 / 3.0);
+// ---- parameter set -> record (QuickCBC.c:3698-3755 / 3795-3850)
+
+// start frequency: 3PN inversion of t(f) for time params[5] before merger (Utilities.c:587-629),
+// split into the part before and after the log of theta.
+struct FbeginHead { double M, eta, chi, th; };
+__device__ __forceinline__ FbeginHead fbegin_head(const double* p) {
+  FbeginHead h;
+  double Mc = MO::exp(p[0]) / kMsun * kTsunCBC, M = MO::exp(p[1]) / kMsun * kTsunCBC;
+  double eta = MO::pow(Mc / M, 5.0 / 3.0);
   if (eta > 0.25) eta = 0.25;
   double dm = sqrt(1.0 - 4.0 * eta), m1 = M * (1.0 + dm) / 2.0, m2 = M * (1.0 - dm) / 2.0;
-  double c1 = p[2], c2 = p[3], chi = (m1 * c1 + m2 * c2) / M, tc = p[5];
-  double th = pow(eta * tc / (5.0 * M), -1.0 / 8.0);
+  h.M = M;
+  h.eta = eta;
+  h.chi = (m1 * p[2] + m2 * p[3]) / M;
+  h.th = MO::pow(eta * p[5] / (5.0 * M), -1.0 / 8.0);
+  return h;
+}
+__device__ __forceinline__ double fbegin_tail(const FbeginHead& h, double c1, double c2) {
+  const double gE = 0.5772156649;
+  double M = h.M, eta = h.eta, chi = h.chi, th = h.th;
   double t2 = th * th, t3 = t2 * th, t4 = t2 * t2, t5 = t2 * t3, t6 = t3 * t3;
   double PN1 = (11.0 / 32.0 * eta + 743.0 / 2688.0) * t2;
   double PN15 = -3.0 * kPi / 10.0 * t3 + (1.0 / 160.0) * (113.0 * chi - 38.0 * eta * (c1 + c2)) * t3;
@@ -419,7 +486,7 @@ __device__ double fbegin_dev(const double* p) {
   double PN25 = -(7729.0 / 21504.0 - 13.0 / 256.0 * eta) * kPi * t5;
   double PN3 = (-720817631400877.0 / 288412611379200.0 + 53.0 / 200.0 * kPi * kPi + 107.0 / 280.0 * gE +
                 (25302017977.0 / 4161798144.0 - 451.0 / 2048.0 * kPi * kPi) * eta - 30913.0 / 1835008.0 * eta * eta +
-                235925.0 / 1769472.0 * eta * eta * eta + 107.0 / 280.0 * log(2.0 * th)) * t6;
+                235925.0 / 1769472.0 * eta * eta * eta + 107.0 / 280.0 * MO::log(2.0 * th)) * t6;
   return t3 / (8.0 * M * kPi) * (1.0 + PN1 + PN15 + PN2 + PN25 + PN3);
 }
 
@@ -427,23 +494,27 @@ __device__ __forceinline__ double bin_freq(const NetGeom& g, int i) {
   return g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
 }
 
-// Full parameter set -> record: waveform coefficients + per-detector projection
-// (QuickCBC.c:3698-3755 / 3795-3850).  Returns status bits.
-__device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, const QnmTable& q) {
-  double fs = fbegin_dev(p);
-  double mc = exp(p[0]), mt = exp(p[1]);
-  double eta = pow((mc / mt), (5.0 / 3.0));
+// Physical inputs of phd_setup from a parameter set (QuickCBC.c:3702-3712).
+struct SetPhys { double m1, m2, dist; };
+__device__ __forceinline__ SetPhys set_phys(const double* p) {
+  double mc = MO::exp(p[0]), mt = MO::exp(p[1]);
+  double eta = MO::pow((mc / mt), (5.0 / 3.0));
   double dm = eta > 0.25 ? 0.0 : sqrt(1.0 - 4.0 * eta);
   double m1 = mt * (1.0 + dm) / 2.0, m2 = mt * (1.0 - dm) / 2.0;
-  int st = phd_setup(c, 0.5 * p[4], kFref, m1 / kMsun, m2 / kMsun, p[2], p[3], exp(p[6]), q);
-  c.fs = fs;
-  c.ts = g.Tobs - p[5];
-  c.sqT = sqrt(g.Tobs);
+  SetPhys s;
+  s.m1 = m1 / kMsun;
+  s.m2 = m2 / kMsun;
+  s.dist = MO::exp(p[6]);
+  return s;
+}
+
+// Per-detector projection: |F|, polarisation phase lambda, geocentre delay (QuickCBC.c:3724-3750).
+__device__ __forceinline__ void set_projection(PhdRec& c, const double* p, const NetGeom& g) {
   double Ap = (1.0 + p[10] * p[10]) / 2.0, Ac = -p[10];
   double cd = sqrt(1.0 - p[8] * p[8]);
   double sa, ca, sps, cps;
-  sincos(g.GMST - p[7], &sa, &ca);      // Times() angle; F_ant uses alpha - GMST = -(GMST - alpha)
-  sincos(p[9], &sps, &cps);
+  MO::sincos(g.GMST - p[7], &sa, &ca);      // Times() angle; F_ant uses alpha - GMST = -(GMST - alpha)
+  MO::sincos(p[9], &sps, &cps);
   double mp[21], mx[18];
   antenna_basis(cps, sps, cd, p[8], ca, -sa, mp, mx);
   for (int id = 0; id < g.nifo; id++) {
@@ -454,17 +525,25 @@ __device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, 
 #pragma unroll
     for (int k = 0; k < 18; k++) fx += c_antX[l][k] * mx[k];
     c.Fs[id] = sqrt(Ap * Ap * fp * fp + Ac * Ac * fx * fx);
-    double lam = atan2(Ac * fx, Ap * fp);
+    double lam = MO::atan2(Ac * fx, Ap * fp);
     if (lam < 0.0) lam += kTwoPi;
     c.lam[id] = lam;
     double r = c_detpos[l][0] * cd * ca + c_detpos[l][1] * cd * sa + c_detpos[l][2] * p[8];
     c.td[id] = -r / kClight;
   }
-  // bins that carry signal: f > fbegin (QuickCBC.c:3758) and f <= fCut (IMRPhenomD.c:530),
-  // inside the band and inside [1, N/2) (bin N/2 of the template is zero, QuickCBC.c:3754)
-  int lo = g.imin > 1 ? g.imin : 1;
+}
+
+// Bins that carry signal: f > fbegin (QuickCBC.c:3758) and f <= fCut (IMRPhenomD.c:530), inside
+// the band and inside [1, N/2) (bin N/2 of the template is zero, QuickCBC.c:3754).  The two ends
+// are found independently from the band limits.
+__device__ __forceinline__ int band_lo(const NetGeom& g) { return g.imin > 1 ? g.imin : 1; }
+__device__ __forceinline__ int band_hi(const NetGeom& g) {
   int hi = g.imax - 1;
   if (hi > g.N / 2 - 1) hi = g.N / 2 - 1;
+  return hi;
+}
+__device__ __forceinline__ int first_bin_above(const NetGeom& g, double fs) {
+  int lo = band_lo(g), hi = band_hi(g);
   if (fs == fs) {
     double x = fs * g.Tobs;
     if (x >= (double)hi + 1.0) lo = hi + 1;
@@ -477,47 +556,284 @@ __device__ int record_from_params(PhdRec& c, const double* p, const NetGeom& g, 
   } else {
     lo = hi + 1;                                   // NaN start frequency: template is zero
   }
-  {
-    double x = c.fCut * g.Tobs;
-    if (x < (double)hi) {
-      int c1 = x < 0.0 ? -1 : (int)floor(x);
-      for (int k = 0; k < 3 && c1 + 1 <= hi && bin_freq(g, c1 + 1) <= c.fCut; k++) c1++;
-      for (int k = 0; k < 3 && c1 >= 0 && bin_freq(g, c1) > c.fCut; k++) c1--;
-      if (c1 < hi) hi = c1;
-    }
+  return lo;
+}
+__device__ __forceinline__ int last_bin_below(const NetGeom& g, double fCut) {
+  int hi = band_hi(g);
+  double x = fCut * g.Tobs;
+  if (x < (double)hi) {
+    int c1 = x < 0.0 ? -1 : (int)floor(x);
+    for (int k = 0; k < 3 && c1 + 1 <= hi && bin_freq(g, c1 + 1) <= fCut; k++) c1++;
+    for (int k = 0; k < 3 && c1 >= 0 && bin_freq(g, c1) > fCut; k++) c1--;
+    if (c1 < hi) hi = c1;
   }
-  c.i_lo = lo;
-  c.i_hi = hi;
-  c.mdf = c.Msec * g.df;
-  c.mdf_third = cbrt(c.mdf);
-  c.mdf_rthird = 1.0 / c.mdf_third;
-  c.mdf_log = log(c.mdf);
-  {
-    double sixth = sqrt(c.mdf_third), sq = sqrt(c.mdf);
-    c.mdf_m76 = 1.0 / (c.mdf * sixth);
-    c.mdf_34 = sqrt(c.mdf * sq);
-  }
-  return st;
+  return hi;
 }
 
-__global__ void k_setup(const double* __restrict__ params, int B, NetGeom g, QnmTable q, PhdRec* __restrict__ recs,
-                        int* __restrict__ status) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
+// Scales of Mf = (Msec df) i for the per-bin tables of the mixed kernel.
+__device__ __forceinline__ void set_mdf(PhdRec& c, const NetGeom& g) {
+  c.mdf = c.Msec * g.df;
+  c.mdf_third = MO::cbrt(c.mdf);
+  c.mdf_rthird = 1.0 / c.mdf_third;
+  c.mdf_log = MO::log(c.mdf);
+  double sixth = sqrt(c.mdf_third), sq = sqrt(c.mdf);
+  c.mdf_m76 = 1.0 / (c.mdf * sixth);
+  c.mdf_34 = sqrt(c.mdf * sq);
+}
+
+// ---- coefficients of the mixed-precision kernel (MixPoly), from the finished FP64 record
+constexpr double kInv2PiD = 0.15915494309189533577;
+constexpr double kLnPi = 1.1447298858494002;
+
+// smallest bin i >= 0 with Msec f_i >= X (the comparison the FP64 evaluation makes)
+__device__ __forceinline__ int first_bin_mf_at_least(const NetGeom& g, double Msec, double X) {
+  double x = X / Msec * g.Tobs;
+  if (!(x < 2.0e9)) return 2000000000;
+  int i = x <= 0.0 ? 0 : (int)ceil(x);
+  for (int k = 0; k < 3 && i > 0 && Msec * bin_freq(g, i - 1) >= X; k++) i--;
+  for (int k = 0; k < 3 && !(Msec * bin_freq(g, i) >= X); k++) i++;
+  return i;
+}
+
+// inspiral phase but its constant, and the intermediate / ringdown pieces but the parts that
+// need the ringdown join (needs pq, alpha/beta, the intermediate join, t0, the mdf scales)
+__device__ __forceinline__ void mix_phase_main(PhdRec& c) {
+  MixPoly& P = c.mix;
+  const double* q = c.pq;
+  const double K = kInv2PiD, T = c.mdf_third, U = c.mdf_rthird, m = c.mdf, ie = c.inv_eta;
+  const double third = 1.0 / 3.0, lam3 = (c.mdf_log + kLnPi) * third;
+  const double T2 = T * T, U2 = U * U, U3 = U2 * U, U5 = U3 * U2, U9 = U3 * U3 * U3;
+  P.pins.At = K * (q[2] * T + q[3] * T * lam3);
+  P.pins.Att = K * (q[1] * T2);
+  P.pins.AtL = K * (q[3] * T * third);
+  P.pins.AL = K * (q[4] * third);
+  P.pins.Au = K * (q[5] * U);
+  P.pins.Auu = K * (q[6] * U2);
+  P.pins.Au3 = K * (q[7] * U3);
+  P.pins.Au5 = K * (q[8] * U5);
+  P.pins.Ai = K * (ie * q[9] * m - c.t0 * m);
+  P.pins.Ait = K * (ie * q[10] * T * m);
+  P.pins.Aitt = K * (ie * q[11] * T2 * m);
+  P.pins.Aii = K * (ie * q[12] * m * m);
+  P.pint.Bi = K * (c.b1 * m * ie + c.C2Int * m - c.t0 * m);
+  P.pint.Bu9 = K * (-(c.b3 * third) * U9 * ie);
+  P.pint.BL = K * (c.b2 * ie);
+  P.pmrd.Ru3 = K * (-c.al2 * U3 * ie);
+  P.pmrd.Rs = K * ((4.0 / 3.0) * c.al3 * c.mdf_34 * ie);
+  P.pmrd.Rat = K * (c.al4 * ie);
+  const double rdm = 1.0 / c.fDM;
+  P.pmrd.D1 = m * rdm;
+  P.pmrd.D0 = c.al5 * c.fRD * rdm;
+}
+
+// the rest of the phase pieces: constants (phi_pre) and the ringdown slope (C2MRD)
+__device__ __forceinline__ void mix_phase_join(PhdRec& c) {
+  MixPoly& P = c.mix;
+  const double K = kInv2PiD, m = c.mdf, ie = c.inv_eta;
+  const double shift = c.t0 * c.MfRef - c.phi_pre;
+  P.pins.A0 = K * (c.pq[0] + c.pq[4] * ((c.mdf_log + kLnPi) * (1.0 / 3.0)) + shift);
+  P.pint.B0 = K * (c.b2 * ie * c.mdf_log + c.C1Int + shift);
+  P.pmrd.R0 = K * (c.C1MRD + shift);
+  P.pmrd.Ri = K * (c.al1 * m * ie + c.C2MRD * m - c.t0 * m);
+}
+
+// FP32 amplitude coefficients (needs ai, the intermediate Newton form, g1..g3, fDM)
+__device__ __forceinline__ void mix_amp(PhdRec& c) {
+  MixPoly& P = c.mix;
+  const double T = c.mdf_third, m = c.mdf, T2 = T * T, m2 = m * m;
+  float* al = P.ains.al;
+  al[0] = (float)(c.ai[0] * T2);
+  al[1] = (float)(c.ai[1] * m);
+  al[2] = (float)(c.ai[2] * m * T);
+  al[3] = (float)(c.ai[3] * m * T2);
+  al[4] = (float)(c.ai[4] * m2);
+  al[5] = (float)(c.ai[5] * m2 * T);
+  al[6] = (float)(c.ai[6] * m2 * T2);
+  al[7] = (float)(c.ai[7] * m2 * m);
+  P.aint.m = m;
+  P.aint.hx1 = c.hx1;
+  P.aint.h21 = (float)(c.hx2 - c.hx1);
+  P.aint.h31 = (float)(c.hx3 - c.hx1);
+  for (int k = 0; k < 5; k++) P.aint.hc[k] = (float)c.hc[k];
+  const double fg = c.fDM * c.g3;
+  P.amrd.m = m;
+  P.amrd.fRD = c.fRD;
+  P.amrd.g2_over_fg = (float)(c.g2 / fg);
+  P.amrd.fg_g1 = (float)(fg * c.g1);
+  P.amrd.fg2 = (float)(fg * fg);
+}
+
+// first bins of the intermediate / ringdown pieces (needs Msec, fmax, fRD)
+__device__ __forceinline__ void mix_bins(PhdRec& c, const NetGeom& g) {
+  MixPoly& P = c.mix;
+  P.iA = first_bin_mf_at_least(g, c.Msec, kAmpJoin);
+  P.iF = first_bin_mf_at_least(g, c.Msec, c.fmax);
+  P.iP = first_bin_mf_at_least(g, c.Msec, kPhiJoin);
+  P.iM = first_bin_mf_at_least(g, c.Msec, 0.5 * c.fRD);
+}
+
+// ---- cooperative setup: a block of 4 warps builds the records of 32 parameter sets, lane l
+// of every warp working on set l.  Each warp takes a different independent piece of the
+// record in each of four phases, so the dependency chain of one record is about a third of
+// the serial one and the lanes of a warp still run the same code:
+//   phase 1  w0 masses/scales        w1 fbegin head, ts      w2 antenna projection   w3 -
+//   phase 2  w0 fRD, fDM             w1 fits, fbegin, lo     w2 a0, ai[0..4], mdf     w3 TaylorF2, MfRef, hi
+//   phase 3  w0 fmax, intermediate   w1 join int, phi(fRef)  w2 MRD join pieces       w3 t0
+//   phase 4  w0 MRD join, phi_pre,   w1 mixed-kernel phase    w2 mixed-kernel          w3 mixed-kernel
+//            mixed-kernel constants                              amplitude                piece bins
+struct SetupScratch {
   double p[11];
+  PhdMass m;
+  FbeginHead fb;
+  double v2, s[4], pv[8], pvl[8];
+  MrdJoin mj;
+  double phr_raw;
+  int phr_branch, st, lo, hi, live;
+};
+
+constexpr int kSetupSets = 32;
+constexpr int kSetupThreads = 128;
+
+// geometry of set b: one shared NetGeom, or the event table of a multi-event launch
+struct GeomOne {
+  NetGeom g;
+  __device__ bool get(int, NetGeom& out, int& e) const { out = g; e = 0; return true; }
+};
+struct GeomTable {
+  const int* event_of;
+  const EventDesc* events;
+  int n_events;
+  __device__ bool get(int b, NetGeom& out, int& e) const {
+    e = event_of[b];
+    if (e < 0 || e >= n_events || events[e].g.nifo == 0) return false;     // out of range or an empty slot
+    out = events[e].g;
+    return true;
+  }
+};
+
+template <class Geom>
+__device__ __forceinline__ void setup_coop_block(const double* __restrict__ params, int B, const Geom& geo,
+                                                 const QnmTable& q, int tile_bins, PhdRec* __restrict__ recs,
+                                                 int* __restrict__ status, int* __restrict__ ntile) {
+  __shared__ __align__(16) PhdRec s_rec[kSetupSets];
+  __shared__ SetupScratch s_x[kSetupSets];
+  __shared__ NetGeom s_g[kSetupSets];
+  __shared__ int s_ev[kSetupSets];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int b0 = blockIdx.x * kSetupSets, nb = min(kSetupSets, B - b0);
+  const int b = b0 + lane;
+  PhdRec& c = s_rec[lane];
+  SetupScratch& x = s_x[lane];
+  if (w == 0 && lane < nb) {
+    NetGeom g;
+    int e;
+    x.live = geo.get(b, g, e);
+    s_g[lane] = g;
+    s_ev[lane] = e;
 #pragma unroll
-  for (int k = 0; k < 11; k++) p[k] = params[(size_t)b * 11 + k];
-  PhdRec c;
-  int st = record_from_params(c, p, g, q);
-  recs[b] = c;
-  status[b] = st;
+    for (int k = 0; k < 11; k++) x.p[k] = params[(size_t)b * 11 + k];
+  }
+  __syncthreads();
+  const bool on = lane < nb && x.live;
+  // phase 1
+  if (on) {
+    const double* p = x.p;
+    if (w == 0) {
+      SetPhys ph = set_phys(p);
+      x.m = phd_masses(c, ph.m1, ph.m2, p[2], p[3], ph.dist);
+    } else if (w == 1) {
+      x.fb = fbegin_head(p);
+      c.ts = s_g[lane].Tobs - p[5];
+      c.sqT = sqrt(s_g[lane].Tobs);
+    } else if (w == 2) {
+      set_projection(c, p, s_g[lane]);
+    }
+  }
+  __syncthreads();
+  // phase 2
+  if (on) {
+    const NetGeom& g = s_g[lane];
+    if (w == 0) {
+      x.st = x.m.st | phd_ringdown(c, x.m, q);
+    } else if (w == 1) {
+      phd_fits(c, x.m.eta, x.m.chi, x.v2, x.s);
+      c.fs = fbegin_tail(x.fb, x.p[2], x.p[3]);
+      x.lo = first_bin_above(g, c.fs);
+    } else if (w == 2) {
+      phd_amp_prefactors(c, x.m);
+      set_mdf(c, g);
+    } else {
+      phd_taylorf2(c, x.m, x.pv, x.pvl);
+      c.MfRef = c.Msec * kFref;
+      x.hi = last_bin_below(g, c.fCut);
+    }
+  }
+  __syncthreads();
+  // phase 3
+  if (on) {
+    if (w == 0) {
+      c.fmax = phd_fmax(c);
+      phd_amp_int(c, x.v2);
+    } else if (w == 1) {
+      phd_pq_sigma(c, x.s);
+      phd_join_int(c, x.pv, x.pvl, x.s);
+      x.phr_raw = phd_phi_ref_raw(c, x.phr_branch);
+    } else if (w == 2) {
+      x.mj = phd_mrd_pieces(c);
+    } else {
+      c.t0 = dphi_mrd<MO>(c, phd_fmax(c));
+    }
+  }
+  __syncthreads();
+  // phase 4
+  if (on && w != 0) {
+    if (w == 1) mix_phase_main(c);
+    else if (w == 2) mix_amp(c);
+    else mix_bins(c, s_g[lane]);
+  }
+  if (w == 0 && lane < nb) {
+    int st;
+    if (on) {
+      phd_join_mrd(c, x.mj);
+      phd_phi_ref(c, 0.5 * x.p[4], x.phr_raw, x.phr_branch);
+      mix_phase_join(c);
+      st = x.st;
+      c.flags = (st == kStOK) ? kRecValid : 0;
+      c.i_lo = x.lo;
+      c.i_hi = x.hi;
+      c.event = s_ev[lane];
+    } else {
+      st = kStNoEvent;
+      c.flags = 0;
+      c.event = -1;
+      c.i_lo = 1;
+      c.i_hi = 0;
+    }
+    status[b] = st;
+    if (ntile) {
+      int bins = (st == kStOK) ? c.i_hi - c.i_lo + 1 : 0;
+      ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+    }
+  }
+  __syncthreads();
+  // the block's records are contiguous in shared and in global memory
+  const int4* src = reinterpret_cast<const int4*>(s_rec);
+  int4* dst = reinterpret_cast<int4*>(recs + b0);
+  const int words = nb * (int)(sizeof(PhdRec) / 16);
+  for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+}
+
+__global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
+                                                         QnmTable q, PhdRec* __restrict__ recs,
+                                                         int* __restrict__ status) {
+  GeomOne geo{g};
+  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr);
 }
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                   int* d_status, cudaStream_t s) {
   if (B <= 0) return;
-  int th = 32;
-  k_setup<<<(B + th - 1) / th, th, 0, s>>>(d_params, B, g, q, d_recs, d_status);
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -585,24 +901,152 @@ __device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, con
 //    FP32 table R[k] = e^{2 pi i k (blockDim df)(ts - td)} built in FP64;
 //  * amplitude in FP32 without the constant a0 (Msec df)^{-7/6} (applied in FP64 by the finaliser);
 //  * FP32 partial sums over 8 bins, accumulated in FP64.
-struct MixCoef {
-  float ai[8];
-  float hcf[5], h21, h31;            // intermediate: Newton coefficients, node offsets from hx1
-  float fg, g2_over_fg, fg_g1;       // merger-ringdown
-  float inv_fdm;                     // 1/fDM for the ringdown phase's atan
-};
+// ---- mixed-precision tile body (coefficients: MixPoly in the record)
 
-__device__ __forceinline__ int mixed_table_len(int i0, int i1) {
-  return i1 >= i0 ? (i1 - i0 + (int)blockDim.x) / (int)blockDim.x : 0;
+// the three phase pieces in cycles (FP64) and the three amplitude pieces (FP32) at bin xi
+__device__ __forceinline__ double mph_ins(const MixPhIns& q, double xi, double t, double u, double L) {
+  double ph = fma(t, fma(t, q.Att, q.At), q.A0);
+  ph = fma(L, fma(t, q.AtL, q.AL), ph);
+  double pu = fma(u * u, q.Au5, q.Au3);
+  pu = fma(u, pu, q.Auu);
+  pu = fma(u, pu, q.Au);
+  ph = fma(u, pu, ph);
+  double pi = fma(xi, q.Aii, fma(t, fma(t, q.Aitt, q.Ait), q.Ai));
+  return fma(xi, pi, ph);
+}
+__device__ __forceinline__ double mph_int(const MixPhInt& q, double xi, double u, double L) {
+  double u3 = u * u * u;
+  return fma(xi, q.Bi, q.B0) + fma(L, q.BL, (u3 * u3 * u3) * q.Bu9);
+}
+__device__ __forceinline__ double mph_mrd(const MixPhMrd& q, double xi, double u, double s) {
+  double at = (double)atanf((float)fma(xi, q.D1, -q.D0));
+  return fma(xi, q.Ri, q.R0) + fma(u * u * u, q.Ru3, fma(s, q.Rs, q.Rat * at));
+}
+__device__ __forceinline__ float mamp_ins(const MixAmpIns& a, float xf, float tf) {
+  const float* al = a.al;
+  float inner = fmaf(xf, al[7], fmaf(tf, fmaf(tf, al[6], al[5]), al[4]));
+  float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, al[3], al[2]), al[1]));
+  return fmaf(xf, mid, fmaf(tf * tf, al[0], 1.0f));
+}
+__device__ __forceinline__ float mamp_int(const MixAmpInt& a, double xi) {
+  float x = (float)fma(xi, a.m, -a.hx1);
+  return a.hc[0] + x * (a.hc[1] + x * (a.hc[2] + (x - a.h21) * (a.hc[3] + (x - a.h31) * a.hc[4])));
+}
+__device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, double xi) {
+  float dfr = (float)fma(xi, a.m, -a.fRD);
+  return __fdividef(__expf(-dfr * a.g2_over_fg) * a.fg_g1, dfr * dfr + a.fg2);
 }
 
-// Builds the rotation table and FP32 coefficients (shared), then runs the bin loop.  Contains
+// piece of bin i: 0 inspiral, 1 intermediate, 2 merger-ringdown
+__device__ __forceinline__ int amp_piece(const MixPoly& P, int i) { return i < P.iA ? 0 : (i >= P.iF ? 2 : 1); }
+__device__ __forceinline__ int ph_piece(const MixPoly& P, int i) { return i < P.iP ? 0 : (i >= P.iM ? 2 : 1); }
+
+// FP32 partial sums of up to 8 bins per detector: S = sum (wr - i wi) R_k amp e^{-i phi} and
+// sum amp^2 ws; flushed into the FP64 accumulators with the thread's rotation base applied,
+// so that acc[2 id] = sum amp (wr cos x + wi sin x), x = 2 pi f (ts - td) + lambda - phi.
+template <int NIFO>
+struct MixAcc {
+  float sx[NIFO], sy[NIFO], sh[NIFO];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) { sx[id] = 0.f; sy[id] = 0.f; sh[id] = 0.f; }
+  }
+  __device__ __forceinline__ void add(float amp, float cyc, const float4* wv, const float2* rot, int nk) {
+    float sw, cw;
+    __sincosf(6.28318530717958648f * cyc, &sw, &cw);     // |argument| <= pi
+    const float ex = amp * cw, ey = -amp * sw, amp2 = amp * amp;
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) {
+      const float2 R = rot[id * nk];
+      const float qx = fmaf(R.x, ex, -R.y * ey), qy = fmaf(R.x, ey, R.y * ex);
+      sx[id] = fmaf(wv[id].x, qx, fmaf(wv[id].y, qy, sx[id]));
+      sy[id] = fmaf(wv[id].x, qy, fmaf(-wv[id].y, qx, sy[id]));
+      sh[id] = fmaf(amp2, wv[id].z, sh[id]);
+    }
+  }
+  __device__ __forceinline__ void flush(const float2* base, double* acc) {
+#pragma unroll
+    for (int id = 0; id < NIFO; id++) {
+      acc[2 * id] += (double)(base[id].x * sx[id] - base[id].y * sy[id]);
+      acc[2 * id + 1] += (double)sh[id];
+    }
+  }
+};
+
+// Rows [k, k_end) of the thread's bins i = i0 + tid + k bs, all in amplitude piece AP and
+// phase piece PP (-1: decided per bin).  The coefficients of the pieces live in registers.
+template <int NIFO, int AP, int PP>
+__device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot, int nk,
+                                           const float2* base, int k, int k_end, int i, int i1, int bs,
+                                           double* acc) {
+  if (i > i1) return;
+  const int n = min(k_end - k, (i1 - i) / bs + 1);     // rows of this thread in the run
+  MixPhIns qi;
+  MixPhInt qn;
+  MixPhMrd qm;
+  MixAmpIns ai;
+  MixAmpInt an;
+  MixAmpMrd am;
+  if (PP == 0) qi = P.pins;
+  if (PP == 1) qn = P.pint;
+  if (PP == 2) qm = P.pmrd;
+  if (AP == 0) ai = P.ains;
+  if (AP == 1) an = P.aint;
+  if (AP == 2) am = P.amrd;
+  const size_t nh = (size_t)ev.nh;
+  const float2* pr = s_rot + k;
+  const double dbs = (double)bs;
+  const float fbs = (float)bs;
+  double xi = (double)i;
+  float xf = (float)i;
+  int b = i;
+  for (int r = 0; r < n; r += 8) {
+    const int m = min(8, n - r);
+    MixAcc<NIFO> A;
+    A.zero();
+    for (int j = 0; j < m; j++) {
+      const double2 tA = __ldg(ev.tabA + b), tB = __ldg(ev.tabB + b);
+      float4 wv[NIFO];
+#pragma unroll
+      for (int id = 0; id < NIFO; id++) wv[id] = __ldg(ev.w4 + id * nh + b);
+      double ph;
+      float a;
+      if (PP == 0) ph = mph_ins(qi, xi, tA.x, tA.y, tB.x);
+      else if (PP == 1) ph = mph_int(qn, xi, tA.y, tB.x);
+      else if (PP == 2) ph = mph_mrd(qm, xi, tA.y, tB.y);
+      else {
+        const int pp = ph_piece(P, b);
+        ph = pp == 0 ? mph_ins(P.pins, xi, tA.x, tA.y, tB.x)
+                     : (pp == 1 ? mph_int(P.pint, xi, tA.y, tB.x) : mph_mrd(P.pmrd, xi, tA.y, tB.y));
+      }
+      if (AP == 0) a = mamp_ins(ai, xf, (float)tA.x);
+      else if (AP == 1) a = mamp_int(an, xi);
+      else if (AP == 2) a = mamp_mrd(am, xi);
+      else {
+        const int ap = amp_piece(P, b);
+        a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x) : (ap == 1 ? mamp_int(P.aint, xi) : mamp_mrd(P.amrd, xi));
+      }
+      A.add(wv[0].w * a, (float)(ph - rint(ph)), wv, pr, nk);
+      b += bs;
+      pr++;
+      xi += dbs;
+      xf += fbs;
+    }
+    A.flush(base, acc);
+  }
+}
+
+__device__ __forceinline__ int mixed_table_len(int i0, int i1, int bs) {
+  return i1 >= i0 ? (i1 - i0 + bs) / bs : 0;
+}
+
+// Builds the rotation table (shared), then runs the bin loop in runs of rows that share their
+// waveform pieces.  The tile is walked by bs threads (tid = 0..bs-1).  Contains
 // __syncthreads(): every thread of the block must call it.
 template <int NIFO>
 __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
-                                           MixCoef& mc, float2* s_rot, double* acc) {
-  const int bs = blockDim.x, tid = threadIdx.x;
-  const int nk = mixed_table_len(i0, i1);
+                                           int tid, int bs, float2* s_rot, double* acc) {
+  const int nk = mixed_table_len(i0, i1, bs);
   constexpr double kInv2Pi = 0.15915494309189533577;
   const double Dstep = (double)bs * g.df;
   for (int k = tid; k < nk; k += bs) {
@@ -613,17 +1057,6 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
       sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
       s_rot[id * nk + k] = make_float2((float)cv, (float)sv);
     }
-  }
-  if (tid == 0) {
-    for (int k = 0; k < 8; k++) mc.ai[k] = (float)c.ai[k];
-    for (int k = 0; k < 5; k++) mc.hcf[k] = (float)c.hc[k];
-    mc.h21 = (float)(c.hx2 - c.hx1);
-    mc.h31 = (float)(c.hx3 - c.hx1);
-    double fg = c.fDM * c.g3;
-    mc.fg = (float)fg;
-    mc.g2_over_fg = (float)(c.g2 / fg);
-    mc.fg_g1 = (float)(fg * c.g1);
-    mc.inv_fdm = (float)(1.0 / c.fDM);
   }
   __syncthreads();
   int i = i0 + tid;
@@ -637,76 +1070,37 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
     sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
     base[id] = make_float2((float)cv, (float)sv);
   }
-  const size_t nh = (size_t)ev.nh;
-  const float4* w4 = ev.w4;
-  const double Dmf = c.Msec * Dstep;
-  double Mf = c.Msec * f;
-  const double lnpi = 1.1447298858494002;     // log(pi)
+  const MixPoly& P = c.mix;
   int k = 0;
-  while (k < nk && i <= i1) {
-    float sd[NIFO], sh[NIFO];
-#pragma unroll
-    for (int id = 0; id < NIFO; id++) { sd[id] = 0.f; sh[id] = 0.f; }
-    for (int kk = 0; kk < 8 && k < nk && i <= i1; kk++, k++, i += bs, Mf += Dmf) {
-      const double2 tA = __ldg(ev.tabA + i), tB = __ldg(ev.tabB + i);
-      float4 wv[NIFO];
-#pragma unroll
-      for (int id = 0; id < NIFO; id++) wv[id] = __ldg(w4 + (size_t)id * nh + i);
-      double third = tA.x * c.mdf_third;
-      double r = tA.y * c.mdf_rthird;
-      double logMf = tB.x + c.mdf_log;
-      float m76 = wv[0].w;
-      // amplitude (relative to a0 (Msec df)^{-7/6}), FP32
-      float a;
-      if (Mf < kAmpJoin) {
-        float th = (float)third, m = (float)Mf;
-        float t2 = th * th, p43 = m * th, p53 = p43 * th, p2 = m * m;
-        a = 1.0f + t2 * mc.ai[0] + m * mc.ai[1] + p43 * mc.ai[2] + p53 * mc.ai[3] + p2 * mc.ai[4] +
-            (p2 * th) * mc.ai[5] + (p2 * t2) * mc.ai[6] + (m * p2) * mc.ai[7];
-      } else if (Mf >= c.fmax) {
-        float dfr = (float)(Mf - c.fRD);
-        a = __expf(-dfr * mc.g2_over_fg) * mc.fg_g1 / (dfr * dfr + mc.fg * mc.fg);
-      } else {
-        float x = (float)(Mf - c.hx1), x2 = x - mc.h21, x3 = x - mc.h31;
-        a = mc.hcf[0] + x * (mc.hcf[1] + x * (mc.hcf[2] + x2 * (mc.hcf[3] + x3 * mc.hcf[4])));
-      }
-      float amp = m76 * a;
-      // phase, FP64
-      double ph;
-      if (Mf < kPhiJoin) {
-        const double* q = c.pq;
-        double logv = (logMf + lnpi) * (1.0 / 3.0);
-        double r2 = r * r, r3 = r2 * r;
-        ph = q[0] + third * (q[2] + q[1] * third) + (q[3] * third + q[4]) * logv + r * q[5] + r2 * q[6] +
-             r3 * (q[7] + r2 * q[8]) + c.inv_eta * (Mf * (q[9] + third * (q[10] + third * q[11]) + q[12] * Mf));
-      } else if (Mf >= c.fMRDJoin) {
-        double f34 = tB.y * c.mdf_34;
-        double at = (double)atanf((float)(Mf - c.al5 * c.fRD) * mc.inv_fdm);
-        ph = (c.al1 * Mf - c.al2 * (r * r * r) + (4.0 / 3.0) * c.al3 * f34 + c.al4 * at) * c.inv_eta + c.C1MRD +
-             c.C2MRD * Mf;
-      } else {
-        double r3 = r * r * r;
-        ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r3 * r3 * r3 + c.b2 * logMf) * c.inv_eta + c.C1Int + c.C2Int * Mf;
-      }
-      ph -= c.t0 * (Mf - c.MfRef) + c.phi_pre;
-      double phc = ph * kInv2Pi;
-      float u = (float)(phc - rint(phc));
-      float sw, cw;
-      sincospif(2.0f * u, &sw, &cw);
-      float amp2 = amp * amp;
-#pragma unroll
-      for (int id = 0; id < NIFO; id++) {
-        float2 R = s_rot[id * nk + k];
-        float rc = base[id].x * R.x - base[id].y * R.y;
-        float rs = base[id].x * R.y + base[id].y * R.x;
-        float cx = rc * cw + rs * sw;            // e^{ix} = rot * e^{-i phi}
-        float sx = rs * cw - rc * sw;
-        sd[id] = fmaf(amp, fmaf(wv[id].x, cx, wv[id].y * sx), sd[id]);
-        sh[id] = fmaf(amp2, wv[id].z, sh[id]);
+  while (k < nk) {                 // block-uniform: depends on k only
+    const int r0 = i0 + k * bs, r1 = min(r0 + bs - 1, i1);
+    if (r0 > i1) break;
+    const int a0 = amp_piece(P, r0), p0 = ph_piece(P, r0);
+    int k_end;
+    if (a0 != amp_piece(P, r1) || p0 != ph_piece(P, r1)) {
+      k_end = k + 1;
+      mixed_rows<NIFO, -1, -1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc);
+    } else {
+      int nxt = i1 + 1;              // the pieces can only change at a threshold
+      if (P.iA > r0 && P.iA < nxt) nxt = P.iA;
+      if (P.iF > r0 && P.iF < nxt) nxt = P.iF;
+      if (P.iP > r0 && P.iP < nxt) nxt = P.iP;
+      if (P.iM > r0 && P.iM < nxt) nxt = P.iM;
+      k_end = nxt > i1 ? nk : max(k + 1, (nxt - i0 - bs) / bs + 1);
+      switch (a0 * 3 + p0) {
+        case 0: mixed_rows<NIFO, 0, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 1: mixed_rows<NIFO, 0, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 2: mixed_rows<NIFO, 0, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 3: mixed_rows<NIFO, 1, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 4: mixed_rows<NIFO, 1, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 5: mixed_rows<NIFO, 1, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 6: mixed_rows<NIFO, 2, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 7: mixed_rows<NIFO, 2, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        default: mixed_rows<NIFO, 2, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
       }
     }
-#pragma unroll
-    for (int id = 0; id < NIFO; id++) { acc[2 * id] += (double)sd[id]; acc[2 * id + 1] += (double)sh[id]; }
+    k = k_end;
+    i = i0 + tid + k * bs;
   }
 }
 
@@ -753,17 +1147,38 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
 }
 
 #ifndef QCBC_MIXED_MINBLOCKS
-#define QCBC_MIXED_MINBLOCKS 4
+#define QCBC_MIXED_MINBLOCKS 2
 #endif
+// Sums over the threads of each group of gs threads (gs a multiple of 32) in a fixed order;
+// the first thread of each group holds its group's sums.
+template <int NV>
+__device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][NV] */, int gs) {
+#pragma unroll
+  for (int k = 0; k < NV; k++)
+    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < NV; k++) smem[w * NV + k] = v[k];
+  __syncthreads();
+  if (threadIdx.x % gs == 0) {
+    const int w0 = w, nw = gs >> 5;
+    for (int k = 0; k < NV; k++) {
+      double x = smem[w0 * NV + k];
+      for (int j = 1; j < nw; j++) x += smem[(w0 + j) * NV + k];
+      v[k] = x;
+    }
+  }
+}
+
+// Mixed-precision full lnL over one tile of bins of one parameter set.
 template <int NIFO>
 __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
                                                                                EventData ev, int tiles,
                                                                                double* __restrict__ partials) {
   __shared__ PhdRec rec;
-  __shared__ MixCoef mc;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ float2 s_rot[];   // [NIFO][nk]
-  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  const int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -771,8 +1186,8 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   double acc[2 * NIFO];
 #pragma unroll
   for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
-  tile_mixed<NIFO>(rec, g, ev, i0, i1, mc, s_rot, acc);
-  block_sum<2 * NIFO>(acc, red);
+  tile_mixed<NIFO>(rec, g, ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
+  group_sum<2 * NIFO>(acc, red, blockDim.x);
   if (threadIdx.x == 0) {
     double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
 #pragma unroll
@@ -792,8 +1207,6 @@ static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const Event
                            double* part, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_lnl_full_mixed<NIFO>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
 }
 
@@ -874,40 +1287,21 @@ void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_
 }
 
 // ---------------------------------------------------------------- multi-event launches
-__global__ void k_setup_multi(const double* __restrict__ params, const int* __restrict__ event_of, int B,
-                              const EventDesc* __restrict__ events, int n_events, QnmTable q, int tile_bins,
-                              PhdRec* __restrict__ recs, int* __restrict__ status, int* __restrict__ ntile) {
-  int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B) return;
-  int e = event_of[b];
-  PhdRec c;
-  if (e < 0 || e >= n_events || events[e].g.nifo == 0) {     // out of range or an empty slot
-    c.flags = 0;
-    c.event = -1;
-    c.i_lo = 1;
-    c.i_hi = 0;
-    recs[b] = c;
-    status[b] = kStNoEvent;
-    ntile[b] = 0;
-    return;
-  }
-  double p[11];
-#pragma unroll
-  for (int k = 0; k < 11; k++) p[k] = params[(size_t)b * 11 + k];
-  NetGeom g = events[e].g;
-  int st = record_from_params(c, p, g, q);
-  c.event = e;
-  recs[b] = c;
-  status[b] = st;
-  int bins = (st == kStOK) ? c.i_hi - c.i_lo + 1 : 0;
-  ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+__global__ void __launch_bounds__(kSetupThreads) k_setup_multi(const double* __restrict__ params,
+                                                               const int* __restrict__ event_of, int B,
+                                                               const EventDesc* __restrict__ events, int n_events,
+                                                               QnmTable q, int tile_bins, PhdRec* __restrict__ recs,
+                                                               int* __restrict__ status, int* __restrict__ ntile) {
+  GeomTable geo{event_of, events, n_events};
+  setup_coop_block(params, B, geo, q, tile_bins, recs, status, ntile);
 }
 
 void launch_setup_multi(const double* d_params, const int* d_event_of, int B, const EventDesc* d_events, int n_events,
                         const QnmTable& q, int tile_bins, PhdRec* d_recs, int* d_status, int* d_ntile, cudaStream_t s) {
   if (B <= 0) return;
-  k_setup_multi<<<(B + 31) / 32, 32, 0, s>>>(d_params, d_event_of, B, d_events, n_events, q, tile_bins, d_recs,
-                                             d_status, d_ntile);
+  k_setup_multi<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, d_event_of, B, d_events,
+                                                                           n_events, q, tile_bins, d_recs, d_status,
+                                                                           d_ntile);
 }
 
 // One block: exclusive scan of ntile into off[0..B], then expansion into items (bounded by items_cap).
@@ -952,18 +1346,22 @@ void launch_scan_expand(const int* d_ntile, int B, int* d_off, int* d_items, int
   k_scan_expand<<<1, 1024, 0, s>>>(d_ntile, B, d_off, d_items, items_cap);
 }
 
+#ifndef QCBC_MULTI_MINBLOCKS
+#define QCBC_MULTI_MINBLOCKS 2
+#endif
+// The FP64 body is light on registers and wants occupancy; the mixed body keeps its piece
+// coefficients in registers.
 template <int PREC>
-__global__ void __launch_bounds__(256, 4) k_lnl_multi(const PhdRec* __restrict__ recs,
+__global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS) k_lnl_multi(const PhdRec* __restrict__ recs,
                                                       const EventDesc* __restrict__ events,
                                                       const int* __restrict__ off, const int* __restrict__ items,
                                                       int B, int tile_bins, int items_cap, int* __restrict__ counter,
                                                       double* __restrict__ partials) {
   __shared__ PhdRec rec;
-  __shared__ MixCoef mc;
   __shared__ EventDesc evd;
   __shared__ int s_item, s_b;
   __shared__ double red[32 * 2 * kMaxIfo];
-  extern __shared__ float2 s_rot[];   // [3][nk]
+  extern __shared__ float2 s_rot[];   // mixed: rotation table [3][nk]
   int total = off[B];
   if (total > items_cap) total = items_cap;
   for (;;) {
@@ -991,9 +1389,9 @@ __global__ void __launch_bounds__(256, 4) k_lnl_multi(const PhdRec* __restrict__
       else if (nifo == 2) tile_fp64<2>(rec, evd.g, evd.ev, i0, i1, acc);
       else tile_fp64<3>(rec, evd.g, evd.ev, i0, i1, acc);
     } else {
-      if (nifo == 1) tile_mixed<1>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
-      else if (nifo == 2) tile_mixed<2>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
-      else tile_mixed<3>(rec, evd.g, evd.ev, i0, i1, mc, s_rot, acc);
+      if (nifo == 1) tile_mixed<1>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
+      else if (nifo == 2) tile_mixed<2>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
+      else tile_mixed<3>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
     }
     block_sum<2 * kMaxIfo>(acc, red);
     if (threadIdx.x == 0) {
@@ -1005,14 +1403,15 @@ __global__ void __launch_bounds__(256, 4) k_lnl_multi(const PhdRec* __restrict__
   }
 }
 
-static size_t multi_smem(int threads, int tile_bins) {
+static size_t multi_smem(Precision prec, int threads, int tile_bins) {
+  if (prec == kFP64) return 0;
   int nk = (tile_bins + threads - 1) / threads + 1;
   return (size_t)nk * kMaxIfo * sizeof(float2);
 }
 
 int multi_blocks_per_sm(Precision prec, int threads, int tile_bins) {
   int n = 0;
-  size_t smem = multi_smem(threads, tile_bins);
+  size_t smem = multi_smem(prec, threads, tile_bins);
   if (prec == kFP64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lnl_multi<kFP64>, threads, smem);
   else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_lnl_multi<kMixed>, threads, smem);
   return n > 0 ? n : 1;
@@ -1022,18 +1421,35 @@ void launch_lnl_multi(const PhdRec* d_recs, const EventDesc* d_events, const int
                       int tile_bins, int items_cap, Precision prec, int threads, int blocks, int* d_counter,
                       double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  size_t smem = multi_smem(threads, tile_bins);
+  size_t smem = multi_smem(prec, threads, tile_bins);
   const int cap = items_cap;
   if (prec == kFP64) {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_multi<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_lnl_multi<kFP64><<<blocks, threads, smem, s>>>(d_recs, d_events, d_off, d_items, B, tile_bins, cap, d_counter,
                                                      d_partials);
   } else {
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_lnl_multi<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_lnl_multi<kMixed><<<blocks, threads, smem, s>>>(d_recs, d_events, d_off, d_items, B, tile_bins, cap, d_counter,
                                                       d_partials);
   }
 }
+
+// Lets the kernels whose rotation tables live in dynamic shared memory use up to the device's
+// opt-in limit (long tiles).  Set once per device at initialisation, outside any stream capture.
+void allow_dynamic_smem() {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  auto allow = [&](const void* f) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, f) == cudaSuccess)
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+  };
+  allow((const void*)k_lnl_full_mixed<1>);
+  allow((const void*)k_lnl_full_mixed<2>);
+  allow((const void*)k_lnl_full_mixed<3>);
+  allow((const void*)k_lnl_multi<kFP64>);
+  allow((const void*)k_lnl_multi<kMixed>);
+}
+
 
 __global__ void k_finalize_multi(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
                                  const int* __restrict__ status, const int* __restrict__ off,
@@ -1241,16 +1657,6 @@ void launch_amp_phase(const double* d_freq, int n, double phi0, double fRef, dou
   k_amp_phase<<<blocks, 256, 0, s>>>(d_rec, d_freq, n, d_amp, d_phase);
 }
 
-__global__ void k_setup_one(const double* __restrict__ params, NetGeom g, QnmTable q, PhdRec* rec, int* status) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double p[11];
-    for (int k = 0; k < 11; k++) p[k] = params[k];
-    PhdRec c;
-    status[0] = record_from_params(c, p, g, q);
-    *rec = c;
-  }
-}
-
 // fulltemplates: h[id][i] = A cos x, h[id][N-i] = A sin x for f > fbegin, else 0 (QuickCBC.c:3752-3772)
 __global__ void k_fulltemplates(const PhdRec* __restrict__ recp, NetGeom g, const double* __restrict__ freq,
                                 double* __restrict__ h) {
@@ -1283,7 +1689,7 @@ __global__ void k_fulltemplates(const PhdRec* __restrict__ recp, NetGeom g, cons
 
 void launch_fulltemplates(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq,
                           PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s) {
-  k_setup_one<<<1, 32, 0, s>>>(d_params, g, q, d_rec, d_status);
+  launch_setup(d_params, 1, g, q, d_rec, d_status, s);
   int blocks = (g.N / 2 + 256) / 256;
   if (blocks > 2368) blocks = 2368;
   k_fulltemplates<<<blocks, 256, 0, s>>>(d_rec, g, d_freq, d_h);
@@ -1311,7 +1717,7 @@ __global__ void k_fullphaseamp(const PhdRec* __restrict__ recp, NetGeom g, const
 
 void launch_fullphaseamp(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq, int n,
                          PhdRec* d_rec, int* d_status, double* d_amp, double* d_phase, cudaStream_t s) {
-  k_setup_one<<<1, 32, 0, s>>>(d_params, g, q, d_rec, d_status);
+  launch_setup(d_params, 1, g, q, d_rec, d_status, s);
   int blocks = (n + 255) / 256;
   if (blocks > 2368) blocks = 2368;
   if (blocks < 1) blocks = 1;

@@ -108,5 +108,6 @@ void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const
 int multi_blocks_per_sm(Precision prec, int threads, int tile_bins);
 
 void upload_tables();    // constant-memory tables; call once per device
+void allow_dynamic_smem();   // dynamic shared-memory limit of the mixed kernels; once per device
 
 }  // namespace qcbc
