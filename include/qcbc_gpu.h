@@ -78,6 +78,12 @@ int qcbc_lnl_full(qcbc_event* ev, const double* params, int B, double* lnl, doub
 /* Same with device pointers on a caller stream (cudaStream_t passed as void*, NULL = the thread's stream). */
 int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho, int precision,
                       void* stream);
+/* Batched log_likelihood_intrinsic (QuickCBC.c:4093-4140): params [B][7 + 3 (nifo - 1)] in the
+ * intrinsic layout of templates (QuickCBC.c:3527-3598: Mc, Mt, chi1, chi2, phic, tc, DL, then
+ * phase offset, time offset and amplitude ratio of each detector after the first; phi0 =
+ * params[4]).  lnL = sum over detectors of (HD - HH/2), set to 0 when nifo > 1 and fewer than
+ * two detectors have SNR^2 = 2 (HD - HH/2) > 25.  snrsq [B][nifo] may be NULL. */
+int qcbc_lnl_intrinsic(qcbc_event* ev, const double* params, int B, double* lnl, double* snrsq, int precision);
 
 /* ---- many events in one launch ---- */
 /* A batch groups open events (same device) so that parameter sets of different
@@ -121,6 +127,13 @@ int qcbc_het_export(const qcbc_event* ev, int* fgrid, double* freq, double* amp,
                     double* SL, double* lc, double* ls, double* aa, double* rc, double* rs, double* logLb);
 int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double* lnl, int precision);
 int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, int precision, void* stream);
+/* Batched het_diff (QuickCBC.c:4966-5051): out[b] = heterodyned squared distance between the
+ * templates of params_a[b] and params_b[b] ([B][11] each), FP64. */
+int qcbc_het_diff(qcbc_event* ev, const double* params_a, const double* params_b, int B, double* out);
+/* Batched Fisher_Het (QuickCBC.c:5446-5617): fish [B][11][11] for params [B][11], from central
+ * differences with step 1e-5 of all 23 waveforms of each set computed in one launch.  A set with
+ * |chi1| or |chi2| >= 0.9999 gets 1e4 on the diagonal and zeros elsewhere, as in the reference. */
+int qcbc_het_fisher(qcbc_event* ev, const double* params, int B, double* fish);
 
 /* ---- allocation-free form (no counterpart in the reference) ---- */
 /* Some callers cannot allocate device memory at call time: code that runs inside

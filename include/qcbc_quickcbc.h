@@ -115,7 +115,20 @@ int IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVector* freq, 
 /* replaces Utilities.c:716 */
 double fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N);
 
-/* The same seven functions under prefixed names, for a forwarding object that
+/* Secondary consumers of the waveform (declared in QuickCBC.h:95-151). */
+/* replaces QuickCBC.c:4093; params in the intrinsic layout (7 + 3 (Nifo - 1) entries) */
+double log_likelihood_intrinsic(struct Net* net, double** D, double* params, RealVector* freq, double** SN, int N,
+                                double Tobs);
+/* replaces QuickCBC.c:3527; params in the intrinsic layout */
+void templates(struct Net* net, double** hwave, RealVector* freq, double* params, int N);
+/* replaces QuickCBC.c:3395; writes Af[i], Pf[i] for i in [1, N/2) */
+void AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N);
+/* replaces QuickCBC.c:4966 (tables as for log_likelihood_het) */
+double het_diff(struct Net* net, struct Het* het, double* params, double* dparams);
+/* replaces QuickCBC.c:5446; fish is the reference's NP x NP row-pointer matrix */
+void Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs);
+
+/* The same functions under prefixed names, for a forwarding object that
  * gives an unchanged QuickCBC build strong definitions. */
 double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
                                     double* rho, int N, double Tobs);
@@ -128,6 +141,12 @@ int qcbc_gpu_IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22, RealVecto
                                              const double fRef_in, const double m1_SI, const double m2_SI,
                                              const double chi1, const double chi2, const double distance);
 double qcbc_gpu_fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N);
+double qcbc_gpu_log_likelihood_intrinsic(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
+                                         int N, double Tobs);
+void qcbc_gpu_templates(struct Net* net, double** hwave, RealVector* freq, double* params, int N);
+void qcbc_gpu_AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N);
+double qcbc_gpu_het_diff(struct Net* net, struct Het* het, double* params, double* dparams);
+void qcbc_gpu_Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs);
 
 #ifdef __cplusplus
 }

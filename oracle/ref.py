@@ -68,6 +68,13 @@ def lib():
         L.ref_lnl_test.restype = C.c_double
         L.ref_lnl_test.argtypes = [vp, vp, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double]
         L.ref_het_free.argtypes = [vp, vp]
+        L.ref_templates.argtypes = [vp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.ref_lnl_intrinsic.restype = C.c_double
+        L.ref_lnl_intrinsic.argtypes = [vp, _dp, _dp, _dp, _dp, C.c_int, C.c_int, C.c_double]
+        L.ref_AmpPhase.argtypes = [_dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.ref_het_diff.restype = C.c_double
+        L.ref_het_diff.argtypes = [vp, vp, _dp, _dp]
+        L.ref_Fisher_Het.argtypes = [vp, vp, _dp, _dp, C.c_double]
         _lib = L
     return _lib
 
@@ -143,6 +150,28 @@ def lnl_full(net: RefNet, D, params, freq, SN, N, Tobs):
     return L, rho[: net.nifo]
 
 
+def templates(net: RefNet, freq, params, N):
+    """templates (QuickCBC.c:3527): intrinsic parameters, 7 + 3 (Nifo - 1) entries."""
+    h = np.zeros((net.nifo, N))
+    f = _f64(freq)
+    lib().ref_templates(net.ptr, h, f, len(f), _f64(params).copy(), N)
+    return h
+
+
+def lnl_intrinsic(net: RefNet, D, params, freq, SN, N, Tobs):
+    SN = _f64(SN)
+    return lib().ref_lnl_intrinsic(net.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN, SN.shape[1], N, Tobs)
+
+
+def AmpPhase(freq, params, N):
+    """AmpPhase (QuickCBC.c:3395): (Af, Pf) over N/2 bins, entry 0 left at zero."""
+    Af = np.zeros(N // 2)
+    Pf = np.zeros(N // 2)
+    f = _f64(freq)
+    lib().ref_AmpPhase(Af, Pf, f, len(f), _f64(params).copy(), N)
+    return Af, Pf
+
+
 def lnl_full_batch(net: RefNet, D, params, freq, SN, N, Tobs, nthreads=0):
     P = _f64(params)
     out = np.zeros(P.shape[0])
@@ -211,6 +240,14 @@ class RefHet:
         out = np.zeros(P.shape[0])
         secs = lib().ref_lnl_het_batch(self.net.ptr, self.ptr, P, P.shape[0], Tobs, out, nthreads)
         return out, secs
+
+    def het_diff(self, params, dparams):
+        return lib().ref_het_diff(self.net.ptr, self.ptr, _f64(params).copy(), _f64(dparams).copy())
+
+    def fisher(self, params, Tobs):
+        F = np.zeros((11, 11))
+        lib().ref_Fisher_Het(self.net.ptr, self.ptr, F, _f64(params).copy(), Tobs)
+        return F
 
     def lnl_test(self, D, params, freq, SN, N, Tobs):
         SN = _f64(SN)

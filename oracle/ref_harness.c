@@ -15,6 +15,9 @@
  *   IMRPhenomDGenerateh22FDAmpPhase  IMRPhenomD.c:186
  *   F_ant / Times        Utilities.c:995 / 1078     fbegin Utilities.c:587
  *   fourier_nwip         Utilities.c:716
+ *   templates            QuickCBC.c:3527     AmpPhase       QuickCBC.c:3395
+ *   log_likelihood_intrinsic  QuickCBC.c:4093
+ *   het_diff             QuickCBC.c:4966     Fisher_Het     QuickCBC.c:5446
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -137,6 +140,31 @@ double ref_lnl_full_batch(struct Net *net, double *Dflat, const double *params, 
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+/* intrinsic parametrisation: params of length NX + 3 (Nifo - 1) */
+void ref_templates(struct Net *net, double *hflat, const double *freq, int nfreq, double *params, int N) {
+  double **h = rows(hflat, net->Nifo, N);
+  RealVector *fv = wrap_freq(freq, nfreq);
+  templates(net, h, fv, params, N);
+  free(fv); free(h);
+}
+
+double ref_lnl_intrinsic(struct Net *net, double *Dflat, double *params, const double *freq, double *SNflat,
+                         int sn_stride, int N, double Tobs) {
+  double **D = rows(Dflat, net->Nifo, N);
+  double **S = rows(SNflat, net->Nifo, sn_stride);
+  RealVector *fv = wrap_freq(freq, N / 2);
+  double L = log_likelihood_intrinsic(net, D, params, fv, S, N, Tobs);
+  free(fv); free(D); free(S);
+  return L;
+}
+
+/* Af, Pf: N/2 entries; entry 0 is left as passed in */
+void ref_AmpPhase(double *Af, double *Pf, const double *freq, int nfreq, double *params, int N) {
+  RealVector *fv = wrap_freq(freq, nfreq);
+  AmpPhase(Af, Pf, fv, params, N);
+  free(fv);
+}
+
 /* ---------------- heterodyne ---------------- */
 struct Het *ref_het_new(void) { return (struct Het *)calloc(1, sizeof(struct Het)); }
 
@@ -226,6 +254,17 @@ double ref_lnl_test(struct Net *net, struct Het *het, double *Dflat, double *par
   double L = log_likelihood_test(net, het, D, params, fv, S, N, Tobs);
   free(fv); free(D); free(S);
   return L;
+}
+
+double ref_het_diff(struct Net *net, struct Het *het, double *params, double *dparams) {
+  return het_diff(net, het, params, dparams);
+}
+
+/* fish: 11 x 11 (NP, ConstCBC.h:68) row-major */
+void ref_Fisher_Het(struct Net *net, struct Het *het, double *fishflat, double *params, double Tobs) {
+  double **F = rows(fishflat, 11, 11);
+  Fisher_Het(net, het, F, params, Tobs);
+  free(F);
 }
 
 void ref_het_free(struct Net *net, struct Het *het) {

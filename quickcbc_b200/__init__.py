@@ -7,9 +7,10 @@ C ABI (include/qcbc_gpu.h, include/qcbc_quickcbc.h).  See ``engine`` for the
 host interface and ``synth`` for the seeded synthetic workloads.
 """
 from ._lib import FP64, MIXED, QcbcError, launch_count  # noqa: F401
-from .engine import (Event, Batch, DeviceBuffer, amp_phase, fourier_nwip, fullphaseamp, fulltemplates,  # noqa: F401
-                     log_likelihood_full, set_band, LegacyHet, time_lnl_full, time_lnl_het)
+from .engine import (Event, Batch, DeviceBuffer, amp_phase, ampphase, fourier_nwip, fullphaseamp,  # noqa: F401
+                     fulltemplates, templates, log_likelihood_full, log_likelihood_intrinsic, set_band, LegacyHet,
+                     time_lnl_full, time_lnl_het)
 
-__all__ = ["FP64", "MIXED", "QcbcError", "Event", "Batch", "DeviceBuffer", "amp_phase", "fourier_nwip", "fullphaseamp",
-           "fulltemplates", "log_likelihood_full", "set_band", "LegacyHet", "time_lnl_full", "time_lnl_het",
-           "launch_count"]
+__all__ = ["FP64", "MIXED", "QcbcError", "Event", "Batch", "DeviceBuffer", "amp_phase", "ampphase", "fourier_nwip",
+           "fullphaseamp", "fulltemplates", "templates", "log_likelihood_full", "log_likelihood_intrinsic", "set_band",
+           "LegacyHet", "time_lnl_full", "time_lnl_het", "launch_count"]

@@ -95,6 +95,9 @@ def lib():
         L.qcbc_het_sizes.argtypes = [vp, pi, pi, pi, pi, pi]
         L.qcbc_het_export.argtypes = [vp, pi] + [_PD] * 11
         L.qcbc_lnl_het.argtypes = [vp, _PD, i, _PD, i]
+        L.qcbc_lnl_intrinsic.argtypes = [vp, _PD, i, _PD, _PD, i]
+        L.qcbc_het_diff.argtypes = [vp, _PD, _PD, i, _PD]
+        L.qcbc_het_fisher.argtypes = [vp, _PD, i, _PD]
         L.qcbc_lnl_het_dev.argtypes = [vp, vp, i, vp, i, vp]
         L.qcbc_set_full_launch.argtypes = [vp, i, i]
         L.qcbc_get_full_launch.argtypes = [vp, i, i, pi, pi]
@@ -123,6 +126,16 @@ def lib():
                                                        C.POINTER(RealVector)] + [d] * 7
         L.fourier_nwip.restype = d
         L.fourier_nwip.argtypes = [_PD, _PD, _PD, i, i, i]
+        L.log_likelihood_intrinsic.restype = d
+        L.log_likelihood_intrinsic.argtypes = [C.POINTER(Net), _PPD, _PD, C.POINTER(RealVector), _PPD, i, d]
+        L.templates.restype = None
+        L.templates.argtypes = [C.POINTER(Net), _PPD, C.POINTER(RealVector), _PD, i]
+        L.AmpPhase.restype = None
+        L.AmpPhase.argtypes = [_PD, _PD, C.POINTER(RealVector), _PD, i]
+        L.het_diff.restype = d
+        L.het_diff.argtypes = [C.POINTER(Net), C.POINTER(Het), _PD, _PD]
+        L.Fisher_Het.restype = None
+        L.Fisher_Het.argtypes = [C.POINTER(Net), C.POINTER(Het), _PPD, _PD, d]
         _lib = L
     return _lib
 

@@ -495,7 +495,7 @@ extern "C" int qcbc_get_full_launch(qcbc_event* ev, int B, int precision, int* t
 // ------------------------------------------------------------------ full likelihood
 static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
                         int prec, cudaStream_t s, const NetGeom& g, cudaEvent_t k0 = nullptr,
-                        cudaEvent_t k1 = nullptr) {
+                        cudaEvent_t k1 = nullptr, int model = kModelFull) {
   FullLaunch L = choose_launch(ev, B, prec);
   int rc;
   if ((rc = grow(w->d_recs, w->c_recs, (size_t)B))) return rc;
@@ -503,33 +503,36 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   if ((rc = grow(w->d_part, w->c_part, (size_t)B * L.tiles * 2 * kMaxIfo))) return rc;
   DeviceState& ds = g_dev[current_device()];
   EventData ed = event_data(ev);
-  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s);
+  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
   if (k0) cudaEventRecord(k0, s);
   launch_lnl_full(w->d_recs, B, g, ed, prec == QCBC_MIXED ? kMixed : kFP64, L, w->d_part, s);
   if (k1) cudaEventRecord(k1, s);
   launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, prec == QCBC_MIXED ? kMixed : kFP64,
-                       d_lnl, d_rho, s);
+                       d_lnl, d_rho, s, model);
   tls_launches += 3;
   CU(cudaGetLastError());
   return QCBC_OK;
 }
 
 static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int prec,
-                    const NetGeom& g) {
+                    const NetGeom& g, int model = kModelFull) {
   Workspace* w;
   int rc = workspace(w);
   if (rc) return rc;
-  if ((rc = grow(w->d_params, w->c_params, (size_t)B * 11))) return rc;
+  const size_t ps = (size_t)param_stride(model, g.nifo);
+  if ((rc = grow(w->d_params, w->c_params, (size_t)B * ps))) return rc;
   if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
   if ((rc = grow(w->d_rho, w->c_rho, (size_t)B * kMaxIfo))) return rc;
-  if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * 11))) return rc;
+  if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * ps))) return rc;
   if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
   if ((rc = grow_host(w->h_rho, w->ch_rho, (size_t)B * kMaxIfo))) return rc;
   if ((rc = grow_host(w->h_status, w->ch_status, (size_t)B))) return rc;
-  memcpy(w->h_params, params, sizeof(double) * 11 * (size_t)B);
+  memcpy(w->h_params, params, sizeof(double) * ps * (size_t)B);
   cudaStream_t s = w->stream;
-  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyHostToDevice, s));
-  if ((rc = enqueue_full(w, ev, w->d_params, B, w->d_lnl, rho ? w->d_rho : nullptr, prec, s, g))) return rc;
+  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * ps * (size_t)B, cudaMemcpyHostToDevice, s));
+  if ((rc = enqueue_full(w, ev, w->d_params, B, w->d_lnl, rho ? w->d_rho : nullptr, prec, s, g, nullptr, nullptr,
+                         model)))
+    return rc;
   CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
   if (rho) CU(cudaMemcpyAsync(w->h_rho, w->d_rho, sizeof(double) * B * g.nifo, cudaMemcpyDeviceToHost, s));
   CU(cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
@@ -560,6 +563,15 @@ extern "C" int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, 
   if (rc) return rc;
   cudaStream_t s = stream ? (cudaStream_t)stream : w->stream;
   return enqueue_full(w, ev, d_params, B, d_lnl, d_rho, precision, s, ev->g);
+}
+
+extern "C" int qcbc_lnl_intrinsic(qcbc_event* ev, const double* params, int B, double* lnl, double* snrsq,
+                                  int precision) {
+  if (!ev || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (B < 0) return fail(QCBC_EINVAL, "B < 0");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B == 0) return QCBC_OK;
+  return run_full(ev, params, B, lnl, snrsq, precision, ev->g, kModelIntrinsic);
 }
 
 // ------------------------------------------------------------------ heterodyne
@@ -813,6 +825,96 @@ extern "C" int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, d
   if (rc) return rc;
   cudaStream_t s = stream ? (cudaStream_t)stream : w->stream;
   return enqueue_het(w, ev, d_params, B, d_lnl, precision, s, ev->g);
+}
+
+// Waves of the sets in d_params (FP64 fullphaseamp on the heterodyne grid) into w->d_a:
+// amplitude [nset][nifo][M] followed by phase [nset][nifo][M].
+static int het_waves(Workspace* w, qcbc_event* ev, const double* d_params, int nset, cudaStream_t s, double** amp,
+                     double** ph) {
+  const size_t per = (size_t)nset * ev->g.nifo * ev->het.M;
+  int rc;
+  if ((rc = grow(w->d_recs, w->c_recs, (size_t)nset))) return rc;
+  if ((rc = grow(w->d_status, w->c_status, (size_t)nset))) return rc;
+  if ((rc = grow(w->d_a, w->c_a, 2 * per))) return rc;
+  DeviceState& ds = g_dev[current_device()];
+  launch_setup(d_params, nset, ev->g, ds.qnm, w->d_recs, w->d_status, s);
+  launch_het_waves(w->d_recs, nset, ev->g, het_data(ev), w->d_a, w->d_a + per, s);
+  tls_launches += 2;
+  *amp = w->d_a;
+  *ph = w->d_a + per;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_diff(qcbc_event* ev, const double* params_a, const double* params_b, int B, double* out) {
+  if (!ev || !params_a || !params_b || !out) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->het.buf) return fail(QCBC_EINVAL, "event has no heterodyne tables");
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_params, w->c_params, (size_t)2 * B * 11))) return rc;
+  if ((rc = grow_host(w->h_params, w->ch_params, (size_t)2 * B * 11))) return rc;
+  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
+  if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
+  for (int p = 0; p < B; p++) {
+    memcpy(w->h_params + (size_t)(2 * p) * 11, params_a + (size_t)p * 11, 11 * sizeof(double));
+    memcpy(w->h_params + (size_t)(2 * p + 1) * 11, params_b + (size_t)p * 11, 11 * sizeof(double));
+  }
+  cudaStream_t s = w->stream;
+  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * 22 * (size_t)B, cudaMemcpyHostToDevice, s));
+  double *amp, *ph;
+  if ((rc = het_waves(w, ev, w->d_params, 2 * B, s, &amp, &ph))) return rc;
+  launch_het_diff(amp, ph, B, ev->g, het_data(ev), w->d_lnl, s);
+  tls_launches += 1;
+  CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  memcpy(out, w->h_lnl, sizeof(double) * B);
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_fisher(qcbc_event* ev, const double* params, int B, double* fish) {
+  constexpr int NP = 11, NSET = 2 * NP + 1;
+  constexpr double eps = 1.0e-5;                 // QuickCBC.c:5489
+  if (!ev || !params || !fish) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->het.buf) return fail(QCBC_EINVAL, "event has no heterodyne tables");
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  const size_t nset = (size_t)B * NSET;
+  if ((rc = grow(w->d_params, w->c_params, nset * NP))) return rc;
+  if ((rc = grow_host(w->h_params, w->ch_params, nset * NP))) return rc;
+  if ((rc = grow(w->d_b, w->c_b, (size_t)B * NP * NP))) return rc;
+  if ((rc = grow_host(w->h_b, w->ch_b, (size_t)B * NP * NP))) return rc;
+  for (int b = 0; b < B; b++) {
+    double* q = w->h_params + (size_t)b * NSET * NP;
+    for (int k = 0; k < NSET; k++) memcpy(q + (size_t)k * NP, params + (size_t)b * NP, NP * sizeof(double));
+    for (int i = 0; i < NP; i++) {
+      q[(size_t)(1 + 2 * i) * NP + i] += eps;
+      q[(size_t)(2 + 2 * i) * NP + i] -= eps;
+    }
+  }
+  cudaStream_t s = w->stream;
+  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * nset * NP, cudaMemcpyHostToDevice, s));
+  double *amp, *ph;
+  if ((rc = het_waves(w, ev, w->d_params, (int)nset, s, &amp, &ph))) return rc;
+  launch_het_fisher(amp, ph, B, ev->g, het_data(ev), eps, w->d_b, s);
+  tls_launches += 1;
+  CU(cudaMemcpyAsync(w->h_b, w->d_b, sizeof(double) * B * NP * NP, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  for (int b = 0; b < B; b++) {
+    double* F = fish + (size_t)b * NP * NP;
+    const double* G = w->h_b + (size_t)b * NP * NP;
+    const double* p = params + (size_t)b * NP;
+    if (fabs(p[2]) < 0.9999 && fabs(p[3]) < 0.9999) {
+      for (int i = 0; i < NP; i++)
+        for (int j = i; j < NP; j++) F[i * NP + j] = F[j * NP + i] = G[i * NP + j];
+    } else {                                     // QuickCBC.c:5459-5469
+      for (int i = 0; i < NP * NP; i++) F[i] = 0.0;
+      for (int i = 0; i < NP; i++) F[i * NP + i] = 1.0e4;
+    }
+  }
+  return QCBC_OK;
 }
 
 // ------------------------------------------------------------------ device memory helpers
@@ -1489,6 +1591,109 @@ extern "C" double fourier_nwip(double* a, double* b, double* Sn, int imin, int i
   return out;
 }
 
+extern "C" double log_likelihood_intrinsic(struct Net* net, double** D, double* params, RealVector* freq,
+                                           double** SN, int N, double Tobs) {
+  (void)freq;   // the grid is i/Tobs (QuickCBC.c:419-420)
+  if (!net || !D || !SN || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
+  if (ensure_init()) return -1.0e20;
+  qcbc_event* ev = nullptr;
+  bool temp = false;
+  {
+    std::lock_guard<std::mutex> lk(g_bind_mu);
+    auto it = g_bound.find(BindKey{net, D, SN, N});
+    if (it != g_bound.end()) ev = it->second;
+  }
+  if (!ev) {
+    ev = open_from_rows(net, D, SN, N, Tobs);
+    if (!ev) return -1.0e20;
+    temp = true;
+  }
+  NetGeom g = ev->g;
+  fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, ev->fmin, ev->fmax);
+  double lnl = -1.0e20;
+  int rc = run_full(ev, params, 1, &lnl, nullptr, QCBC_FP64, g, kModelIntrinsic);
+  if (temp) qcbc_event_close(ev);
+  return rc == QCBC_OK ? lnl : -1.0e20;
+}
+
+extern "C" void templates(struct Net* net, double** hwave, RealVector* freq, double* params, int N) {
+  if (!net || !hwave || !freq || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  Workspace* w;
+  if (workspace(w)) return;
+  if (check_geom(net->Nifo, net->labels, 1.0, N)) return;
+  cudaStream_t s = w->stream;
+  double* d_freq;
+  if (stage_freq(w, freq, (size_t)N / 2, &d_freq)) return;
+  double Tobs = 1.0 / freq->data[1];   // QuickCBC.c:3539
+  NetGeom g;
+  fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, 0.0, 1.0);
+  const int nI = net->Nifo, ps = param_stride(kModelIntrinsic, nI);
+  if (grow(w->d_a, w->c_a, (size_t)nI * N) || grow(w->d_params, w->c_params, (size_t)ps) ||
+      grow(w->d_recs, w->c_recs, 1) || grow(w->d_status, w->c_status, 1) || grow_host(w->h_a, w->ch_a, (size_t)nI * N))
+    return;
+  if (cudaMemcpyAsync(w->d_params, params, ps * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess) return;
+  DeviceState& ds = g_dev[current_device()];
+  launch_fulltemplates(w->d_params, g, ds.qnm, d_freq, w->d_recs, w->d_status, w->d_a, s, kModelIntrinsic);
+  tls_launches += 2;
+  cudaMemcpyAsync(w->h_a, w->d_a, sizeof(double) * nI * N, cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "templates failed"); return; }
+  for (int id = 0; id < nI; id++) memcpy(hwave[id], w->h_a + (size_t)id * N, sizeof(double) * N);
+}
+
+extern "C" void AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N) {
+  if (!Af || !Pf || !freq || !freq->data || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  const int n = N / 2;
+  if (n < 2 || freq->length < (size_t)n) { fail(QCBC_EINVAL, "freq shorter than N/2"); return; }
+  Workspace* w;
+  if (workspace(w)) return;
+  // physical parameters exactly as QuickCBC.c:3406-3431 forms them
+  const double Tobs = 1.0 / freq->data[1];
+  const double mc = exp(params[0]), mt = exp(params[1]);
+  const double eta = pow((mc / mt), (5.0 / 3.0));
+  const double dm = eta > 0.25 ? 0.0 : sqrt(1.0 - 4.0 * eta);
+  const double m1_SI = mt * (1.0 + dm) / 2.0, m2_SI = mt * (1.0 - dm) / 2.0;
+  const double ts = Tobs - params[5], distance = exp(params[6]);
+  cudaStream_t s = w->stream;
+  double* d_freq;
+  if (stage_freq(w, freq, (size_t)n, &d_freq)) return;
+  if (grow(w->d_a, w->c_a, (size_t)4 * n) || grow(w->d_recs, w->c_recs, 1) || grow(w->d_status, w->c_status, 1) ||
+      grow_host(w->h_a, w->ch_a, (size_t)2 * n) || grow_host(w->h_status, w->ch_status, 1))
+    return;
+  DeviceState& ds = g_dev[current_device()];
+  double *d_amp = w->d_a, *d_ph = w->d_a + n, *d_Af = w->d_a + 2 * n, *d_Pf = w->d_a + 3 * n;
+  launch_amp_phase(d_freq, n, params[4], kFref, m1_SI / kMsun, m2_SI / kMsun, params[2], params[3], distance, ds.qnm,
+                   w->d_recs, d_amp, d_ph, w->d_status, s);
+  launch_ampphase_out(d_freq, d_amp, d_ph, n, ts, d_Af, d_Pf, s);
+  tls_launches += 3;
+  cudaMemcpyAsync(w->h_a, d_Af, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s);
+  cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (cudaStreamSynchronize(s) != cudaSuccess) { fail(QCBC_ECUDA, "AmpPhase failed"); return; }
+  if (w->h_status[0] != 0) fail(QCBC_EDOM, "IMRPhenomD input outside its domain");
+  memcpy(Af + 1, w->h_a + 1, sizeof(double) * (n - 1));
+  memcpy(Pf + 1, w->h_a + n + 1, sizeof(double) * (n - 1));
+}
+
+extern "C" double het_diff(struct Net* net, struct Het* het, double* params, double* dparams) {
+  if (!net || !het || !params || !dparams) { fail(QCBC_EINVAL, "NULL argument"); return 0.0; }
+  if (ensure_init()) return 0.0;
+  qcbc_event* ev = het_event_for(net, het);
+  if (!ev) return 0.0;
+  double out = 0.0;
+  return qcbc_het_diff(ev, params, dparams, 1, &out) == QCBC_OK ? out : 0.0;
+}
+
+extern "C" void Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs) {
+  (void)Tobs;   // fullphaseamp on the heterodyne grid uses net->Tobs (QuickCBC.c:3797)
+  if (!net || !het || !fish || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  if (ensure_init()) return;
+  qcbc_event* ev = het_event_for(net, het);
+  if (!ev) return;
+  double F[11 * 11];
+  if (qcbc_het_fisher(ev, params, 1, F) != QCBC_OK) return;
+  for (int i = 0; i < 11; i++)
+    for (int j = 0; j < 11; j++) fish[i][j] = F[i * 11 + j];
+}
+
 // ------------------------------------------------------------------ prefixed aliases
 extern "C" double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq,
                                                double** SN, double* rho, int N, double Tobs) {
@@ -1515,6 +1720,22 @@ extern "C" int qcbc_gpu_IMRPhenomDGenerateh22FDAmpPhase(AmpPhaseFDWaveform** h22
 }
 extern "C" double qcbc_gpu_fourier_nwip(double* a, double* b, double* Sn, int imin, int imax, int N) {
   return fourier_nwip(a, b, Sn, imin, imax, N);
+}
+extern "C" double qcbc_gpu_log_likelihood_intrinsic(struct Net* net, double** D, double* params, RealVector* freq,
+                                                    double** SN, int N, double Tobs) {
+  return log_likelihood_intrinsic(net, D, params, freq, SN, N, Tobs);
+}
+extern "C" void qcbc_gpu_templates(struct Net* net, double** hwave, RealVector* freq, double* params, int N) {
+  templates(net, hwave, freq, params, N);
+}
+extern "C" void qcbc_gpu_AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N) {
+  AmpPhase(Af, Pf, freq, params, N);
+}
+extern "C" double qcbc_gpu_het_diff(struct Net* net, struct Het* het, double* params, double* dparams) {
+  return het_diff(net, het, params, dparams);
+}
+extern "C" void qcbc_gpu_Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs) {
+  Fisher_Het(net, het, fish, params, Tobs);
 }
 
 // ------------------------------------------------------------------ allocation-free entry point

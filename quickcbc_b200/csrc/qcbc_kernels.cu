@@ -533,6 +533,21 @@ __device__ __forceinline__ void set_projection(PhdRec& c, const double* p, const
   }
 }
 
+// Per-detector offsets of the intrinsic parametrisation (QuickCBC.c:3570-3598): detector 0 is
+// the reference; detector j > 0 has phase offset p[NX+3(j-1)], time offset p[NX+3(j-1)+1] and
+// amplitude ratio p[NX+3(j-1)+2], entering the template x = 2 pi f (ts - td) + pd - phi with
+// amplitude Ar h22fac A / sqrt(T) exactly where lambda, td and |F| enter the full template.
+__device__ __forceinline__ void set_offsets(PhdRec& c, const double* p, int nifo) {
+  c.Fs[0] = 1.0;
+  c.lam[0] = 0.0;
+  c.td[0] = 0.0;
+  for (int j = 1; j < nifo; j++) {
+    c.lam[j] = p[kNX + 3 * (j - 1)];
+    c.td[j] = p[kNX + 3 * (j - 1) + 1];
+    c.Fs[j] = p[kNX + 3 * (j - 1) + 2];
+  }
+}
+
 // Bins that carry signal: f > fbegin (QuickCBC.c:3758) and f <= fCut (IMRPhenomD.c:530), inside
 // the band and inside [1, N/2) (bin N/2 of the template is zero, QuickCBC.c:3754).  The two ends
 // are found independently from the band limits.
@@ -677,12 +692,13 @@ __device__ __forceinline__ void mix_bins(PhdRec& c, const NetGeom& g) {
 // record in each of four phases, so the dependency chain of one record is about a third of
 // the serial one and the lanes of a warp still run the same code:
 //   phase 1  w0 masses/scales        w1 fbegin head, ts      w2 antenna projection   w3 -
+//                                                            (or detector offsets)
 //   phase 2  w0 fRD, fDM             w1 fits, fbegin, lo     w2 a0, ai[0..4], mdf     w3 TaylorF2, MfRef, hi
 //   phase 3  w0 fmax, intermediate   w1 join int, phi(fRef)  w2 MRD join pieces       w3 t0
 //   phase 4  w0 MRD join, phi_pre,   w1 mixed-kernel phase    w2 mixed-kernel          w3 mixed-kernel
 //            mixed-kernel constants                              amplitude                piece bins
 struct SetupScratch {
-  double p[11];
+  double p[kMaxParams];
   PhdMass m;
   FbeginHead fb;
   double v2, s[4], pv[8], pvl[8];
@@ -714,7 +730,7 @@ struct GeomTable {
 template <class Geom>
 __device__ __forceinline__ void setup_coop_block(const double* __restrict__ params, int B, const Geom& geo,
                                                  const QnmTable& q, int tile_bins, PhdRec* __restrict__ recs,
-                                                 int* __restrict__ status, int* __restrict__ ntile) {
+                                                 int* __restrict__ status, int* __restrict__ ntile, int model) {
   __shared__ __align__(16) PhdRec s_rec[kSetupSets];
   __shared__ SetupScratch s_x[kSetupSets];
   __shared__ NetGeom s_g[kSetupSets];
@@ -730,8 +746,8 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     x.live = geo.get(b, g, e);
     s_g[lane] = g;
     s_ev[lane] = e;
-#pragma unroll
-    for (int k = 0; k < 11; k++) x.p[k] = params[(size_t)b * 11 + k];
+    const int ps = x.live ? param_stride(model, g.nifo) : 0;
+    for (int k = 0; k < ps; k++) x.p[k] = params[(size_t)b * ps + k];
   }
   __syncthreads();
   const bool on = lane < nb && x.live;
@@ -746,7 +762,8 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
       c.ts = s_g[lane].Tobs - p[5];
       c.sqT = sqrt(s_g[lane].Tobs);
     } else if (w == 2) {
-      set_projection(c, p, s_g[lane]);
+      if (model == kModelIntrinsic) set_offsets(c, p, s_g[lane].nifo);
+      else set_projection(c, p, s_g[lane]);
     }
   }
   __syncthreads();
@@ -795,7 +812,7 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     int st;
     if (on) {
       phd_join_mrd(c, x.mj);
-      phd_phi_ref(c, 0.5 * x.p[4], x.phr_raw, x.phr_branch);
+      phd_phi_ref(c, model == kModelIntrinsic ? x.p[4] : 0.5 * x.p[4], x.phr_raw, x.phr_branch);
       mix_phase_join(c);
       st = x.st;
       c.flags = (st == kStOK) ? kRecValid : 0;
@@ -825,15 +842,15 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
 
 __global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
                                                          QnmTable q, PhdRec* __restrict__ recs,
-                                                         int* __restrict__ status) {
+                                                         int* __restrict__ status, int model) {
   GeomOne geo{g};
-  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr);
+  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model);
 }
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
-                  int* d_status, cudaStream_t s) {
+                  int* d_status, cudaStream_t s, int model) {
   if (B <= 0) return;
-  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status);
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -1239,7 +1256,7 @@ void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventD
 
 __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
                                 const int* __restrict__ status, int B, int tiles, NetGeom g, EventData ev,
-                                int mixed, double* __restrict__ lnl, double* __restrict__ rho) {
+                                int mixed, int model, double* __restrict__ lnl, double* __restrict__ rho) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
   const PhdRec& c = recs[b];
@@ -1249,6 +1266,7 @@ __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRe
     return;
   }
   double L = 0.0;
+  int loud = 0;
   for (int id = 0; id < g.nifo; id++) {
     double sd = 0.0, sh = 0.0;
     for (int t = 0; t < tiles; t++) {
@@ -1259,18 +1277,25 @@ __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRe
     double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * ev.inv_sigma[id];
     if (mixed) K *= c.a0 * c.mdf_m76;       // the mixed kernel sums the amplitude without this factor
     double HD = K * sd, HH = K * K * sh;
-    if (rho) rho[(size_t)b * g.nifo + id] = HD / sqrt(HH);
-    L += HD - 0.5 * HH;
+    double x = HD - 0.5 * HH;
+    if (model == kModelIntrinsic) {
+      if (rho) rho[(size_t)b * g.nifo + id] = 2.0 * x;
+      loud += 2.0 * x > 25.0;
+    } else if (rho) {
+      rho[(size_t)b * g.nifo + id] = HD / sqrt(HH);
+    }
+    L += x;
   }
+  if (model == kModelIntrinsic && g.nifo > 1 && loud < 2) L = 0.0;   // a signal in at least two detectors
   lnl[b] = L;
 }
 
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
                           const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
-                          cudaStream_t s) {
+                          cudaStream_t s, int model) {
   if (B <= 0) return;
   k_finalize_full<<<(B + 127) / 128, 128, 0, s>>>(d_partials, d_recs, d_status, B, tiles, g, ev,
-                                                  prec == kMixed ? 1 : 0, d_lnl, d_rho);
+                                                  prec == kMixed ? 1 : 0, model, d_lnl, d_rho);
 }
 
 __global__ void k_fill_bin_tables(double2* __restrict__ A, double2* __restrict__ Bt, int n) {
@@ -1293,7 +1318,7 @@ __global__ void __launch_bounds__(kSetupThreads) k_setup_multi(const double* __r
                                                                QnmTable q, int tile_bins, PhdRec* __restrict__ recs,
                                                                int* __restrict__ status, int* __restrict__ ntile) {
   GeomTable geo{event_of, events, n_events};
-  setup_coop_block(params, B, geo, q, tile_bins, recs, status, ntile);
+  setup_coop_block(params, B, geo, q, tile_bins, recs, status, ntile, kModelFull);
 }
 
 void launch_setup_multi(const double* d_params, const int* d_event_of, int B, const EventDesc* d_events, int n_events,
@@ -1621,6 +1646,164 @@ void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetG
   }
 }
 
+// ---------------------------------------------------------------- heterodyne-grid waveforms, het_diff, Fisher_Het
+// fullphaseamp on the heterodyne frequencies (QuickCBC.c:3850-3866), FP64, for B records:
+// A = |F| h22fac amp / sqrt(T) x taper, x = 2 pi f (ts - td) + lambda - phi.
+__global__ void k_het_waves(const PhdRec* __restrict__ recs, NetGeom g, HetData h, double* __restrict__ amp_out,
+                            double* __restrict__ ph_out) {
+  __shared__ PhdRec rec;
+  const int b = blockIdx.y;
+  load_record(rec, recs + b);
+  __syncthreads();
+  const PhdRec& c = rec;
+  const int M = h.M, nifo = g.nifo;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
+    const double f = __ldg(h.freq + j);
+    double y = 1.0;
+    if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);
+    double amp = 0.0, ph = 0.0;
+    if (!(f > c.fCut)) { phd_eval64(c, c.Msec * f, amp, ph); amp *= c.amp_scale; }
+    for (int id = 0; id < nifo; id++) {
+      const size_t o = ((size_t)b * nifo + id) * M + j;
+      amp_out[o] = c.Fs[id] * kH22fac * amp / c.sqT * y;
+      ph_out[o] = __dadd_rn(__dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, f), c.ts - c.td[id]), c.lam[id]), -ph);
+    }
+  }
+}
+
+void launch_het_waves(const PhdRec* d_recs, int B, const NetGeom& g, const HetData& h, double* d_amp,
+                      double* d_phase, cudaStream_t s) {
+  if (B <= 0) return;
+  dim3 grid((unsigned)((h.M + 127) / 128), (unsigned)B);
+  k_het_waves<<<grid, 128, 0, s>>>(d_recs, g, h, d_amp, d_phase);
+}
+
+// The slow-term quadrature of the heterodyne summary for one detector and the regions
+// r = r0, r0 + rstep, ...: sum_r (IP[r] v_r) . SL[r][id], and separately the over-counted edge
+// values sum_{r < NR-2} aa[id][r+1] v[rJ + J] (QuickCBC.c:5005-5035, 5571-5597).
+__device__ __forceinline__ void het_slow_terms(const HetData& h, int nifo, int id, const double* v, int r0, int rstep,
+                                               double& hh, double& edge) {
+  const int J = h.J, J1 = J + 1, NR = h.NR;
+  for (int r = r0; r < NR; r += rstep) {
+    const double* ip = h.IP + (size_t)r * J1 * J1;
+    const double* sl = h.SL + ((size_t)r * nifo + id) * J1;
+    const double* vv = v + r * J;
+    for (int a = 0; a < J1; a++) {
+      double u = 0.0;
+      for (int k = 0; k < J1; k++) u += __ldg(ip + a * J1 + k) * vv[k];
+      hh += u * __ldg(sl + a);
+    }
+    if (r < NR - 2) edge += __ldg(h.aa + id * NR + r + 1) * vv[J];
+  }
+}
+
+// het_diff: one block per pair p of wave sets (2p, 2p+1); d_out[p] = sum over detectors of the
+// slow-term quadrature of cc = 4 |h_2p - h_2p+1|^2 / Aref^2 (QuickCBC.c:4995-5040).
+__global__ void __launch_bounds__(256) k_het_diff(const double* __restrict__ amp, const double* __restrict__ ph,
+                                                  NetGeom g, HetData h, double* __restrict__ out) {
+  extern __shared__ double s_cc[];   // [M]
+  __shared__ double red[32 * 2];
+  const int p = blockIdx.x, M = h.M, nifo = g.nifo;
+  double tot = 0.0;
+  for (int id = 0; id < nifo; id++) {
+    const double* Ar = amp + ((size_t)(2 * p) * nifo + id) * M;
+    const double* Ap = amp + ((size_t)(2 * p + 1) * nifo + id) * M;
+    const double* Pr = ph + ((size_t)(2 * p) * nifo + id) * M;
+    const double* Pp = ph + ((size_t)(2 * p + 1) * nifo + id) * M;
+    for (int j = threadIdx.x; j < M; j += blockDim.x) {
+      const double d = Pr[j] - Pp[j];
+      const double re = Ar[j] - Ap[j] * cos(d), im = Ap[j] * sin(d);
+      const double aref = __ldg(h.amp + id * M + j);
+      s_cc[j] = 4.0 * (re * re + im * im) / (aref * aref);
+    }
+    __syncthreads();
+    double v[2] = {0.0, 0.0};
+    het_slow_terms(h, nifo, id, s_cc, threadIdx.x, blockDim.x, v[0], v[1]);
+    block_sum<2>(v, red);
+    if (threadIdx.x == 0) tot += v[0] - v[1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[p] = tot;
+}
+
+void launch_het_diff(const double* d_amp, const double* d_phase, int npair, const NetGeom& g, const HetData& h,
+                     double* d_out, cudaStream_t s) {
+  if (npair <= 0) return;
+  k_het_diff<<<npair, 256, (size_t)h.M * sizeof(double), s>>>(d_amp, d_phase, g, h, d_out);
+}
+
+// Fisher_Het: one block per (matrix f, pair i <= j).  Central differences of the amplitude and
+// phase (wave sets 23 f + 1 + 2 i and 23 f + 2 + 2 i, step eps), then per detector the slow-term
+// quadrature of cc = 4 (dA_i dA_j + A^2 dphi_i dphi_j) / Aref^2 (QuickCBC.c:5503-5600).
+constexpr int kNP = 11;
+constexpr int kFisherSets = 2 * kNP + 1;
+__global__ void __launch_bounds__(256) k_het_fisher(const double* __restrict__ amp, const double* __restrict__ ph,
+                                                    NetGeom g, HetData h, double eps, double* __restrict__ fish) {
+  extern __shared__ double s_cc[];   // [M]
+  __shared__ double red[32 * 2];
+  __shared__ int s_ij[2];
+  const int f = blockIdx.y, M = h.M, nifo = g.nifo;
+  if (threadIdx.x == 0) {           // pair index -> (i, j >= i) in row-major order of the upper triangle
+    int q = blockIdx.x, i = 0;
+    while (q >= kNP - i) { q -= kNP - i; i++; }
+    s_ij[0] = i;
+    s_ij[1] = i + q;
+  }
+  __syncthreads();
+  const int i = s_ij[0], j = s_ij[1];
+  const size_t set0 = (size_t)f * kFisherSets;
+  double tot = 0.0;
+  for (int id = 0; id < nifo; id++) {
+    const double* A0 = amp + (set0 * nifo + id) * M;
+    const double* Api = amp + ((set0 + 1 + 2 * i) * nifo + id) * M;
+    const double* Ami = amp + ((set0 + 2 + 2 * i) * nifo + id) * M;
+    const double* Apj = amp + ((set0 + 1 + 2 * j) * nifo + id) * M;
+    const double* Amj = amp + ((set0 + 2 + 2 * j) * nifo + id) * M;
+    const double* Ppi = ph + ((set0 + 1 + 2 * i) * nifo + id) * M;
+    const double* Pmi = ph + ((set0 + 2 + 2 * i) * nifo + id) * M;
+    const double* Ppj = ph + ((set0 + 1 + 2 * j) * nifo + id) * M;
+    const double* Pmj = ph + ((set0 + 2 + 2 * j) * nifo + id) * M;
+    for (int k = threadIdx.x; k < M; k += blockDim.x) {
+      const double dAi = (Api[k] - Ami[k]) / (2.0 * eps), dAj = (Apj[k] - Amj[k]) / (2.0 * eps);
+      const double dPi = (Ppi[k] - Pmi[k]) / (2.0 * eps), dPj = (Ppj[k] - Pmj[k]) / (2.0 * eps);
+      const double aref = __ldg(h.amp + id * M + k);
+      s_cc[k] = 4.0 * (dAi * dAj + A0[k] * A0[k] * dPi * dPj) / (aref * aref);
+    }
+    __syncthreads();
+    double v[2] = {0.0, 0.0};
+    het_slow_terms(h, nifo, id, s_cc, threadIdx.x, blockDim.x, v[0], v[1]);
+    block_sum<2>(v, red);
+    if (threadIdx.x == 0) tot += v[0] - v[1];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) fish[((size_t)f * kNP + i) * kNP + j] = tot;
+}
+
+void launch_het_fisher(const double* d_amp, const double* d_phase, int nmat, const NetGeom& g, const HetData& h,
+                       double eps, double* d_fish, cudaStream_t s) {
+  if (nmat <= 0) return;
+  dim3 grid(kNP * (kNP + 1) / 2, (unsigned)nmat);
+  k_het_fisher<<<grid, 256, (size_t)h.M * sizeof(double), s>>>(d_amp, d_phase, g, h, eps, d_fish);
+}
+
+// AmpPhase outputs for bins [1, n) (QuickCBC.c:3435-3440)
+__global__ void k_ampphase_out(const double* __restrict__ freq, const double* __restrict__ amp,
+                               const double* __restrict__ phase, int n, double ts, double* __restrict__ Af,
+                               double* __restrict__ Pf) {
+  for (int i = 1 + blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    Pf[i] = __dadd_rn(__dmul_rn(__dmul_rn(kTwoPi, freq[i]), ts), -phase[i]);
+    Af[i] = kH22fac * amp[i];
+  }
+}
+
+void launch_ampphase_out(const double* d_freq, const double* d_amp, const double* d_phase, int n, double ts,
+                         double* d_Af, double* d_Pf, cudaStream_t s) {
+  int blocks = (n + 255) / 256;
+  if (blocks > 1184) blocks = 1184;
+  if (blocks < 1) blocks = 1;
+  k_ampphase_out<<<blocks, 256, 0, s>>>(d_freq, d_amp, d_phase, n, ts, d_Af, d_Pf);
+}
+
 // ---------------------------------------------------------------- waveform outputs
 __global__ void k_setup_phys(double phi0, double fRef, double m1, double m2, double chi1, double chi2, double dist,
                              QnmTable q, PhdRec* rec, int* status) {
@@ -1688,8 +1871,8 @@ __global__ void k_fulltemplates(const PhdRec* __restrict__ recp, NetGeom g, cons
 }
 
 void launch_fulltemplates(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq,
-                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s) {
-  launch_setup(d_params, 1, g, q, d_rec, d_status, s);
+                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s, int model) {
+  launch_setup(d_params, 1, g, q, d_rec, d_status, s, model);
   int blocks = (g.N / 2 + 256) / 256;
   if (blocks > 2368) blocks = 2368;
   k_fulltemplates<<<blocks, 256, 0, s>>>(d_rec, g, d_freq, d_h);

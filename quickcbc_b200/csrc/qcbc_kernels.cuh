@@ -57,18 +57,44 @@ struct FullLaunch {
   int threads;           // threads per block
 };
 
+// Parameter models of a set.  Full: the 11 parameters of log_likelihood_full (sky position,
+// polarisation, inclination -> antenna response; phi0 = params[4] / 2).  Intrinsic: the
+// NX + 3 (Nifo - 1) parameters of log_likelihood_intrinsic / templates (QuickCBC.c:3527-3598):
+// per-detector phase offset, time offset and amplitude ratio relative to detector 0 in place of
+// the antenna response, phi0 = params[4].
+enum ParamModel { kModelFull = 0, kModelIntrinsic = 1 };
+constexpr int kNX = 7;
+constexpr int kMaxParams = kNX + 3 * (kMaxIfo - 1);
+__host__ __device__ constexpr int param_stride(int model, int nifo) {
+  return model == kModelIntrinsic ? kNX + 3 * (nifo - 1) : 11;
+}
+
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
-                  int* d_status, cudaStream_t s);
+                  int* d_status, cudaStream_t s, int model = kModelFull);
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s);
+// d_rho: full model rho[id] = HD / sqrt(HH); intrinsic model the per-detector SNR^2 = 2 (HD - HH/2)
+// (and lnL = 0 unless at least two detectors exceed 25 when Nifo > 1, QuickCBC.c:4117-4128)
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
                           const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
-                          cudaStream_t s);
+                          cudaStream_t s, int model = kModelFull);
 // fill the per-bin tables for bins [0, n)
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, int threads, double* d_lnl, cudaStream_t s);
 size_t het_smem_bytes(const NetGeom& g, const HetData& h);
+// fullphaseamp on the heterodyne grid (QuickCBC.c:3850-3866) for B records:
+// amp/phase [B][nifo][M]
+void launch_het_waves(const PhdRec* d_recs, int B, const NetGeom& g, const HetData& h, double* d_amp,
+                      double* d_phase, cudaStream_t s);
+// het_diff (QuickCBC.c:4966-5051) for npair pairs of wave sets (2p, 2p+1) -> d_out[npair]
+void launch_het_diff(const double* d_amp, const double* d_phase, int npair, const NetGeom& g, const HetData& h,
+                     double* d_out, cudaStream_t s);
+// Fisher_Het (QuickCBC.c:5446-5617) for nmat matrices; matrix f uses the wave sets 23 f + k:
+// k = 0 the point, k = 1 + 2 i / 2 + 2 i the point +/- eps along parameter i.  Writes the upper
+// triangle (j >= i) of d_fish[nmat][11][11].
+void launch_het_fisher(const double* d_amp, const double* d_phase, int nmat, const NetGeom& g, const HetData& h,
+                       double eps, double* d_fish, cudaStream_t s);
 
 // waveform outputs for the reference-signature entry points
 void launch_amp_phase(const double* d_freq, int n, double phi0, double fRef, double m1_Msun, double m2_Msun,
@@ -78,7 +104,10 @@ void launch_amp_phase(const double* d_freq, int n, double phi0, double fRef, dou
 void launch_nwip(const double* d_a, const double* d_b, const double* d_S, int imin, int imax, int N, double* d_out,
                  cudaStream_t s);
 void launch_fulltemplates(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq,
-                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s);
+                          PhdRec* d_rec, int* d_status, double* d_h, cudaStream_t s, int model = kModelFull);
+// AmpPhase outputs (QuickCBC.c:3435-3440): Pf[i] = 2 pi f_i ts - phase[i], Af[i] = h22fac amp[i], i in [1, n)
+void launch_ampphase_out(const double* d_freq, const double* d_amp, const double* d_phase, int n, double ts,
+                         double* d_Af, double* d_Pf, cudaStream_t s);
 void launch_fullphaseamp(const double* d_params, const NetGeom& g, const QnmTable& q, const double* d_freq, int n,
                          PhdRec* d_rec, int* d_status, double* d_amp, double* d_phase, cudaStream_t s);
 

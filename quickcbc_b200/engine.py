@@ -90,6 +90,20 @@ class Event:
             check(rc)
         return (out, r) if rho else out
 
+    def lnl_intrinsic(self, params, precision=FP64, snrsq=False, allow_invalid=False):
+        """Batched log_likelihood_intrinsic: params [B][7 + 3 (nifo - 1)] (templates' layout)."""
+        P = _f64(np.atleast_2d(params))
+        if P.shape[1] != 7 + 3 * (self.nifo - 1):
+            raise ValueError(f"intrinsic parameter sets have {7 + 3 * (self.nifo - 1)} entries for {self.nifo} detectors")
+        B = P.shape[0]
+        out = np.zeros(B)
+        r = np.zeros((B, self.nifo)) if snrsq else None
+        rc = lib().qcbc_lnl_intrinsic(self._h, _ptr(P), B, _ptr(out), _ptr(r) if snrsq else None,
+                                      precision_code(precision))
+        if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
+            check(rc)
+        return (out, r) if snrsq else out
+
     def set_launch(self, tiles=0, threads=0):
         check(lib().qcbc_set_full_launch(self._h, tiles, threads))
 
@@ -135,6 +149,20 @@ class Event:
         if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
             check(rc)
         return out
+
+    def het_diff(self, params_a, params_b):
+        """Heterodyned squared distance between the templates of paired rows (het_diff)."""
+        A, Bp = _f64(np.atleast_2d(params_a)), _f64(np.atleast_2d(params_b))
+        out = np.zeros(A.shape[0])
+        check(lib().qcbc_het_diff(self._h, _ptr(A), _ptr(Bp), A.shape[0], _ptr(out)))
+        return out
+
+    def het_fisher(self, params):
+        """Fisher matrices [B][11][11] from the heterodyne tables (Fisher_Het), one launch for all sets."""
+        P = _f64(np.atleast_2d(params))
+        F = np.zeros((P.shape[0], 11, 11))
+        check(lib().qcbc_het_fisher(self._h, _ptr(P), P.shape[0], _ptr(F)))
+        return F
 
 
 class Batch:
@@ -311,6 +339,33 @@ def amp_phase(freq, phi0, fRef, m1_SI, m2_SI, chi1, chi2, dist):
     return st, amp, ph
 
 
+def templates(labels, GMST, freq, params, N):
+    """templates (QuickCBC.c:3527) through the drop-in symbol; intrinsic parameters."""
+    nh = _NetHolder(labels, 1.0 / freq[1], GMST)
+    h = np.zeros((len(nh.labels), N))
+    f, rv = _rv(freq)
+    p = _f64(params).copy()
+    lib().templates(nh.ref, _rows(h), C.byref(rv), _ptr(p), N)
+    return h
+
+
+def ampphase(freq, params, N):
+    """AmpPhase (QuickCBC.c:3395) through the drop-in symbol: (Af, Pf) over N/2 bins, entry 0 zero."""
+    f, rv = _rv(freq)
+    Af, Pf = np.zeros(N // 2), np.zeros(N // 2)
+    p = _f64(params).copy()
+    lib().AmpPhase(_ptr(Af), _ptr(Pf), C.byref(rv), _ptr(p), N)
+    return Af, Pf
+
+
+def log_likelihood_intrinsic(labels, GMST, D, params, freq, SN, N, Tobs):
+    nh = _NetHolder(labels, Tobs, GMST)
+    D, SN = _f64(D), _f64(SN)
+    f, rv = _rv(freq)
+    p = _f64(params).copy()
+    return lib().log_likelihood_intrinsic(nh.ref, _rows(D), _ptr(p), C.byref(rv), _rows(SN), N, Tobs)
+
+
 def fourier_nwip(a, b, S, imin, imax, N):
     a, b, S = _f64(a), _f64(b), _f64(S)
     return lib().fourier_nwip(_ptr(a), _ptr(b), _ptr(S), imin, imax, N)
@@ -357,6 +412,16 @@ class LegacyHet:
     def lnl(self, params):
         p = _f64(params).copy()
         return lib().log_likelihood_het(self.nh.ref, C.byref(self.het), _ptr(p), self.Tobs)
+
+    def het_diff(self, params, dparams):
+        p, q = _f64(params).copy(), _f64(dparams).copy()
+        return lib().het_diff(self.nh.ref, C.byref(self.het), _ptr(p), _ptr(q))
+
+    def fisher(self, params):
+        F = np.zeros((11, 11))
+        p = _f64(params).copy()
+        lib().Fisher_Het(self.nh.ref, C.byref(self.het), _rows(F), _ptr(p), self.Tobs)
+        return F
 
     def tables(self):
         h, nI, M, J, NR = self.het, self.nh.net.Nifo, self.het.M, self.het.J, self.het.NR

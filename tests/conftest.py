@@ -61,6 +61,7 @@ class GoldenEvent:
         self.SN = z["SN"]
         self.inj = z["inj"]
         self.freq = np.arange(self.N // 2, dtype=np.float64) / self.Tobs
+        self.freq[0] = 1.0 / self.Tobs          # the reference's grid (QuickCBC.c:418-419)
         self.freq[0] = 1.0 / self.Tobs
 
     @property

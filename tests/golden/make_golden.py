@@ -6,7 +6,7 @@ The reference ships no golden vectors or known-answer tests, so these
 fixtures pin the CPU oracle and the CUDA kernels on machines where the
 reference tree is absent.  Regenerate with:
 
-    make -C oracle ref && python tests/golden/make_golden.py
+    make -C oracle ref && python tests/golden/make_golden.py [wave cfg1 het1 grid3 secondary1]
 
 Contents (float64 unless noted):
   wave.npz     amp/phase of IMRPhenomDGenerateh22FDAmpPhase for 6 systems on a
@@ -16,6 +16,9 @@ Contents (float64 unless noted):
   het1.npz     reference heterodyne grid (het_space) and tables for config 1,
                reference het lnL at 16 nearby parameter sets
   grid3.npz    reference heterodyne grid for config 3 (3 det, 128 s, 4096 Hz)
+  secondary1.npz  config 1: templates and log_likelihood_intrinsic on intrinsic-layout
+               parameter sets, AmpPhase, and het_diff / Fisher_Het on the reference's
+               heterodyne tables of het1.npz's grid
 """
 from __future__ import annotations
 
@@ -133,11 +136,78 @@ def make_grid3():
                         logLb=t["logLb"], params=P, lnl=L, inj=ev.inj, GMST=ev.GMST)
 
 
+def intrinsic_equivalent(p, labels, GMST):
+    """Intrinsic-layout parameters (QuickCBC.c:3570-3582) of the template that equals the full
+    template of p (QuickCBC.c:3722-3760) in every detector: detector 0's response |F0|,
+    polarisation phase lambda0 and delay td0 go into the distance, phase and merger time;
+    detectors j > 0 get lambda_j - lambda0, td_j - td0 and |F_j| / |F0|."""
+    alpha, sind, psi, ci = p[7], p[8], p[9], p[10]
+    Ap, Ac = (1.0 + ci * ci) / 2.0, -ci
+    dt = ref.Times(alpha, sind, GMST)
+    Fs, lam, td = [], [], []
+    for l in labels:
+        fp, fx = ref.F_ant(psi, alpha, sind, GMST, int(l))
+        Fs.append(np.sqrt(Ap * Ap * fp * fp + Ac * Ac * fx * fx))
+        lam.append(np.mod(np.arctan2(Ac * fx, Ap * fp), 2 * np.pi))
+        td.append(dt[int(l)])
+    q = [p[0], p[1], p[2], p[3], (p[4] + lam[0]) / 2.0, p[5] + td[0], p[6] - np.log(Fs[0])]
+    for j in range(1, len(labels)):
+        q += [lam[j] - lam[0], td[j] - td[0], Fs[j] / Fs[0]]
+    return np.array(q)
+
+
+def intrinsic_sets(rng, n, inj, labels, GMST):
+    """Intrinsic-layout sets about the intrinsic equivalent of the injection; the last two are
+    far away (fewer than two detectors with SNR^2 > 25, so the reference returns 0)."""
+    c = intrinsic_equivalent(inj, labels, GMST)
+    P = np.tile(c, (n, 1))
+    P[:, 0] += 1e-4 * rng.normal(size=n)
+    P[:, 1] += 1e-3 * rng.normal(size=n)
+    P[:, 2:4] = np.clip(P[:, 2:4] + 1e-2 * rng.normal(size=(n, 2)), -0.95, 0.95)
+    P[:, 4] += 0.05 * rng.normal(size=n)
+    P[:, 5] += 1e-4 * rng.normal(size=n)
+    P[:, 6] += 0.05 * rng.normal(size=n)
+    P[:, 7:] += np.array([0.05, 1e-4, 0.05]) * rng.normal(size=(n, 3))
+    P[n - 2:, 6] += np.log(50.0)
+    return P
+
+
+def make_secondary1():
+    ev = synth.config_event(1, ref_template_factory())
+    net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+    rng = np.random.default_rng(1700)
+    PI = intrinsic_sets(rng, 8, ev.inj, ev.labels, ev.GMST)
+    L = np.array([ref.lnl_intrinsic(net, ev.D, p, ev.freq, ev.SN, ev.N, ev.Tobs) for p in PI])
+    H = np.array([ref.templates(net, ev.freq, PI[k], ev.N) for k in (0, 5)])
+    PA = synth.jitter_params(rng, 2, ev.inj, scale=1e-2)
+    AP = [ref.AmpPhase(ev.freq, p, ev.N) for p in PA]
+    h1 = np.load(os.path.join(OUT, "het1.npz"))
+    het = ref.RefHet(net)
+    het.set_grid(h1["fgrid"], int(h1["MN"]), int(h1["MM"]), int(h1["J"]), ev.Tobs)
+    het.heterodyne(ev.D, h1["pref"], ev.freq, ev.SN, ev.N, ev.Tobs)
+    DA = synth.jitter_params(rng, 4, h1["pref"], scale=1e-4)
+    DB = synth.jitter_params(rng, 4, h1["pref"], scale=1e-4)
+    dif = np.array([het.het_diff(a, b) for a, b in zip(DA, DB)])
+    FP = np.vstack([h1["pref"], synth.jitter_params(rng, 1, h1["pref"], scale=1e-4)])
+    fish = np.array([het.fisher(p, ev.Tobs) for p in FP])
+    np.savez_compressed(os.path.join(OUT, "secondary1.npz"), int_params=PI, int_lnl=L, int_h=H,
+                        int_h_idx=np.array([0, 5]), ap_params=PA, ap_amp=np.array([a for a, _ in AP]),
+                        ap_phase=np.array([p for _, p in AP]), diff_a=DA, diff_b=DB, diff=dif, fisher_params=FP,
+                        fisher=fish)
+
+
 if __name__ == "__main__":
-    make_wave()
-    ev, net = make_cfg1()
-    make_het1(ev, net)
-    make_grid3()
+    which = set(sys.argv[1:]) or {"wave", "cfg1", "het1", "grid3", "secondary1"}
+    if "wave" in which:
+        make_wave()
+    if which & {"cfg1", "het1"}:
+        ev, net = make_cfg1()
+        if "het1" in which:
+            make_het1(ev, net)
+    if "grid3" in which:
+        make_grid3()
+    if "secondary1" in which:
+        make_secondary1()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))

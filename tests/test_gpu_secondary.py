@@ -1,0 +1,109 @@
+"""Secondary reference-signature entry points (QuickCBC.h:95-151) against the
+reference's own outputs (tests/golden/secondary1.npz, made by running the
+reference): templates, log_likelihood_intrinsic, AmpPhase, het_diff and
+Fisher_Het, plus their batched C-ABI forms.
+
+Tolerances:
+  FP64 waveform outputs   1e-11 of the largest |h| (templates), 1e-12 relative (AmpPhase amp),
+                          1e-9 of the largest |phase| (AmpPhase phase)
+  FP64 likelihoods        1e-8 absolute (intrinsic lnL), 1e-9 relative (het_diff)
+  mixed likelihoods       1e-3 absolute
+  Fisher_Het              1e-6 of sqrt(F_ii F_jj) per entry (central differences with step 1e-5)
+"""
+import numpy as np
+import pytest
+
+import quickcbc_b200 as q
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def sec(golden):
+    return golden("secondary1.npz")
+
+
+@pytest.fixture(scope="module")
+def ev1(cfg1_event):
+    ev, z = cfg1_event
+    e = q.Event.from_synthetic(ev)
+    yield ev, e
+    e.close()
+
+
+def test_templates_vs_reference(ev1, sec):
+    ev, _ = ev1
+    for H, k in zip(sec["int_h"], sec["int_h_idx"]):
+        h = q.templates(ev.labels, ev.GMST, ev.freq, sec["int_params"][k], ev.N)
+        np.testing.assert_allclose(h, H, rtol=0, atol=1e-11 * np.abs(H).max())
+
+
+def test_lnl_intrinsic_vs_reference(ev1, sec):
+    ev, e = ev1
+    Lref = sec["int_lnl"]
+    assert np.count_nonzero(Lref == 0.0) == 2 and np.all(Lref[:6] > 200), "fixture covers both branches of the rule"
+    L = np.array([q.log_likelihood_intrinsic(ev.labels, ev.GMST, ev.D, p, ev.freq, ev.SN, ev.N, ev.Tobs)
+                  for p in sec["int_params"]])
+    np.testing.assert_allclose(L, Lref, rtol=0, atol=1e-8)
+    Lb, snr2 = e.lnl_intrinsic(sec["int_params"], q.FP64, snrsq=True)
+    np.testing.assert_allclose(Lb, Lref, rtol=0, atol=1e-8)
+    loud = (snr2 > 25.0).sum(axis=1)
+    assert np.array_equal(Lref == 0.0, loud < 2)
+    Lm = e.lnl_intrinsic(sec["int_params"], q.MIXED)
+    np.testing.assert_allclose(Lm, Lref, rtol=0, atol=1e-3)
+
+
+def test_lnl_intrinsic_rejects_wrong_layout(ev1, sec):
+    _, e = ev1
+    with pytest.raises(ValueError):
+        e.lnl_intrinsic(sec["int_params"][:, :9])
+
+
+def test_ampphase_vs_reference(ev1, sec):
+    ev, _ = ev1
+    for p, Ar, Pr in zip(sec["ap_params"], sec["ap_amp"], sec["ap_phase"]):
+        Af, Pf = q.ampphase(ev.freq, p, ev.N)
+        np.testing.assert_allclose(Af[1:], Ar[1:], rtol=1e-12, atol=1e-40)
+        np.testing.assert_allclose(Pf[1:], Pr[1:], rtol=0, atol=1e-9 * np.abs(Pr).max())
+
+
+@pytest.fixture(scope="module")
+def het1(ev1, golden):
+    ev, _ = ev1
+    h = golden("het1.npz")
+    H = q.LegacyHet(ev.labels, ev.GMST, ev.Tobs, h["fgrid"], int(h["MN"]), int(h["MM"]), int(h["J"]))
+    H.heterodyne(ev.D, h["pref"], ev.freq, ev.SN, ev.N)
+    return H
+
+
+def test_het_diff_vs_reference(het1, sec):
+    d = np.array([het1.het_diff(a, b) for a, b in zip(sec["diff_a"], sec["diff_b"])])
+    np.testing.assert_allclose(d, sec["diff"], rtol=1e-9, atol=0)
+    assert het1.het_diff(sec["diff_a"][0], sec["diff_a"][0]) == 0.0
+
+
+def fisher_close(F, G):
+    s = np.sqrt(np.outer(np.diag(G), np.diag(G)))
+    assert np.all(np.abs(F - G) <= 1e-6 * s), np.max(np.abs(F - G) / s)
+
+
+def test_fisher_het_vs_reference(het1, sec):
+    for p, G in zip(sec["fisher_params"], sec["fisher"]):
+        F = het1.fisher(p)
+        assert np.array_equal(F, F.T)
+        fisher_close(F, G)
+
+
+def test_batched_het_forms_match_drop_ins(ev1, het1, sec):
+    _, e = ev1
+    e.het_set(het1.tables())
+    F = e.het_fisher(sec["fisher_params"])
+    for k, G in enumerate(sec["fisher"]):
+        fisher_close(F[k], G)
+    d = e.het_diff(sec["diff_a"], sec["diff_b"])
+    np.testing.assert_allclose(d, sec["diff"], rtol=1e-9, atol=0)
+    # near-extremal spins: the reference's fallback matrix
+    p = sec["fisher_params"][0].copy()
+    p[2] = 0.99995
+    F1 = e.het_fisher(p)[0]
+    assert np.array_equal(F1, np.diag(np.full(11, 1.0e4)))
