@@ -127,23 +127,33 @@ def cpu_baseline_reference(ev, P, budget_s=12.0, impl_note=""):
         S = ev.SN.copy()
         S[:, int(16.0 * ev.Tobs):int(ev.fmin * ev.Tobs)] = np.inf   # reference built with fmin = 16 Hz
         kind, cores = "reference", ref.max_threads()
-        run = lambda X: ref.lnl_full_batch(net, ev.D, X, ev.freq, S, ev.N, ev.Tobs)  # noqa: E731
+        run = lambda X, nt=cores: ref.lnl_full_batch(net, ev.D, X, ev.freq, S, ev.N, ev.Tobs, nthreads=nt)  # noqa: E731
     except Exception:
         from oracle import ora
         kind, cores = "port", os.cpu_count()
-        run = lambda X: ora.lnl_full_batch(ev, X)  # noqa: E731
-    n, secs, chunk = 0, 0.0, 64
-    t_end = time.perf_counter() + budget_s
-    k = 0
-    while time.perf_counter() < t_end:
-        X = P[(k * chunk) % len(P):(k * chunk) % len(P) + chunk]
-        _, s = run(X)
-        n += len(X)
-        secs += s
-        k += 1
-    return {"value": n / secs, "unit": "lnL evals/s", "cores": int(cores), "kind": kind,
-            "sample": f"{n} parameter sets of the benchmark batch in chunks of {chunk}, OpenMP over sets, "
-                      f"{secs:.1f} s wall{impl_note}"}
+        run = lambda X, nt=cores: ora.lnl_full_batch(ev, X)  # noqa: E731
+
+    def sample(seconds, nt, chunk):
+        n, secs, k = 0, 0.0, 0
+        t_end = time.perf_counter() + seconds
+        while time.perf_counter() < t_end:
+            X = P[(k * chunk) % len(P):(k * chunk) % len(P) + chunk]
+            _, s = run(X, nt)
+            n += len(X)
+            secs += s
+            k += 1
+        return n, secs
+
+    chunk = 64
+    n, secs = sample(budget_s, cores, chunk)
+    out = {"value": n / secs, "unit": "lnL evals/s", "cores": int(cores), "kind": kind,
+           "sample": f"{n} parameter sets of the benchmark batch in chunks of {chunk}, OpenMP over sets, "
+                     f"{secs:.1f} s wall{impl_note}"}
+    if kind == "reference":
+        n1, s1 = sample(3.0, 1, 4)
+        run(P[:1], cores)                 # restore the thread count
+        out["single_thread"] = {"value": n1 / s1, "unit": "lnL evals/s", "sample": f"{n1} sets, 1 thread, {s1:.1f} s"}
+    return out
 
 
 def run_reference_arm(args):
