@@ -127,6 +127,15 @@ int qcbc_het_export(const qcbc_event* ev, int* fgrid, double* freq, double* amp,
                     double* SL, double* lc, double* ls, double* aa, double* rc, double* rs, double* logLb);
 int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double* lnl, int precision);
 int qcbc_lnl_het_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, int precision, void* stream);
+/* Heterodyne grid search het_space (QuickCBC.c:4570-4910) on the event's PSD about params, within
+ * the prior box [pmin, pmax] (11 each): limits (4275) -> Fisher_All (2695) -> eigen-directions
+ * (FisherEvec, 2449) scaled by efix (4387) to a squared distance of ~30 -> adaptive grid with
+ * J = 2 points per region.  The waveforms run on the device, the control logic on the host.
+ * Returns the grid size M and the band [MN, MM]; qcbc_het_space_grid copies the M bins.
+ * Feed them to qcbc_het_setup (J = 2). */
+int qcbc_het_space(qcbc_event* ev, const double* params, const double* pmin, const double* pmax, int* M, int* MN,
+                   int* MM);
+int qcbc_het_space_grid(const qcbc_event* ev, int* fgrid);
 /* Batched het_diff (QuickCBC.c:4966-5051): out[b] = heterodyned squared distance between the
  * templates of params_a[b] and params_b[b] ([B][11] each), FP64. */
 int qcbc_het_diff(qcbc_event* ev, const double* params_a, const double* params_b, int B, double* out);

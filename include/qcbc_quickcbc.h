@@ -127,6 +127,10 @@ void AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N);
 double het_diff(struct Net* net, struct Het* het, double* params, double* dparams);
 /* replaces QuickCBC.c:5446; fish is the reference's NP x NP row-pointer matrix */
 void Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs);
+/* replaces QuickCBC.c:4570; sets het->MN, MM, J, NR, M, freq, fgrid (malloc'd as the reference
+ * allocates them); writes no diagnostic files */
+void het_space(struct Net* net, struct Het* het, double* params, double* min, double* max, RealVector* freq,
+               double** SN, int N, double Tobs);
 
 /* The same functions under prefixed names, for a forwarding object that
  * gives an unchanged QuickCBC build strong definitions. */
@@ -147,6 +151,8 @@ void qcbc_gpu_templates(struct Net* net, double** hwave, RealVector* freq, doubl
 void qcbc_gpu_AmpPhase(double* Af, double* Pf, RealVector* freq, double* params, int N);
 double qcbc_gpu_het_diff(struct Net* net, struct Het* het, double* params, double* dparams);
 void qcbc_gpu_Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs);
+void qcbc_gpu_het_space(struct Net* net, struct Het* het, double* params, double* min, double* max, RealVector* freq,
+                        double** SN, int N, double Tobs);
 
 #ifdef __cplusplus
 }

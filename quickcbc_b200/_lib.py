@@ -98,6 +98,8 @@ def lib():
         L.qcbc_lnl_intrinsic.argtypes = [vp, _PD, i, _PD, _PD, i]
         L.qcbc_het_diff.argtypes = [vp, _PD, _PD, i, _PD]
         L.qcbc_het_fisher.argtypes = [vp, _PD, i, _PD]
+        L.qcbc_het_space.argtypes = [vp, _PD, _PD, _PD, pi, pi, pi]
+        L.qcbc_het_space_grid.argtypes = [vp, pi]
         L.qcbc_lnl_het_dev.argtypes = [vp, vp, i, vp, i, vp]
         L.qcbc_set_full_launch.argtypes = [vp, i, i]
         L.qcbc_get_full_launch.argtypes = [vp, i, i, pi, pi]
@@ -134,6 +136,8 @@ def lib():
         L.AmpPhase.argtypes = [_PD, _PD, C.POINTER(RealVector), _PD, i]
         L.het_diff.restype = d
         L.het_diff.argtypes = [C.POINTER(Net), C.POINTER(Het), _PD, _PD]
+        L.het_space.restype = None
+        L.het_space.argtypes = [C.POINTER(Net), C.POINTER(Het), _PD, _PD, _PD, C.POINTER(RealVector), _PPD, i, d]
         L.Fisher_Het.restype = None
         L.Fisher_Het.argtypes = [C.POINTER(Net), C.POINTER(Het), _PPD, _PD, d]
         _lib = L

@@ -13,6 +13,7 @@
 #include <algorithm>
 
 #include "qcbc_kernels.cuh"
+#include "qcbc_hetspace.h"
 #include "../../include/qcbc_gpu.h"
 #include "../../include/qcbc_quickcbc.h"
 #include "_gen/qnm_table.h"
@@ -268,6 +269,9 @@ struct HetDev {
 
 struct qcbc_event {
   int device = 0;
+  // the last grid found by qcbc_het_space
+  std::vector<int> space_grid;
+  int space_MN = 0, space_MM = 0;
   NetGeom g{};
   double fmin = 16.0, fmax = 1024.0;
   int nh = 0;
@@ -914,6 +918,50 @@ extern "C" int qcbc_het_fisher(qcbc_event* ev, const double* params, int B, doub
       for (int i = 0; i < NP; i++) F[i * NP + i] = 1.0e4;
     }
   }
+  return QCBC_OK;
+}
+
+// ------------------------------------------------------------------ heterodyne grid search
+static int run_het_space(const NetGeom& g, const double* h_S, int sn_stride, const double* h_freq, int N, double Tobs,
+                         double fmin, double fmax, const double* params, const double* pmin, const double* pmax,
+                         HetSpaceOut& out) {
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  HetSpaceIn in{g, g_dev[current_device()].qnm, h_S, sn_stride, h_freq, N, Tobs, fmin, fmax, w->stream};
+  std::string err;
+  rc = het_space_run(in, params, pmin, pmax, out, err);
+  tls_launches += out.launches;
+  if (rc == -3) return fail(QCBC_ECUDA, "%s", err.c_str());
+  if (rc) return fail(QCBC_EINVAL, "%s", err.c_str());
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_space(qcbc_event* ev, const double* params, const double* pmin, const double* pmax, int* M,
+                              int* MN, int* MM) {
+  if (!ev || !params || !pmin || !pmax) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->has_data) return fail(QCBC_EINVAL, "event has no data");
+  const int nI = ev->g.nifo, nh = ev->nh;
+  std::vector<double> S((size_t)nI * (nh + 1)), freq((size_t)nh);
+  CU(cudaMemcpy(S.data(), ev->d_S, S.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  CU(cudaMemcpy(freq.data(), ev->d_freq, freq.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  HetSpaceOut out;
+  int rc = run_het_space(ev->g, S.data(), nh + 1, freq.data(), ev->g.N, ev->g.Tobs, ev->fmin, ev->fmax, params, pmin,
+                         pmax, out);
+  if (rc) return rc;
+  ev->space_grid = out.fgrid;
+  ev->space_MN = out.MN;
+  ev->space_MM = out.MM;
+  if (M) *M = out.M;
+  if (MN) *MN = out.MN;
+  if (MM) *MM = out.MM;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_het_space_grid(const qcbc_event* ev, int* fgrid) {
+  if (!ev || !fgrid) return fail(QCBC_EINVAL, "NULL argument");
+  if (ev->space_grid.empty()) return fail(QCBC_EINVAL, "no grid: call qcbc_het_space first");
+  memcpy(fgrid, ev->space_grid.data(), ev->space_grid.size() * sizeof(int));
   return QCBC_OK;
 }
 
@@ -1694,6 +1742,37 @@ extern "C" void Fisher_Het(struct Net* net, struct Het* het, double** fish, doub
     for (int j = 0; j < 11; j++) fish[i][j] = F[i * 11 + j];
 }
 
+extern "C" void het_space(struct Net* net, struct Het* het, double* params, double* min, double* max,
+                          RealVector* freq, double** SN, int N, double Tobs) {
+  if (!net || !het || !params || !min || !max || !freq || !freq->data || !SN) { fail(QCBC_EINVAL, "NULL argument"); return; }
+  if (ensure_init()) return;
+  if (check_geom(net->Nifo, net->labels, net->Tobs, N)) return;
+  const int nI = net->Nifo, nh = N / 2;
+  if (freq->length < (size_t)nh) { fail(QCBC_EINVAL, "freq shorter than N/2"); return; }
+  std::vector<double> S((size_t)nI * nh);
+  for (int id = 0; id < nI; id++) memcpy(&S[(size_t)id * nh], SN[id], sizeof(double) * nh);
+  NetGeom g;
+  fill_geom(g, nI, net->labels, net->Tobs, net->GMST, N, g_band_fmin, g_band_fmax);
+  HetSpaceOut out;
+  if (run_het_space(g, S.data(), nh, freq->data, N, Tobs, g_band_fmin, g_band_fmax, params, min, max, out)) return;
+  // the struct Het fields het_space sets, allocated as CreateRealVector / int_vector do
+  // (IMRPhenomD_internals.c:148-156, Utilities.c:2941-2944) so freehet releases them
+  het->MN = out.MN;
+  het->MM = out.MM;
+  het->J = out.J;
+  het->NR = out.NR;
+  het->M = out.M;
+  RealVector* fv = (RealVector*)malloc(sizeof(RealVector));
+  fv->length = (size_t)out.M;
+  fv->data = (double*)malloc(sizeof(double) * (size_t)out.M);
+  het->fgrid = (int*)malloc(sizeof(int) * (size_t)(out.M + 1));
+  for (int i = 0; i < out.M; i++) {
+    het->fgrid[i] = out.fgrid[i];
+    fv->data[i] = ((double)out.fgrid[i]) / Tobs;
+  }
+  het->freq = fv;
+}
+
 // ------------------------------------------------------------------ prefixed aliases
 extern "C" double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq,
                                                double** SN, double* rho, int N, double Tobs) {
@@ -1733,6 +1812,10 @@ extern "C" void qcbc_gpu_AmpPhase(double* Af, double* Pf, RealVector* freq, doub
 }
 extern "C" double qcbc_gpu_het_diff(struct Net* net, struct Het* het, double* params, double* dparams) {
   return het_diff(net, het, params, dparams);
+}
+extern "C" void qcbc_gpu_het_space(struct Net* net, struct Het* het, double* params, double* min, double* max,
+                                   RealVector* freq, double** SN, int N, double Tobs) {
+  het_space(net, het, params, min, max, freq, SN, N, Tobs);
 }
 extern "C" void qcbc_gpu_Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs) {
   Fisher_Het(net, het, fish, params, Tobs);

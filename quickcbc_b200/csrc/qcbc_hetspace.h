@@ -1,0 +1,33 @@
+// Heterodyne grid search (het_space, QuickCBC.c:4570-4910): host control logic over device
+// waveforms.  Internal interface between qcbc_hetspace.cu and the C ABI.
+#pragma once
+#include <string>
+#include <vector>
+
+#include "qcbc_kernels.cuh"
+
+namespace qcbc {
+
+struct HetSpaceIn {
+  NetGeom g;                 // network; g.Tobs is the Tobs the waveforms use (net->Tobs)
+  QnmTable qnm;
+  const double* h_S;         // host PSD rows [nifo][sn_stride], entries [0, N/2)
+  int sn_stride;
+  const double* h_freq;      // host frequencies [N/2] (freq[0] = 1/Tobs, freq[i] = i/Tobs)
+  int N;
+  double Tobs;               // the Tobs argument of het_space (bin <-> frequency)
+  double fmin, fmax;         // analysis band (ConstCBC.h:33-34)
+  cudaStream_t stream;
+};
+
+struct HetSpaceOut {
+  int MN = 0, MM = 0, J = 2, M = 0, NR = 0;
+  std::vector<int> fgrid;    // bins of the M grid points
+  int launches = 0;
+};
+
+// Returns 0, or -2 (bad input: empty band, runaway grid) / -3 (CUDA error) with err set.
+int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin, const double* pmax,
+                  HetSpaceOut& out, std::string& err);
+
+}  // namespace qcbc

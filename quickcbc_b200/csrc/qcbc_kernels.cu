@@ -1647,18 +1647,20 @@ void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetG
 }
 
 // ---------------------------------------------------------------- heterodyne-grid waveforms, het_diff, Fisher_Het
-// fullphaseamp on the heterodyne frequencies (QuickCBC.c:3850-3866), FP64, for B records:
-// A = |F| h22fac amp / sqrt(T) x taper, x = 2 pi f (ts - td) + lambda - phi.
-__global__ void k_het_waves(const PhdRec* __restrict__ recs, NetGeom g, HetData h, double* __restrict__ amp_out,
-                            double* __restrict__ ph_out) {
+constexpr int kNP = 11;                       // parameters of a full set (NP, ConstCBC.h:68)
+constexpr int kFisherSets = 2 * kNP + 1;      // the point and +/- eps along each parameter
+// fullphaseamp (QuickCBC.c:3850-3866), FP64, for B records on the frequencies freq[0..M):
+// A = |F| h22fac amp / sqrt(T) x taper, x = 2 pi f (ts - td) + lambda - phi; out [B][nifo][M].
+__global__ void k_waves(const PhdRec* __restrict__ recs, NetGeom g, const double* __restrict__ freq, int M,
+                        double* __restrict__ amp_out, double* __restrict__ ph_out) {
   __shared__ PhdRec rec;
   const int b = blockIdx.y;
   load_record(rec, recs + b);
   __syncthreads();
   const PhdRec& c = rec;
-  const int M = h.M, nifo = g.nifo;
+  const int nifo = g.nifo;
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < M; j += gridDim.x * blockDim.x) {
-    const double f = __ldg(h.freq + j);
+    const double f = __ldg(freq + j);
     double y = 1.0;
     if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);
     double amp = 0.0, ph = 0.0;
@@ -1671,11 +1673,131 @@ __global__ void k_het_waves(const PhdRec* __restrict__ recs, NetGeom g, HetData 
   }
 }
 
+void launch_waves(const PhdRec* d_recs, int B, const NetGeom& g, const double* d_freq, int M, double* d_amp,
+                  double* d_phase, cudaStream_t s) {
+  if (B <= 0 || M <= 0) return;
+  int bx = (M + 255) / 256;
+  if (bx > 296) bx = 296;
+  dim3 grid((unsigned)bx, (unsigned)B);
+  k_waves<<<grid, 256, 0, s>>>(d_recs, g, d_freq, M, d_amp, d_phase);
+}
+
 void launch_het_waves(const PhdRec* d_recs, int B, const NetGeom& g, const HetData& h, double* d_amp,
                       double* d_phase, cudaStream_t s) {
+  launch_waves(d_recs, B, g, h.freq, h.M, d_amp, d_phase, s);
+}
+
+// Fisher_All (QuickCBC.c:2695-2817): one block per (matrix f, pair i <= j) over the full band:
+// sum over detectors and bins k in [imin, imax) of 4 (dA_i dA_j + A^2 dphi_i dphi_j) / S, with
+// the central differences of the 23 wave sets of matrix f (as k_het_fisher) on n bins.
+__global__ void __launch_bounds__(256) k_fisher_full(const double* __restrict__ amp, const double* __restrict__ ph,
+                                                     NetGeom g, int n, const double* __restrict__ S, int sn_stride,
+                                                     int imin, int imax, double eps, double* __restrict__ fish) {
+  __shared__ double red[32];
+  __shared__ int s_ij[2];
+  const int f = blockIdx.y, nifo = g.nifo;
+  if (threadIdx.x == 0) {
+    int q = blockIdx.x, i = 0;
+    while (q >= kNP - i) { q -= kNP - i; i++; }
+    s_ij[0] = i;
+    s_ij[1] = i + q;
+  }
+  __syncthreads();
+  const int i = s_ij[0], j = s_ij[1];
+  const size_t set0 = (size_t)f * kFisherSets;
+  double acc[1] = {0.0};
+  for (int id = 0; id < nifo; id++) {
+    const double* A0 = amp + (set0 * nifo + id) * n;
+    const double* Api = amp + ((set0 + 1 + 2 * i) * nifo + id) * n;
+    const double* Ami = amp + ((set0 + 2 + 2 * i) * nifo + id) * n;
+    const double* Apj = amp + ((set0 + 1 + 2 * j) * nifo + id) * n;
+    const double* Amj = amp + ((set0 + 2 + 2 * j) * nifo + id) * n;
+    const double* Ppi = ph + ((set0 + 1 + 2 * i) * nifo + id) * n;
+    const double* Pmi = ph + ((set0 + 2 + 2 * i) * nifo + id) * n;
+    const double* Ppj = ph + ((set0 + 1 + 2 * j) * nifo + id) * n;
+    const double* Pmj = ph + ((set0 + 2 + 2 * j) * nifo + id) * n;
+    const double* Sd = S + (size_t)id * sn_stride;
+    for (int k = imin + threadIdx.x; k < imax; k += blockDim.x) {
+      const double dAi = (Api[k] - Ami[k]) / (2.0 * eps), dAj = (Apj[k] - Amj[k]) / (2.0 * eps);
+      const double dPi = (Ppi[k] - Pmi[k]) / (2.0 * eps), dPj = (Ppj[k] - Pmj[k]) / (2.0 * eps);
+      acc[0] += 4.0 * (dAi * dAj + A0[k] * A0[k] * dPi * dPj) / Sd[k];
+    }
+  }
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) fish[((size_t)f * kNP + i) * kNP + j] = acc[0];
+}
+
+void launch_fisher_full(const double* d_amp, const double* d_phase, int nmat, const NetGeom& g, int n,
+                        const double* d_S, int sn_stride, int imin, int imax, double eps, double* d_fish,
+                        cudaStream_t s) {
+  if (nmat <= 0) return;
+  dim3 grid(kNP * (kNP + 1) / 2, (unsigned)nmat);
+  k_fisher_full<<<grid, 256, 0, s>>>(d_amp, d_phase, g, n, d_S, sn_stride, imin, imax, eps, d_fish);
+}
+
+// diff (QuickCBC.c:4913-4964): out[b] = sum over detectors and bins j in [imin, m) of
+// 4 |h_ref - h_b|^2 / S, for the reference waves (one set) and B other wave sets on n bins.
+__global__ void __launch_bounds__(256) k_diff_full(const double* __restrict__ amp_ref, const double* __restrict__ ph_ref,
+                                                   const double* __restrict__ amp, const double* __restrict__ ph,
+                                                   NetGeom g, int n, int imin, int m, const double* __restrict__ S,
+                                                   int sn_stride, double* __restrict__ out) {
+  __shared__ double red[32];
+  const int b = blockIdx.x, nifo = g.nifo;
+  double acc[1] = {0.0};
+  for (int id = 0; id < nifo; id++) {
+    const double* Ar = amp_ref + (size_t)id * n;
+    const double* Pr = ph_ref + (size_t)id * n;
+    const double* Ap = amp + ((size_t)b * nifo + id) * n;
+    const double* Pp = ph + ((size_t)b * nifo + id) * n;
+    const double* Sd = S + (size_t)id * sn_stride;
+    for (int j = imin + threadIdx.x; j < m; j += blockDim.x) {
+      const double d = Pr[j] - Pp[j];
+      const double re = Ar[j] - Ap[j] * cos(d), im = Ap[j] * sin(d);
+      acc[0] += 4.0 * (re * re + im * im) / Sd[j];
+    }
+  }
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) out[b] = acc[0];
+}
+
+void launch_diff_full(const double* d_amp_ref, const double* d_ph_ref, const double* d_amp, const double* d_ph, int B,
+                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, double* d_out,
+                      cudaStream_t s) {
   if (B <= 0) return;
-  dim3 grid((unsigned)((h.M + 127) / 128), (unsigned)B);
-  k_het_waves<<<grid, 128, 0, s>>>(d_recs, g, h, d_amp, d_phase);
+  k_diff_full<<<B, 256, 0, s>>>(d_amp_ref, d_ph_ref, d_amp, d_ph, g, n, imin, m, d_S, sn_stride, d_out);
+}
+
+// het_space's ratios to the reference waveform (QuickCBC.c:4688-4702) for the wave sets
+// 1..nset-1 against set 0, bins [j0, j1) of n: Cs = 1 - Ap/Ar cos(Pr - Pp), Sn = Ap/Ar sin(Pr - Pp),
+// DH = Cs^2 + Sn^2, each [nset-1][nifo][j1-j0].
+__global__ void k_hs_ratios(const double* __restrict__ amp, const double* __restrict__ ph, int nset, int nifo, int n,
+                            int j0, int j1, double* __restrict__ Cs, double* __restrict__ Sn,
+                            double* __restrict__ DH) {
+  const int w = j1 - j0;
+  const long long total = (long long)(nset - 1) * nifo * w;
+  for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int jj = (int)(t % w);
+    const long long r = t / w;
+    const int id = (int)(r % nifo), i = (int)(r / nifo);
+    const int j = j0 + jj;
+    const double Ar = amp[(size_t)id * n + j], Pr = ph[(size_t)id * n + j];
+    const double Ap = amp[((size_t)(i + 1) * nifo + id) * n + j], Pp = ph[((size_t)(i + 1) * nifo + id) * n + j];
+    const double c = 1.0 - Ap / Ar * cos(Pr - Pp);
+    const double sv = Ap / Ar * sin(Pr - Pp);
+    Cs[t] = c;
+    Sn[t] = sv;
+    DH[t] = c * c + sv * sv;
+  }
+}
+
+void launch_hs_ratios(const double* d_amp, const double* d_ph, int nset, int nifo, int n, int j0, int j1,
+                      double* d_Cs, double* d_Sn, double* d_DH, cudaStream_t s) {
+  long long total = (long long)(nset - 1) * nifo * (j1 - j0);
+  if (total <= 0) return;
+  long long blocks = (total + 255) / 256;
+  if (blocks > 4736) blocks = 4736;
+  k_hs_ratios<<<(unsigned)blocks, 256, 0, s>>>(d_amp, d_ph, nset, nifo, n, j0, j1, d_Cs, d_Sn, d_DH);
 }
 
 // The slow-term quadrature of the heterodyne summary for one detector and the regions
@@ -1735,8 +1857,6 @@ void launch_het_diff(const double* d_amp, const double* d_phase, int npair, cons
 // Fisher_Het: one block per (matrix f, pair i <= j).  Central differences of the amplitude and
 // phase (wave sets 23 f + 1 + 2 i and 23 f + 2 + 2 i, step eps), then per detector the slow-term
 // quadrature of cc = 4 (dA_i dA_j + A^2 dphi_i dphi_j) / Aref^2 (QuickCBC.c:5503-5600).
-constexpr int kNP = 11;
-constexpr int kFisherSets = 2 * kNP + 1;
 __global__ void __launch_bounds__(256) k_het_fisher(const double* __restrict__ amp, const double* __restrict__ ph,
                                                     NetGeom g, HetData h, double eps, double* __restrict__ fish) {
   extern __shared__ double s_cc[];   // [M]

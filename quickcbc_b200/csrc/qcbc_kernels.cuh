@@ -87,6 +87,21 @@ size_t het_smem_bytes(const NetGeom& g, const HetData& h);
 // amp/phase [B][nifo][M]
 void launch_het_waves(const PhdRec* d_recs, int B, const NetGeom& g, const HetData& h, double* d_amp,
                       double* d_phase, cudaStream_t s);
+// fullphaseamp on any frequency list freq[0..M) for B records: amp/phase [B][nifo][M]
+void launch_waves(const PhdRec* d_recs, int B, const NetGeom& g, const double* d_freq, int M, double* d_amp,
+                  double* d_phase, cudaStream_t s);
+// Fisher_All (QuickCBC.c:2695-2817) from the 23 wave sets per matrix (layout of launch_het_fisher) on n
+// bins, PSD rows S [nifo][sn_stride], bins [imin, imax): upper triangle of d_fish[nmat][11][11]
+void launch_fisher_full(const double* d_amp, const double* d_phase, int nmat, const NetGeom& g, int n,
+                        const double* d_S, int sn_stride, int imin, int imax, double eps, double* d_fish,
+                        cudaStream_t s);
+// diff (QuickCBC.c:4913-4964) of B wave sets against one reference wave set, bins [imin, m) of n
+void launch_diff_full(const double* d_amp_ref, const double* d_ph_ref, const double* d_amp, const double* d_ph, int B,
+                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, double* d_out,
+                      cudaStream_t s);
+// het_space ratios Cs, Sn, DH (QuickCBC.c:4688-4702) of wave sets 1..nset-1 to set 0, bins [j0, j1)
+void launch_hs_ratios(const double* d_amp, const double* d_ph, int nset, int nifo, int n, int j0, int j1,
+                      double* d_Cs, double* d_Sn, double* d_DH, cudaStream_t s);
 // het_diff (QuickCBC.c:4966-5051) for npair pairs of wave sets (2p, 2p+1) -> d_out[npair]
 void launch_het_diff(const double* d_amp, const double* d_phase, int npair, const NetGeom& g, const HetData& h,
                      double* d_out, cudaStream_t s);

@@ -150,6 +150,15 @@ class Event:
             check(rc)
         return out
 
+    def het_space(self, params, pmin, pmax):
+        """Heterodyne grid search about params (het_space): returns (fgrid, MN, MM) for het_setup."""
+        M, MN, MM = C.c_int(), C.c_int(), C.c_int()
+        check(lib().qcbc_het_space(self._h, _ptr(_f64(params)), _ptr(_f64(pmin)), _ptr(_f64(pmax)), C.byref(M),
+                                   C.byref(MN), C.byref(MM)))
+        g = np.zeros(M.value, dtype=np.int32)
+        check(lib().qcbc_het_space_grid(self._h, g.ctypes.data_as(C.POINTER(C.c_int))))
+        return g, MN.value, MM.value
+
     def het_diff(self, params_a, params_b):
         """Heterodyned squared distance between the templates of paired rows (het_diff)."""
         A, Bp = _f64(np.atleast_2d(params_a)), _f64(np.atleast_2d(params_b))
@@ -386,6 +395,25 @@ def log_likelihood_full(labels, GMST, D, params, freq, SN, N, Tobs, bind=False):
     p = _f64(params).copy()
     L = lib().log_likelihood_full(nh.ref, Dr, _ptr(p), C.byref(rv), Sr, _ptr(rho), N, Tobs)
     return L, rho[: len(nh.labels)]
+
+
+def het_space(labels, GMST, Tobs, params, pmin, pmax, freq, SN, N):
+    """het_space (QuickCBC.c:4570) through the drop-in symbol: (fgrid, MN, MM, J, NR)."""
+    nh = _NetHolder(labels, Tobs, GMST)
+    SN = _f64(SN)
+    f, rv = _rv(freq)
+    het = _lib.Het()
+    lib().het_space(nh.ref, C.byref(het), _ptr(_f64(params).copy()), _ptr(_f64(pmin).copy()),
+                    _ptr(_f64(pmax).copy()), C.byref(rv), _rows(SN), N, Tobs)
+    if not het.fgrid:
+        raise QcbcError(-1, _lib.last_error())
+    g = np.array([het.fgrid[i] for i in range(het.M)], dtype=np.int32)
+    libc = C.CDLL(None)
+    libc.free.argtypes = [C.c_void_p]
+    libc.free(C.cast(het.freq.contents.data, C.c_void_p))
+    libc.free(C.cast(het.freq, C.c_void_p))
+    libc.free(C.cast(het.fgrid, C.c_void_p))
+    return g, het.MN, het.MM, het.J, het.NR
 
 
 class LegacyHet:
