@@ -228,21 +228,85 @@ def bench_cfg1_percall(q, eng, _lib):
             "value": steps * 16 / dt, "unit": "lnL evals/s", "us_per_call": 1e6 * dt / (steps * 16)}
 
 
+def prior_box(Tobs):
+    """MCMC_all's prior box (QuickCBC.c:1871-1896, ConstCBC.h:48-57)."""
+    from quickcbc_b200 import synth
+    M, PC = synth.MSUN_SI, synth.PC_SI
+    pmin = np.array([np.log(0.5 * M), np.log(0.5 * M), -0.85, -0.85, 0.0, max(Tobs - 3.5, 1.5),
+                     np.log(1e6 * PC), 0.0, -1.0, 0.0, -1.0])
+    pmax = np.array([np.log(160 * M), np.log(300 * M), 0.85, 0.85, 2 * np.pi, Tobs - 0.5,
+                     np.log(1e10 * PC), 2 * np.pi, 1.0, np.pi, 1.0])
+    return pmin, pmax
+
+
+def reference_het_space_child():
+    """Child process: the reference's het_space + heterodyne (oracle/_ref) on config 3; prints
+    the wall seconds as JSON.  Runs apart from the GPU process because the reference's
+    het_space reads its grid after freeing it (QuickCBC.c:4866-4893)."""
+    import tempfile
+    from oracle import ora, ref
+    from quickcbc_b200 import synth
+
+    def tmpl(info, p):
+        return ora.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    ev = synth.config_event(3, tmpl)
+    pmin, pmax = prior_box(ev.Tobs)
+    net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+    S = ev.SN.copy()
+    S[:, int(16.0 * ev.Tobs):int(ev.fmin * ev.Tobs)] = np.inf   # reference built with fmin = 16 Hz
+    het = ref.RefHet(net)
+    with tempfile.TemporaryDirectory() as d:
+        t0 = time.perf_counter()
+        het.space(ev.inj, pmin, pmax, ev.freq, S, ev.N, ev.Tobs, d)
+        het.heterodyne(ev.D, ev.inj, ev.freq, S, ev.N, ev.Tobs)
+        dt = time.perf_counter() - t0
+    print(json.dumps({"seconds": dt, "M": het.sizes()["M"]}))
+
+
+def reference_het_space_seconds():
+    """Wall time of the reference's het_space + heterodyne on this host (child process), or the
+    reason it is missing.  glibc's mmap threshold is raised in the child so that the grid the
+    reference frees stays mapped when it reads it back."""
+    try:
+        from oracle import ref
+        if not ref.available():
+            return {"unavailable": "oracle/_ref not built"}
+        env = dict(os.environ, MALLOC_MMAP_THRESHOLD_=str(1 << 30))
+        r = subprocess.run([sys.executable, os.path.abspath(__file__), "--ref-het-space-child"], env=env,
+                           capture_output=True, text=True, timeout=300)
+        lines = [x for x in r.stdout.splitlines() if x.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": f"reference het_space exited with {r.returncode}"}
+        return json.loads(lines[-1])
+    except Exception as exc:
+        return {"unavailable": f"{type(exc).__name__}: {exc}"}
+
+
 def bench_cfg3_het(q):
-    """Config 3: 3 det, 128 s, 4096 Hz BNS; heterodyned lnL on the reference's het_space grid
-    (tests/golden/grid3.npz) for 4096 sets, and the full lnL for 512 sets."""
+    """Config 3: 3 det, 128 s, 4096 Hz BNS; heterodyne grid search and tables on the GPU
+    (het_space + heterodyne, the analysis-admission latency), then the heterodyned lnL for
+    4096 sets and the full lnL for 512 sets."""
     from quickcbc_b200 import synth
 
     def tmpl(info, p):
         return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
-    g = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
+    g3 = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
     ev = synth.config_event(3, tmpl)
     e = q.Event.from_synthetic(ev)
-    e.het_setup(ev.inj, g["fgrid"], int(g["MN"]), int(g["MM"]), int(g["J"]))
+    pmin, pmax = prior_box(ev.Tobs)
+    e.het_space(ev.inj, pmin, pmax)                       # warm-up
+    t0 = time.perf_counter()
+    fgrid, MN, MM = e.het_space(ev.inj, pmin, pmax)
+    t1 = time.perf_counter()
+    e.het_setup(ev.inj, fgrid, MN, MM, 2)
+    t2 = time.perf_counter()
     P = synth.jitter_params(np.random.default_rng(3000 + 500000), 4096, ev.inj, scale=1e-6)
     dP = q.DeviceBuffer(P.nbytes)
     dP.upload(P)
-    out = {"workload": "config 3: 3 det, 128 s, 4096 Hz, BNS 1.45+1.30, het grid M=%d" % len(g["fgrid"])}
+    out = {"workload": "config 3: 3 det, 128 s, 4096 Hz, BNS 1.45+1.30, het grid M=%d" % len(fgrid),
+           "het_space_s": t1 - t0, "heterodyne_s": t2 - t1,
+           "grid_equals_reference": bool(np.array_equal(fgrid, g3["fgrid"])),
+           "reference_het_space_heterodyne": reference_het_space_seconds()}
     Lh64 = e.lnl_het(P, q.FP64)
     Lhm = e.lnl_het(P, q.MIXED)
     for prec, name in ((q.MIXED, "het_mixed"), (q.FP64, "het_fp64")):
@@ -355,8 +419,11 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--ref-het-space-child", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.ref_het_space_child:
+        return reference_het_space_child()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.profile:

@@ -311,12 +311,18 @@ int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin
   const int imin_d = (in.fmin > fs) ? (int)(Tobs * in.fmin) : (int)(Tobs * fs);
   double* trial_a = d_amp + (size_t)nifo * M;        // one trial set after the reference waves
   double* trial_p = d_ph + (size_t)nifo * M;
+  constexpr int kChunks = 148;
+  double* d_part;
+  HS_CU(sc.alloc(&d_part, (size_t)kChunks));
   auto diff = [&](const double* px, double& z) -> int {
     if ((rc = waves(px, 1, M, trial_a, trial_p))) return rc;
-    launch_diff_full(d_amp, d_ph, trial_a, trial_p, 1, g, M, imin_d, M, d_S, ss, d_out, s);
+    launch_diff_full(d_amp, d_ph, trial_a, trial_p, 1, g, M, imin_d, M, d_S, ss, kChunks, d_part, s);
     launches += 1;
-    HS_CU(cudaMemcpyAsync(&z, d_out, sizeof(double), cudaMemcpyDeviceToHost, s));
+    double part[kChunks];
+    HS_CU(cudaMemcpyAsync(part, d_part, sizeof(part), cudaMemcpyDeviceToHost, s));
     HS_CU(cudaStreamSynchronize(s));
+    z = 0.0;
+    for (int c = 0; c < kChunks; c++) z += part[c];
     return 0;
   };
   {
@@ -355,7 +361,7 @@ int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin
     }
   }
 
-  // ---- grid walk (QuickCBC.c:4624-4765)
+  // ---- grid walk (QuickCBC.c:4624-4765): the 12 sets' waves, their ratios and the walk on the device
   std::vector<double> P((size_t)(NP + 1) * NP);
   memcpy(P.data(), params, NP * sizeof(double));
   for (int i = 0; i < NP; ++i) {
@@ -364,48 +370,26 @@ int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin
     step_point(params, 1.0, e, pmin, pmax, &P[(size_t)(1 + i) * NP]);
   }
   if ((rc = waves(P.data(), NP + 1, MM, d_amp, d_ph))) return rc;
-  const int W = MM - MN;
-  const size_t per = (size_t)NP * nifo * W;
-  double *d_Cs, *d_Sn, *d_DH;
-  HS_CU(sc.alloc(&d_Cs, per));
-  HS_CU(sc.alloc(&d_Sn, per));
-  HS_CU(sc.alloc(&d_DH, per));
+  const int W = MM - MN, per = NP * nifo;
+  double *d_Cs, *d_Sn, *d_DH, *d_ratio;
+  int *d_grid, *d_count;
+  HS_CU(sc.alloc(&d_Cs, (size_t)per * W));
+  HS_CU(sc.alloc(&d_Sn, (size_t)per * W));
+  HS_CU(sc.alloc(&d_DH, (size_t)per * W));
+  HS_CU(sc.alloc(&d_ratio, ratio.size()));
+  HS_CU(sc.alloc(&d_grid, (size_t)W + 2));
+  HS_CU(sc.alloc(&d_count, 1));
+  HS_CU(cudaMemcpyAsync(d_ratio, ratio.data(), sizeof(double) * ratio.size(), cudaMemcpyHostToDevice, s));
   launch_hs_ratios(d_amp, d_ph, NP + 1, nifo, MM, MN, MM, d_Cs, d_Sn, d_DH, s);
-  launches += 1;
-  std::vector<double> Cs(per), Sn(per), DH(per);
-  HS_CU(cudaMemcpyAsync(Cs.data(), d_Cs, sizeof(double) * per, cudaMemcpyDeviceToHost, s));
-  HS_CU(cudaMemcpyAsync(Sn.data(), d_Sn, sizeof(double) * per, cudaMemcpyDeviceToHost, s));
-  HS_CU(cudaMemcpyAsync(DH.data(), d_DH, sizeof(double) * per, cudaMemcpyDeviceToHost, s));
-  HS_CU(cudaStreamSynchronize(s));
-  auto at = [&](const std::vector<double>& v, int i, int id, int j) { return v[((size_t)i * nifo + id) * W + (j - MN)]; };
-
   const int djmax = (int)(100.0 * Tobs);                 // maximum spacing
-  std::vector<int> fgrid;
-  int jmin = MN;
-  fgrid.push_back(jmin);
-  for (int j = MN; j < MM; j++) {
-    bool flag = false;
-    double tl = tol * ratio[j];                          // tolerance scaled by the SNR contribution
-    if (tl < tol) tl = tol;
-    for (int id = 0; id < nifo; id++)
-      for (int i = 0; i < NP; i++) {
-        const int jmid = (j + jmin) / 2;                 // linear interpolation at the mid-point
-        const double cmid = (at(Cs, i, id, jmin) * (double)(j - jmid) + at(Cs, i, id, j) * (double)(jmid - jmin)) /
-                            (double)(j - jmin);
-        const double smid = (at(Sn, i, id, jmin) * (double)(j - jmid) + at(Sn, i, id, j) * (double)(jmid - jmin)) /
-                            (double)(j - jmin);
-        const double dmid = (at(DH, i, id, jmin) * (double)(j - jmid) + at(DH, i, id, j) * (double)(jmid - jmin)) /
-                            (double)(j - jmin);
-        if (fabs(at(Cs, i, id, jmid) - cmid) > tl || fabs(at(Sn, i, id, jmid) - smid) > tl ||
-            fabs(at(DH, i, id, jmid) - dmid) > tl)
-          flag = true;
-      }
-    if ((j - jmin) > djmax) flag = true;
-    if (flag) {
-      jmin = j;
-      fgrid.push_back(jmin);
-    }
-  }
+  launch_hs_walk(d_Cs, d_Sn, d_DH, d_ratio, per, MN, MM, djmax, tol, W + 2, d_grid, d_count, s);
+  launches += 2;
+  int count = 0;
+  HS_CU(cudaMemcpyAsync(&count, d_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+  HS_CU(cudaStreamSynchronize(s));
+  if (count < 1) { err = "het_space: grid walk did not finish"; return -2; }
+  std::vector<int> fgrid((size_t)count);
+  HS_CU(cudaMemcpy(fgrid.data(), d_grid, sizeof(int) * count, cudaMemcpyDeviceToHost));
   const int Mr = (int)fgrid.size() - 1;
 
   // ---- spacing per bin and the flattened grid with J = 2 points per region (QuickCBC.c:4767-4864)

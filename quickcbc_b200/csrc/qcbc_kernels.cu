@@ -1735,14 +1735,17 @@ void launch_fisher_full(const double* d_amp, const double* d_phase, int nmat, co
   k_fisher_full<<<grid, 256, 0, s>>>(d_amp, d_phase, g, n, d_S, sn_stride, imin, imax, eps, d_fish);
 }
 
-// diff (QuickCBC.c:4913-4964): out[b] = sum over detectors and bins j in [imin, m) of
-// 4 |h_ref - h_b|^2 / S, for the reference waves (one set) and B other wave sets on n bins.
+// diff (QuickCBC.c:4913-4964): partial sums over detectors and bins j in [imin, m) of
+// 4 |h_ref - h_b|^2 / S for the reference waves (one set) and B other wave sets on n bins; block
+// (c, b) covers chunk c of the bins of set b and writes out[b * gridDim.x + c].
 __global__ void __launch_bounds__(256) k_diff_full(const double* __restrict__ amp_ref, const double* __restrict__ ph_ref,
                                                    const double* __restrict__ amp, const double* __restrict__ ph,
                                                    NetGeom g, int n, int imin, int m, const double* __restrict__ S,
                                                    int sn_stride, double* __restrict__ out) {
   __shared__ double red[32];
-  const int b = blockIdx.x, nifo = g.nifo;
+  const int b = blockIdx.y, nifo = g.nifo;
+  const int span = (m - imin + gridDim.x - 1) / gridDim.x;
+  const int j0 = imin + blockIdx.x * span, j1 = min(m, j0 + span);
   double acc[1] = {0.0};
   for (int id = 0; id < nifo; id++) {
     const double* Ar = amp_ref + (size_t)id * n;
@@ -1750,37 +1753,37 @@ __global__ void __launch_bounds__(256) k_diff_full(const double* __restrict__ am
     const double* Ap = amp + ((size_t)b * nifo + id) * n;
     const double* Pp = ph + ((size_t)b * nifo + id) * n;
     const double* Sd = S + (size_t)id * sn_stride;
-    for (int j = imin + threadIdx.x; j < m; j += blockDim.x) {
+    for (int j = j0 + threadIdx.x; j < j1; j += blockDim.x) {
       const double d = Pr[j] - Pp[j];
       const double re = Ar[j] - Ap[j] * cos(d), im = Ap[j] * sin(d);
       acc[0] += 4.0 * (re * re + im * im) / Sd[j];
     }
   }
   block_sum<1>(acc, red);
-  if (threadIdx.x == 0) out[b] = acc[0];
+  if (threadIdx.x == 0) out[(size_t)b * gridDim.x + blockIdx.x] = acc[0];
 }
 
 void launch_diff_full(const double* d_amp_ref, const double* d_ph_ref, const double* d_amp, const double* d_ph, int B,
-                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, double* d_out,
-                      cudaStream_t s) {
-  if (B <= 0) return;
-  k_diff_full<<<B, 256, 0, s>>>(d_amp_ref, d_ph_ref, d_amp, d_ph, g, n, imin, m, d_S, sn_stride, d_out);
+                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, int chunks,
+                      double* d_out, cudaStream_t s) {
+  if (B <= 0 || chunks <= 0) return;
+  dim3 grid((unsigned)chunks, (unsigned)B);
+  k_diff_full<<<grid, 256, 0, s>>>(d_amp_ref, d_ph_ref, d_amp, d_ph, g, n, imin, m, d_S, sn_stride, d_out);
 }
 
 // het_space's ratios to the reference waveform (QuickCBC.c:4688-4702) for the wave sets
 // 1..nset-1 against set 0, bins [j0, j1) of n: Cs = 1 - Ap/Ar cos(Pr - Pp), Sn = Ap/Ar sin(Pr - Pp),
-// DH = Cs^2 + Sn^2, each [nset-1][nifo][j1-j0].
+// DH = Cs^2 + Sn^2, each [j1-j0][nset-1][nifo] (bin-major, as the grid walk reads them).
 __global__ void k_hs_ratios(const double* __restrict__ amp, const double* __restrict__ ph, int nset, int nifo, int n,
                             int j0, int j1, double* __restrict__ Cs, double* __restrict__ Sn,
                             double* __restrict__ DH) {
-  const int w = j1 - j0;
-  const long long total = (long long)(nset - 1) * nifo * w;
+  const int per = (nset - 1) * nifo;
+  const long long total = (long long)per * (j1 - j0);
   for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
        t += (long long)gridDim.x * blockDim.x) {
-    const int jj = (int)(t % w);
-    const long long r = t / w;
-    const int id = (int)(r % nifo), i = (int)(r / nifo);
-    const int j = j0 + jj;
+    const int r = (int)(t % per);
+    const int j = j0 + (int)(t / per);
+    const int id = r % nifo, i = r / nifo;
     const double Ar = amp[(size_t)id * n + j], Pr = ph[(size_t)id * n + j];
     const double Ap = amp[((size_t)(i + 1) * nifo + id) * n + j], Pp = ph[((size_t)(i + 1) * nifo + id) * n + j];
     const double c = 1.0 - Ap / Ar * cos(Pr - Pp);
@@ -1798,6 +1801,64 @@ void launch_hs_ratios(const double* d_amp, const double* d_ph, int nset, int nif
   long long blocks = (total + 255) / 256;
   if (blocks > 4736) blocks = 4736;
   k_hs_ratios<<<(unsigned)blocks, 256, 0, s>>>(d_amp, d_ph, nset, nifo, n, j0, j1, d_Cs, d_Sn, d_DH);
+}
+
+// het_space's grid walk (QuickCBC.c:4720-4765) in one block: from the current grid point jmin,
+// the next one is the first bin j > jmin at which the linear interpolation between jmin and j of
+// any ratio (Cs, Sn, DH of any direction and detector) misses its value at the mid-point by more
+// than tl = max(tol ratio[j], tol), or at which j - jmin exceeds djmax.  The block tests 1024
+// consecutive bins at a time and keeps the first hit.  grid[0..*count) gets the points; the walk
+// stops at the cap (*count = -1 then).
+__global__ void __launch_bounds__(1024) k_hs_walk(const double* __restrict__ Cs, const double* __restrict__ Sn,
+                                                  const double* __restrict__ DH, const double* __restrict__ ratio,
+                                                  int per, int MN, int MM, int djmax, double tol, int cap,
+                                                  int* __restrict__ grid, int* __restrict__ count) {
+  __shared__ int s_first;
+  int jmin = MN, nout = 0;
+  if (threadIdx.x == 0) grid[nout] = jmin;
+  nout++;
+  for (;;) {
+    int found = MM;
+    for (int base = jmin + 1; base < MM && found == MM; base += blockDim.x) {
+      if (threadIdx.x == 0) s_first = MM;
+      __syncthreads();
+      const int j = base + threadIdx.x;
+      bool flag = false;
+      if (j < MM) {
+        double tl = tol * ratio[j];
+        if (tl < tol) tl = tol;
+        const int jmid = (j + jmin) / 2;
+        const double w0 = (double)(j - jmid), w1 = (double)(jmid - jmin), dw = (double)(j - jmin);
+        const size_t oa = (size_t)(jmin - MN) * per, ob = (size_t)(j - MN) * per, om = (size_t)(jmid - MN) * per;
+        for (int r = 0; r < per && !flag; r++) {
+          const double cmid = (Cs[oa + r] * w0 + Cs[ob + r] * w1) / dw;
+          const double smid = (Sn[oa + r] * w0 + Sn[ob + r] * w1) / dw;
+          const double dmid = (DH[oa + r] * w0 + DH[ob + r] * w1) / dw;
+          if (fabs(Cs[om + r] - cmid) > tl || fabs(Sn[om + r] - smid) > tl || fabs(DH[om + r] - dmid) > tl)
+            flag = true;
+        }
+        if (j - jmin > djmax) flag = true;
+      }
+      if (flag) atomicMin(&s_first, j);
+      __syncthreads();
+      found = s_first;
+      __syncthreads();
+    }
+    if (found >= MM) break;
+    jmin = found;
+    if (nout >= cap) {
+      if (threadIdx.x == 0) *count = -1;
+      return;
+    }
+    if (threadIdx.x == 0) grid[nout] = jmin;
+    nout++;
+  }
+  if (threadIdx.x == 0) *count = nout;
+}
+
+void launch_hs_walk(const double* d_Cs, const double* d_Sn, const double* d_DH, const double* d_ratio, int per, int MN,
+                    int MM, int djmax, double tol, int cap, int* d_grid, int* d_count, cudaStream_t s) {
+  k_hs_walk<<<1, 1024, 0, s>>>(d_Cs, d_Sn, d_DH, d_ratio, per, MN, MM, djmax, tol, cap, d_grid, d_count);
 }
 
 // The slow-term quadrature of the heterodyne summary for one detector and the regions

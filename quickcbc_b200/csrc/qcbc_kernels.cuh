@@ -95,13 +95,19 @@ void launch_waves(const PhdRec* d_recs, int B, const NetGeom& g, const double* d
 void launch_fisher_full(const double* d_amp, const double* d_phase, int nmat, const NetGeom& g, int n,
                         const double* d_S, int sn_stride, int imin, int imax, double eps, double* d_fish,
                         cudaStream_t s);
-// diff (QuickCBC.c:4913-4964) of B wave sets against one reference wave set, bins [imin, m) of n
+// diff (QuickCBC.c:4913-4964) of B wave sets against one reference wave set, bins [imin, m) of n,
+// as `chunks` partial sums per set: d_out[B][chunks] (sum them in order)
 void launch_diff_full(const double* d_amp_ref, const double* d_ph_ref, const double* d_amp, const double* d_ph, int B,
-                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, double* d_out,
-                      cudaStream_t s);
-// het_space ratios Cs, Sn, DH (QuickCBC.c:4688-4702) of wave sets 1..nset-1 to set 0, bins [j0, j1)
+                      const NetGeom& g, int n, int imin, int m, const double* d_S, int sn_stride, int chunks,
+                      double* d_out, cudaStream_t s);
+// het_space ratios Cs, Sn, DH (QuickCBC.c:4688-4702) of wave sets 1..nset-1 to set 0, bins [j0, j1),
+// bin-major [j1-j0][nset-1][nifo]
 void launch_hs_ratios(const double* d_amp, const double* d_ph, int nset, int nifo, int n, int j0, int j1,
                       double* d_Cs, double* d_Sn, double* d_DH, cudaStream_t s);
+// het_space grid walk (QuickCBC.c:4720-4765) over the ratios (per = (nset-1) nifo values per bin) and
+// the per-bin tolerance scale ratio[j]: d_grid[0..*d_count) (count -1 when it would exceed cap)
+void launch_hs_walk(const double* d_Cs, const double* d_Sn, const double* d_DH, const double* d_ratio, int per, int MN,
+                    int MM, int djmax, double tol, int cap, int* d_grid, int* d_count, cudaStream_t s);
 // het_diff (QuickCBC.c:4966-5051) for npair pairs of wave sets (2p, 2p+1) -> d_out[npair]
 void launch_het_diff(const double* d_amp, const double* d_phase, int npair, const NetGeom& g, const HetData& h,
                      double* d_out, cudaStream_t s);
