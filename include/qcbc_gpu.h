@@ -110,6 +110,12 @@ int qcbc_batch_autotune(qcbc_batch* batch, const int* event_of, const double* pa
 /* event_of[B] indexes the batch's events; rho is [B][3] (unused detectors 0) or NULL. */
 int qcbc_lnl_multi(qcbc_batch* batch, const int* event_of, const double* params, int B, double* lnl, double* rho,
                    int precision);
+/* Heterodyned lnL (log_likelihood_het, QuickCBC.c:5303) of sets of many events: each set uses
+ * the heterodyne tables its event had when its slot was set (qcbc_het_setup / qcbc_het_set
+ * before qcbc_batch_set_slot; set the slot again after re-heterodyning).  Sets whose event has
+ * no tables get lnL = -1e20 and the call returns QCBC_EDOM. */
+int qcbc_lnl_multi_het(qcbc_batch* batch, const int* event_of, const double* params, int B, double* lnl,
+                       int precision);
 /* Device time of `iters` graph launches on inputs already uploaded by a previous
  * qcbc_lnl_multi call with the same B (no host copies inside the timed span). */
 int qcbc_time_lnl_multi(qcbc_batch* batch, int B, int precision, int iters, int flush_l2, float* ms);

@@ -47,7 +47,14 @@ typedef struct {
   int n_temps, n_chains, n_steps, burn_in, thin;
   double ladder;            /* temperature ratio (1.15 in ConstCBC.h:44) */
   unsigned long long seed;
+  int likelihood;           /* QCBC_LNL_FULL, or QCBC_LNL_HET: at admission the heterodyne grid search
+                               and tables are built about `start` (het_space + heterodyne,
+                               QuickCBC.c:4570, 5112) and every step uses the heterodyned lnL
+                               (log_likelihood_het, QuickCBC.c:5303), as the reference's sampler does */
 } qcbc_run_spec;
+
+#define QCBC_LNL_FULL 0
+#define QCBC_LNL_HET 1
 
 #define QCBC_RUN_QUEUED 0
 #define QCBC_RUN_LIVE 1

@@ -100,6 +100,7 @@ def lib():
         L.qcbc_het_fisher.argtypes = [vp, _PD, i, _PD]
         L.qcbc_het_space.argtypes = [vp, _PD, _PD, _PD, pi, pi, pi]
         L.qcbc_het_space_grid.argtypes = [vp, pi]
+        L.qcbc_lnl_multi_het.argtypes = [vp, pi, _PD, i, _PD, i]
         L.qcbc_lnl_het_dev.argtypes = [vp, vp, i, vp, i, vp]
         L.qcbc_set_full_launch.argtypes = [vp, i, i]
         L.qcbc_get_full_launch.argtypes = [vp, i, i, pi, pi]

@@ -1043,10 +1043,28 @@ struct MultiGraph {
   cudaGraphExec_t exec_full = nullptr, exec_dev = nullptr;
 };
 
+// Scratch of the heterodyned multi-event path (grown on demand).
+struct HetMultiScratch {
+  int cap = 0;
+  double* d_params = nullptr; int* d_eof = nullptr; PhdRec* d_recs = nullptr; int* d_status = nullptr;
+  int* d_ntile = nullptr; double* d_lnl = nullptr;
+  double* h_params = nullptr; int* h_eof = nullptr; double* h_lnl = nullptr; int* h_status = nullptr;
+};
+
+static void free_het_scratch(HetMultiScratch& h) {
+  cudaFree(h.d_params); cudaFree(h.d_eof); cudaFree(h.d_recs); cudaFree(h.d_status); cudaFree(h.d_ntile);
+  cudaFree(h.d_lnl);
+  cudaFreeHost(h.h_params); cudaFreeHost(h.h_eof); cudaFreeHost(h.h_lnl); cudaFreeHost(h.h_status);
+  h = HetMultiScratch();
+}
+
 struct qcbc_batch {
   int device = 0;
   std::vector<qcbc_event*> events;
   EventDesc* d_events = nullptr;
+  HetData* d_het = nullptr;            // per slot: the event's heterodyne tables (M = 0: none)
+  std::vector<size_t> het_smem;        // per slot: shared memory of its heterodyned lnL
+  HetMultiScratch hs;
   int nh_max = 0;
   int tile_bins = 2048, threads = 256;
   cudaStream_t stream = nullptr;
@@ -1077,14 +1095,20 @@ extern "C" qcbc_batch* qcbc_batch_create_slots(int capacity, int max_bins) {
   bt->device = current_device();
   bt->nh_max = max_bins;
   bt->events.assign(capacity, nullptr);
+  bt->het_smem.assign(capacity, 0);
   std::vector<EventDesc> h(capacity);
   memset(h.data(), 0, sizeof(EventDesc) * capacity);   // nifo = 0 marks an empty slot
+  std::vector<HetData> hh(capacity);
+  memset(hh.data(), 0, sizeof(HetData) * capacity);
   if (cudaMalloc(&bt->d_events, sizeof(EventDesc) * capacity) != cudaSuccess ||
       cudaMemcpy(bt->d_events, h.data(), sizeof(EventDesc) * capacity, cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMalloc(&bt->d_het, sizeof(HetData) * capacity) != cudaSuccess ||
+      cudaMemcpy(bt->d_het, hh.data(), sizeof(HetData) * capacity, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaStreamCreateWithFlags(&bt->stream, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&bt->e0) != cudaSuccess || cudaEventCreate(&bt->e1) != cudaSuccess) {
     fail(QCBC_ECUDA, "batch allocation failed");
     cudaFree(bt->d_events);
+    cudaFree(bt->d_het);
     delete bt;
     return nullptr;
   }
@@ -1099,16 +1123,25 @@ extern "C" int qcbc_batch_set_slot(qcbc_batch* bt, int slot, qcbc_event* ev) {
   if (!bt || slot < 0 || slot >= (int)bt->events.size()) return fail(QCBC_EINVAL, "bad batch or slot");
   EventDesc d;
   memset(&d, 0, sizeof(d));
+  HetData hd;
+  memset(&hd, 0, sizeof(hd));
+  size_t smem = 0;
   if (ev) {
     if (!ev->has_data || ev->device != bt->device) return fail(QCBC_EINVAL, "event has no data or another device");
     if (ev->nh > bt->nh_max) return fail(QCBC_EINVAL, "event has %d bins, batch holds at most %d", ev->nh, bt->nh_max);
     d.g = ev->g;
     d.ev = event_data(ev);
+    if (ev->het.buf) {               // tables as of now; set the slot again after a re-heterodyne
+      hd = het_data(ev);
+      smem = het_smem_bytes(ev->g, hd);
+    }
   }
   std::lock_guard<std::mutex> lk(bt->mu);
   CU(cudaMemcpyAsync(bt->d_events + slot, &d, sizeof(d), cudaMemcpyHostToDevice, bt->stream));
+  CU(cudaMemcpyAsync(bt->d_het + slot, &hd, sizeof(hd), cudaMemcpyHostToDevice, bt->stream));
   CU(cudaStreamSynchronize(bt->stream));
   bt->events[slot] = ev;
+  bt->het_smem[slot] = smem;
   return QCBC_OK;
 }
 
@@ -1140,6 +1173,8 @@ extern "C" int qcbc_batch_destroy(qcbc_batch* bt) {
     bt->graphs.clear();
   }
   cudaFree(bt->d_events);
+  cudaFree(bt->d_het);
+  free_het_scratch(bt->hs);
   cudaFree(bt->d_flush);
   cudaEventDestroy(bt->e0);
   cudaEventDestroy(bt->e1);
@@ -1265,6 +1300,53 @@ extern "C" int qcbc_lnl_multi(qcbc_batch* bt, const int* event_of, const double*
   if (dev != bt->device) return fail(QCBC_EINVAL, "batch lives on device %d, %d is current", bt->device, dev);
   std::lock_guard<std::mutex> lk(bt->mu);
   return run_multi(bt, event_of, params, B, lnl, rho, precision);
+}
+
+extern "C" int qcbc_lnl_multi_het(qcbc_batch* bt, const int* event_of, const double* params, int B, double* lnl,
+                                  int precision) {
+  if (!bt || !event_of || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  std::lock_guard<std::mutex> lk(bt->mu);
+  HetMultiScratch& h = bt->hs;
+  if (B > h.cap) {
+    free_het_scratch(h);
+    const size_t n = (size_t)B;
+    CU(cudaMalloc(&h.d_params, n * 11 * sizeof(double)));
+    CU(cudaMalloc(&h.d_eof, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_recs, n * sizeof(PhdRec)));
+    CU(cudaMalloc(&h.d_status, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_ntile, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_lnl, n * sizeof(double)));
+    CU(cudaMallocHost(&h.h_params, n * 11 * sizeof(double)));
+    CU(cudaMallocHost(&h.h_eof, n * sizeof(int)));
+    CU(cudaMallocHost(&h.h_lnl, n * sizeof(double)));
+    CU(cudaMallocHost(&h.h_status, n * sizeof(int)));
+    h.cap = B;
+  }
+  size_t smem = 0;
+  for (size_t k = 0; k < bt->het_smem.size(); k++) smem = std::max(smem, bt->het_smem[k]);
+  memcpy(h.h_params, params, sizeof(double) * 11 * (size_t)B);
+  memcpy(h.h_eof, event_of, sizeof(int) * (size_t)B);
+  cudaStream_t s = bt->stream;
+  CU(cudaMemcpyAsync(h.d_params, h.h_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(h.d_eof, h.h_eof, sizeof(int) * (size_t)B, cudaMemcpyHostToDevice, s));
+  DeviceState& ds = g_dev[current_device()];
+  launch_setup_multi(h.d_params, h.d_eof, B, bt->d_events, (int)bt->events.size(), ds.qnm, bt->tile_bins, h.d_recs,
+                     h.d_status, h.d_ntile, s);
+  launch_lnl_het_multi(h.d_recs, h.d_status, B, bt->d_events, bt->d_het, smem,
+                       precision == QCBC_MIXED ? kMixed : kFP64, h.d_lnl, s);
+  tls_launches += 2;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(h.h_lnl, h.d_lnl, sizeof(double) * (size_t)B, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(h.h_status, h.d_status, sizeof(int) * (size_t)B, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  memcpy(lnl, h.h_lnl, sizeof(double) * (size_t)B);
+  int bad = 0;
+  for (int b = 0; b < B; b++) bad += h.h_status[b] != 0 || h.h_lnl[b] <= -1.0e19;
+  if (bad) return fail(QCBC_EDOM, "%d of %d sets without a valid event, heterodyne tables or waveform (lnL=-1e20)",
+                       bad, B);
+  return QCBC_OK;
 }
 
 extern "C" int qcbc_time_lnl_multi(qcbc_batch* bt, int B, int precision, int iters, int flush, float* ms) {

@@ -1457,23 +1457,6 @@ void launch_lnl_multi(const PhdRec* d_recs, const EventDesc* d_events, const int
   }
 }
 
-// Lets the kernels whose rotation tables live in dynamic shared memory use up to the device's
-// opt-in limit (long tiles).  Set once per device at initialisation, outside any stream capture.
-void allow_dynamic_smem() {
-  int dev = 0, optin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  auto allow = [&](const void* f) {
-    cudaFuncAttributes a;
-    if (cudaFuncGetAttributes(&a, f) == cudaSuccess)
-      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
-  };
-  allow((const void*)k_lnl_full_mixed<1>);
-  allow((const void*)k_lnl_full_mixed<2>);
-  allow((const void*)k_lnl_full_mixed<3>);
-  allow((const void*)k_lnl_multi<kFP64>);
-  allow((const void*)k_lnl_multi<kMixed>);
-}
 
 
 __global__ void k_finalize_multi(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
@@ -1524,25 +1507,11 @@ void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const
 // shared memory.  Phase 2: per region r, uu = IP[r] v for v in {cc, hc, hs},
 // contracted with SL / lc / ls and the edge over-count correction
 // (QuickCBC.c:5347-5425); block sum; lnL = logLb - sum (HR + HH/2).
+// Body of one heterodyned lnL for record c (shared memory: sm [3][nifo][M], red [32][4 kMaxIfo]);
+// thread 0 writes *out.
 template <int PREC>
-__global__ void __launch_bounds__(256) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
-                                                 NetGeom g, HetData h, double* __restrict__ lnl) {
-  extern __shared__ double sm[];
-  __shared__ PhdRec rec;
-  __shared__ double red[32 * 4 * kMaxIfo];
-  int b = blockIdx.x;
-  {
-    const int nw = sizeof(PhdRec) / 8;
-    const double* src = reinterpret_cast<const double*>(recs + b);
-    double* dst = reinterpret_cast<double*>(&rec);
-    for (int k = threadIdx.x; k < nw; k += blockDim.x) dst[k] = src[k];
-  }
-  __syncthreads();
-  const PhdRec& c = rec;
-  if (status[b] != kStOK) {
-    if (threadIdx.x == 0) lnl[b] = -1.0e20;
-    return;
-  }
+__device__ __forceinline__ void het_block(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm, double* red,
+                                          double* out) {
   const int M = h.M, nifo = g.nifo;
   double* s_hc = sm;                 // [nifo][M]
   double* s_hs = sm + nifo * M;
@@ -1627,11 +1596,54 @@ __global__ void __launch_bounds__(256) k_lnl_het(const PhdRec* __restrict__ recs
       double HH = acc[4 * id] - acc[4 * id + 2], HR = acc[4 * id + 1] - acc[4 * id + 3];
       L -= (HR + 0.5 * HH);
     }
-    lnl[b] = L;
+    *out = L;
   }
 }
 
+template <int PREC>
+__global__ void __launch_bounds__(256) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+                                                 NetGeom g, HetData h, double* __restrict__ lnl) {
+  extern __shared__ double sm[];
+  __shared__ PhdRec rec;
+  __shared__ double red[32 * 4 * kMaxIfo];
+  const int b = blockIdx.x;
+  load_record(rec, recs + b);
+  __syncthreads();
+  if (status[b] != kStOK) {
+    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+    return;
+  }
+  het_block<PREC>(rec, g, h, sm, red, lnl + b);
+}
+
+// Heterodyned lnL of sets of many events: set b uses the geometry and heterodyne tables of its
+// record's event (het[e].M == 0: the event has no tables, lnL = -1e20).
+template <int PREC>
+__global__ void __launch_bounds__(256) k_lnl_het_multi(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+                                                       const EventDesc* __restrict__ events,
+                                                       const HetData* __restrict__ het, double* __restrict__ lnl) {
+  extern __shared__ double sm[];
+  __shared__ PhdRec rec;
+  __shared__ double red[32 * 4 * kMaxIfo];
+  const int b = blockIdx.x;
+  load_record(rec, recs + b);
+  __syncthreads();
+  const int e = rec.event;
+  if (status[b] != kStOK || e < 0 || het[e].M == 0) {
+    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+    return;
+  }
+  het_block<PREC>(rec, events[e].g, het[e], sm, red, lnl + b);
+}
+
 size_t het_smem_bytes(const NetGeom& g, const HetData& h) { return (size_t)3 * g.nifo * h.M * sizeof(double); }
+
+void launch_lnl_het_multi(const PhdRec* d_recs, const int* d_status, int B, const EventDesc* d_events,
+                          const HetData* d_het, size_t smem, Precision prec, double* d_lnl, cudaStream_t s) {
+  if (B <= 0) return;
+  if (prec == kFP64) k_lnl_het_multi<kFP64><<<B, 128, smem, s>>>(d_recs, d_status, d_events, d_het, d_lnl);
+  else k_lnl_het_multi<kMixed><<<B, 128, smem, s>>>(d_recs, d_status, d_events, d_het, d_lnl);
+}
 
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, int threads, double* d_lnl, cudaStream_t s) {
@@ -2210,6 +2222,27 @@ __global__ void k_nwip(const double* __restrict__ a, const double* __restrict__ 
 void launch_nwip(const double* d_a, const double* d_b, const double* d_S, int imin, int imax, int N, double* d_out,
                  cudaStream_t s) {
   k_nwip<<<1, 1024, 0, s>>>(d_a, d_b, d_S, imin, imax, N, d_out);
+}
+
+// Lets the kernels with large dynamic shared memory (rotation tables of long tiles, heterodyne
+// grids) use up to the device's opt-in limit.  Set once per device at initialisation, outside
+// any stream capture.
+void allow_dynamic_smem() {
+  int dev = 0, optin = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  auto allow = [&](const void* f) {
+    cudaFuncAttributes a;
+    if (cudaFuncGetAttributes(&a, f) == cudaSuccess)
+      cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin - (int)a.sharedSizeBytes);
+  };
+  allow((const void*)k_lnl_full_mixed<1>);
+  allow((const void*)k_lnl_full_mixed<2>);
+  allow((const void*)k_lnl_full_mixed<3>);
+  allow((const void*)k_lnl_multi<kFP64>);
+  allow((const void*)k_lnl_multi<kMixed>);
+  allow((const void*)k_lnl_het_multi<kFP64>);
+  allow((const void*)k_lnl_het_multi<kMixed>);
 }
 
 }  // namespace qcbc

@@ -83,6 +83,10 @@ void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, int threads, double* d_lnl, cudaStream_t s);
 size_t het_smem_bytes(const NetGeom& g, const HetData& h);
+// heterodyned lnL of sets of many events (records from launch_setup_multi); d_het [n_events] (M = 0:
+// no tables); smem = the largest het_smem_bytes over the events
+void launch_lnl_het_multi(const PhdRec* d_recs, const int* d_status, int B, const EventDesc* d_events,
+                          const HetData* d_het, size_t smem, Precision prec, double* d_lnl, cudaStream_t s);
 // fullphaseamp on the heterodyne grid (QuickCBC.c:3850-3866) for B records:
 // amp/phase [B][nifo][M]
 void launch_het_waves(const PhdRec* d_recs, int B, const NetGeom& g, const HetData& h, double* d_amp,

@@ -1,6 +1,7 @@
 // Continuous-batching PT-MCMC service over the multi-event likelihood
 // (declared in include/qcbc_serve.h).  Host code only: every likelihood goes
-// through the public C ABI (qcbc_event_open, qcbc_batch_*, qcbc_lnl_multi).
+// through the public C ABI (qcbc_event_open, qcbc_batch_*, qcbc_lnl_multi,
+// qcbc_lnl_multi_het, qcbc_het_space, qcbc_het_setup).
 //
 // The sampler follows the reference's parallel-tempered scheme in outline
 // (QuickCBC.c:1781-2236 MCMC_all, 2238-2405 update): Metropolis updates at
@@ -83,6 +84,7 @@ struct Run {
   double start[11], sigma[11], pmin[11], pmax[11];
   int n_temps = 1, n_chains = 1, n_steps = 0, burn_in = 0, thin = 1;
   double ladder = 1.15;
+  int likelihood = QCBC_LNL_FULL;
   // live state
   qcbc_event* ev = nullptr;
   int slot = -1;
@@ -116,10 +118,9 @@ struct qcbc_server {
   long long next_id = 0;
   std::chrono::steady_clock::time_point t0;
   std::mutex mu;
-  // launch staging
-  std::vector<int> eo;
-  std::vector<double> params, out;
-  std::vector<std::pair<long long, int>> owner;  // (run, chain) per set
+  // launch staging: full and heterodyned sets
+  std::vector<int> eo, eo_h;
+  std::vector<double> params, out, params_h, out_h;
 };
 
 static double now_s(const qcbc_server* s) {
@@ -217,6 +218,11 @@ extern "C" long long qcbc_server_submit(qcbc_server* s, const qcbc_run_spec* sp)
   r->burn_in = sp->burn_in;
   r->thin = sp->thin;
   r->ladder = sp->ladder;
+  if (sp->likelihood != QCBC_LNL_FULL && sp->likelihood != QCBC_LNL_HET) {
+    delete r;
+    return sfail(QCBC_EINVAL, "likelihood %d", sp->likelihood);
+  }
+  r->likelihood = sp->likelihood;
   r->rng.seed(sp->seed);
   r->bytes = estimate_bytes(*r);
   std::lock_guard<std::mutex> lk(s->mu);
@@ -251,6 +257,16 @@ extern "C" int qcbc_server_cancel(qcbc_server* s, long long id) {
   return QCBC_OK;
 }
 
+// Heterodyne grid search and tables of a run's event about its starting point.
+static int het_tables(Run* r) {
+  int M = 0, MN = 0, MM = 0;
+  int rc = qcbc_het_space(r->ev, r->start, r->pmin, r->pmax, &M, &MN, &MM);
+  if (rc != QCBC_OK) return rc;
+  std::vector<int> grid(M);
+  if ((rc = qcbc_het_space_grid(r->ev, grid.data())) != QCBC_OK) return rc;
+  return qcbc_het_setup(r->ev, r->start, grid.data(), M, MN, MM, 2);
+}
+
 // Admit queued runs in arrival order while a slot and the budget allow.
 static void admit(qcbc_server* s) {
   while (!s->queue.empty()) {
@@ -263,6 +279,10 @@ static void admit(qcbc_server* s) {
     s->queue.pop_front();
     r->ev = qcbc_event_open(r->nifo, r->labels, r->Tobs, r->GMST, r->N, r->D.data(), r->N, r->SN.data(),
                             r->sn_stride, r->fmin, r->fmax);
+    if (r->ev && r->likelihood == QCBC_LNL_HET && het_tables(r) != QCBC_OK) {
+      qcbc_event_close(r->ev);
+      r->ev = nullptr;
+    }
     if (!r->ev || qcbc_batch_set_slot(s->batch, slot, r->ev) != QCBC_OK) {
       if (r->ev) qcbc_event_close(r->ev);
       r->ev = nullptr;
@@ -320,10 +340,14 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
   double t0 = now_s(s);
   s->eo.clear();
   s->params.clear();
-  s->owner.clear();
+  s->eo_h.clear();
+  s->params_h.clear();
   // proposals (or the starting points of newly admitted runs)
   for (long long id : s->live) {
     Run* r = s->runs[id];
+    const bool het = r->likelihood == QCBC_LNL_HET;
+    std::vector<int>& eo = het ? s->eo_h : s->eo;
+    std::vector<double>& P = het ? s->params_h : s->params;
     int nc = r->n_temps * r->n_chains;
     for (int c = 0; c < nc; c++) {
       double y[11];
@@ -336,42 +360,52 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
         for (int j = 0; j < 11; j++) y[j] = x[j];
       }
       bool ok = in_prior(r, y);
-      s->eo.push_back(ok ? r->slot : -1);
-      s->params.insert(s->params.end(), y, y + 11);
-      s->owner.push_back({id, c});
+      eo.push_back(ok ? r->slot : -1);
+      P.insert(P.end(), y, y + 11);
     }
   }
-  int B = (int)s->eo.size();
+  const int Bf = (int)s->eo.size(), Bh = (int)s->eo_h.size();
   double t1 = now_s(s);
-  if (B > 0) {
-    s->out.assign(B, -1e20);
-    int rc = qcbc_lnl_multi(s->batch, s->eo.data(), s->params.data(), B, s->out.data(), nullptr, s->precision);
+  if (Bf > 0) {
+    s->out.assign(Bf, -1e20);
+    int rc = qcbc_lnl_multi(s->batch, s->eo.data(), s->params.data(), Bf, s->out.data(), nullptr, s->precision);
     if (rc != QCBC_OK && rc != QCBC_EDOM) return rc;   // EDOM: out-of-prior or invalid sets, lnL = -1e20
     s->launches++;
-    s->evals += B;
+    s->evals += Bf;
+  }
+  if (Bh > 0) {
+    s->out_h.assign(Bh, -1e20);
+    int rc = qcbc_lnl_multi_het(s->batch, s->eo_h.data(), s->params_h.data(), Bh, s->out_h.data(), s->precision);
+    if (rc != QCBC_OK && rc != QCBC_EDOM) return rc;
+    s->launches++;
+    s->evals += Bh;
   }
   double t2 = now_s(s);
   // accept / reject, swaps, adaptation, samples
-  size_t k = 0;
+  size_t kf = 0, kh = 0;
   std::vector<long long> finished;
   for (long long id : s->live) {
     Run* r = s->runs[id];
+    const bool het = r->likelihood == QCBC_LNL_HET;
+    const double* out = het ? s->out_h.data() : s->out.data();
+    const double* P = het ? s->params_h.data() : s->params.data();
+    size_t& k = het ? kh : kf;
     int nc = r->n_temps * r->n_chains;
     r->evals += nc;
     if (!r->initialised) {
-      for (int c = 0; c < nc; c++, k++) r->lnl[c] = s->out[k];
+      for (int c = 0; c < nc; c++, k++) r->lnl[c] = out[k];
       r->initialised = true;
       continue;
     }
     for (int c = 0; c < nc; c++, k++) {
       int t = c % r->n_temps;
-      double Ly = s->out[k];
+      double Ly = out[k];
       r->prop[t]++;
       if (t == 0) r->cold_prop++;
       if (Ly > -1e19) {
         double la = (Ly - r->lnl[c]) / r->temp[c];
         if (la >= 0.0 || std::log(r->rng.uniform()) < la) {
-          std::memcpy(&r->x[(size_t)c * 11], &s->params[k * 11], 11 * sizeof(double));
+          std::memcpy(&r->x[(size_t)c * 11], &P[k * 11], 11 * sizeof(double));
           r->lnl[c] = Ly;
           r->acc[t]++;
           if (t == 0) r->cold_acc++;

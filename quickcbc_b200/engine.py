@@ -228,6 +228,20 @@ class Batch:
             check(rc)
         return (out, r) if rho else out
 
+    def lnl_het(self, event_of, params, precision=MIXED, allow_invalid=False):
+        """Heterodyned lnL of sets of many events (each event's tables as of when the batch
+        took it; events without tables give -1e20)."""
+        eo = np.ascontiguousarray(event_of, dtype=np.int32)
+        P = _f64(np.atleast_2d(params))
+        B = P.shape[0]
+        assert eo.shape == (B,)
+        out = np.zeros(B)
+        rc = lib().qcbc_lnl_multi_het(self._h, eo.ctypes.data_as(C.POINTER(C.c_int)), _ptr(P), B, _ptr(out),
+                                      precision_code(precision))
+        if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
+            check(rc)
+        return out
+
     def time(self, B, precision=MIXED, iters=10, flush_l2=True):
         ms = (C.c_float * iters)()
         check(lib().qcbc_time_lnl_multi(self._h, int(B), precision_code(precision), iters, int(flush_l2), ms))

@@ -79,3 +79,14 @@ def oracle_template(ora):
     def t(info, p):
         return ora.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
     return t
+
+
+def prior_bounds(Tobs):
+    """MCMC_all's prior box (QuickCBC.c:1871-1896, ConstCBC.h:48-57), as the fixtures used."""
+    from quickcbc_b200 import synth
+    M, PC = synth.MSUN_SI, synth.PC_SI
+    pmin = np.array([np.log(0.5 * M), np.log(0.5 * M), -0.85, -0.85, 0.0, max(Tobs - 3.5, 1.5),
+                     np.log(1e6 * PC), 0.0, -1.0, 0.0, -1.0])
+    pmax = np.array([np.log(160 * M), np.log(300 * M), 0.85, 0.85, 2 * np.pi, Tobs - 0.5,
+                     np.log(1e10 * PC), 2 * np.pi, 1.0, np.pi, 1.0])
+    return pmin, pmax

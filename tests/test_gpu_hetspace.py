@@ -7,19 +7,9 @@ import pytest
 
 import quickcbc_b200 as q
 from quickcbc_b200 import synth
-from conftest import oracle_template, load_golden
+from conftest import oracle_template, load_golden, prior_bounds
 
 pytestmark = pytest.mark.gpu
-
-
-def prior_bounds(Tobs):
-    # MCMC_all's prior box (QuickCBC.c:1871-1896, ConstCBC.h:48-57), as the fixtures used
-    M, PC = synth.MSUN_SI, synth.PC_SI
-    pmin = np.array([np.log(0.5 * M), np.log(0.5 * M), -0.85, -0.85, 0.0, max(Tobs - 3.5, 1.5),
-                     np.log(1e6 * PC), 0.0, -1.0, 0.0, -1.0])
-    pmax = np.array([np.log(160 * M), np.log(300 * M), 0.85, 0.85, 2 * np.pi, Tobs - 0.5,
-                     np.log(1e10 * PC), 2 * np.pi, 1.0, np.pi, 1.0])
-    return pmin, pmax
 
 
 def test_het_space_config1_matches_reference(cfg1_event, golden):

@@ -6,7 +6,7 @@ import pytest
 
 import quickcbc_b200 as q
 from quickcbc_b200 import synth
-from conftest import oracle_template
+from conftest import oracle_template, prior_bounds
 
 pytestmark = pytest.mark.gpu
 
@@ -88,3 +88,31 @@ def test_autotune_keeps_results(uneven):
     assert tb > 0 and th in (64, 128, 256)
     np.testing.assert_allclose(batch.lnl(eo, P, q.FP64), before, rtol=0, atol=1e-9)
     assert np.all(batch.time(len(P), q.MIXED, iters=3) > 0)
+
+
+def test_multi_het_matches_single_event(uneven):
+    """qcbc_lnl_multi_het: each set uses its own event's heterodyne tables (grid search and tables
+    built on the GPU about each injection); equal to the single-event heterodyned lnL."""
+    evs, handles, _ = uneven
+    sel_events = [0, 1, 2, 3]
+    for e in sel_events:
+        pmin, pmax = prior_bounds(evs[e].Tobs)
+        g, MN, MM = handles[e].het_space(evs[e].inj, pmin, pmax)
+        handles[e].het_setup(evs[e].inj, g, MN, MM, 2)
+    batch = q.Batch([handles[e] for e in sel_events] + [handles[5]])     # the last one has no tables
+    rng = np.random.default_rng(4400)
+    eo, P = [], []
+    for k, e in enumerate(sel_events):
+        P.append(synth.jitter_params(rng, 6, evs[e].inj, scale=1e-5))
+        eo += [k] * 6
+    eo, P = np.array(eo, dtype=np.int32), np.vstack(P)
+    for prec, tol in ((q.FP64, 1e-9), (q.MIXED, 1e-9)):
+        L = batch.lnl_het(eo, P, prec)
+        for k, e in enumerate(sel_events):
+            Ls = handles[e].lnl_het(P[eo == k], prec)
+            np.testing.assert_allclose(L[eo == k], Ls, rtol=0, atol=tol)
+    alone = batch.lnl_het(eo[eo == 2], P[eo == 2], q.MIXED)
+    assert np.array_equal(alone, batch.lnl_het(eo, P, q.MIXED)[eo == 2])
+    Lx = batch.lnl_het(np.array([4, 0], dtype=np.int32), P[:2], q.FP64, allow_invalid=True)
+    assert Lx[0] == -1e20 and Lx[1] > -1e19
+    batch.close()

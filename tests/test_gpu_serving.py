@@ -99,3 +99,35 @@ def test_stream_driver_reports_latency(events):
     assert res["p50_s"] > 0 and res["p99_s"] >= res["p50_s"]
     assert res["lnl_evals"] == sum(2 * 2 * 41 for _ in events)
     srv.close()
+
+
+def test_het_runs_same_alone_and_in_mix(events):
+    """Heterodyned runs: grid search and tables at admission; a run evolves identically alone and
+    in a mix that also holds full-likelihood runs."""
+    alone = serving.Server(max_live=8, max_bins=1 << 15)
+    r = alone.submit(events[0], seed=21, likelihood="het", **SAMPLER)
+    alone.run_until_idle()
+    s_alone = alone.samples(r)
+    mix = serving.Server(max_live=8, max_bins=1 << 15)
+    ids = [mix.submit(ev, seed=21 + k, likelihood="het" if k % 2 == 0 else "full", **SAMPLER)
+           for k, ev in enumerate(events)]
+    mix.run_until_idle()
+    assert all(mix.info(i)["state"] == serving.RUN_DONE for i in ids)
+    assert s_alone.shape == (SAMPLER["n_chains"] * 8, 12)
+    assert np.array_equal(s_alone, mix.samples(ids[0]))
+    alone.close()
+    mix.close()
+
+
+def test_het_chains_concentrate_on_injection(ora):
+    ev = synth.config_event(1, oracle_template(ora), snr=40.0)
+    srv = serving.Server(max_live=4, max_bins=1 << 13)
+    r = srv.submit(ev, start=ev.inj.copy(), n_temps=4, n_chains=4, n_steps=400, burn_in=200, thin=4, seed=3,
+                   likelihood="het")
+    srv.run_until_idle()
+    s = srv.samples(r)
+    assert srv.info(r)["state"] == serving.RUN_DONE
+    Linj, _ = ora.lnl_full(ev, ev.inj)
+    assert np.max(s[:, 11]) > Linj - 5.0
+    assert abs(np.median(s[:, 0]) - ev.inj[0]) < 0.05
+    srv.close()
