@@ -360,7 +360,8 @@ def bench_cfg4_uneven(q):
     return out
 
 
-def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64"), rate_hz=2.0):
+def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64", "mixed-het", "mixed-dev",
+                                                                 "mixed-het-dev"), rate_hz=2.0, device_steps=16):
     """Config 5: Poisson arrivals (mean rate_hz) of PT-MCMC analyses of config-4-like events
     (16 temperatures x 8 chains x n_steps), device-resident runs admitted by a 150 GB budget,
     every step of every live run merged into one multi-event launch."""
@@ -372,12 +373,18 @@ def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64")
     out = {"workload": "config 5: %d runs, Poisson %.1f/s, 16 temps x 8 chains x %d steps, config-4 events, "
                        "HBM budget 150 GB" % (n_runs, rate_hz, n_steps)}
     for name in precisions:
-        prec = q.MIXED if name == "mixed" else q.FP64
-        srv = serving.Server(hbm_budget_bytes=150 * 10**9, max_live=256, max_bins=1 << 17, precision=prec)
+        # "<precision>" samples the full lnL; "<precision>-het" builds each run's heterodyne grid and
+        # tables on the GPU at admission and samples the heterodyned lnL, as the reference does;
+        # "-dev" keeps the chains on the device, up to device_steps steps per host call
+        parts = name.split("-")
+        prec = q.MIXED if parts[0] == "mixed" else q.FP64
+        lik = "het" if "het" in parts else "full"
+        srv = serving.Server(hbm_budget_bytes=150 * 10**9, max_live=256, max_bins=1 << 17, precision=prec,
+                             device_steps=device_steps if "dev" in parts else 0)
         srv.set_tiling(8192, 256)
         res = serving.serve_stream(srv, evs, rate_hz=rate_hz, seed=5,
                                    sampler=dict(n_temps=16, n_chains=8, n_steps=n_steps, burn_in=n_steps // 4,
-                                                thin=max(1, n_steps // 200)))
+                                                thin=max(1, n_steps // 200), likelihood=lik))
         st = srv.stats()
         res.pop("ttp_s")
         res["launches"] = st["launches"]
@@ -415,7 +422,8 @@ def main():
     ap.add_argument("--serve", action="store_true", help="config 5 serving stream only")
     ap.add_argument("--serve-runs", type=int, default=32)
     ap.add_argument("--serve-steps", type=int, default=20000)
-    ap.add_argument("--serve-prec", default="mixed,fp64")
+    ap.add_argument("--serve-prec", default="mixed,fp64,mixed-het,mixed-dev,mixed-het-dev")
+    ap.add_argument("--serve-dev-steps", type=int, default=16)
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
@@ -433,7 +441,7 @@ def main():
         from quickcbc_b200 import _lib
         _lib.check(_lib.lib().qcbc_init(0))
         res = bench_cfg5_serving(q, n_runs=args.serve_runs, n_steps=args.serve_steps,
-                                 precisions=tuple(args.serve_prec.split(",")))
+                                 precisions=tuple(args.serve_prec.split(",")), device_steps=args.serve_dev_steps)
         print(json.dumps({"metric": "time-to-posterior p50/p99 and aggregate lnL evals/s (config 5)", **res}))
         return
 

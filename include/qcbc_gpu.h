@@ -116,6 +116,15 @@ int qcbc_lnl_multi(qcbc_batch* batch, const int* event_of, const double* params,
  * no tables get lnL = -1e20 and the call returns QCBC_EDOM. */
 int qcbc_lnl_multi_het(qcbc_batch* batch, const int* event_of, const double* params, int B, double* lnl,
                        int precision);
+/* Device-buffer forms of qcbc_lnl_multi / qcbc_lnl_multi_het: event_of, params and lnl are device
+ * pointers; the work is queued on `stream` (a cudaStream_t as void*, NULL = the batch's stream)
+ * with no host copy and no synchronisation.  Sets outside the waveform domain or without an event
+ * (or tables) get lnL = -1e20; no status is returned for them.  Calls on one batch share its
+ * buffers: keep them on one stream. */
+int qcbc_lnl_multi_dev(qcbc_batch* batch, const int* d_event_of, const double* d_params, int B, double* d_lnl,
+                       int precision, void* stream);
+int qcbc_lnl_multi_het_dev(qcbc_batch* batch, const int* d_event_of, const double* d_params, int B, double* d_lnl,
+                           int precision, void* stream);
 /* Device time of `iters` graph launches on inputs already uploaded by a previous
  * qcbc_lnl_multi call with the same B (no host copies inside the timed span). */
 int qcbc_time_lnl_multi(qcbc_batch* batch, int B, int precision, int iters, int flush_l2, float* ms);

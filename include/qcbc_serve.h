@@ -93,6 +93,13 @@ int qcbc_server_stats(qcbc_server* s, long long* lnl_evals, long long* launches,
 int qcbc_server_timing(qcbc_server* s, double* propose_s, double* lnl_s, double* update_s);
 /* Tiling of the merged launches (see qcbc_batch_set_tiling). */
 int qcbc_server_set_tiling(qcbc_server* s, int tile_bins, int threads);
+/* Device-resident stepping: with steps > 0 the chains of the live runs stay on the device and
+ * every qcbc_server_step() queues up to `steps` whole steps on one stream (proposal, merged lnL
+ * launches, acceptance, swaps, adaptation, thinning as kernels), stopping early when a run
+ * finishes; 0 (the default) steps on the host.  Each chain draws from its own generator stream,
+ * so a run evolves identically alone, in any mix and for any `steps`.  Set before submitting
+ * runs; at most 64 temperatures per run in this mode. */
+int qcbc_server_set_device_steps(qcbc_server* s, int steps);
 
 #ifdef __cplusplus
 }

@@ -21,8 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 GEN = os.path.join(CSRC, "_gen")
 LIB = os.path.join(HERE, "libqcbc_gpu.so")
-SOURCES = ["qcbc_kernels.cu", "qcbc_capi.cu", "qcbc_serve.cu", "qcbc_hetspace.cu"]
-HEADERS = ["qcbc_device.cuh", "qcbc_kernels.cuh", "qcbc_hetspace.h"]
+SOURCES = ["qcbc_kernels.cu", "qcbc_capi.cu", "qcbc_serve.cu", "qcbc_hetspace.cu", "qcbc_ptstep.cu"]
+HEADERS = ["qcbc_device.cuh", "qcbc_kernels.cuh", "qcbc_hetspace.h", "qcbc_ptstep.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "--expt-relaxed-constexpr"]
 

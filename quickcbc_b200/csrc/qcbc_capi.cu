@@ -1302,6 +1302,64 @@ extern "C" int qcbc_lnl_multi(qcbc_batch* bt, const int* event_of, const double*
   return run_multi(bt, event_of, params, B, lnl, rho, precision);
 }
 
+// Device-buffer forms for callers that keep parameter sets and results on the device (the
+// service's device-resident sampler): no host copies, no synchronisation; work is ordered on
+// `stream`.  Calls on one batch must not overlap (they share the batch's graph buffers).
+extern "C" int qcbc_lnl_multi_dev(qcbc_batch* bt, const int* d_event_of, const double* d_params, int B, double* d_lnl,
+                                  int precision, void* stream) {
+  if (!bt || !d_event_of || !d_params || !d_lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  std::lock_guard<std::mutex> lk(bt->mu);
+  MultiGraph* m = nullptr;
+  int rc = multi_graph(bt, bucket_of(B), precision, &m);
+  if (rc) return rc;
+  cudaStream_t s = stream ? (cudaStream_t)stream : bt->stream;
+  CU(cudaMemcpyAsync(m->d_params, d_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyDeviceToDevice, s));
+  CU(cudaMemcpyAsync(m->d_eof, d_event_of, sizeof(int) * (size_t)B, cudaMemcpyDeviceToDevice, s));
+  if (m->Bcap > B) CU(cudaMemsetAsync(m->d_eof + B, 0xFF, sizeof(int) * (size_t)(m->Bcap - B), s));   // -1: no work
+  CU(cudaGraphLaunch(m->exec_dev, s));
+  CU(cudaMemcpyAsync(d_lnl, m->d_lnl, sizeof(double) * (size_t)B, cudaMemcpyDeviceToDevice, s));
+  tls_launches += 4;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_lnl_multi_het_dev(qcbc_batch* bt, const int* d_event_of, const double* d_params, int B,
+                                      double* d_lnl, int precision, void* stream) {
+  if (!bt || !d_event_of || !d_params || !d_lnl) return fail(QCBC_EINVAL, "NULL argument");
+  if (precision != QCBC_FP64 && precision != QCBC_MIXED) return fail(QCBC_EINVAL, "precision %d", precision);
+  if (B <= 0) return B == 0 ? QCBC_OK : fail(QCBC_EINVAL, "B < 0");
+  std::lock_guard<std::mutex> lk(bt->mu);
+  HetMultiScratch& h = bt->hs;
+  cudaStream_t s = stream ? (cudaStream_t)stream : bt->stream;
+  if (B > h.cap) {                 // grown once; device memory only
+    CU(cudaStreamSynchronize(s));
+    free_het_scratch(h);
+    const size_t n = (size_t)B;
+    CU(cudaMalloc(&h.d_params, n * 11 * sizeof(double)));
+    CU(cudaMalloc(&h.d_eof, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_recs, n * sizeof(PhdRec)));
+    CU(cudaMalloc(&h.d_status, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_ntile, n * sizeof(int)));
+    CU(cudaMalloc(&h.d_lnl, n * sizeof(double)));
+    CU(cudaMallocHost(&h.h_params, n * 11 * sizeof(double)));
+    CU(cudaMallocHost(&h.h_eof, n * sizeof(int)));
+    CU(cudaMallocHost(&h.h_lnl, n * sizeof(double)));
+    CU(cudaMallocHost(&h.h_status, n * sizeof(int)));
+    h.cap = B;
+  }
+  size_t smem = 0;
+  for (size_t k = 0; k < bt->het_smem.size(); k++) smem = std::max(smem, bt->het_smem[k]);
+  DeviceState& ds = g_dev[current_device()];
+  launch_setup_multi(d_params, d_event_of, B, bt->d_events, (int)bt->events.size(), ds.qnm, bt->tile_bins, h.d_recs,
+                     h.d_status, h.d_ntile, s);
+  launch_lnl_het_multi(h.d_recs, h.d_status, B, bt->d_events, bt->d_het, smem,
+                       precision == QCBC_MIXED ? kMixed : kFP64, d_lnl, s);
+  tls_launches += 2;
+  CU(cudaGetLastError());
+  return QCBC_OK;
+}
+
 extern "C" int qcbc_lnl_multi_het(qcbc_batch* bt, const int* event_of, const double* params, int B, double* lnl,
                                   int precision) {
   if (!bt || !event_of || !params || !lnl) return fail(QCBC_EINVAL, "NULL argument");

@@ -1,0 +1,188 @@
+// Device-resident parallel-tempering step (see qcbc_ptstep.h).  The scheme is the host
+// service's (qcbc_serve.cu, after the reference's MCMC_all / update, QuickCBC.c:1781-2405): a
+// symmetric step with per-temperature adapted scales, angles wrapped and sin/cos parameters
+// reflected, the prior box and symmetric-mass-ratio limits (QuickCBC.c:1871-1896, 2341-2364),
+// Metropolis acceptance at T = ladder^t, one swap attempt between a random adjacent pair of
+// temperatures per ladder, scale adaptation towards 25 % acceptance every 50 burn-in steps, and
+// thinned samples of the T = 1 chains after burn-in.  Every chain draws from its own xoshiro256**
+// stream and the swap draws come from the ladder's coldest chain, so a run evolves the same
+// alone, in any mix of runs and for any number of steps per host call.
+#include "qcbc_ptstep.h"
+
+#include <cmath>
+
+namespace qcbc {
+namespace {
+
+constexpr double kTwoPiP = 6.2831853071795862319959269370884;
+constexpr double kPiP = 3.1415926535897931159979634685442;
+
+struct Xoshiro {
+  uint64_t s[4];
+  __device__ static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
+  __device__ uint64_t next() {
+    const uint64_t r = rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
+    s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
+    s[2] ^= t; s[3] = rotl(s[3], 45);
+    return r;
+  }
+  __device__ double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
+  // symmetric, zero-mean, unit-variance step: (u1 + u2 + u3 + u4 - 2) sqrt(3)
+  __device__ double step() {
+    const uint64_t a = next(), b = next();
+    const double k = 1.0 / 4294967296.0;
+    const double s4 = ((double)(uint32_t)a + (double)(a >> 32) + (double)(uint32_t)b + (double)(b >> 32)) * k;
+    return (s4 - 2.0) * 1.7320508075688772;
+  }
+  __device__ void load(const uint64_t* p) { for (int i = 0; i < 4; i++) s[i] = p[i]; }
+  __device__ void store(uint64_t* p) const { for (int i = 0; i < 4; i++) p[i] = s[i]; }
+};
+
+__device__ void wrap(double* y) {
+  y[4] = fmod(y[4], kTwoPiP);
+  if (y[4] < 0) y[4] += kTwoPiP;
+  y[7] = fmod(y[7], kTwoPiP);
+  if (y[7] < 0) y[7] += kTwoPiP;
+  y[9] = fmod(y[9], kPiP);
+  if (y[9] < 0) y[9] += kPiP;
+  for (int j = 8; j <= 10; j += 2) {
+    if (y[j] > 1.0) y[j] = 2.0 - y[j];
+    if (y[j] < -1.0) y[j] = -2.0 - y[j];
+  }
+}
+
+__device__ bool in_prior(const PtRun& r, const double* y) {
+  for (int j = 0; j < kPtNP; j++)
+    if (y[j] < r.pmin[j] || y[j] > r.pmax[j]) return false;
+  const double leta = (5.0 / 3.0) * (y[0] - y[1]);
+  return leta <= log(0.25) && leta >= log(0.05);
+}
+
+__device__ double chain_temp(const PtRun& r, int t) { return pow(r.ladder, (double)t); }
+
+__global__ void k_pt_propose(PtRun* __restrict__ runs, PtChains c, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  const PtRun& r = runs[c.run[b]];
+  double y[kPtNP];
+  const double* x = c.x + (size_t)b * kPtNP;
+  if (r.init) {
+    const int t = (b - r.off) % r.n_temps;
+    Xoshiro g;
+    g.load(c.rng + (size_t)b * 4);
+    for (int j = 0; j < kPtNP; j++) y[j] = x[j] + r.scale[t] * r.sigma[j] * g.step();
+    g.store(c.rng + (size_t)b * 4);
+    wrap(y);
+  } else {
+    for (int j = 0; j < kPtNP; j++) y[j] = x[j];
+  }
+  for (int j = 0; j < kPtNP; j++) c.y[(size_t)b * kPtNP + j] = y[j];
+  c.eo[b] = in_prior(r, y) ? r.slot : -1;
+}
+
+__global__ void k_pt_accept(PtRun* __restrict__ runs, PtChains c, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B) return;
+  PtRun& r = runs[c.run[b]];
+  const double Ly = c.lnly[b];
+  if (!r.init) {                       // the starting point's lnL
+    c.lnl[b] = Ly;
+    return;
+  }
+  const int t = (b - r.off) % r.n_temps;
+  atomicAdd(&r.prop[t], 1);
+  if (t == 0) atomicAdd(&r.cold_prop, 1ULL);
+  if (!(Ly > -1e19)) return;
+  const double la = (Ly - c.lnl[b]) / chain_temp(r, t);
+  bool ok = la >= 0.0;
+  if (!ok) {
+    Xoshiro g;
+    g.load(c.rng + (size_t)b * 4);
+    ok = log(g.uniform()) < la;
+    g.store(c.rng + (size_t)b * 4);
+  }
+  if (ok) {
+    for (int j = 0; j < kPtNP; j++) c.x[(size_t)b * kPtNP + j] = c.y[(size_t)b * kPtNP + j];
+    c.lnl[b] = Ly;
+    atomicAdd(&r.acc[t], 1);
+    if (t == 0) atomicAdd(&r.cold_acc, 1ULL);
+  }
+}
+
+// block (run): threads over the run's ladders for the swaps, then thread 0 .. n_temps-1 for the
+// adaptation and the ladders again for the samples
+__global__ void k_pt_swap_finish(PtRun* __restrict__ runs, PtChains c) {
+  PtRun& r = runs[blockIdx.x];
+  if (!r.init) {
+    __syncthreads();
+    if (threadIdx.x == 0) r.init = 1;
+    return;
+  }
+  if (r.n_temps > 1) {
+    for (int ch = threadIdx.x; ch < r.n_chains; ch += blockDim.x) {
+      const size_t cold = (size_t)r.off + (size_t)ch * r.n_temps;
+      Xoshiro g;
+      g.load(c.rng + cold * 4);
+      const int t = (int)(g.uniform() * (r.n_temps - 1));
+      const size_t a = cold + t, b = a + 1;
+      const double la = (c.lnl[b] - c.lnl[a]) * (1.0 / chain_temp(r, t) - 1.0 / chain_temp(r, t + 1));
+      atomicAdd(&r.swap_tries, 1ULL);
+      bool ok = la >= 0.0;
+      if (!ok) ok = log(g.uniform()) < la;
+      g.store(c.rng + cold * 4);
+      if (ok) {
+        for (int j = 0; j < kPtNP; j++) {
+          const double v = c.x[a * kPtNP + j];
+          c.x[a * kPtNP + j] = c.x[b * kPtNP + j];
+          c.x[b * kPtNP + j] = v;
+        }
+        const double v = c.lnl[a];
+        c.lnl[a] = c.lnl[b];
+        c.lnl[b] = v;
+        atomicAdd(&r.swaps, 1ULL);
+      }
+    }
+  }
+  __syncthreads();
+  const int step = r.steps_done + 1;
+  if (step <= r.burn_in && step % 50 == 0) {
+    for (int t = threadIdx.x; t < r.n_temps; t += blockDim.x) {
+      const double rate = r.prop[t] ? (double)r.acc[t] / r.prop[t] : 0.25;
+      const double f = exp(rate - 0.25);
+      r.scale[t] = fmin(fmax(r.scale[t] * f, 1e-3), 1e3);
+      r.acc[t] = 0;
+      r.prop[t] = 0;
+    }
+  }
+  if (step > r.burn_in && (step - r.burn_in) % r.thin == 0) {
+    for (int ch = threadIdx.x; ch < r.n_chains; ch += blockDim.x) {
+      const int row = r.n_samples + ch;
+      if (row < r.cap_samples) {
+        const size_t cold = (size_t)r.off + (size_t)ch * r.n_temps;
+        double* o = r.samples + (size_t)row * 12;
+        for (int j = 0; j < kPtNP; j++) o[j] = c.x[cold * kPtNP + j];
+        o[11] = c.lnl[cold];
+      }
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (step > r.burn_in && (step - r.burn_in) % r.thin == 0) r.n_samples = min(r.n_samples + r.n_chains, r.cap_samples);
+    r.steps_done = step;
+  }
+}
+
+}  // namespace
+
+void launch_pt_propose(PtRun* d_runs, PtChains c, int B, cudaStream_t s) {
+  if (B > 0) k_pt_propose<<<(B + 127) / 128, 128, 0, s>>>(d_runs, c, B);
+}
+void launch_pt_accept(PtRun* d_runs, PtChains c, int B, cudaStream_t s) {
+  if (B > 0) k_pt_accept<<<(B + 127) / 128, 128, 0, s>>>(d_runs, c, B);
+}
+void launch_pt_swap_finish(PtRun* d_runs, int nrun, int max_ladders, PtChains c, cudaStream_t s) {
+  (void)max_ladders;
+  if (nrun > 0) k_pt_swap_finish<<<nrun, 64, 0, s>>>(d_runs, c);
+}
+
+}  // namespace qcbc

@@ -21,8 +21,11 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda_runtime.h>
+
 #include "../../include/qcbc_gpu.h"
 #include "../../include/qcbc_serve.h"
+#include "qcbc_ptstep.h"
 
 extern "C" int qcbc_internal_fail(int code, const char* msg);
 
@@ -85,6 +88,7 @@ struct Run {
   int n_temps = 1, n_chains = 1, n_steps = 0, burn_in = 0, thin = 1;
   double ladder = 1.15;
   int likelihood = QCBC_LNL_FULL;
+  unsigned long long seed = 0;
   // live state
   qcbc_event* ev = nullptr;
   int slot = -1;
@@ -97,6 +101,9 @@ struct Run {
   std::vector<double> samples;               // rows of 12
   double t_arrival = 0, t_admit = -1, t_done = -1;
   Rng rng;
+  // device-resident stepping: per-chain generator states and the kernels' view of the run
+  std::vector<uint64_t> rng_chains;          // [nc][4]
+  qcbc::PtRun pt{};
 };
 
 long long estimate_bytes(const Run& r) {
@@ -121,7 +128,21 @@ struct qcbc_server {
   // launch staging: full and heterodyned sets
   std::vector<int> eo, eo_h;
   std::vector<double> params, out, params_h, out_h;
+  // device-resident stepping (dev_steps > 0): the live runs packed into flat device arrays,
+  // full-likelihood runs first; repacked when the live set changes
+  int dev_steps = 0;
+  cudaStream_t dstream = nullptr;
+  qcbc::PtChains dc{};
+  qcbc::PtRun* d_runs = nullptr;
+  int capB = 0, capR = 0, Bpk = 0, Bfpk = 0;
+  std::vector<long long> packed;
+  bool dirty = true;
 };
+
+static void free_dev(qcbc_server* s);
+static int dev_init_run(Run* r, unsigned long long seed);
+static int dev_pull(qcbc_server* s);
+static int dev_samples(Run* r);
 
 static double now_s(const qcbc_server* s) {
   return std::chrono::duration<double>(std::chrono::steady_clock::now() - s->t0).count();
@@ -146,6 +167,11 @@ extern "C" qcbc_server* qcbc_server_create(long long budget, int max_live, int m
 }
 
 static void retire(qcbc_server* s, Run* r, int state) {
+  if (r->pt.samples) {
+    cudaFree(r->pt.samples);
+    r->pt.samples = nullptr;
+  }
+  s->dirty = true;
   if (r->slot >= 0) {
     qcbc_batch_set_slot(s->batch, r->slot, nullptr);
     s->slot_run[r->slot] = -1;
@@ -167,10 +193,13 @@ static void retire(qcbc_server* s, Run* r, int state) {
 extern "C" int qcbc_server_destroy(qcbc_server* s) {
   if (!s) return QCBC_OK;
   std::lock_guard<std::mutex> lk(s->mu);
+  if (s->dstream) cudaStreamSynchronize(s->dstream);
   for (auto& kv : s->runs) {
     if (kv.second->state == QCBC_RUN_LIVE) retire(s, kv.second, QCBC_RUN_CANCELLED);
     delete kv.second;
   }
+  free_dev(s);
+  if (s->dstream) cudaStreamDestroy(s->dstream);
   qcbc_batch_destroy(s->batch);
   delete s;
   return QCBC_OK;
@@ -189,6 +218,8 @@ extern "C" long long qcbc_server_submit(qcbc_server* s, const qcbc_run_spec* sp)
       sp->n_chains < 1 || sp->n_steps < 1 || sp->thin < 1 || sp->burn_in < 0 || !(sp->ladder >= 1.0))
     return sfail(QCBC_EINVAL, "bad run specification");
   if (sp->N / 2 > s->max_bins) return sfail(QCBC_EINVAL, "run has %d bins, server holds %d", sp->N / 2, s->max_bins);
+  if (s->dev_steps > 0 && sp->n_temps > qcbc::kPtMaxTemps)
+    return sfail(QCBC_EINVAL, "device-resident stepping takes at most %d temperatures", qcbc::kPtMaxTemps);
   Run* r = new Run();
   r->nifo = sp->nifo;
   r->N = sp->N;
@@ -223,6 +254,7 @@ extern "C" long long qcbc_server_submit(qcbc_server* s, const qcbc_run_spec* sp)
     return sfail(QCBC_EINVAL, "likelihood %d", sp->likelihood);
   }
   r->likelihood = sp->likelihood;
+  r->seed = sp->seed;
   r->rng.seed(sp->seed);
   r->bytes = estimate_bytes(*r);
   std::lock_guard<std::mutex> lk(s->mu);
@@ -250,6 +282,11 @@ extern "C" int qcbc_server_cancel(qcbc_server* s, long long id) {
     r->state = QCBC_RUN_CANCELLED;
     r->t_done = now_s(s);
   } else if (r->state == QCBC_RUN_LIVE) {
+    if (s->dev_steps > 0) {          // keep what the device sampler has so far
+      int rc = dev_pull(s);
+      if (rc == QCBC_OK) rc = dev_samples(r);
+      if (rc != QCBC_OK) return rc;
+    }
     retire(s, r, QCBC_RUN_CANCELLED);
     for (size_t k = 0; k < s->live.size(); k++)
       if (s->live[k] == id) { s->live.erase(s->live.begin() + k); break; }
@@ -309,6 +346,13 @@ static void admit(qcbc_server* s) {
       for (int j = 0; j < 11; j++) r->x[(size_t)c * 11 + j] = r->start[j];
     }
     for (int t = 0; t < r->n_temps; t++) r->scale[t] = std::sqrt(std::pow(r->ladder, t));
+    if (s->dev_steps > 0) {
+      if (dev_init_run(r, r->seed) != QCBC_OK) {
+        retire(s, r, QCBC_RUN_FAILED);
+        continue;
+      }
+      s->dirty = true;
+    }
     s->live.push_back(r->id);
   }
 }
@@ -333,10 +377,232 @@ static void wrap(double* y) {
   }
 }
 
+// ---------------------------------------------------------------- device-resident stepping
+static void free_dev(qcbc_server* s) {
+  qcbc::PtChains& c = s->dc;
+  cudaFree(c.x); cudaFree(c.lnl); cudaFree(c.y); cudaFree(c.lnly); cudaFree(c.eo); cudaFree(c.run); cudaFree(c.rng);
+  cudaFree(s->d_runs);
+  c = qcbc::PtChains{};
+  s->d_runs = nullptr;
+  s->capB = s->capR = 0;
+}
+
+// Device view of a newly live run: starting points, per-chain generators seeded from the run's
+// seed, scales sqrt(ladder^t), and the device buffer for its thinned samples.
+static int dev_init_run(Run* r, unsigned long long seed) {
+  qcbc::PtRun& p = r->pt;
+  memset(&p, 0, sizeof(p));
+  p.slot = r->slot;
+  p.nc = r->n_temps * r->n_chains;
+  p.n_temps = r->n_temps;
+  p.n_chains = r->n_chains;
+  p.burn_in = r->burn_in;
+  p.thin = r->thin;
+  p.n_steps = r->n_steps;
+  p.ladder = r->ladder;
+  for (int j = 0; j < 11; j++) { p.sigma[j] = r->sigma[j]; p.pmin[j] = r->pmin[j]; p.pmax[j] = r->pmax[j]; }
+  for (int t = 0; t < r->n_temps; t++) p.scale[t] = std::sqrt(std::pow(r->ladder, t));
+  int rows = r->n_steps > r->burn_in ? (r->n_steps - r->burn_in) / r->thin : 0;
+  p.cap_samples = rows * r->n_chains;
+  if (p.cap_samples > 0 &&
+      cudaMalloc(&p.samples, sizeof(double) * 12 * (size_t)p.cap_samples) != cudaSuccess)
+    return sfail(QCBC_ENOMEM, "sample buffer of %d rows", p.cap_samples);
+  r->rng_chains.assign((size_t)p.nc * 4, 0);
+  for (int c = 0; c < p.nc; c++) {
+    uint64_t v = seed + 0x632BE59BD9B4E019ULL * (uint64_t)(c + 1);
+    for (int k = 0; k < 4; k++) r->rng_chains[(size_t)c * 4 + k] = Rng::splitmix(v);
+  }
+  return QCBC_OK;
+}
+
+// Device state of the packed runs back into their Run objects (the device stays authoritative).
+static int dev_pull(qcbc_server* s) {
+  if (s->packed.empty()) return QCBC_OK;
+  const int B = s->Bpk, R = (int)s->packed.size();
+  std::vector<double> x((size_t)B * 11), lnl(B);
+  std::vector<uint64_t> rng((size_t)B * 4);
+  std::vector<qcbc::PtRun> pr(R);
+  if (cudaStreamSynchronize(s->dstream) != cudaSuccess ||
+      cudaMemcpy(x.data(), s->dc.x, x.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(lnl.data(), s->dc.lnl, lnl.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(rng.data(), s->dc.rng, rng.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess ||
+      cudaMemcpy(pr.data(), s->d_runs, sizeof(qcbc::PtRun) * R, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return sfail(QCBC_ECUDA, "device sampler state download failed");
+  for (int k = 0; k < R; k++) {
+    Run* r = s->runs[s->packed[k]];
+    if (r->state != QCBC_RUN_LIVE) continue;
+    const qcbc::PtRun& p = pr[k];
+    r->pt = p;
+    memcpy(r->x.data(), &x[(size_t)p.off * 11], sizeof(double) * 11 * p.nc);
+    memcpy(r->lnl.data(), &lnl[p.off], sizeof(double) * p.nc);
+    memcpy(r->rng_chains.data(), &rng[(size_t)p.off * 4], sizeof(uint64_t) * 4 * p.nc);
+    r->cold_acc = (long long)p.cold_acc;
+    r->cold_prop = (long long)p.cold_prop;
+    r->swaps = (long long)p.swaps;
+    r->swap_tries = (long long)p.swap_tries;
+  }
+  return QCBC_OK;
+}
+
+// The thinned samples a device run holds so far into its host copy.
+static int dev_samples(Run* r) {
+  r->samples.assign((size_t)r->pt.n_samples * 12, 0.0);
+  if (r->pt.n_samples > 0 && r->pt.samples &&
+      cudaMemcpy(r->samples.data(), r->pt.samples, r->samples.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return sfail(QCBC_ECUDA, "sample download failed");
+  return QCBC_OK;
+}
+
+template <class T>
+static int dev_grow(T** p, size_t n) {
+  cudaFree(*p);
+  *p = nullptr;
+  return cudaMalloc(p, sizeof(T) * (n > 0 ? n : 1)) == cudaSuccess ? QCBC_OK : QCBC_ENOMEM;
+}
+
+// Live runs into the flat device arrays: full-likelihood runs first, then heterodyned ones.
+static int dev_pack(qcbc_server* s) {
+  std::vector<long long> order;
+  for (int pass = 0; pass < 2; pass++)
+    for (long long id : s->live)
+      if ((s->runs[id]->likelihood == QCBC_LNL_HET) == (pass == 1)) order.push_back(id);
+  int B = 0, Bf = 0;
+  for (long long id : order) {
+    Run* r = s->runs[id];
+    r->pt.off = B;
+    B += r->pt.nc;
+    if (r->likelihood != QCBC_LNL_HET) Bf = B;
+  }
+  const int R = (int)order.size();
+  if (B > s->capB) {
+    int rc = 0;
+    qcbc::PtChains& c = s->dc;
+    rc |= dev_grow(&c.x, (size_t)B * 11) | dev_grow(&c.lnl, (size_t)B) | dev_grow(&c.y, (size_t)B * 11) |
+          dev_grow(&c.lnly, (size_t)B) | dev_grow(&c.eo, (size_t)B) | dev_grow(&c.run, (size_t)B) |
+          dev_grow(&c.rng, (size_t)B * 4);
+    if (rc) return sfail(QCBC_ENOMEM, "device sampler arrays for %d chains", B);
+    s->capB = B;
+  }
+  if (R > s->capR) {
+    if (dev_grow(&s->d_runs, (size_t)R)) return sfail(QCBC_ENOMEM, "device run table");
+    s->capR = R;
+  }
+  std::vector<double> x((size_t)B * 11), lnl(B);
+  std::vector<uint64_t> rng((size_t)B * 4);
+  std::vector<int> run(B);
+  std::vector<qcbc::PtRun> pr(R);
+  for (int k = 0; k < R; k++) {
+    Run* r = s->runs[order[k]];
+    const qcbc::PtRun& p = r->pt;
+    pr[k] = p;
+    memcpy(&x[(size_t)p.off * 11], r->x.data(), sizeof(double) * 11 * p.nc);
+    memcpy(&lnl[p.off], r->lnl.data(), sizeof(double) * p.nc);
+    memcpy(&rng[(size_t)p.off * 4], r->rng_chains.data(), sizeof(uint64_t) * 4 * p.nc);
+    for (int c = 0; c < p.nc; c++) run[p.off + c] = k;
+  }
+  if (B > 0 &&
+      (cudaMemcpy(s->dc.x, x.data(), x.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(s->dc.lnl, lnl.data(), lnl.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(s->dc.rng, rng.data(), rng.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(s->dc.run, run.data(), run.size() * sizeof(int), cudaMemcpyHostToDevice) != cudaSuccess ||
+       cudaMemcpy(s->d_runs, pr.data(), sizeof(qcbc::PtRun) * R, cudaMemcpyHostToDevice) != cudaSuccess))
+    return sfail(QCBC_ECUDA, "device sampler state upload failed");
+  s->packed = order;
+  s->Bpk = B;
+  s->Bfpk = Bf;
+  s->dirty = false;
+  return QCBC_OK;
+}
+
+// Up to dev_steps steps of every live run on the device, stopping when a run finishes.
+static int dev_step(qcbc_server* s) {
+  double t0 = now_s(s);
+  int rc;
+  if (s->dirty) {
+    if ((rc = dev_pull(s))) return rc;
+    if ((rc = dev_pack(s))) return rc;
+  }
+  if (s->packed.empty()) return QCBC_OK;
+  int K = s->dev_steps;
+  for (long long id : s->packed) {
+    Run* r = s->runs[id];
+    K = std::min(K, r->n_steps - r->steps_done + (r->initialised ? 0 : 1));
+  }
+  const int B = s->Bpk, Bf = s->Bfpk, Bh = B - Bf, R = (int)s->packed.size();
+  double t1 = now_s(s);
+  qcbc::PtChains c = s->dc;
+  for (int k = 0; k < K; k++) {
+    qcbc::launch_pt_propose(s->d_runs, c, B, s->dstream);
+    if (Bf > 0 && (rc = qcbc_lnl_multi_dev(s->batch, c.eo, c.y, Bf, c.lnly, s->precision, s->dstream))) return rc;
+    if (Bh > 0 &&
+        (rc = qcbc_lnl_multi_het_dev(s->batch, c.eo + Bf, c.y + (size_t)Bf * 11, Bh, c.lnly + Bf, s->precision,
+                                     s->dstream)))
+      return rc;
+    qcbc::launch_pt_accept(s->d_runs, c, B, s->dstream);
+    qcbc::launch_pt_swap_finish(s->d_runs, R, 0, c, s->dstream);
+  }
+  cudaError_t e = cudaStreamSynchronize(s->dstream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) return sfail(QCBC_ECUDA, "device steps: %s", cudaGetErrorString(e));
+  double t2 = now_s(s);
+  s->launches += (long long)K * ((Bf > 0) + (Bh > 0));
+  s->evals += (long long)K * B;
+  std::vector<long long> finished;
+  for (long long id : s->packed) {
+    Run* r = s->runs[id];
+    r->evals += (long long)K * r->pt.nc;
+    r->steps_done += r->initialised ? K : K - 1;
+    r->initialised = true;
+    if (r->steps_done >= r->n_steps) finished.push_back(id);
+  }
+  if (!finished.empty()) {
+    if ((rc = dev_pull(s))) return rc;
+    for (long long id : finished) {
+      Run* r = s->runs[id];
+      if ((rc = dev_samples(r))) return rc;
+      retire(s, r, QCBC_RUN_DONE);
+      for (size_t q = 0; q < s->live.size(); q++)
+        if (s->live[q] == id) { s->live.erase(s->live.begin() + q); break; }
+    }
+    s->packed.clear();
+    s->dirty = true;
+  }
+  double t3 = now_s(s);
+  s->t_propose += t1 - t0;
+  s->t_lnl += t2 - t1;
+  s->t_update += t3 - t2;
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_server_set_device_steps(qcbc_server* s, int steps) {
+  if (!s || steps < 0) return sfail(QCBC_EINVAL, "NULL server or negative step count");
+  std::lock_guard<std::mutex> lk(s->mu);
+  if (!s->live.empty() || !s->queue.empty()) return sfail(QCBC_EINVAL, "set the stepping mode before submitting runs");
+  if (steps > 0 && !s->dstream && cudaStreamCreateWithFlags(&s->dstream, cudaStreamNonBlocking) != cudaSuccess)
+    return sfail(QCBC_ECUDA, "stream creation failed");
+  s->dev_steps = steps;
+  return QCBC_OK;
+}
+
+static void step_counts(qcbc_server* s, int* n_live, int* n_queued, int* n_done) {
+  if (n_live) *n_live = (int)s->live.size();
+  if (n_queued) *n_queued = (int)s->queue.size();
+  if (n_done) {
+    int d = 0;
+    for (auto& kv : s->runs) d += kv.second->state >= QCBC_RUN_DONE;
+    *n_done = d;
+  }
+}
+
 extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int* n_done) {
   if (!s) return sfail(QCBC_EINVAL, "NULL server");
   std::lock_guard<std::mutex> lk(s->mu);
   admit(s);
+  if (s->dev_steps > 0) {
+    int rc = dev_step(s);
+    step_counts(s, n_live, n_queued, n_done);
+    return rc;
+  }
   double t0 = now_s(s);
   s->eo.clear();
   s->params.clear();
@@ -467,7 +733,12 @@ extern "C" int qcbc_server_run_info(qcbc_server* s, long long id, qcbc_run_info*
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->runs.find(id);
   if (it == s->runs.end()) return sfail(QCBC_EINVAL, "no run %lld", id);
-  const Run* r = it->second;
+  Run* r = it->second;
+  if (s->dev_steps > 0 && r->state == QCBC_RUN_LIVE) {   // the device holds the live counters
+    int rc = dev_pull(s);
+    if (rc == QCBC_OK) rc = dev_samples(r);
+    if (rc != QCBC_OK) return rc;
+  }
   o->state = r->state;
   o->steps_done = r->steps_done;
   o->t_arrival = r->t_arrival;
@@ -486,6 +757,11 @@ extern "C" int qcbc_server_run_samples(qcbc_server* s, long long id, double* out
   std::lock_guard<std::mutex> lk(s->mu);
   auto it = s->runs.find(id);
   if (it == s->runs.end()) return sfail(QCBC_EINVAL, "no run %lld", id);
+  if (s->dev_steps > 0 && it->second->state == QCBC_RUN_LIVE) {
+    int rc = dev_pull(s);
+    if (rc == QCBC_OK) rc = dev_samples(it->second);
+    if (rc != QCBC_OK) return rc;
+  }
   int n = (int)std::min<size_t>(it->second->samples.size() / 12, (size_t)std::max(max_rows, 0));
   std::memcpy(out, it->second->samples.data(), sizeof(double) * 12 * (size_t)n);
   *n_rows = n;

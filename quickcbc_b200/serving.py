@@ -55,17 +55,27 @@ def _bind():
     L.qcbc_server_stats.argtypes = [vp, C.POINTER(ll), C.POINTER(ll), C.POINTER(ll)]
     L.qcbc_server_set_tiling.argtypes = [vp, i, i]
     L.qcbc_server_timing.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d)]
+    L.qcbc_server_set_device_steps.argtypes = [vp, i]
     L._serve_bound = True
     return L
 
 
 class Server:
-    def __init__(self, hbm_budget_bytes=150 * 10**9, max_live=256, max_bins=1 << 17, precision=MIXED):
+    """device_steps > 0 keeps the chains on the device and advances every live run by up to that
+    many steps per step() call (qcbc_server_set_device_steps); 0 steps the chains on the host."""
+
+    def __init__(self, hbm_budget_bytes=150 * 10**9, max_live=256, max_bins=1 << 17, precision=MIXED,
+                 device_steps=0):
         L = _bind()
         check(L.qcbc_init(0))
         self._h = L.qcbc_server_create(int(hbm_budget_bytes), int(max_live), int(max_bins), int(precision))
         if not self._h:
             raise QcbcError(-1, _lib.last_error())
+        if device_steps:
+            self.set_device_steps(device_steps)
+
+    def set_device_steps(self, steps):
+        check(_bind().qcbc_server_set_device_steps(self._h, int(steps)))
 
     def close(self):
         if getattr(self, "_h", None):
