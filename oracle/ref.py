@@ -75,6 +75,11 @@ def lib():
         L.ref_het_diff.restype = C.c_double
         L.ref_het_diff.argtypes = [vp, vp, _dp, _dp]
         L.ref_Fisher_Het.argtypes = [vp, vp, _dp, _dp, C.c_double]
+        L.ref_framed_count.argtypes = [C.c_char_p]
+        L.ref_framed_count.restype = C.c_int
+        L.ref_condition.argtypes = [_dp, C.c_int, C.c_double, _dp]
+        L.makespec.argtypes = [C.c_int, C.c_int] + [_dp] * 8 + [C.c_double, C.c_int]
+        L.makespec.restype = None
         _lib = L
     return _lib
 
@@ -253,3 +258,24 @@ class RefHet:
         SN = _f64(SN)
         return lib().ref_lnl_test(self.net.ptr, self.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN,
                                   SN.shape[1], N, Tobs)
+
+
+def framed_count(path):
+    """Row count of a framed file as QuickCBC.c:205-211 computes it (-2: unreadable content)."""
+    return lib().ref_framed_count(str(path).encode())
+
+
+def condition(x, Tobs):
+    """QuickCBC.c:244-258 + 309-313 on one time series: tukey, GSL real FFT, sqrt(Tobs)/N."""
+    x = _f64(x)
+    D = np.zeros(len(x))
+    lib().ref_condition(x, len(x), float(Tobs), D)
+    return D
+
+
+def makespec(ffit, Sspline, linef, lineh, lineQ, linew, deltafmax, Tobs, N):
+    """The reference's makespec (Utilities.c:1908): SN[N/2]."""
+    a = [_f64(v).copy() for v in (ffit, Sspline, linef, lineh, lineQ, linew, deltafmax)]
+    SN = np.zeros(N // 2)
+    lib().makespec(len(a[0]), len(a[2]), *a, SN, float(Tobs), int(N))
+    return SN

@@ -18,6 +18,11 @@
  *   templates            QuickCBC.c:3527     AmpPhase       QuickCBC.c:3395
  *   log_likelihood_intrinsic  QuickCBC.c:4093
  *   het_diff             QuickCBC.c:4966     Fisher_Het     QuickCBC.c:5446
+ *   tukey                Utilities.c:635     makespec       Utilities.c:1908 (called directly)
+ * and two restatements of input steps that live inside QuickCBC.c's main():
+ *   ref_framed_count     the row count of QuickCBC.c:205-211 (same fscanf / feof loop)
+ *   ref_condition        QuickCBC.c:244-258 + 309-313: tukey, gsl_fft_real_radix2_transform,
+ *                        times sqrt(Tobs)/N
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -271,4 +276,29 @@ void ref_het_free(struct Net *net, struct Het *het) {
   if (!het) return;
   if (het->IP) freehet(net, het);
   free(het);
+}
+
+/* Row count of a framed file by the loop of QuickCBC.c:205-211: one fscanf of two values per
+ * pass until the end-of-file flag is set, starting from -1. */
+int ref_framed_count(const char *path) {
+  FILE *in = fopen(path, "r");
+  if (!in) return -1;
+  double x, y;
+  int N = -1;
+  while (!feof(in)) {
+    if (fscanf(in, "%lf%lf", &x, &y) == 0) { N = -2; break; }   /* the reference would loop forever */
+    N++;
+  }
+  fclose(in);
+  return N;
+}
+
+/* D = FFT(tukey(x)) sqrt(Tobs)/N in GSL half-complex layout (QuickCBC.c:244-258, 309-313). */
+void ref_condition(const double *x, int N, double Tobs, double *D) {
+  memcpy(D, x, sizeof(double) * (size_t)N);
+  double alpha = 2.0 * 0.4 / Tobs;
+  tukey(D, alpha, N);
+  gsl_fft_real_radix2_transform(D, 1, N);
+  double fac = sqrt(Tobs) / (double)N;
+  for (int i = 0; i < N; i++) D[i] *= fac;
 }

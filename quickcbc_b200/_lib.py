@@ -85,6 +85,7 @@ def lib():
         L.qcbc_batch_create.restype = vp
         L.qcbc_batch_create.argtypes = [C.POINTER(vp), i]
         L.qcbc_batch_destroy.argtypes = [vp]
+        L.qcbc_batch_set_slot.argtypes = [vp, i, vp]
         L.qcbc_batch_set_tiling.argtypes = [vp, i, i]
         L.qcbc_batch_get_tiling.argtypes = [vp, pi, pi]
         L.qcbc_batch_autotune.argtypes = [vp, pi, _PD, i, i]
@@ -141,6 +142,25 @@ def lib():
         L.het_space.argtypes = [C.POINTER(Net), C.POINTER(Het), _PD, _PD, _PD, C.POINTER(RealVector), _PPD, i, d]
         L.Fisher_Het.restype = None
         L.Fisher_Het.argtypes = [C.POINTER(Net), C.POINTER(Het), _PPD, _PD, d]
+        # input stage (include/qcbc_ingest.h)
+        cp = C.c_char_p
+        L.qcbc_framed_length.argtypes = [cp, pi]
+        L.qcbc_read_framed.argtypes = [cp, i, _PD, _PD]
+        L.qcbc_read_spec.argtypes = [cp, i, _PD, _PD]
+        L.qcbc_analysis_paths.argtypes = [cp, d, d, i, cp, cp, i]
+        L.qcbc_condition_data.argtypes = [i, i, d, _PD, i, _PD, i]
+        L.qcbc_load_analysis.argtypes = [cp, d, d, i, pi, i, _PD, i, _PD, _PD, i]
+        L.qcbc_psd_model_open.restype = vp
+        L.qcbc_psd_model_open.argtypes = [cp, i, pi]
+        L.qcbc_psd_model_create.restype = vp
+        L.qcbc_psd_model_create.argtypes = [i, pi, pi, i, i, i, _PD, _PD, _PD]
+        L.qcbc_psd_model_info.argtypes = [vp, pi, pi, pi, pi]
+        L.qcbc_psd_model_close.argtypes = [vp]
+        L.qcbc_psd_draw.argtypes = [vp, i, d, i, _PD, i]
+        L.qcbc_event_set_psd_sample.argtypes = [vp, vp, i]
+        L.qcbc_event_set_psd.argtypes = [vp, _PD, i]
+        L.makespec.restype = None
+        L.makespec.argtypes = [i, i] + [_PD] * 8 + [d, i]
         _lib = L
     return _lib
 

@@ -21,8 +21,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 GEN = os.path.join(CSRC, "_gen")
 LIB = os.path.join(HERE, "libqcbc_gpu.so")
-SOURCES = ["qcbc_kernels.cu", "qcbc_capi.cu", "qcbc_serve.cu", "qcbc_hetspace.cu", "qcbc_ptstep.cu"]
-HEADERS = ["qcbc_device.cuh", "qcbc_kernels.cuh", "qcbc_hetspace.h", "qcbc_ptstep.h"]
+SOURCES = ["qcbc_kernels.cu", "qcbc_capi.cu", "qcbc_serve.cu", "qcbc_hetspace.cu", "qcbc_ptstep.cu", "qcbc_ingest.cu"]
+HEADERS = ["qcbc_device.cuh", "qcbc_kernels.cuh", "qcbc_hetspace.h", "qcbc_ptstep.h", "qcbc_ingest_dev.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall", "--expt-relaxed-constexpr"]
 
@@ -74,7 +74,8 @@ def _stale(target, deps):
 def build(force: bool = False, verbose: bool = False) -> str:
     qnm = gen_qnm()
     deps = [os.path.join(CSRC, s) for s in SOURCES + HEADERS] + [qnm, __file__]
-    deps += [os.path.join(HERE, "..", "include", h) for h in ("qcbc_gpu.h", "qcbc_quickcbc.h", "qcbc_serve.h")]
+    deps += [os.path.join(HERE, "..", "include", h) for h in ("qcbc_gpu.h", "qcbc_quickcbc.h", "qcbc_serve.h",
+                                                                   "qcbc_ingest.h")]
     if not force and not _stale(LIB, deps):
         return LIB
     nvcc = os.environ.get("NVCC", "nvcc")

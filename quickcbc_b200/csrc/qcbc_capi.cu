@@ -14,6 +14,7 @@
 
 #include "qcbc_kernels.cuh"
 #include "qcbc_hetspace.h"
+#include "qcbc_ingest_dev.h"
 #include "../../include/qcbc_gpu.h"
 #include "../../include/qcbc_quickcbc.h"
 #include "_gen/qnm_table.h"
@@ -174,6 +175,8 @@ static int ensure_init() {
   return qcbc_init(d);
 }
 
+extern "C" int qcbc_internal_ensure_init(void) { return ensure_init(); }
+
 extern "C" int qcbc_set_qnm_table(const double* a, const double* fring, const double* fdamp, int n) {
   if (!a || !fring || !fdamp || n < 4) return fail(QCBC_EINVAL, "bad QNM table");
   for (int i = 1; i < n; i++)
@@ -265,6 +268,8 @@ struct HetDev {
   int* d_fgrid = nullptr;
   size_t bytes = 0;
   std::vector<int> fgrid;
+  double pref[11] = {0};       // reference point of tables built by qcbc_het_setup
+  bool has_pref = false;
 };
 
 struct qcbc_event {
@@ -607,6 +612,7 @@ extern "C" int qcbc_het_set(qcbc_event* ev, const qcbc_het_tables* t) {
   if ((rc = het_alloc(ev, t->M, t->J, t->MN, t->MM))) return rc;
   HetDev& h = ev->het;
   h.logLb = t->logLb;
+  h.has_pref = false;
   h.fgrid.assign(t->fgrid, t->fgrid + t->M);
   HetData d = het_data(ev);
   int nI = ev->g.nifo, M = h.M, NR = h.NR, J1 = h.J + 1;
@@ -769,6 +775,8 @@ extern "C" int qcbc_het_setup(qcbc_event* ev, const double* pref, const int* fgr
   for (int id = 0; id < nI; id++) L += pairs[2 * id + 1] + 0.5 * pairs[2 * id];
   h.logLb = L;
   h.fgrid.assign(fgrid, fgrid + M);
+  memcpy(h.pref, pref, sizeof(h.pref));
+  h.has_pref = true;
   CU(cudaMemcpy((void*)hd.freq, freq.data(), M * 8, cudaMemcpyHostToDevice));
   CU(cudaMemcpy((void*)hd.amp, amp.data(), amp.size() * 8, cudaMemcpyHostToDevice));
   CU(cudaMemcpy((void*)hd.phase, ph.data(), ph.size() * 8, cudaMemcpyHostToDevice));
@@ -2024,4 +2032,70 @@ extern "C" int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int
   tls_launches += 3;
   CU(cudaGetLastError());
   return QCBC_OK;
+}
+
+// ================================================================== PSD changes (noise marginalisation)
+// After the event's device PSD rows changed: the in-band minimum of each detector (device reduction),
+// sigma = sqrt(min) as at upload, the weighted data rebuilt on the device with the same arithmetic
+// as event_upload, and heterodyne tables built by qcbc_het_setup rebuilt about the same reference
+// point and grid (QuickCBC.c:1994-2010).  Tables given by qcbc_het_set are dropped.
+static int event_psd_changed(qcbc_event* ev, Workspace* w) {
+  const int nI = ev->g.nifo, nh = ev->nh;
+  const int lo = std::max(ev->g.imin, 1), hi = std::min(ev->g.imax, nh);
+  int rc;
+  if ((rc = grow(w->d_b, w->c_b, (size_t)2 * kMaxIfo))) return rc;
+  cudaStream_t s = w->stream;
+  qcbc::launch_band_min(ev->d_S, nh + 1, nI, lo, hi, w->d_b, s);
+  double smin[kMaxIfo];
+  CU(cudaMemcpyAsync(smin, w->d_b, sizeof(double) * nI, cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  qcbc::Sigmas sg{{1.0, 1.0, 1.0}};
+  for (int id = 0; id < nI; id++) {
+    double m = smin[id];
+    if (!(m < HUGE_VAL)) m = 1.0;
+    sg.v[id] = sqrt(m);
+    ev->inv_sigma[id] = 1.0 / sg.v[id];
+  }
+  qcbc::launch_event_weights(ev->d_D, ev->g.N, ev->d_S, nh + 1, nI, lo, hi, sg, ev->d_w64, ev->d_w4, s);
+  tls_launches += 2;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(s));
+  HetDev& h = ev->het;
+  if (h.buf && h.has_pref) {
+    double pref[11];
+    memcpy(pref, h.pref, sizeof(pref));
+    std::vector<int> grid = h.fgrid;
+    return qcbc_het_setup(ev, pref, grid.data(), h.M, h.MN, h.MM, h.J);
+  }
+  if (h.buf) {
+    cudaFree(h.buf);
+    cudaFree(h.d_fgrid);
+    h = HetDev();
+  }
+  return QCBC_OK;
+}
+
+extern "C" int qcbc_event_set_psd_sample(qcbc_event* ev, qcbc_psd_model* m, int k) {
+  if (!ev || !m) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->has_data) return fail(QCBC_EINVAL, "event has no data");
+  if (qcbc::psd_model_nifo(m) != ev->g.nifo)
+    return fail(QCBC_EINVAL, "model has %d detectors, event %d", qcbc::psd_model_nifo(m), ev->g.nifo);
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = qcbc::psd_model_draw_dev(m, k, ev->g.Tobs, ev->g.N, ev->d_S, ev->nh + 1, w->stream))) return rc;
+  return event_psd_changed(ev, w);
+}
+
+extern "C" int qcbc_event_set_psd(qcbc_event* ev, const double* SN, int sn_stride) {
+  if (!ev || !SN) return fail(QCBC_EINVAL, "NULL argument");
+  if (!ev->has_data) return fail(QCBC_EINVAL, "event has no data");
+  if (sn_stride < ev->nh) return fail(QCBC_EINVAL, "sn_stride < N/2");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  for (int id = 0; id < ev->g.nifo; id++)
+    CU(cudaMemcpyAsync(ev->d_S + (size_t)id * (ev->nh + 1), SN + (size_t)id * sn_stride, sizeof(double) * ev->nh,
+                       cudaMemcpyHostToDevice, w->stream));
+  return event_psd_changed(ev, w);
 }

@@ -166,6 +166,19 @@ class Event:
         check(lib().qcbc_het_diff(self._h, _ptr(A), _ptr(Bp), A.shape[0], _ptr(out)))
         return out
 
+    def set_psd(self, SN):
+        """A new PSD, SN [nifo, >= N/2] (qcbc_event_set_psd): weighted data and heterodyne tables
+        built by het_setup are rebuilt on the device."""
+        SN = _f64(np.atleast_2d(SN))
+        if SN.shape[0] != self.nifo or SN.shape[1] < self.N // 2:
+            raise ValueError("SN must be [nifo, >= N/2]")
+        check(lib().qcbc_event_set_psd(self._h, _ptr(SN), SN.shape[1]))
+
+    def set_psd_sample(self, model, k):
+        """noisemarg redraw (qcbc_event_set_psd_sample): PSD sample k of `model` (ingest.PsdModel)
+        evaluated on the device into this event, then the same rebuilds as set_psd."""
+        check(lib().qcbc_event_set_psd_sample(self._h, model.handle, int(k)))
+
     def het_fisher(self, params):
         """Fisher matrices [B][11][11] from the heterodyne tables (Fisher_Het), one launch for all sets."""
         P = _f64(np.atleast_2d(params))
@@ -188,6 +201,12 @@ class Batch:
         self._h = lib().qcbc_batch_create(arr, len(self.events))
         if not self._h:
             raise QcbcError(-1, _lib.last_error())
+
+    def set_slot(self, slot, event):
+        """(Re)fill slot `slot` with `event` (qcbc_batch_set_slot), e.g. after its PSD or heterodyne
+        tables changed; None empties it."""
+        check(lib().qcbc_batch_set_slot(self._h, int(slot), event.handle if event is not None else None))
+        self.events[slot] = event
 
     def close(self):
         if getattr(self, "_h", None):

@@ -23,6 +23,7 @@ network optimal SNR over the analysis band equals the requested value.
 """
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass, field
 import numpy as np
 
@@ -247,3 +248,77 @@ def uneven_params(events, chains=32, proposals=8, seed=4000 + 500000, scale=1e-3
     P = np.vstack([jitter_params(rng, n, ev.inj, scale=scale) for ev in events])
     eo = np.repeat(np.arange(len(events), dtype=np.int32), n)
     return eo, P
+
+
+# --- analysis input files ------------------------------------------------------
+def time_series(ev):
+    """Strain time series whose scaled FFT is the event's data: x = irfft of D (half-complex,
+    scaled by sqrt(Tobs)/N) times N/sqrt(Tobs).  [Nifo, N]."""
+    N = ev.N
+    M = N // 2
+    out = np.zeros((len(ev.labels), N))
+    for i in range(len(ev.labels)):
+        d = ev.D[i]
+        X = np.zeros(M + 1, dtype=complex)
+        X[0] = d[0]
+        X[M] = d[M]
+        X[1:M] = d[1:M] + 1j * d[N - 1:M:-1]
+        out[i] = np.fft.irfft(X, n=N) * N / np.sqrt(ev.Tobs)
+    return out
+
+
+def psd_model_arrays(rng, nifo, Tobs, N, nsample=3, nknots=(24, 20, 16), nlines=(6, 4, 5)):
+    """A spline-plus-lines PSD model of `nsample` samples per detector: knots from 1/Tobs to
+    (N/2)/Tobs, log PSD of the analytic curve with 5 % scatter per sample, lines near 60 Hz
+    multiples and calibration-like frequencies with heights 10-1000 and Q 500-5000.
+    Returns (nspline, nlines, ffit [nifo, nsp], xspline [nifo, nsample, nsp],
+    lines [nifo, nsample, nlm, 5])."""
+    ns = np.array(nknots[:nifo], dtype=np.int32)
+    nl = np.array(nlines[:nifo], dtype=np.int32)
+    nsp, nlm = int(ns.max()), int(nl.max())
+    ffit = np.zeros((nifo, nsp))
+    xs = np.zeros((nifo, nsample, nsp))
+    L = np.zeros((nifo, nsample, nlm, 5))
+    fhi = (N // 2) / Tobs
+    base = np.array([60.0, 120.0, 35.9, 331.3, 502.5, 999.7])
+    for i in range(nifo):
+        n = ns[i]
+        ffit[i, :n] = np.concatenate([[1.0 / Tobs], np.geomspace(6.0, 0.8 * fhi, n - 2), [fhi]])
+        for s in range(nsample):
+            xs[i, s, :n] = np.log(psd(ffit[i, :n])) + 0.05 * rng.normal(size=n)
+            for j in range(nl[i]):
+                lf = base[j] * (1.0 + 1e-3 * rng.normal())
+                L[i, s, j] = [lf, 10.0 ** rng.uniform(1, 3), rng.uniform(500, 5000), rng.uniform(0.5, 4.0),
+                              rng.uniform(0.05, 0.5)]
+    return ns, nl, ffit, xs, L
+
+
+def write_analysis_files(directory, labels, Tobs, ttrig, x, SN, SM=None):
+    """framed_ and spec_ files as SpecFit writes them (SpecFit.c:207-213, 888-897): rows
+    "t x" with %.16e, rows "f SN SM PS" with %.15e (PS written as 0)."""
+    N = x.shape[1]
+    dt = Tobs / N
+    for i, lab in enumerate(labels):
+        fr = os.path.join(directory, "framed_%d_%d_%d.dat" % (int(Tobs), int(ttrig), lab))
+        with open(fr, "w") as f:
+            f.writelines("%.16e %.16e\n" % (k * dt, v) for k, v in enumerate(x[i]))
+        sp = os.path.join(directory, "spec_%d_%d_%d.dat" % (int(Tobs), int(ttrig), lab))
+        sm = SN[i] if SM is None else SM[i]
+        with open(sp, "w") as f:
+            f.writelines("%.15e %.15e %.15e %.15e\n" % (k / Tobs, SN[i][k], sm[k], 0.0) for k in range(N // 2))
+
+
+def write_psd_model_files(directory, labels, nspline, nlines, ffit, xspline, lines):
+    """summary_, ffile_, sfile_ and lfile_ files in the layout QuickCBC.c:322-378 reads."""
+    nsample = xspline.shape[1]
+    for i, lab in enumerate(labels):
+        n, m = int(nspline[i]), int(nlines[i])
+        with open(os.path.join(directory, "summary_%d.dat" % lab), "w") as f:
+            f.write("%d %d %d\n" % (n, m, nsample))
+        with open(os.path.join(directory, "ffile_%d.dat" % lab), "w") as f:
+            f.writelines("%.16e\n" % v for v in ffit[i, :n])
+        with open(os.path.join(directory, "sfile_%d.dat" % lab), "w") as f:
+            f.writelines(" ".join("%.16e" % v for v in xspline[i, s, :n]) + "\n" for s in range(nsample))
+        with open(os.path.join(directory, "lfile_%d.dat" % lab), "w") as f:
+            for s in range(nsample):
+                f.writelines(" ".join("%.16e" % v for v in lines[i, s, j]) + "\n" for j in range(m))

@@ -19,6 +19,11 @@ Contents (float64 unless noted):
   secondary1.npz  config 1: templates and log_likelihood_intrinsic on intrinsic-layout
                parameter sets, AmpPhase, and het_diff / Fisher_Het on the reference's
                heterodyne tables of het1.npz's grid
+  ingest1.npz  config-1 input stage: time series x whose conditioned data (the reference's
+               tukey + real FFT + sqrt(Tobs)/N) are D; the spec-file PSD SN as read back from
+               its %.15e text; a 3-sample spline-plus-lines PSD model and the reference's
+               makespec of every sample and detector; reference lnL on (D, SN) and on
+               (D, makespec sample 1)
 """
 from __future__ import annotations
 
@@ -196,8 +201,31 @@ def make_secondary1():
                         fisher=fish)
 
 
+def make_ingest1():
+    ev = synth.config_event(1, ref_template_factory())
+    net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+    x = synth.time_series(ev)
+    D = np.array([ref.condition(xi, ev.Tobs) for xi in x])
+    nh = ev.N // 2
+    # the spec file's PSD column as the reference reads it back (%.15e text)
+    SN = np.array([[float("%.15e" % v) for v in row[:nh]] for row in ev.SN])
+    ns, nl, ffit, xs, L = synth.psd_model_arrays(np.random.default_rng(1800), len(ev.labels), ev.Tobs, ev.N)
+    S = np.zeros((xs.shape[1], len(ev.labels), nh))
+    for k in range(xs.shape[1]):
+        for i in range(len(ev.labels)):
+            n, m = ns[i], nl[i]
+            S[k, i] = ref.makespec(ffit[i, :n], xs[i, k, :n], L[i, k, :m, 0], L[i, k, :m, 1], L[i, k, :m, 2],
+                                   L[i, k, :m, 3], L[i, k, :m, 4], ev.Tobs, ev.N)
+    P = synth.jitter_params(np.random.default_rng(1801), 6, ev.inj)
+    lnl = np.array([ref.lnl_full(net, D, p, ev.freq, SN, ev.N, ev.Tobs)[0] for p in P])
+    lnl_s1 = np.array([ref.lnl_full(net, D, p, ev.freq, S[1], ev.N, ev.Tobs)[0] for p in P])
+    np.savez_compressed(os.path.join(OUT, "ingest1.npz"), labels=ev.labels, Tobs=ev.Tobs, N=ev.N, fmin=ev.fmin,
+                        GMST=ev.GMST, inj=ev.inj, x=x, D=D, SN=SN, nspline=ns, nlines=nl, ffit=ffit, xspline=xs,
+                        lines=L, makespec=S, params=P, lnl=lnl, lnl_sample1=lnl_s1)
+
+
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"wave", "cfg1", "het1", "grid3", "secondary1"}
+    which = set(sys.argv[1:]) or {"wave", "cfg1", "het1", "grid3", "secondary1", "ingest1"}
     if "wave" in which:
         make_wave()
     if which & {"cfg1", "het1"}:
@@ -208,6 +236,8 @@ if __name__ == "__main__":
         make_grid3()
     if "secondary1" in which:
         make_secondary1()
+    if "ingest1" in which:
+        make_ingest1()
     for f in sorted(os.listdir(OUT)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(OUT, f)))
