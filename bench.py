@@ -329,6 +329,62 @@ def bench_cfg3_het(q):
     return out
 
 
+def bench_input_stage(q):
+    """Input stage at config 3 sizes (3 det, 128 s, 4096 Hz, N = 2^19): data conditioning
+    (Tukey window, FFT, sqrt(Tobs)/N) and the noisemarg PSD redraw of an event holding heterodyne
+    tables (makespec of every detector, weighted data, heterodyne tables rebuilt), on the GPU and
+    with the reference's CPU code (tukey + GSL-layout FFT; makespec + heterodyne, one thread)."""
+    from quickcbc_b200 import ingest, synth
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    ev = synth.config_event(3, tmpl)
+    g3 = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
+    x = synth.time_series(ev)
+    ingest.condition_data(x, ev.Tobs)
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        D = ingest.condition_data(x, ev.Tobs)
+        ts.append(time.perf_counter() - t0)
+    ns, nl, ffit, xs, L = synth.psd_model_arrays(np.random.default_rng(3800), 3, ev.Tobs, ev.N, nsample=4,
+                                                 nknots=(64, 64, 64), nlines=(6, 6, 6))
+    m = ingest.PsdModel(ffit, xs, L, ns, nl)
+    e = q.Event(ev.labels, ev.Tobs, ev.GMST, ev.N, D, m.draw(0, ev.Tobs, ev.N), fmin=ev.fmin)
+    e.het_setup(ev.inj, g3["fgrid"], int(g3["MN"]), int(g3["MM"]), 2)
+    e.set_psd_sample(m, 1)
+    tr = []
+    for k in range(6):
+        t0 = time.perf_counter()
+        e.set_psd_sample(m, k % 4)
+        tr.append(time.perf_counter() - t0)
+    out = {"workload": "config 3 input stage: 3 det x N = 2^19; PSD model 64 knots + 6 lines x 4 samples, "
+                       "het grid M=%d" % len(g3["fgrid"]),
+           "condition_data_s": float(np.median(ts)), "noisemarg_redraw_s": float(np.median(tr))}
+    try:
+        from oracle import ref
+        if ref.available():
+            t0 = time.perf_counter()
+            Dr = np.array([ref.condition(xi, ev.Tobs) for xi in x])
+            out["reference_condition_s"] = time.perf_counter() - t0
+            out["condition_max_rel_diff"] = float(np.max(np.abs(D - Dr)) / np.max(np.abs(Dr)))
+            net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+            het = ref.RefHet(net)
+            het.set_grid(g3["fgrid"], int(g3["MN"]), int(g3["MM"]), 2, ev.Tobs)
+            t0 = time.perf_counter()
+            S = np.zeros((3, ev.N // 2 + 1))
+            for i in range(3):
+                S[i, :ev.N // 2] = ref.makespec(ffit[i], xs[i, 1], *L[i, 1].T, ev.Tobs, ev.N)
+            het.heterodyne(Dr, ev.inj, ev.freq, S, ev.N, ev.Tobs)
+            out["reference_redraw_s"] = time.perf_counter() - t0
+            out["reference_cores"] = 1
+    except Exception as exc:
+        out["reference"] = f"unavailable: {type(exc).__name__}: {exc}"
+    e.close()
+    m.close()
+    return out
+
+
 def bench_cfg4_uneven(q):
     """Config 4: 256 uneven events x (32 chains x 8 proposals) in one graph-captured
     persistent launch, autotuned tiling, mixed and FP64."""
@@ -420,6 +476,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true", help="skip configs 1, 3, 4 and the reduced config 5")
     ap.add_argument("--serve", action="store_true", help="config 5 serving stream only")
+    ap.add_argument("--input-stage", action="store_true", help="config 3 input stage only")
     ap.add_argument("--serve-runs", type=int, default=32)
     ap.add_argument("--serve-steps", type=int, default=20000)
     ap.add_argument("--serve-prec", default="mixed,fp64,mixed-het,mixed-dev,mixed-het-dev")
@@ -443,6 +500,12 @@ def main():
         res = bench_cfg5_serving(q, n_runs=args.serve_runs, n_steps=args.serve_steps,
                                  precisions=tuple(args.serve_prec.split(",")), device_steps=args.serve_dev_steps)
         print(json.dumps({"metric": "time-to-posterior p50/p99 and aggregate lnL evals/s (config 5)", **res}))
+        return
+    if args.input_stage:
+        import quickcbc_b200 as q
+        from quickcbc_b200 import _lib
+        _lib.check(_lib.lib().qcbc_init(0))
+        print(json.dumps({"metric": "input-stage seconds (config 3)", **bench_input_stage(q)}))
         return
 
     from quickcbc_b200.replicas import Replicas
@@ -551,6 +614,7 @@ def main():
         out["config1_per_call"] = bench_cfg1_percall(q, eng, _lib)
         out["config3"] = bench_cfg3_het(q)
         out["config4_uneven"] = bench_cfg4_uneven(q)
+        out["input_stage"] = bench_input_stage(q)
         out["config5_serving_reduced"] = bench_cfg5_serving(q, n_runs=16, n_steps=1000, rate_hz=2.0)
         out["config5_serving_reduced"]["note"] = ("reduced: 16 runs x 1000 steps per run (config 5 specifies "
                                                   "20000 steps; full run: bench.py --serve)")
