@@ -175,16 +175,44 @@ void step_point(const double* params, double a, const double* e, const double* p
     }                                                                              \
   } while (0)
 
-// Device scratch of one grid search, released on every exit path.
+// Device scratch of the grid searches of one host thread, kept from call to call (grow-only, per
+// device).  The Fisher waves alone are (2 NP + 1) nifo N/2 doubles twice, about 290 MB at 128 s and
+// 4096 Hz, and allocating and releasing them on every call cost up to a second.  A search ends with
+// its stream synchronised, so the next search of the thread may reuse the buffers.  They are
+// released with the process.
+struct ScratchCache {
+  std::vector<void*> p[16];
+  std::vector<size_t> cap[16];
+};
+thread_local ScratchCache tls_scratch;
+
+// Hands out the cached buffers in the order a search asks for them; on every exit path the search's
+// stream is drained before the buffers can be handed out again.
 struct Scratch {
-  std::vector<void*> p;
-  ~Scratch() { for (void* q : p) cudaFree(q); }
+  int device = 0;
+  size_t next = 0;
+  cudaStream_t stream;
+  explicit Scratch(cudaStream_t s) : stream(s) { cudaGetDevice(&device); }
+  ~Scratch() { cudaStreamSynchronize(stream); }
   template <class T>
   cudaError_t alloc(T** out, size_t n) {
-    void* q = nullptr;
-    cudaError_t e = cudaMalloc(&q, n * sizeof(T) > 0 ? n * sizeof(T) : 1);
-    if (e == cudaSuccess) { p.push_back(q); *out = static_cast<T*>(q); }
-    return e;
+    std::vector<void*>& p = tls_scratch.p[device];
+    std::vector<size_t>& cap = tls_scratch.cap[device];
+    const size_t bytes = n * sizeof(T) > 0 ? n * sizeof(T) : 1;
+    if (next == p.size()) {
+      p.push_back(nullptr);
+      cap.push_back(0);
+    }
+    if (cap[next] < bytes) {
+      cudaFree(p[next]);
+      p[next] = nullptr;
+      cap[next] = 0;
+      cudaError_t e = cudaMalloc(&p[next], bytes);
+      if (e != cudaSuccess) return e;
+      cap[next] = bytes;
+    }
+    *out = static_cast<T*>(p[next++]);
+    return cudaSuccess;
   }
 };
 
@@ -197,7 +225,7 @@ int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin
   const double Tobs = in.Tobs;
   const int ss = in.sn_stride;
   cudaStream_t s = in.stream;
-  Scratch sc;
+  Scratch sc(s);
   double *d_freq, *d_S, *d_par, *d_amp, *d_ph, *d_out;
   PhdRec* d_rec;
   int* d_st;

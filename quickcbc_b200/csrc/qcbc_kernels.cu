@@ -920,38 +920,54 @@ __device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, con
 //  * FP32 partial sums over 8 bins, accumulated in FP64.
 // ---- mixed-precision tile body (coefficients: MixPoly in the record)
 
+// The piece coefficients of a parameter set stay in shared memory (the block's record) and are
+// re-read at every use: asm volatile keeps each load in the bin loop, so the coefficients pin no
+// registers and three blocks of 256 threads fit an SM (80 registers per thread).
+__device__ __forceinline__ double sld(const double& x) {
+  double v;
+  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((uint32_t)__cvta_generic_to_shared(&x)));
+  return v;
+}
+__device__ __forceinline__ float sld(const float& x) {
+  float v;
+  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"((uint32_t)__cvta_generic_to_shared(&x)));
+  return v;
+}
+
 // the three phase pieces in cycles (FP64) and the three amplitude pieces (FP32) at bin xi
 __device__ __forceinline__ double mph_ins(const MixPhIns& q, double xi, double t, double u, double L) {
-  double ph = fma(t, fma(t, q.Att, q.At), q.A0);
-  ph = fma(L, fma(t, q.AtL, q.AL), ph);
-  double pu = fma(u * u, q.Au5, q.Au3);
-  pu = fma(u, pu, q.Auu);
-  pu = fma(u, pu, q.Au);
+  double ph = fma(t, fma(t, sld(q.Att), sld(q.At)), sld(q.A0));
+  ph = fma(L, fma(t, sld(q.AtL), sld(q.AL)), ph);
+  double pu = fma(u * u, sld(q.Au5), sld(q.Au3));
+  pu = fma(u, pu, sld(q.Auu));
+  pu = fma(u, pu, sld(q.Au));
   ph = fma(u, pu, ph);
-  double pi = fma(xi, q.Aii, fma(t, fma(t, q.Aitt, q.Ait), q.Ai));
+  double pi = fma(xi, sld(q.Aii), fma(t, fma(t, sld(q.Aitt), sld(q.Ait)), sld(q.Ai)));
   return fma(xi, pi, ph);
 }
 __device__ __forceinline__ double mph_int(const MixPhInt& q, double xi, double u, double L) {
   double u3 = u * u * u;
-  return fma(xi, q.Bi, q.B0) + fma(L, q.BL, (u3 * u3 * u3) * q.Bu9);
+  return fma(xi, sld(q.Bi), sld(q.B0)) + fma(L, sld(q.BL), (u3 * u3 * u3) * sld(q.Bu9));
 }
 __device__ __forceinline__ double mph_mrd(const MixPhMrd& q, double xi, double u, double s) {
-  double at = (double)atanf((float)fma(xi, q.D1, -q.D0));
-  return fma(xi, q.Ri, q.R0) + fma(u * u * u, q.Ru3, fma(s, q.Rs, q.Rat * at));
+  const double at = (double)atanf((float)fma(xi, sld(q.D1), -sld(q.D0)));
+  return fma(xi, sld(q.Ri), sld(q.R0)) + fma(u * u * u, sld(q.Ru3), fma(s, sld(q.Rs), sld(q.Rat) * at));
 }
 __device__ __forceinline__ float mamp_ins(const MixAmpIns& a, float xf, float tf) {
   const float* al = a.al;
-  float inner = fmaf(xf, al[7], fmaf(tf, fmaf(tf, al[6], al[5]), al[4]));
-  float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, al[3], al[2]), al[1]));
-  return fmaf(xf, mid, fmaf(tf * tf, al[0], 1.0f));
+  float inner = fmaf(xf, sld(al[7]), fmaf(tf, fmaf(tf, sld(al[6]), sld(al[5])), sld(al[4])));
+  float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, sld(al[3]), sld(al[2])), sld(al[1])));
+  return fmaf(xf, mid, fmaf(tf * tf, sld(al[0]), 1.0f));
 }
 __device__ __forceinline__ float mamp_int(const MixAmpInt& a, double xi) {
-  float x = (float)fma(xi, a.m, -a.hx1);
-  return a.hc[0] + x * (a.hc[1] + x * (a.hc[2] + (x - a.h21) * (a.hc[3] + (x - a.h31) * a.hc[4])));
+  float x = (float)fma(xi, sld(a.m), -sld(a.hx1));
+  return sld(a.hc[0]) +
+         x * (sld(a.hc[1]) +
+              x * (sld(a.hc[2]) + (x - sld(a.h21)) * (sld(a.hc[3]) + (x - sld(a.h31)) * sld(a.hc[4]))));
 }
 __device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, double xi) {
-  float dfr = (float)fma(xi, a.m, -a.fRD);
-  return __fdividef(__expf(-dfr * a.g2_over_fg) * a.fg_g1, dfr * dfr + a.fg2);
+  float dfr = (float)fma(xi, sld(a.m), -sld(a.fRD));
+  return __fdividef(__expf(-dfr * sld(a.g2_over_fg)) * sld(a.fg_g1), dfr * dfr + sld(a.fg2));
 }
 
 // piece of bin i: 0 inspiral, 1 intermediate, 2 merger-ringdown
@@ -998,18 +1014,12 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
                                            double* acc) {
   if (i > i1) return;
   const int n = min(k_end - k, (i1 - i) / bs + 1);     // rows of this thread in the run
-  MixPhIns qi;
-  MixPhInt qn;
-  MixPhMrd qm;
-  MixAmpIns ai;
-  MixAmpInt an;
-  MixAmpMrd am;
-  if (PP == 0) qi = P.pins;
-  if (PP == 1) qn = P.pint;
-  if (PP == 2) qm = P.pmrd;
-  if (AP == 0) ai = P.ains;
-  if (AP == 1) an = P.aint;
-  if (AP == 2) am = P.amrd;
+  const MixPhIns& qi = P.pins;      // in shared memory, read per use (sld)
+  const MixPhInt& qn = P.pint;
+  const MixPhMrd& qm = P.pmrd;
+  const MixAmpIns& ai = P.ains;
+  const MixAmpInt& an = P.aint;
+  const MixAmpMrd& am = P.amrd;
   const size_t nh = (size_t)ev.nh;
   const float2* pr = s_rot + k;
   const double dbs = (double)bs;
@@ -1021,6 +1031,7 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
     const int m = min(8, n - r);
     MixAcc<NIFO> A;
     A.zero();
+#pragma unroll 1
     for (int j = 0; j < m; j++) {
       const double2 tA = __ldg(ev.tabA + b), tB = __ldg(ev.tabB + b);
       float4 wv[NIFO];
@@ -1041,7 +1052,8 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       else if (AP == 2) a = mamp_mrd(am, xi);
       else {
         const int ap = amp_piece(P, b);
-        a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x) : (ap == 1 ? mamp_int(P.aint, xi) : mamp_mrd(P.amrd, xi));
+        a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x)
+                    : (ap == 1 ? mamp_int(P.aint, xi) : mamp_mrd(P.amrd, xi));
       }
       A.add(wv[0].w * a, (float)(ph - rint(ph)), wv, pr, nk);
       b += bs;
@@ -1164,7 +1176,7 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
 }
 
 #ifndef QCBC_MIXED_MINBLOCKS
-#define QCBC_MIXED_MINBLOCKS 2
+#define QCBC_MIXED_MINBLOCKS 3     // 80 registers: the piece coefficients are read from shared memory
 #endif
 // Sums over the threads of each group of gs threads (gs a multiple of 32) in a fixed order;
 // the first thread of each group holds its group's sums.
@@ -1187,6 +1199,7 @@ __device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][
   }
 }
 
+// Mixed-precision full lnL over one tile of bins of one parameter set.
 // Mixed-precision full lnL over one tile of bins of one parameter set.
 template <int NIFO>
 __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
@@ -1372,10 +1385,10 @@ void launch_scan_expand(const int* d_ntile, int B, int* d_off, int* d_items, int
 }
 
 #ifndef QCBC_MULTI_MINBLOCKS
-#define QCBC_MULTI_MINBLOCKS 2
+#define QCBC_MULTI_MINBLOCKS 3
 #endif
-// The FP64 body is light on registers and wants occupancy; the mixed body keeps its piece
-// coefficients in registers.
+// Both bodies are held to the register budget of three or more blocks per SM: the FP64 body is
+// light on registers, the mixed body reads its piece coefficients from shared memory.
 template <int PREC>
 __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS) k_lnl_multi(const PhdRec* __restrict__ recs,
                                                       const EventDesc* __restrict__ events,
