@@ -10,9 +10,11 @@
  * runs keep their data on the device and their chains on the host.  Every
  * qcbc_server_step() advances every live run by one step: one proposal per
  * chain (Gaussian, per-parameter scales adapted towards 25% acceptance during
- * burn-in, angles wrapped, sin/cos reflected), all proposals of all live runs
- * evaluated in ONE multi-event launch (qcbc_lnl_multi), Metropolis acceptance
- * at each chain's temperature, one swap attempt between adjacent temperatures
+ * burn-in, angles wrapped, sin/cos reflected; or the reference's mixture, see
+ * qcbc_run_spec.proposal), all proposals of all live runs evaluated in ONE
+ * multi-event launch (qcbc_lnl_multi), Metropolis acceptance at each chain's
+ * temperature with the reference's prior density (flat in m1, m2, uniform in
+ * volume: QuickCBC.c:2352-2381), one swap attempt between adjacent temperatures
  * per ladder, thinned samples of the T = 1 chains kept after burn-in.  Finished
  * runs release their slot and device memory.  A run's chains use their own
  * random stream and the lnL of a set does not depend on the other sets of the
@@ -51,10 +53,18 @@ typedef struct {
                                and tables are built about `start` (het_space + heterodyne,
                                QuickCBC.c:4570, 5112) and every step uses the heterodyned lnL
                                (log_likelihood_het, QuickCBC.c:5303), as the reference's sampler does */
+  int proposal;             /* QCBC_PROPOSE_GAUSS: Gaussian steps with scales adapted during burn-in;
+                               QCBC_PROPOSE_REFERENCE (device-resident stepping only): the reference's
+                               mixture (update, QuickCBC.c:2266-2333) of Fisher eigen-jumps, differential
+                               evolution and jiggles; its Fisher matrix and jump sizes (Fisher_Het,
+                               FisherEvec, efix) are computed at the starting point at admission, from
+                               heterodyne tables built there for either likelihood */
 } qcbc_run_spec;
 
 #define QCBC_LNL_FULL 0
 #define QCBC_LNL_HET 1
+#define QCBC_PROPOSE_GAUSS 0
+#define QCBC_PROPOSE_REFERENCE 1
 
 #define QCBC_RUN_QUEUED 0
 #define QCBC_RUN_LIVE 1

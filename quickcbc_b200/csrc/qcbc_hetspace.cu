@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -218,6 +219,47 @@ struct Scratch {
 
 }  // namespace
 
+void fisher_evec_11(const double (&F)[11][11], double* ej, double (&ev)[11][11]) { fisher_evec(F, ej, ev); }
+
+int efix_run(const double* params, const double* pmin, const double* pmax, double* eval, const double (&evec)[11][11],
+             double zs, const std::function<int(const double*, double&)>& dist) {
+  const double zmx = zs * 2.0, zmn = zs / 2.0;
+  double px[NP], e[NP];
+  int rc;
+  for (int i = 0; i < NP; ++i) {
+    double dzmin = 1.0e20, alpham = 1.0, alpha0 = 1.0, z0 = 0.0, z = 0.0;
+    for (int j = 0; j < NP; j++) e[j] = eval[i] * evec[i][j];
+    int k = 0;
+    do {
+      step_point(params, alpha0, e, pmin, pmax, px);
+      if ((rc = dist(px, z0))) return rc;
+      double dz = fabs(z0 - zs);
+      if (dz < dzmin) { dzmin = dz; alpham = alpha0; }
+      if (z0 < zmn) alpha0 *= 2.0;
+      if (z0 > zmx) alpha0 /= 1.9;
+      k++;
+    } while ((z0 > zmx || z0 < zmn) && k < 15 && fabs(alpha0 < 1.0e4));
+    double alpha = alpha0 * 1.1;
+    k = 0;
+    do {
+      step_point(params, alpha, e, pmin, pmax, px);
+      if ((rc = dist(px, z))) return rc;
+      double alphanew;
+      if (alpha > alpha0) alphanew = alpha0 + (zs - z0) / (z - z0) * (alpha - alpha0);
+      else alphanew = alpha + (zs - z) / (z0 - z) * (alpha0 - alpha);
+      double dz = fabs(z - zs);
+      if (dz < dzmin) { dzmin = dz; alpham = alpha; }
+      z0 = z;
+      alpha0 = alpha;
+      alpha = alphanew;
+      k++;
+    } while (fabs(z - zs) > 0.2 && k < 10 && fabs(alpha < 1.0e4));
+    if (dzmin / zs > 1.0) alpham = 0.0;               // kill any failed direction
+    eval[i] *= alpham;
+  }
+  return 0;
+}
+
 int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin, const double* pmax,
                   HetSpaceOut& out, std::string& err) {
   const NetGeom& g = in.g;
@@ -353,41 +395,9 @@ int het_space_run(const HetSpaceIn& in, const double* params, const double* pmin
     for (int c = 0; c < kChunks; c++) z += part[c];
     return 0;
   };
-  {
-    const double zs = 30.0, zmx = zs * 2.0, zmn = zs / 2.0;
-    double px[NP], e[NP];
-    for (int i = 0; i < NP; ++i) {
-      double dzmin = 1.0e20, alpham = 1.0, alpha0 = 1.0, z0 = 0.0, z = 0.0;
-      for (int j = 0; j < NP; j++) e[j] = eval[i] * evec[i][j];
-      int k = 0;
-      do {
-        step_point(params, alpha0, e, pmin, pmax, px);
-        if ((rc = diff(px, z0))) return rc;
-        double dz = fabs(z0 - zs);
-        if (dz < dzmin) { dzmin = dz; alpham = alpha0; }
-        if (z0 < zmn) alpha0 *= 2.0;
-        if (z0 > zmx) alpha0 /= 1.9;
-        k++;
-      } while ((z0 > zmx || z0 < zmn) && k < 15 && fabs(alpha0 < 1.0e4));
-      double alpha = alpha0 * 1.1;
-      k = 0;
-      do {
-        step_point(params, alpha, e, pmin, pmax, px);
-        if ((rc = diff(px, z))) return rc;
-        double alphanew;
-        if (alpha > alpha0) alphanew = alpha0 + (zs - z0) / (z - z0) * (alpha - alpha0);
-        else alphanew = alpha + (zs - z) / (z0 - z) * (alpha0 - alpha);
-        double dz = fabs(z - zs);
-        if (dz < dzmin) { dzmin = dz; alpham = alpha; }
-        z0 = z;
-        alpha0 = alpha;
-        alpha = alphanew;
-        k++;
-      } while (fabs(z - zs) > 0.2 && k < 10 && fabs(alpha < 1.0e4));
-      if (dzmin / zs > 1.0) alpham = 0.0;               // kill any failed direction
-      eval[i] *= alpham;
-    }
-  }
+  auto dist = [&](const double* px, double& z) -> int { return diff(px, z); };
+  rc = efix_run(params, pmin, pmax, eval, evec, 30.0, dist);
+  if (rc != 0) return rc;
 
   // ---- grid walk (QuickCBC.c:4624-4765): the 12 sets' waves, their ratios and the walk on the device
   std::vector<double> P((size_t)(NP + 1) * NP);

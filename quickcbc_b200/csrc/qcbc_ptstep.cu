@@ -1,12 +1,21 @@
-// Device-resident parallel-tempering step (see qcbc_ptstep.h).  The scheme is the host
-// service's (qcbc_serve.cu, after the reference's MCMC_all / update, QuickCBC.c:1781-2405): a
-// symmetric step with per-temperature adapted scales, angles wrapped and sin/cos parameters
-// reflected, the prior box and symmetric-mass-ratio limits (QuickCBC.c:1871-1896, 2341-2364),
-// Metropolis acceptance at T = ladder^t, one swap attempt between a random adjacent pair of
-// temperatures per ladder, scale adaptation towards 25 % acceptance every 50 burn-in steps, and
-// thinned samples of the T = 1 chains after burn-in.  Every chain draws from its own xoshiro256**
-// stream and the swap draws come from the ladder's coldest chain, so a run evolves the same
-// alone, in any mix of runs and for any number of steps per host call.
+// Device-resident parallel-tempering step (see qcbc_ptstep.h), after the reference's MCMC_all /
+// update (QuickCBC.c:1781-2405):
+//   * proposals: kProposeGauss, the host service's symmetric step with per-temperature adapted
+//     scales (angles wrapped, sin/cos parameters reflected); or kProposeReference, update's mixture
+//     (QuickCBC.c:2266-2333): Fisher eigen-jumps sqrt(T) ejump[i] N(0,1) along evec[i] (50 %),
+//     differential evolution from the temperature's history (20 %, de_jump QuickCBC.c:2407-2425),
+//     jiggles of 0.01 10^-floor(3U) sqrt(T) N(0,1) in every parameter (10 %); the reference's
+//     sky-ring move (20 %) is not built here and its share goes to the Fisher jump;
+//   * the prior box and symmetric-mass-ratio limits (QuickCBC.c:1871-1896, 2341-2364) and the
+//     prior density of update (QuickCBC.c:2352-2381): flat in m1, m2 (2 ln Mt + ln eta
+//     - ln(1 - 4 eta) / 2 in the ln Mc, ln Mt coordinates) and uniform in volume (3 ln D);
+//   * Metropolis acceptance at T = ladder^t, one swap attempt between a random adjacent pair of
+//     temperatures per ladder, scale adaptation towards 25 % acceptance every 50 burn-in steps
+//     (Gauss proposal only), the history rows of every temperature refreshed every 20 steps, and
+//     thinned samples of the T = 1 chains after burn-in.
+// Every chain draws from its own xoshiro256** stream and the swap draws come from the ladder's
+// coldest chain, so a run evolves the same alone, in any mix of runs and for any number of steps
+// per host call.
 #include "qcbc_ptstep.h"
 
 #include <cmath>
@@ -34,9 +43,33 @@ struct Xoshiro {
     const double s4 = ((double)(uint32_t)a + (double)(a >> 32) + (double)(uint32_t)b + (double)(b >> 32)) * k;
     return (s4 - 2.0) * 1.7320508075688772;
   }
+  // standard normal by the Box-Muller transform
+  __device__ double gauss() {
+    const double u1 = 1.0 - uniform(), u2 = uniform();     // u1 in (0, 1]
+    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+  }
   __device__ void load(const uint64_t* p) { for (int i = 0; i < 4; i++) s[i] = p[i]; }
   __device__ void store(uint64_t* p) const { for (int i = 0; i < 4; i++) p[i] = s[i]; }
 };
+
+// log prior density of update (QuickCBC.c:2352-2381) up to a constant: flat in m1, m2 and uniform
+// in volume, in the sampled ln Mc, ln Mt, ln D coordinates
+__device__ double log_prior(const double* p) {
+  const double leta = (5.0 / 3.0) * (p[0] - p[1]);
+  const double eta = exp(leta);
+  return 2.0 * p[1] + leta - 0.5 * log(fmax(1.0 - 4.0 * eta, 1e-16)) + 3.0 * p[6];   // finite at eta = 1/4
+}
+
+// angles into [0, 2 pi) / [0, pi) (QuickCBC.c:2336-2341); sin/cos parameters are left to the
+// prior box, as the reference does
+__device__ void wrap_angles(double* y) {
+  y[4] = fmod(y[4], kTwoPiP);
+  if (y[4] < 0) y[4] += kTwoPiP;
+  y[7] = fmod(y[7], kTwoPiP);
+  if (y[7] < 0) y[7] += kTwoPiP;
+  y[9] = fmod(y[9], kPiP);
+  if (y[9] < 0) y[9] += kPiP;
+}
 
 __device__ void wrap(double* y) {
   y[4] = fmod(y[4], kTwoPiP);
@@ -66,7 +99,30 @@ __global__ void k_pt_propose(PtRun* __restrict__ runs, PtChains c, int B) {
   const PtRun& r = runs[c.run[b]];
   double y[kPtNP];
   const double* x = c.x + (size_t)b * kPtNP;
-  if (r.init) {
+  if (r.init && r.proposal == kProposeReference) {
+    const int t = (b - r.off) % r.n_temps;
+    const double sT = sqrt(chain_temp(r, t));
+    Xoshiro g;
+    g.load(c.rng + (size_t)b * 4);
+    const double alpha = g.uniform();
+    if (alpha > 0.3 && alpha <= 0.5) {                // differential evolution
+      const double* H = r.hist + (size_t)t * kPtHist * kPtNP;
+      const int i = (int)(g.uniform() * kPtHist);
+      int j = (int)(g.uniform() * kPtHist);
+      for (int k = 0; j == i && k < 64; k++) j = (int)(g.uniform() * kPtHist);
+      const double a = g.uniform() < 0.9 ? 0.5 * g.gauss() : 1.0;
+      for (int k = 0; k < kPtNP; k++) y[k] = x[k] + a * (H[(size_t)i * kPtNP + k] - H[(size_t)j * kPtNP + k]);
+    } else if (alpha > 0.2 && alpha <= 0.3) {         // jiggle
+      const double beta = 0.01 * exp10(-floor(3.0 * g.uniform())) * sT;
+      for (int k = 0; k < kPtNP; k++) y[k] = x[k] + beta * g.gauss();
+    } else {                                          // Fisher eigen-jump (and the sky-ring share)
+      const int i = min((int)(g.uniform() * kPtNP), kPtNP - 1);
+      const double beta = sT * r.ejump[i] * g.gauss();
+      for (int k = 0; k < kPtNP; k++) y[k] = x[k] + beta * r.evec[i][k];
+    }
+    g.store(c.rng + (size_t)b * 4);
+    wrap_angles(y);
+  } else if (r.init) {
     const int t = (b - r.off) % r.n_temps;
     Xoshiro g;
     g.load(c.rng + (size_t)b * 4);
@@ -93,7 +149,9 @@ __global__ void k_pt_accept(PtRun* __restrict__ runs, PtChains c, int B) {
   atomicAdd(&r.prop[t], 1);
   if (t == 0) atomicAdd(&r.cold_prop, 1ULL);
   if (!(Ly > -1e19)) return;
-  const double la = (Ly - c.lnl[b]) / chain_temp(r, t);
+  const double* x = c.x + (size_t)b * kPtNP;
+  const double* y = c.y + (size_t)b * kPtNP;
+  const double la = (Ly - c.lnl[b]) / chain_temp(r, t) + log_prior(y) - log_prior(x);
   bool ok = la >= 0.0;
   if (!ok) {
     Xoshiro g;
@@ -145,7 +203,15 @@ __global__ void k_pt_swap_finish(PtRun* __restrict__ runs, PtChains c) {
   }
   __syncthreads();
   const int step = r.steps_done + 1;
-  if (step <= r.burn_in && step % 50 == 0) {
+  if (r.proposal == kProposeReference && step % 20 == 0) {   // history rows (QuickCBC.c:2068-2080)
+    for (int e = threadIdx.x; e < r.n_chains * r.n_temps; e += blockDim.x) {
+      const int ch = e / r.n_temps, t = e - ch * r.n_temps;
+      const size_t src = (size_t)r.off + (size_t)ch * r.n_temps + t;
+      double* h = r.hist + ((size_t)t * kPtHist + (size_t)((r.hist_pos + ch) % kPtHist)) * kPtNP;
+      for (int j = 0; j < kPtNP; j++) h[j] = c.x[src * kPtNP + j];
+    }
+  }
+  if (r.proposal == kProposeGauss && step <= r.burn_in && step % 50 == 0) {
     for (int t = threadIdx.x; t < r.n_temps; t += blockDim.x) {
       const double rate = r.prop[t] ? (double)r.acc[t] / r.prop[t] : 0.25;
       const double f = exp(rate - 0.25);
@@ -168,6 +234,7 @@ __global__ void k_pt_swap_finish(PtRun* __restrict__ runs, PtChains c) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (step > r.burn_in && (step - r.burn_in) % r.thin == 0) r.n_samples = min(r.n_samples + r.n_chains, r.cap_samples);
+    if (r.proposal == kProposeReference && step % 20 == 0) r.hist_pos = (r.hist_pos + r.n_chains) % kPtHist;
     r.steps_done = step;
   }
 }

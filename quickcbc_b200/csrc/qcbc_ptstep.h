@@ -10,6 +10,9 @@ namespace qcbc {
 
 constexpr int kPtMaxTemps = 64;
 constexpr int kPtNP = 11;
+constexpr int kPtHist = 1000;        // differential-evolution history per temperature (NH, ConstCBC.h:72)
+
+enum PtProposal { kProposeGauss = 0, kProposeReference = 1 };
 
 // One live run, as the kernels see it.  Chains of the run are [off, off + nc) of the packed chain
 // arrays; chain c has temperature index c % n_temps and ladder c / n_temps.
@@ -23,6 +26,12 @@ struct PtRun {
   unsigned long long cold_acc, cold_prop, swaps, swap_tries;
   double* samples;                    // device, rows of 12 (11 parameters, lnL)
   int n_samples, cap_samples;
+  // kProposeReference: the reference's proposal mixture (update, QuickCBC.c:2238-2405)
+  int proposal;
+  int hist_pos;                       // next history row of every temperature
+  double* hist;                       // device [n_temps][kPtHist][11]
+  double ejump[kPtNP];                // Fisher jump sizes (FisherEvec + efix at the start point)
+  double evec[kPtNP][kPtNP];          // their eigen-directions
 };
 
 struct PtChains {

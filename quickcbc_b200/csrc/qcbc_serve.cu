@@ -25,6 +25,7 @@
 
 #include "../../include/qcbc_gpu.h"
 #include "../../include/qcbc_serve.h"
+#include "qcbc_hetspace.h"
 #include "qcbc_ptstep.h"
 
 extern "C" int qcbc_internal_fail(int code, const char* msg);
@@ -88,7 +89,9 @@ struct Run {
   int n_temps = 1, n_chains = 1, n_steps = 0, burn_in = 0, thin = 1;
   double ladder = 1.15;
   int likelihood = QCBC_LNL_FULL;
+  int proposal = QCBC_PROPOSE_GAUSS;
   unsigned long long seed = 0;
+  double ejump[11], evec[11][11];            // reference proposal: Fisher jumps at the start point
   // live state
   qcbc_event* ev = nullptr;
   int slot = -1;
@@ -170,6 +173,10 @@ static void retire(qcbc_server* s, Run* r, int state) {
   if (r->pt.samples) {
     cudaFree(r->pt.samples);
     r->pt.samples = nullptr;
+  }
+  if (r->pt.hist) {
+    cudaFree(r->pt.hist);
+    r->pt.hist = nullptr;
   }
   s->dirty = true;
   if (r->slot >= 0) {
@@ -253,7 +260,16 @@ extern "C" long long qcbc_server_submit(qcbc_server* s, const qcbc_run_spec* sp)
     delete r;
     return sfail(QCBC_EINVAL, "likelihood %d", sp->likelihood);
   }
+  if (sp->proposal != QCBC_PROPOSE_GAUSS && sp->proposal != QCBC_PROPOSE_REFERENCE) {
+    delete r;
+    return sfail(QCBC_EINVAL, "proposal %d", sp->proposal);
+  }
+  if (sp->proposal == QCBC_PROPOSE_REFERENCE && s->dev_steps == 0) {
+    delete r;
+    return sfail(QCBC_EINVAL, "the reference proposal runs with device-resident stepping only");
+  }
   r->likelihood = sp->likelihood;
+  r->proposal = sp->proposal;
   r->seed = sp->seed;
   r->rng.seed(sp->seed);
   r->bytes = estimate_bytes(*r);
@@ -304,6 +320,21 @@ static int het_tables(Run* r) {
   return qcbc_het_setup(r->ev, r->start, grid.data(), M, MN, MM, 2);
 }
 
+// Fisher jumps of the reference proposal at the run's starting point: Fisher_Het (QuickCBC.c:5446)
+// from the heterodyne tables, FisherEvec (2449) and efix with het_diff to distance 1 (4387), as
+// MCMC_all prepares them (QuickCBC.c:1917-1923).
+static int fisher_jumps(Run* r) {
+  double F[11][11];
+  int rc = qcbc_het_fisher(r->ev, r->start, 1, &F[0][0]);
+  if (rc != QCBC_OK) return rc;
+  qcbc::fisher_evec_11(F, r->ejump, r->evec);
+  auto dist = [&](const double* px, double& z) -> int {
+    if (qcbc_het_diff(r->ev, r->start, px, 1, &z) != QCBC_OK || !(z == z)) z = 1.0e20;
+    return 0;
+  };
+  return qcbc::efix_run(r->start, r->pmin, r->pmax, r->ejump, r->evec, 1.0, dist);
+}
+
 // Admit queued runs in arrival order while a slot and the budget allow.
 static void admit(qcbc_server* s) {
   while (!s->queue.empty()) {
@@ -316,7 +347,9 @@ static void admit(qcbc_server* s) {
     s->queue.pop_front();
     r->ev = qcbc_event_open(r->nifo, r->labels, r->Tobs, r->GMST, r->N, r->D.data(), r->N, r->SN.data(),
                             r->sn_stride, r->fmin, r->fmax);
-    if (r->ev && r->likelihood == QCBC_LNL_HET && het_tables(r) != QCBC_OK) {
+    const bool need_het = r->likelihood == QCBC_LNL_HET || r->proposal == QCBC_PROPOSE_REFERENCE;
+    if (r->ev && need_het && (het_tables(r) != QCBC_OK ||
+                              (r->proposal == QCBC_PROPOSE_REFERENCE && fisher_jumps(r) != QCBC_OK))) {
       qcbc_event_close(r->ev);
       r->ev = nullptr;
     }
@@ -355,6 +388,14 @@ static void admit(qcbc_server* s) {
     }
     s->live.push_back(r->id);
   }
+}
+
+// log prior density of update (QuickCBC.c:2352-2381) up to a constant: flat in m1, m2 and uniform
+// in volume, in the sampled ln Mc, ln Mt, ln D coordinates
+static double log_prior(const double* p) {
+  const double leta = (5.0 / 3.0) * (p[0] - p[1]);
+  const double eta = std::exp(leta);
+  return 2.0 * p[1] + leta - 0.5 * std::log(std::max(1.0 - 4.0 * eta, 1e-16)) + 3.0 * p[6];
 }
 
 static bool in_prior(const Run* r, const double* y) {
@@ -402,6 +443,20 @@ static int dev_init_run(Run* r, unsigned long long seed) {
   p.ladder = r->ladder;
   for (int j = 0; j < 11; j++) { p.sigma[j] = r->sigma[j]; p.pmin[j] = r->pmin[j]; p.pmax[j] = r->pmax[j]; }
   for (int t = 0; t < r->n_temps; t++) p.scale[t] = std::sqrt(std::pow(r->ladder, t));
+  p.proposal = r->proposal == QCBC_PROPOSE_REFERENCE ? qcbc::kProposeReference : qcbc::kProposeGauss;
+  if (p.proposal == qcbc::kProposeReference) {
+    memcpy(p.ejump, r->ejump, sizeof(p.ejump));
+    memcpy(p.evec, r->evec, sizeof(p.evec));
+    // the history of every temperature starts at the starting point (MCMC_all fills it with the
+    // chains' states, QuickCBC.c:1944-1951)
+    const size_t nh = (size_t)r->n_temps * qcbc::kPtHist;
+    std::vector<double> h(nh * 11);
+    for (size_t k = 0; k < nh; k++) memcpy(&h[k * 11], r->start, sizeof(double) * 11);
+    if (cudaMalloc(&p.hist, sizeof(double) * h.size()) != cudaSuccess)
+      return sfail(QCBC_ENOMEM, "history of %d temperatures", r->n_temps);
+    if (cudaMemcpy(p.hist, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return sfail(QCBC_ECUDA, "history upload failed");
+  }
   int rows = r->n_steps > r->burn_in ? (r->n_steps - r->burn_in) / r->thin : 0;
   p.cap_samples = rows * r->n_chains;
   if (p.cap_samples > 0 &&
@@ -669,7 +724,7 @@ extern "C" int qcbc_server_step(qcbc_server* s, int* n_live, int* n_queued, int*
       r->prop[t]++;
       if (t == 0) r->cold_prop++;
       if (Ly > -1e19) {
-        double la = (Ly - r->lnl[c]) / r->temp[c];
+        double la = (Ly - r->lnl[c]) / r->temp[c] + log_prior(&P[k * 11]) - log_prior(&r->x[(size_t)c * 11]);
         if (la >= 0.0 || std::log(r->rng.uniform()) < la) {
           std::memcpy(&r->x[(size_t)c * 11], &P[k * 11], 11 * sizeof(double));
           r->lnl[c] = Ly;

@@ -25,9 +25,10 @@ class RunSpec(C.Structure):
                 ("D", _PD), ("SN", _PD), ("sn_stride", C.c_int), ("fmin", C.c_double), ("fmax", C.c_double),
                 ("start", _PD), ("scales", _PD), ("prior_min", _PD), ("prior_max", _PD), ("n_temps", C.c_int),
                 ("n_chains", C.c_int), ("n_steps", C.c_int), ("burn_in", C.c_int), ("thin", C.c_int),
-                ("ladder", C.c_double), ("seed", C.c_ulonglong), ("likelihood", C.c_int)]
+                ("ladder", C.c_double), ("seed", C.c_ulonglong), ("likelihood", C.c_int), ("proposal", C.c_int)]
 
 LNL_FULL, LNL_HET = 0, 1
+PROPOSE_GAUSS, PROPOSE_REFERENCE = 0, 1
 
 
 class RunInfo(C.Structure):
@@ -95,11 +96,15 @@ class Server:
         check(_bind().qcbc_server_set_tiling(self._h, int(tile_bins), int(threads)))
 
     def submit(self, ev, start=None, n_temps=16, n_chains=8, n_steps=20000, burn_in=None, thin=10, ladder=1.15,
-               seed=0, scales=None, likelihood="full"):
+               seed=0, scales=None, likelihood="full", proposal="gauss"):
         """Submit a synthetic event (synth.Event); returns the run id.  likelihood "het" builds the
-        heterodyne grid and tables about `start` at admission and samples the heterodyned lnL."""
+        heterodyne grid and tables about `start` at admission and samples the heterodyned lnL.
+        proposal "reference" (device-resident stepping only) uses the reference's mixture of
+        Fisher eigen-jumps, differential evolution and jiggles."""
         if likelihood not in ("full", "het"):
             raise ValueError("likelihood is 'full' or 'het'")
+        if proposal not in ("gauss", "reference"):
+            raise ValueError("proposal is 'gauss' or 'reference'")
         keep = dict(labels=np.ascontiguousarray(ev.labels, dtype=np.int32), D=np.ascontiguousarray(ev.D),
                     SN=np.ascontiguousarray(ev.SN),
                     start=np.ascontiguousarray(ev.inj if start is None else start, dtype=np.float64))
@@ -112,7 +117,8 @@ class Server:
                        scales=keep["scales"].ctypes.data_as(_PD) if scales is not None else None,
                        prior_min=None, prior_max=None, n_temps=n_temps, n_chains=n_chains, n_steps=n_steps,
                        burn_in=n_steps // 4 if burn_in is None else burn_in, thin=thin, ladder=ladder,
-                       seed=int(seed), likelihood=LNL_HET if likelihood == "het" else LNL_FULL)
+                       seed=int(seed), likelihood=LNL_HET if likelihood == "het" else LNL_FULL,
+                       proposal=PROPOSE_REFERENCE if proposal == "reference" else PROPOSE_GAUSS)
         rid = _bind().qcbc_server_submit(self._h, C.byref(spec))
         if rid < 0:
             raise QcbcError(int(rid), _lib.last_error())

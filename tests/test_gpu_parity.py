@@ -233,3 +233,16 @@ def test_cfg3_heterodyne_long_signal(ora):
     Lo, _ = ora.lnl_het_batch(ev, to, g["params"])
     np.testing.assert_allclose(L, Lo, rtol=0, atol=1e-7)
     e.close()
+
+
+def test_cfg3_full_lnl_largest_size(ora):
+    """Config 3 at full size (3 det, 128 s, 4096 Hz: 3 x 128512 bins per set), the largest
+    workload of the suite: FP64 against the oracle on 6 sets, mixed against FP64 on 256 sets."""
+    ev = synth.config_event(3, oracle_template(ora))
+    e = q.Event.from_synthetic(ev)
+    P = synth.jitter_params(np.random.default_rng(3303), 256, ev.inj, scale=1e-5)
+    L64 = e.lnl_full(P, q.FP64)
+    Lo, _ = ora.lnl_full_batch(ev, P[:6])
+    np.testing.assert_allclose(L64[:6], Lo, rtol=0, atol=1e-6)
+    assert np.max(np.abs(e.lnl_full(P, q.MIXED) - L64)) <= LNL_ATOL_MIXED
+    e.close()

@@ -127,3 +127,69 @@ def test_device_stream_driver(events):
     assert res["n_done"] == len(events)
     assert res["lnl_evals"] == sum(2 * 2 * 41 for _ in events)
     srv.close()
+
+
+def reference_sampler(n_steps=400):
+    return dict(n_temps=4, n_chains=4, n_steps=n_steps, burn_in=n_steps // 2, thin=4)
+
+
+@pytest.mark.parametrize("likelihood", ["full", "het"])
+def test_reference_proposal_concentrates_on_injection(ora, likelihood):
+    """The reference's proposal mixture (Fisher eigen-jumps from Fisher_Het + FisherEvec + efix at
+    the start point, differential evolution, jiggles) samples the injection's neighbourhood."""
+    ev = synth.config_event(1, oracle_template(ora), snr=40.0)
+    srv = serving.Server(max_live=4, max_bins=1 << 13, device_steps=32)
+    r = srv.submit(ev, start=ev.inj.copy(), seed=3, likelihood=likelihood, proposal="reference",
+                   **reference_sampler())
+    srv.run_until_idle()
+    s, info = srv.samples(r), srv.info(r)
+    assert info["state"] == serving.RUN_DONE and s.shape == (4 * 50, 12)
+    assert 0.02 < info["accept_cold"] < 0.9 and info["swap_rate"] > 0.0
+    Linj, _ = ora.lnl_full(ev, ev.inj)
+    assert np.max(s[:, 11]) > Linj - 5.0
+    assert abs(np.median(s[:, 0]) - ev.inj[0]) < 0.05
+    assert np.std(s[:, 5]) > 0.0 and np.std(s[:, 7]) > 0.0
+    srv.close()
+
+
+def test_reference_proposal_same_alone_mix_and_K(events):
+    kw = dict(SAMPLER, proposal="reference")
+    s1, _ = run_alone(events[0], 1, seed=31, **kw)
+    s16, _ = run_alone(events[0], 16, seed=31, **kw)
+    assert np.array_equal(s1, s16)
+    mix = serving.Server(max_live=8, max_bins=1 << 15, device_steps=5)
+    ids = [mix.submit(ev, seed=31 + k, likelihood="het" if k % 2 else "full", **kw) for k, ev in enumerate(events)]
+    mix.run_until_idle()
+    assert all(mix.info(i)["state"] == serving.RUN_DONE for i in ids)
+    assert np.array_equal(mix.samples(ids[0]), s1)
+    mix.close()
+
+
+def test_reference_proposal_needs_device_steps(events):
+    srv = serving.Server(max_live=2, max_bins=1 << 15)
+    with pytest.raises(q.QcbcError):
+        srv.submit(events[0], proposal="reference", **SAMPLER)
+    srv.close()
+
+
+@pytest.mark.parametrize("device_steps", [0, 16])
+def test_prior_density_uniform_in_volume(events, device_steps):
+    """With a likelihood that is zero everywhere (no data, PSD 1e30 times the curve) the chains
+    sample the prior of update (QuickCBC.c:2352-2381).  Its distance part is uniform in volume,
+    p(ln D) ~ exp(3 ln D) on [ln 1e6 pc, ln 1e10 pc]: mean b - 1/3 at the upper edge b, where a flat
+    prior in ln D would give the box's middle."""
+    ev = events[0]
+    quiet = synth.Event(**{**ev.__dict__, "D": np.zeros_like(ev.D), "SN": ev.SN * 1e30})
+    b = np.log(1e10 * synth.PC_SI)
+    start = ev.inj.copy()
+    start[6] = b - 0.3
+    scales = np.array([1e-4, 1e-3, 0.02, 0.02, 0.1, 1e-4, 0.3, 0.01, 0.01, 0.02, 0.02])
+    srv = serving.Server(max_live=2, max_bins=1 << 15, device_steps=device_steps)
+    r = srv.submit(quiet, start=start, scales=scales, n_temps=1, n_chains=64, n_steps=3000, burn_in=500, thin=10,
+                   seed=5)
+    srv.run_until_idle()
+    s = srv.samples(r)
+    assert np.max(np.abs(s[:, 11])) < 1e-6, "the likelihood is flat"
+    m = np.mean(s[:, 6])
+    assert abs(m - (b - 1.0 / 3.0)) < 0.06, (m, b - 1.0 / 3.0)
+    srv.close()
