@@ -476,7 +476,8 @@ def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64",
     for name in precisions:
         # "<precision>" samples the full lnL; "<precision>-het" builds each run's heterodyne grid and
         # tables on the GPU at admission and samples the heterodyned lnL, as the reference does;
-        # "-dev" keeps the chains on the device, up to device_steps steps per host call
+        # "-dev" keeps the chains on the device, up to device_steps steps per host call; "-ref" uses
+        # the reference's proposal mixture (Fisher jumps, differential evolution, jiggles)
         parts = name.split("-")
         prec = q.MIXED if parts[0] == "mixed" else q.FP64
         lik = "het" if "het" in parts else "full"
@@ -485,7 +486,8 @@ def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64",
         srv.set_tiling(8192, 256)
         res = serving.serve_stream(srv, evs, rate_hz=rate_hz, seed=5,
                                    sampler=dict(n_temps=16, n_chains=8, n_steps=n_steps, burn_in=n_steps // 4,
-                                                thin=max(1, n_steps // 200), likelihood=lik))
+                                                thin=max(1, n_steps // 200), likelihood=lik,
+                                                proposal="reference" if "ref" in parts else "gauss"))
         st = srv.stats()
         res.pop("ttp_s")
         res["launches"] = st["launches"]
