@@ -524,6 +524,7 @@ def main():
     ap.add_argument("--no-extra", action="store_true", help="skip configs 1, 3, 4 and the reduced config 5")
     ap.add_argument("--serve", action="store_true", help="config 5 serving stream only")
     ap.add_argument("--input-stage", action="store_true", help="config 3 input stage only")
+    ap.add_argument("--cfg3", action="store_true", help="config 3 (heterodyned, 128 s BNS) only")
     ap.add_argument("--cfg4", action="store_true", help="config 4 (256 uneven events) only")
     ap.add_argument("--serve-runs", type=int, default=32)
     ap.add_argument("--serve-steps", type=int, default=20000)
@@ -548,6 +549,12 @@ def main():
         res = bench_cfg5_serving(q, n_runs=args.serve_runs, n_steps=args.serve_steps,
                                  precisions=tuple(args.serve_prec.split(",")), device_steps=args.serve_dev_steps)
         print(json.dumps({"metric": "time-to-posterior p50/p99 and aggregate lnL evals/s (config 5)", **res}))
+        return
+    if args.cfg3:
+        import quickcbc_b200 as q
+        from quickcbc_b200 import _lib
+        _lib.check(_lib.lib().qcbc_init(0))
+        print(json.dumps({"metric": "lnL evals/s (config 3)", **bench_cfg3_het(q)}))
         return
     if args.cfg4:
         import quickcbc_b200 as q

@@ -1515,22 +1515,26 @@ void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const
 }
 
 // ---------------------------------------------------------------- heterodyned lnL
-// One block per parameter set.  Phase 1: waveform at the M grid points and the
-// per-detector ratios hc, hs, cc to the reference (QuickCBC.c:5332-5345) into
-// shared memory.  Phase 2: per region r, uu = IP[r] v for v in {cc, hc, hs},
-// contracted with SL / lc / ls and the edge over-count correction
-// (QuickCBC.c:5347-5425); block sum; lnL = logLb - sum (HR + HH/2).
-// Body of one heterodyned lnL for record c (shared memory: sm [3][nifo][M], red [32][4 kMaxIfo]);
-// thread 0 writes *out.
+// One warp per parameter set, several sets per block, no block-wide barrier.  Phase 1: waveform at
+// the M grid points and the per-detector ratios hc, hs, cc to the reference (QuickCBC.c:5332-5345)
+// into the warp's shared memory.  Phase 2: per region r, uu = IP[r] v for v in {cc, hc, hs},
+// contracted with SL / lc / ls and the edge over-count correction (QuickCBC.c:5347-5425); warp sum;
+// lnL = logLb - sum (HR + HH/2).  The warp's shared memory: the record, then [3][nifo][M] doubles.
+constexpr int kRecDoubles = (int)(sizeof(PhdRec) / 8);
+
+// doubles of shared memory one set's warp uses (a multiple of 2, so the next record stays 16-B aligned)
+__host__ __device__ inline int het_warp_doubles(int nifo, int M) { return kRecDoubles + (3 * nifo * M + 1) / 2 * 2; }
+
 template <int PREC>
-__device__ __forceinline__ void het_block(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm, double* red,
-                                          double* out) {
+__device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm,
+                                         double* out) {
+  const int lane = threadIdx.x & 31;
   const int M = h.M, nifo = g.nifo;
   double* s_hc = sm;                 // [nifo][M]
   double* s_hs = sm + nifo * M;
   double* s_cc = sm + 2 * nifo * M;
   constexpr double kInv2Pi = 0.15915494309189533577;
-  for (int j = threadIdx.x; j < M; j += blockDim.x) {
+  for (int j = lane; j < M; j += 32) {
     double f = __ldg(h.freq + j);
     double y = 1.0;
     if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);          // taper below fbegin (QuickCBC.c:3859)
@@ -1568,14 +1572,16 @@ __device__ __forceinline__ void het_block(const PhdRec& c, const NetGeom& g, con
       }
     }
   }
-  __syncthreads();
+  __syncwarp();
   const int J = h.J, J1 = J + 1, NR = h.NR;
   double acc[4 * kMaxIfo];           // per detector: HH, HR, x, y
 #pragma unroll
   for (int k = 0; k < 4 * kMaxIfo; k++) acc[k] = 0.0;
-  for (int r = threadIdx.x; r < NR; r += blockDim.x) {
+  for (int r = lane; r < NR; r += 32) {
     const double* ip = h.IP + (size_t)r * J1 * J1;
-    for (int id = 0; id < nifo; id++) {
+#pragma unroll
+    for (int id = 0; id < kMaxIfo; id++) {     // unrolled: acc stays in registers
+      if (id >= nifo) break;
       const double* sl = h.SL + ((size_t)r * nifo + id) * J1;
       const double* lc = h.lc + ((size_t)r * nifo + id) * J1;
       const double* ls = h.ls + ((size_t)r * nifo + id) * J1;
@@ -1602,8 +1608,10 @@ __device__ __forceinline__ void het_block(const PhdRec& c, const NetGeom& g, con
       }
     }
   }
-  block_sum<4 * kMaxIfo>(acc, red);
-  if (threadIdx.x == 0) {
+#pragma unroll
+  for (int k = 0; k < 4 * kMaxIfo; k++)
+    for (int o = 16; o > 0; o >>= 1) acc[k] += __shfl_xor_sync(0xffffffffu, acc[k], o);
+  if (lane == 0) {
     double L = h.logLb;
     for (int id = 0; id < nifo; id++) {
       double HH = acc[4 * id] - acc[4 * id + 2], HR = acc[4 * id + 1] - acc[4 * id + 3];
@@ -1613,62 +1621,89 @@ __device__ __forceinline__ void het_block(const PhdRec& c, const NetGeom& g, con
   }
 }
 
+// the warp's record into its shared memory
+__device__ __forceinline__ void warp_load_record(double* dst, const PhdRec* src) {
+  const double* s = reinterpret_cast<const double*>(src);
+  for (int k = threadIdx.x & 31; k < kRecDoubles; k += 32) dst[k] = s[k];
+  __syncwarp();
+}
+
 template <int PREC>
-__global__ void __launch_bounds__(256) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
-                                                 NetGeom g, HetData h, double* __restrict__ lnl) {
-  extern __shared__ double sm[];
-  __shared__ PhdRec rec;
-  __shared__ double red[32 * 4 * kMaxIfo];
-  const int b = blockIdx.x;
-  load_record(rec, recs + b);
-  __syncthreads();
+__global__ void __launch_bounds__(128) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+                                                 NetGeom g, HetData h, int B, int warp_doubles,
+                                                 double* __restrict__ lnl) {
+  extern __shared__ __align__(16) double sm[];
+  const int w = threadIdx.x >> 5;
+  const int b = blockIdx.x * (blockDim.x >> 5) + w;
+  if (b >= B) return;                // the whole warp leaves; no block barrier follows
+  double* base = sm + (size_t)w * warp_doubles;
   if (status[b] != kStOK) {
-    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+    if ((threadIdx.x & 31) == 0) lnl[b] = -1.0e20;
     return;
   }
-  het_block<PREC>(rec, g, h, sm, red, lnl + b);
+  warp_load_record(base, recs + b);
+  het_warp<PREC>(*reinterpret_cast<const PhdRec*>(base), g, h, base + kRecDoubles, lnl + b);
 }
 
 // Heterodyned lnL of sets of many events: set b uses the geometry and heterodyne tables of its
 // record's event (het[e].M == 0: the event has no tables, lnL = -1e20).
 template <int PREC>
-__global__ void __launch_bounds__(256) k_lnl_het_multi(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+__global__ void __launch_bounds__(128) k_lnl_het_multi(const PhdRec* __restrict__ recs, const int* __restrict__ status,
                                                        const EventDesc* __restrict__ events,
-                                                       const HetData* __restrict__ het, double* __restrict__ lnl) {
-  extern __shared__ double sm[];
-  __shared__ PhdRec rec;
-  __shared__ double red[32 * 4 * kMaxIfo];
-  const int b = blockIdx.x;
-  load_record(rec, recs + b);
-  __syncthreads();
-  const int e = rec.event;
-  if (status[b] != kStOK || e < 0 || het[e].M == 0) {
-    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+                                                       const HetData* __restrict__ het, int B, int warp_doubles,
+                                                       double* __restrict__ lnl) {
+  extern __shared__ __align__(16) double sm[];
+  const int w = threadIdx.x >> 5;
+  const int b = blockIdx.x * (blockDim.x >> 5) + w;
+  if (b >= B) return;
+  double* base = sm + (size_t)w * warp_doubles;
+  if (status[b] != kStOK) {
+    if ((threadIdx.x & 31) == 0) lnl[b] = -1.0e20;
     return;
   }
-  het_block<PREC>(rec, events[e].g, het[e], sm, red, lnl + b);
+  warp_load_record(base, recs + b);
+  const PhdRec& rec = *reinterpret_cast<const PhdRec*>(base);
+  const int e = rec.event;
+  if (e < 0 || het[e].M == 0) {
+    if ((threadIdx.x & 31) == 0) lnl[b] = -1.0e20;
+    return;
+  }
+  het_warp<PREC>(rec, events[e].g, het[e], base + kRecDoubles, lnl + b);
 }
 
-size_t het_smem_bytes(const NetGeom& g, const HetData& h) { return (size_t)3 * g.nifo * h.M * sizeof(double); }
+size_t het_smem_bytes(const NetGeom& g, const HetData& h) {
+  return (size_t)het_warp_doubles(g.nifo, h.M) * sizeof(double);
+}
+
+// sets per block: four warps while their shared memory stays within 96 KB
+static int het_sets_per_block(size_t warp_bytes) {
+  int n = 4;
+  while (n > 1 && (size_t)n * warp_bytes > 96 * 1024) n >>= 1;
+  return n;
+}
 
 void launch_lnl_het_multi(const PhdRec* d_recs, const int* d_status, int B, const EventDesc* d_events,
                           const HetData* d_het, size_t smem, Precision prec, double* d_lnl, cudaStream_t s) {
   if (B <= 0) return;
-  if (prec == kFP64) k_lnl_het_multi<kFP64><<<B, 128, smem, s>>>(d_recs, d_status, d_events, d_het, d_lnl);
-  else k_lnl_het_multi<kMixed><<<B, 128, smem, s>>>(d_recs, d_status, d_events, d_het, d_lnl);
+  const int spb = het_sets_per_block(smem);
+  const int wd = (int)(smem / sizeof(double));
+  const unsigned grid = (unsigned)((B + spb - 1) / spb);
+  if (prec == kFP64)
+    k_lnl_het_multi<kFP64><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, d_events, d_het, B, wd, d_lnl);
+  else
+    k_lnl_het_multi<kMixed><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, d_events, d_het, B, wd, d_lnl);
 }
 
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, int threads, double* d_lnl, cudaStream_t s) {
+  (void)threads;
   if (B <= 0) return;
-  size_t smem = het_smem_bytes(g, h);
-  if (prec == kFP64) {
-    cudaFuncSetAttribute(k_lnl_het<kFP64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lnl_het<kFP64><<<B, threads, smem, s>>>(d_recs, d_status, g, h, d_lnl);
-  } else {
-    cudaFuncSetAttribute(k_lnl_het<kMixed>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_lnl_het<kMixed><<<B, threads, smem, s>>>(d_recs, d_status, g, h, d_lnl);
-  }
+  const size_t smem = het_smem_bytes(g, h);
+  const int spb = het_sets_per_block(smem);
+  const int wd = het_warp_doubles(g.nifo, h.M);
+  const unsigned grid = (unsigned)((B + spb - 1) / spb);
+  if (prec == kFP64) k_lnl_het<kFP64><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
+  else k_lnl_het<kMixed><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
 }
 
 // ---------------------------------------------------------------- heterodyne-grid waveforms, het_diff, Fisher_Het
@@ -2256,6 +2291,8 @@ void allow_dynamic_smem() {
   allow((const void*)k_lnl_multi<kMixed>);
   allow((const void*)k_lnl_het_multi<kFP64>);
   allow((const void*)k_lnl_het_multi<kMixed>);
+  allow((const void*)k_lnl_het<kFP64>);
+  allow((const void*)k_lnl_het<kMixed>);
 }
 
 }  // namespace qcbc
