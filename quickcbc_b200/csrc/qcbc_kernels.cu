@@ -1521,6 +1521,9 @@ void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const
 // contracted with SL / lc / ls and the edge over-count correction (QuickCBC.c:5347-5425); warp sum;
 // lnL = logLb - sum (HR + HH/2).  The warp's shared memory: the record, then [3][nifo][M] doubles.
 constexpr int kRecDoubles = (int)(sizeof(PhdRec) / 8);
+#ifndef QCBC_HET_MINBLOCKS
+#define QCBC_HET_MINBLOCKS 8     // 64 registers: 32 sets in flight per SM, 4096 sets in one wave
+#endif
 
 // doubles of shared memory one set's warp uses (a multiple of 2, so the next record stays 16-B aligned)
 __host__ __device__ inline int het_warp_doubles(int nifo, int M) { return kRecDoubles + (3 * nifo * M + 1) / 2 * 2; }
@@ -1629,7 +1632,7 @@ __device__ __forceinline__ void warp_load_record(double* dst, const PhdRec* src)
 }
 
 template <int PREC>
-__global__ void __launch_bounds__(128) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+__global__ void __launch_bounds__(128, QCBC_HET_MINBLOCKS) k_lnl_het(const PhdRec* __restrict__ recs, const int* __restrict__ status,
                                                  NetGeom g, HetData h, int B, int warp_doubles,
                                                  double* __restrict__ lnl) {
   extern __shared__ __align__(16) double sm[];
@@ -1648,7 +1651,7 @@ __global__ void __launch_bounds__(128) k_lnl_het(const PhdRec* __restrict__ recs
 // Heterodyned lnL of sets of many events: set b uses the geometry and heterodyne tables of its
 // record's event (het[e].M == 0: the event has no tables, lnL = -1e20).
 template <int PREC>
-__global__ void __launch_bounds__(128) k_lnl_het_multi(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+__global__ void __launch_bounds__(128, QCBC_HET_MINBLOCKS) k_lnl_het_multi(const PhdRec* __restrict__ recs, const int* __restrict__ status,
                                                        const EventDesc* __restrict__ events,
                                                        const HetData* __restrict__ het, int B, int warp_doubles,
                                                        double* __restrict__ lnl) {
