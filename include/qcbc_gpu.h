@@ -125,6 +125,13 @@ int qcbc_lnl_multi_dev(qcbc_batch* batch, const int* d_event_of, const double* d
                        int precision, void* stream);
 int qcbc_lnl_multi_het_dev(qcbc_batch* batch, const int* d_event_of, const double* d_params, int B, double* d_lnl,
                            int precision, void* stream);
+/* Sky-ring proposal map of the reference's sampler (update, QuickCBC.c:2299-2331) on the GPU: x's
+ * sky position turned by `rot` radians about the line between detectors label1 and label2 (ring of
+ * equal time delay, Ring_all), then the distance, polarisation, phase, inclination and geocentre
+ * time that keep the signal in both detectors (skymap_all); *log_jacobian = log |det| of the map's
+ * 4 x 4 Jacobian (skydensity_all).  x, y: [11] host arrays (y's angles not wrapped). */
+int qcbc_sky_ring_map(const double* x, double* y, double GMST, int label1, int label2, double rot,
+                      double* log_jacobian);
 /* Device time of `iters` graph launches on inputs already uploaded by a previous
  * qcbc_lnl_multi call with the same B (no host copies inside the timed span). */
 int qcbc_time_lnl_multi(qcbc_batch* batch, int B, int precision, int iters, int flush_l2, float* ms);

@@ -56,7 +56,7 @@ typedef struct {
   int proposal;             /* QCBC_PROPOSE_GAUSS: Gaussian steps with scales adapted during burn-in;
                                QCBC_PROPOSE_REFERENCE (device-resident stepping only): the reference's
                                mixture (update, QuickCBC.c:2266-2333) of Fisher eigen-jumps, differential
-                               evolution and jiggles; its Fisher matrix and jump sizes (Fisher_Het,
+                               evolution, jiggles and sky-ring moves; its Fisher matrix and jump sizes (Fisher_Het,
                                FisherEvec, efix) are computed at the starting point at admission, from
                                heterodyne tables built there for either likelihood */
 } qcbc_run_spec;

@@ -80,6 +80,10 @@ def lib():
         L.ref_condition.argtypes = [_dp, C.c_int, C.c_double, _dp]
         L.makespec.argtypes = [C.c_int, C.c_int] + [_dp] * 8 + [C.c_double, C.c_int]
         L.makespec.restype = None
+        L.skymap_all.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int]
+        L.skymap_all.restype = None
+        L.skydensity_all.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int]
+        L.skydensity_all.restype = C.c_double
         _lib = L
     return _lib
 
@@ -279,3 +283,18 @@ def makespec(ffit, Sspline, linef, lineh, lineQ, linew, deltafmax, Tobs, N):
     SN = np.zeros(N // 2)
     lib().makespec(len(a[0]), len(a[2]), *a, SN, float(Tobs), int(N))
     return SN
+
+
+def skymap_all(x, y, GMST, ifo1, ifo2):
+    """The reference's skymap_all (QuickCBC.c:7085): fills y's [4, 5, 6, 9, 10] for y's sky position."""
+    x = _f64(x).copy()
+    y = _f64(y).copy()
+    lib().skymap_all(x, y, float(GMST), int(ifo1), int(ifo2))
+    return y
+
+
+def skydensity_all(x, y, GMST, ifo1, ifo2):
+    """The reference's skydensity_all (QuickCBC.c:7411): |det| of the map's 4 x 4 Jacobian."""
+    x = _f64(x).copy()
+    y = _f64(y).copy()
+    return lib().skydensity_all(x, y, float(GMST), int(ifo1), int(ifo2))

@@ -9,9 +9,9 @@ host interface and ``synth`` for the seeded synthetic workloads.
 from ._lib import FP64, MIXED, QcbcError, launch_count  # noqa: F401
 from .engine import (Event, Batch, DeviceBuffer, amp_phase, ampphase, fourier_nwip, fullphaseamp,  # noqa: F401
                      fulltemplates, templates, het_space, log_likelihood_full, log_likelihood_intrinsic, set_band,
-                     LegacyHet,
+                     LegacyHet, sky_ring_map,
                      time_lnl_full, time_lnl_het)
 
 __all__ = ["FP64", "MIXED", "QcbcError", "Event", "Batch", "DeviceBuffer", "amp_phase", "ampphase", "fourier_nwip",
            "fullphaseamp", "fulltemplates", "templates", "het_space", "log_likelihood_full", "log_likelihood_intrinsic", "set_band",
-           "LegacyHet", "time_lnl_full", "time_lnl_het", "launch_count"]
+           "LegacyHet", "sky_ring_map", "time_lnl_full", "time_lnl_het", "launch_count"]

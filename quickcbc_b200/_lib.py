@@ -103,6 +103,7 @@ def lib():
         L.qcbc_het_space_grid.argtypes = [vp, pi]
         L.qcbc_lnl_multi_het.argtypes = [vp, pi, _PD, i, _PD, i]
         L.qcbc_lnl_het_dev.argtypes = [vp, vp, i, vp, i, vp]
+        L.qcbc_sky_ring_map.argtypes = [_PD, _PD, d, i, i, d, C.POINTER(d)]
         L.qcbc_set_full_launch.argtypes = [vp, i, i]
         L.qcbc_get_full_launch.argtypes = [vp, i, i, pi, pi]
         L.qcbc_device_alloc.restype = vp

@@ -2099,3 +2099,25 @@ extern "C" int qcbc_event_set_psd(qcbc_event* ev, const double* SN, int sn_strid
                        cudaMemcpyHostToDevice, w->stream));
   return event_psd_changed(ev, w);
 }
+
+// ================================================================== sky-ring map (one point)
+extern "C" int qcbc_sky_ring_map(const double* x, double* y, double GMST, int label1, int label2, double rot,
+                                 double* log_jacobian) {
+  if (!x || !y || !log_jacobian) return fail(QCBC_EINVAL, "NULL argument");
+  if (label1 < 0 || label1 > 2 || label2 < 0 || label2 > 2 || label1 == label2)
+    return fail(QCBC_EINVAL, "two different detector labels in 0..2");
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  if ((rc = grow(w->d_b, w->c_b, (size_t)2 * kMaxIfo))) return rc;
+  if ((rc = grow(w->d_params, w->c_params, 24))) return rc;
+  cudaStream_t s = w->stream;
+  CU(cudaMemcpyAsync(w->d_params, x, sizeof(double) * 11, cudaMemcpyHostToDevice, s));
+  launch_sky_ring_map(w->d_params, w->d_params + 12, GMST, label1, label2, rot, w->d_b, s);
+  tls_launches += 1;
+  CU(cudaGetLastError());
+  CU(cudaMemcpyAsync(y, w->d_params + 12, sizeof(double) * 11, cudaMemcpyDeviceToHost, s));
+  CU(cudaMemcpyAsync(log_jacobian, w->d_b, sizeof(double), cudaMemcpyDeviceToHost, s));
+  CU(cudaStreamSynchronize(s));
+  return QCBC_OK;
+}

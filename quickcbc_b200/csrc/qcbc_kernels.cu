@@ -15,6 +15,7 @@
 // lnL), 5112-5299 (heterodyne), 5303-5444 (heterodyned lnL); Utilities.c
 // :587-629, 716-736, 995-1109; IMRPhenomD.c:413-563.
 #include "qcbc_kernels.cuh"
+#include "qcbc_ptstep.h"
 #include <cmath>
 #include <cstdio>
 
@@ -2278,6 +2279,198 @@ void launch_nwip(const double* d_a, const double* d_b, const double* d_S, int im
 // Lets the kernels with large dynamic shared memory (rotation tables of long tiles, heterodyne
 // grids) use up to the device's opt-in limit.  Set once per device at initialisation, outside
 // any stream capture.
+// ---------------------------------------------------------------- sky-ring proposal
+// update's fourth move (QuickCBC.c:2299-2331): a new sky position on the ring of equal time delay
+// between two detectors (Ring_all, Utilities.c:1445-1560), the distance, polarisation, phase and
+// inclination that keep the signal in both detectors (skymap_all with uvwz_all, uvwz_sol and
+// exsolve_all, QuickCBC.c:7085-7150, 7295-7405, 7526-7545), and the log of the Jacobian of that
+// map by one-sided differences of step 1e-6 (skydensity_all, QuickCBC.c:7411-7500).
+
+// F+, Fx of detector l at psi = 0 (F_ant with psi = 0), as set_projection evaluates them
+__device__ void sky_ant(int l, double alpha, double sind, double GMST, double& fp, double& fx) {
+  const double cd = sqrt(1.0 - sind * sind);
+  double sa, ca;
+  sincos(GMST - alpha, &sa, &ca);
+  double mp[21], mx[18];
+  antenna_basis(1.0, 0.0, cd, sind, ca, -sa, mp, mx);
+  fp = 0.0;
+  fx = 0.0;
+  for (int k = 0; k < 21; k++) fp += c_antP[l][k] * mp[k];
+  for (int k = 0; k < 18; k++) fx += c_antX[l][k] * mx[k];
+}
+
+// delay from the geocentre to detector l (Times)
+__device__ double sky_delay(int l, double alpha, double sind, double GMST) {
+  const double cd = sqrt(1.0 - sind * sind);
+  double sa, ca;
+  sincos(GMST - alpha, &sa, &ca);
+  return -(c_detpos[l][0] * cd * ca + c_detpos[l][1] * cd * sa + c_detpos[l][2] * sind) / kClight;
+}
+
+// new sky position: the propagation direction turned by `rot` about the line between detectors
+// l1 and l2, which keeps the time delay between them
+__device__ void sky_ring_rotate(const double* x, double* y, int l1, int l2, double GMST, double rot) {
+  double z[3], zm = 0.0;
+  for (int i = 0; i < 3; i++) {
+    z[i] = c_detpos[l1][i] - c_detpos[l2][i];
+    zm += z[i] * z[i];
+  }
+  zm = sqrt(zm);
+  for (int i = 0; i < 3; i++) z[i] /= zm;
+  const double sind = x[8], cosd = sqrt(1.0 - sind * sind);
+  double sa, ca;
+  sincos(x[7] - GMST, &sa, &ca);
+  const double k[3] = {cosd * ca, -cosd * sa, sind};
+  double cmu = z[0] * k[0] + z[1] * k[1] + z[2] * k[2];
+  cmu = fmin(fmax(cmu, -0.999999), 0.999999);
+  const double smu = sqrt(1.0 - cmu * cmu);
+  const double u[3] = {(k[0] - cmu * z[0]) / smu, (k[1] - cmu * z[1]) / smu, (k[2] - cmu * z[2]) / smu};
+  const double v[3] = {(z[1] * k[2] - z[2] * k[1]) / smu, (z[2] * k[0] - z[0] * k[2]) / smu,
+                       (z[0] * k[1] - z[1] * k[0]) / smu};
+  double sr, cr;
+  sincos(rot, &sr, &cr);
+  double kr[3];
+  for (int i = 0; i < 3; i++) kr[i] = cmu * z[i] + smu * (cr * u[i] + sr * v[i]);
+  y[8] = kr[2];
+  double a = GMST - atan2(kr[1], kr[0]);
+  if (a < 0.0) a += kTwoPi;
+  y[7] = a;
+}
+
+// distance, polarisation, phase, inclination and geocentre time at y's sky position that keep the
+// strain in detectors l1 and l2 what it is at x
+__device__ void sky_map(const double* x, double* y, double GMST, int l1, int l2) {
+  double fp1x, fc1x, fp2x, fc2x, fp1y, fc1y, fp2y, fc2y;
+  sky_ant(l1, x[7], x[8], GMST, fp1x, fc1x);
+  sky_ant(l2, x[7], x[8], GMST, fp2x, fc2x);
+  sky_ant(l1, y[7], y[8], GMST, fp1y, fc1y);
+  sky_ant(l2, y[7], y[8], GMST, fp2y, fc2y);
+  // the two polarisation amplitudes of x as (u, v, w, z)
+  const double ci = x[10], Ap = 0.5 * (1.0 + ci * ci), ecc = -ci / Ap, A = Ap / exp(x[6]);
+  double sphi, cphi, s2p, c2p;
+  sincos(x[4], &sphi, &cphi);
+  sincos(2.0 * x[9], &s2p, &c2p);
+  const double ux = A * (cphi * c2p + ecc * sphi * s2p), vx = A * (cphi * s2p - ecc * sphi * c2p);
+  const double wx = A * (sphi * c2p - ecc * cphi * s2p), zx = A * (sphi * s2p + ecc * cphi * c2p);
+  // the same detector responses from y's antenna patterns
+  const double den = fc1y * fp2y - fc2y * fp1y;
+  const double a1 = fc1y * fc2x - fc1x * fc2y, a2 = fc1y * fp2x - fc2y * fp1x;
+  const double b1 = fc1x * fp2y - fc2x * fp1y, b2 = fp2y * fp1x - fp1y * fp2x;
+  const double uy = (vx * a1 + ux * a2) / den, vy = (vx * b1 + ux * b2) / den;
+  const double wy = (zx * a1 + wx * a2) / den, zy = (zx * b1 + wx * b2) / den;
+  // back to phase, polarisation, inclination and distance
+  const double cross = uy * wy + vy * zy, diffn = (uy * uy + vy * vy) - (wy * wy + zy * zy);
+  const double q = 2.0 * cross / diffn, rad = sqrt(1.0 + q * q);
+  double t = atan2(2.0 * cross, diffn);
+  if (t < 0.0) t += kTwoPi;
+  const double phiy = 0.5 * t;
+  const bool f1 = cos(t) > 0.0, f2 = cos(0.5 * t) > 0.0, f3 = sin(0.5 * t) > 0.0;
+  const double pp = ((rad + 1.0) * (uy * uy + vy * vy) + (rad - 1.0) * (wy * wy + zy * zy) + 2.0 * q * cross) /
+                    (2.0 * rad);
+  const double det = uy * zy - vy * wy;
+  const double e = f1 ? det / pp : pp / det;
+  const double ciy = -(1.0 - sqrt(1.0 - e * e)) / e;
+  const double c1 = (1.0 + rad) * uy + q * wy, c2 = (1.0 + rad) * vy + q * zy;
+  double s;
+  if (f1 && f2) s = atan2(c2, c1);
+  else if (f1) s = atan2(-c2, -c1);
+  else if (f3) s = atan2(e * c1, -e * c2);
+  else s = atan2(-e * c1, e * c2);
+  if (s < 0.0) s += kTwoPi;
+  const double Ay = f1 ? sqrt(pp) : sqrt(pp) / fabs(e);
+  y[9] = 0.5 * s;
+  y[10] = ciy;
+  y[6] = log((1.0 + ciy * ciy) / (2.0 * Ay));
+  y[4] = phiy;
+  y[5] = x[5] + sky_delay(l1, x[7], x[8], GMST) - sky_delay(l1, y[7], y[8], GMST);
+}
+
+// log |det| of the 4 x 4 Jacobian of (ln D, psi, phi, cos iota) under sky_map at fixed sky positions
+__device__ double sky_log_jacobian(const double* x, const double* y, double GMST, int l1, int l2) {
+  const double ep = 1.0e-6;
+  const int idx[4] = {6, 9, 4, 10};
+  double J[4][4];
+  for (int i = 0; i < 4; i++) {
+    double xp[11], yp[11];
+    for (int j = 0; j < 11; j++) { xp[j] = x[j]; yp[j] = y[j]; }
+    xp[idx[i]] += ep;
+    sky_map(xp, yp, GMST, l1, l2);
+    // the other branch of the (psi, phi) solution maps back
+    if (fabs(yp[9] + 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] += 0.5 * kPi;
+    if (fabs(yp[9] - 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] -= 0.5 * kPi;
+    if (fabs(yp[4] + kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] += kPi;
+    if (fabs(yp[4] - kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] -= kPi;
+    for (int j = 0; j < 4; j++) J[i][j] = (yp[idx[j]] - y[idx[j]]) / ep;
+  }
+  // determinant by elimination with partial pivoting
+  double d = 1.0;
+  for (int c = 0; c < 4; c++) {
+    int p = c;
+    for (int r = c + 1; r < 4; r++)
+      if (fabs(J[r][c]) > fabs(J[p][c])) p = r;
+    if (J[p][c] == 0.0) return -HUGE_VAL;
+    if (p != c) {
+      for (int k = 0; k < 4; k++) { const double t = J[c][k]; J[c][k] = J[p][k]; J[p][k] = t; }
+      d = -d;
+    }
+    d *= J[c][c];
+    for (int r = c + 1; r < 4; r++) {
+      const double f = J[r][c] / J[c][c];
+      for (int k = c; k < 4; k++) J[r][k] -= f * J[c][k];
+    }
+  }
+  return log(fabs(d));
+}
+
+// ring rotation, signal-preserving map and log Jacobian of one proposal
+__device__ double sky_ring_move(const double* x, double* y, int l1, int l2, double GMST, double rot) {
+  for (int j = 0; j < 11; j++) y[j] = x[j];
+  sky_ring_rotate(x, y, l1, l2, GMST, rot);
+  sky_map(x, y, GMST, l1, l2);
+  return sky_log_jacobian(x, y, GMST, l1, l2);
+}
+
+__global__ void k_pt_skyring(PtRun* __restrict__ runs, PtChains c, int B) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= B || c.kind[b] != kKindSkyRing) return;
+  const PtRun& r = runs[c.run[b]];
+  Xoshiro g;
+  g.load(c.rng + (size_t)b * 4);
+  int id1 = 0, id2 = 1;
+  if (r.nifo > 2) {                  // a random pair of the network's detectors
+    id1 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
+    id2 = id1;
+    for (int k = 0; id2 == id1 && k < 64; k++) id2 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
+    if (id2 == id1) id2 = (id1 + 1) % r.nifo;
+  }
+  double y[11];
+  const double lj = sky_ring_move(c.x + (size_t)b * 11, y, r.labels[id1], r.labels[id2], r.GMST,
+                                  kTwoPi * g.uniform());
+  if (g.uniform() > 0.5) {           // the other half of the (phi, psi) range
+    y[4] += kPi;
+    y[9] += 0.5 * kPi;
+  }
+  g.store(c.rng + (size_t)b * 4);
+  pt_wrap_angles(y);
+  for (int j = 0; j < 11; j++) c.y[(size_t)b * 11 + j] = y[j];
+  c.jack[b] = lj;
+  c.eo[b] = (isfinite(lj) && pt_in_prior(r.pmin, r.pmax, y)) ? r.slot : -1;
+}
+
+void launch_pt_skyring(PtRun* d_runs, PtChains c, int B, cudaStream_t s) {
+  if (B > 0) k_pt_skyring<<<(B + 127) / 128, 128, 0, s>>>(d_runs, c, B);
+}
+
+__global__ void k_sky_ring_map(const double* __restrict__ x, double* __restrict__ y, double GMST, int l1, int l2,
+                               double rot, double* __restrict__ lj) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) *lj = sky_ring_move(x, y, l1, l2, GMST, rot);
+}
+
+void launch_sky_ring_map(const double* d_x, double* d_y, double GMST, int l1, int l2, double rot, double* d_lj,
+                         cudaStream_t s) {
+  k_sky_ring_map<<<1, 32, 0, s>>>(d_x, d_y, GMST, l1, l2, rot, d_lj);
+}
+
 void allow_dynamic_smem() {
   int dev = 0, optin = 0;
   cudaGetDevice(&dev);

@@ -162,6 +162,9 @@ void launch_finalize_multi(const double* d_partials, const PhdRec* d_recs, const
 int multi_blocks_per_sm(Precision prec, int threads, int tile_bins);
 
 void upload_tables();    // constant-memory tables; call once per device
-void allow_dynamic_smem();   // dynamic shared-memory limit of the mixed kernels; once per device
+void allow_dynamic_smem();
+// One sky-ring proposal map (qcbc_sky_ring_map): x -> y on device buffers, log Jacobian in *d_lj.
+void launch_sky_ring_map(const double* d_x, double* d_y, double GMST, int l1, int l2, double rot, double* d_lj,
+                         cudaStream_t s);   // dynamic shared-memory limit of the mixed kernels; once per device
 
 }  // namespace qcbc

@@ -4,8 +4,8 @@
 //     scales (angles wrapped, sin/cos parameters reflected); or kProposeReference, update's mixture
 //     (QuickCBC.c:2266-2333): Fisher eigen-jumps sqrt(T) ejump[i] N(0,1) along evec[i] (50 %),
 //     differential evolution from the temperature's history (20 %, de_jump QuickCBC.c:2407-2425),
-//     jiggles of 0.01 10^-floor(3U) sqrt(T) N(0,1) in every parameter (10 %); the reference's
-//     sky-ring move (20 %) is not built here and its share goes to the Fisher jump;
+//     jiggles of 0.01 10^-floor(3U) sqrt(T) N(0,1) in every parameter (10 %), and the sky ring
+//     (20 %; one detector: Fisher jump instead), which k_pt_skyring (qcbc_kernels.cu) completes;
 //   * the prior box and symmetric-mass-ratio limits (QuickCBC.c:1871-1896, 2341-2364) and the
 //     prior density of update (QuickCBC.c:2352-2381): flat in m1, m2 (2 ln Mt + ln eta
 //     - ln(1 - 4 eta) / 2 in the ln Mc, ln Mt coordinates) and uniform in volume (3 ln D);
@@ -23,53 +23,9 @@
 namespace qcbc {
 namespace {
 
-constexpr double kTwoPiP = 6.2831853071795862319959269370884;
-constexpr double kPiP = 3.1415926535897931159979634685442;
+constexpr double kTwoPiP = kPtTwoPi;
+constexpr double kPiP = kPtPi;
 
-struct Xoshiro {
-  uint64_t s[4];
-  __device__ static uint64_t rotl(uint64_t x, int k) { return (x << k) | (x >> (64 - k)); }
-  __device__ uint64_t next() {
-    const uint64_t r = rotl(s[1] * 5, 7) * 9, t = s[1] << 17;
-    s[2] ^= s[0]; s[3] ^= s[1]; s[1] ^= s[2]; s[0] ^= s[3];
-    s[2] ^= t; s[3] = rotl(s[3], 45);
-    return r;
-  }
-  __device__ double uniform() { return (next() >> 11) * (1.0 / 9007199254740992.0); }
-  // symmetric, zero-mean, unit-variance step: (u1 + u2 + u3 + u4 - 2) sqrt(3)
-  __device__ double step() {
-    const uint64_t a = next(), b = next();
-    const double k = 1.0 / 4294967296.0;
-    const double s4 = ((double)(uint32_t)a + (double)(a >> 32) + (double)(uint32_t)b + (double)(b >> 32)) * k;
-    return (s4 - 2.0) * 1.7320508075688772;
-  }
-  // standard normal by the Box-Muller transform
-  __device__ double gauss() {
-    const double u1 = 1.0 - uniform(), u2 = uniform();     // u1 in (0, 1]
-    return sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
-  }
-  __device__ void load(const uint64_t* p) { for (int i = 0; i < 4; i++) s[i] = p[i]; }
-  __device__ void store(uint64_t* p) const { for (int i = 0; i < 4; i++) p[i] = s[i]; }
-};
-
-// log prior density of update (QuickCBC.c:2352-2381) up to a constant: flat in m1, m2 and uniform
-// in volume, in the sampled ln Mc, ln Mt, ln D coordinates
-__device__ double log_prior(const double* p) {
-  const double leta = (5.0 / 3.0) * (p[0] - p[1]);
-  const double eta = exp(leta);
-  return 2.0 * p[1] + leta - 0.5 * log(fmax(1.0 - 4.0 * eta, 1e-16)) + 3.0 * p[6];   // finite at eta = 1/4
-}
-
-// angles into [0, 2 pi) / [0, pi) (QuickCBC.c:2336-2341); sin/cos parameters are left to the
-// prior box, as the reference does
-__device__ void wrap_angles(double* y) {
-  y[4] = fmod(y[4], kTwoPiP);
-  if (y[4] < 0) y[4] += kTwoPiP;
-  y[7] = fmod(y[7], kTwoPiP);
-  if (y[7] < 0) y[7] += kTwoPiP;
-  y[9] = fmod(y[9], kPiP);
-  if (y[9] < 0) y[9] += kPiP;
-}
 
 __device__ void wrap(double* y) {
   y[4] = fmod(y[4], kTwoPiP);
@@ -84,12 +40,7 @@ __device__ void wrap(double* y) {
   }
 }
 
-__device__ bool in_prior(const PtRun& r, const double* y) {
-  for (int j = 0; j < kPtNP; j++)
-    if (y[j] < r.pmin[j] || y[j] > r.pmax[j]) return false;
-  const double leta = (5.0 / 3.0) * (y[0] - y[1]);
-  return leta <= log(0.25) && leta >= log(0.05);
-}
+__device__ bool in_prior(const PtRun& r, const double* y) { return pt_in_prior(r.pmin, r.pmax, y); }
 
 __device__ double chain_temp(const PtRun& r, int t) { return pow(r.ladder, (double)t); }
 
@@ -115,13 +66,20 @@ __global__ void k_pt_propose(PtRun* __restrict__ runs, PtChains c, int B) {
     } else if (alpha > 0.2 && alpha <= 0.3) {         // jiggle
       const double beta = 0.01 * exp10(-floor(3.0 * g.uniform())) * sT;
       for (int k = 0; k < kPtNP; k++) y[k] = x[k] + beta * g.gauss();
-    } else {                                          // Fisher eigen-jump (and the sky-ring share)
+    } else if (alpha <= 0.2 && r.nifo >= 2) {         // sky ring: completed by k_pt_skyring
+      g.store(c.rng + (size_t)b * 4);
+      for (int j = 0; j < kPtNP; j++) c.y[(size_t)b * kPtNP + j] = x[j];
+      c.kind[b] = kKindSkyRing;
+      c.jack[b] = 0.0;
+      c.eo[b] = -1;
+      return;
+    } else {                                          // Fisher eigen-jump (one detector: also the ring's share)
       const int i = min((int)(g.uniform() * kPtNP), kPtNP - 1);
       const double beta = sT * r.ejump[i] * g.gauss();
       for (int k = 0; k < kPtNP; k++) y[k] = x[k] + beta * r.evec[i][k];
     }
     g.store(c.rng + (size_t)b * 4);
-    wrap_angles(y);
+    pt_wrap_angles(y);
   } else if (r.init) {
     const int t = (b - r.off) % r.n_temps;
     Xoshiro g;
@@ -134,6 +92,8 @@ __global__ void k_pt_propose(PtRun* __restrict__ runs, PtChains c, int B) {
   }
   for (int j = 0; j < kPtNP; j++) c.y[(size_t)b * kPtNP + j] = y[j];
   c.eo[b] = in_prior(r, y) ? r.slot : -1;
+  c.kind[b] = kKindOther;
+  c.jack[b] = 0.0;
 }
 
 __global__ void k_pt_accept(PtRun* __restrict__ runs, PtChains c, int B) {
@@ -151,7 +111,7 @@ __global__ void k_pt_accept(PtRun* __restrict__ runs, PtChains c, int B) {
   if (!(Ly > -1e19)) return;
   const double* x = c.x + (size_t)b * kPtNP;
   const double* y = c.y + (size_t)b * kPtNP;
-  const double la = (Ly - c.lnl[b]) / chain_temp(r, t) + log_prior(y) - log_prior(x);
+  const double la = (Ly - c.lnl[b]) / chain_temp(r, t) + pt_log_prior(y) - pt_log_prior(x) + c.jack[b];
   bool ok = la >= 0.0;
   if (!ok) {
     Xoshiro g;

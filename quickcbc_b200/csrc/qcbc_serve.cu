@@ -140,6 +140,7 @@ struct qcbc_server {
   int capB = 0, capR = 0, Bpk = 0, Bfpk = 0;
   std::vector<long long> packed;
   bool dirty = true;
+  bool any_ref = false;                        // a packed run uses the reference proposal
 };
 
 static void free_dev(qcbc_server* s);
@@ -422,6 +423,7 @@ static void wrap(double* y) {
 static void free_dev(qcbc_server* s) {
   qcbc::PtChains& c = s->dc;
   cudaFree(c.x); cudaFree(c.lnl); cudaFree(c.y); cudaFree(c.lnly); cudaFree(c.eo); cudaFree(c.run); cudaFree(c.rng);
+  cudaFree(c.kind); cudaFree(c.jack);
   cudaFree(s->d_runs);
   c = qcbc::PtChains{};
   s->d_runs = nullptr;
@@ -444,6 +446,9 @@ static int dev_init_run(Run* r, unsigned long long seed) {
   for (int j = 0; j < 11; j++) { p.sigma[j] = r->sigma[j]; p.pmin[j] = r->pmin[j]; p.pmax[j] = r->pmax[j]; }
   for (int t = 0; t < r->n_temps; t++) p.scale[t] = std::sqrt(std::pow(r->ladder, t));
   p.proposal = r->proposal == QCBC_PROPOSE_REFERENCE ? qcbc::kProposeReference : qcbc::kProposeGauss;
+  p.nifo = r->nifo;
+  for (int i = 0; i < r->nifo; i++) p.labels[i] = r->labels[i];
+  p.GMST = r->GMST;
   if (p.proposal == qcbc::kProposeReference) {
     memcpy(p.ejump, r->ejump, sizeof(p.ejump));
     memcpy(p.evec, r->evec, sizeof(p.evec));
@@ -534,7 +539,7 @@ static int dev_pack(qcbc_server* s) {
     qcbc::PtChains& c = s->dc;
     rc |= dev_grow(&c.x, (size_t)B * 11) | dev_grow(&c.lnl, (size_t)B) | dev_grow(&c.y, (size_t)B * 11) |
           dev_grow(&c.lnly, (size_t)B) | dev_grow(&c.eo, (size_t)B) | dev_grow(&c.run, (size_t)B) |
-          dev_grow(&c.rng, (size_t)B * 4);
+          dev_grow(&c.rng, (size_t)B * 4) | dev_grow(&c.kind, (size_t)B) | dev_grow(&c.jack, (size_t)B);
     if (rc) return sfail(QCBC_ENOMEM, "device sampler arrays for %d chains", B);
     s->capB = B;
   }
@@ -565,6 +570,8 @@ static int dev_pack(qcbc_server* s) {
   s->packed = order;
   s->Bpk = B;
   s->Bfpk = Bf;
+  s->any_ref = false;
+  for (long long id : order) s->any_ref |= s->runs[id]->proposal == QCBC_PROPOSE_REFERENCE;
   s->dirty = false;
   return QCBC_OK;
 }
@@ -588,6 +595,7 @@ static int dev_step(qcbc_server* s) {
   qcbc::PtChains c = s->dc;
   for (int k = 0; k < K; k++) {
     qcbc::launch_pt_propose(s->d_runs, c, B, s->dstream);
+    if (s->any_ref) qcbc::launch_pt_skyring(s->d_runs, c, B, s->dstream);
     if (Bf > 0 && (rc = qcbc_lnl_multi_dev(s->batch, c.eo, c.y, Bf, c.lnly, s->precision, s->dstream))) return rc;
     if (Bh > 0 &&
         (rc = qcbc_lnl_multi_het_dev(s->batch, c.eo + Bf, c.y + (size_t)Bf * 11, Bh, c.lnly + Bf, s->precision,

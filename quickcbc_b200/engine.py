@@ -497,3 +497,14 @@ class LegacyHet:
             arr = getattr(h, k)
             t[k] = np.array([[arr[i][r] for r in range(NR)] for i in range(nI)])
         return t
+
+
+def sky_ring_map(x, GMST, label1, label2, rot):
+    """The reference sampler's sky-ring map on the GPU (qcbc_sky_ring_map): x's sky position turned
+    by `rot` about the line between two detectors, the extrinsic parameters that keep their signal,
+    and the log Jacobian of the map.  Returns (y [11], log_jacobian)."""
+    x = _f64(x).copy()
+    y = np.zeros(11)
+    lj = C.c_double()
+    check(lib().qcbc_sky_ring_map(_ptr(x), _ptr(y), float(GMST), int(label1), int(label2), float(rot), C.byref(lj)))
+    return y, lj.value
