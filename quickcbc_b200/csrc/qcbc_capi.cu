@@ -794,7 +794,7 @@ static int enqueue_het(Workspace* w, qcbc_event* ev, const double* d_params, int
   if ((rc = grow(w->d_status, w->c_status, (size_t)B))) return rc;
   DeviceState& ds = g_dev[current_device()];
   launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s);
-  launch_lnl_het(w->d_recs, w->d_status, B, g, het_data(ev), prec == QCBC_MIXED ? kMixed : kFP64, 128, d_lnl, s);
+  launch_lnl_het(w->d_recs, w->d_status, B, g, het_data(ev), prec == QCBC_MIXED ? kMixed : kFP64, d_lnl, s);
   tls_launches += 2;
   CU(cudaGetLastError());
   return QCBC_OK;

@@ -1699,8 +1699,7 @@ void launch_lnl_het_multi(const PhdRec* d_recs, const int* d_status, int B, cons
 }
 
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
-                    Precision prec, int threads, double* d_lnl, cudaStream_t s) {
-  (void)threads;
+                    Precision prec, double* d_lnl, cudaStream_t s) {
   if (B <= 0) return;
   const size_t smem = het_smem_bytes(g, h);
   const int spb = het_sets_per_block(smem);

@@ -81,7 +81,8 @@ void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const 
 // fill the per-bin tables for bins [0, n)
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
-                    Precision prec, int threads, double* d_lnl, cudaStream_t s);
+                    Precision prec, double* d_lnl, cudaStream_t s);
+// shared memory of one set's warp in the heterodyned kernels (its record and [3][nifo][M] doubles)
 size_t het_smem_bytes(const NetGeom& g, const HetData& h);
 // heterodyned lnL of sets of many events (records from launch_setup_multi); d_het [n_events] (M = 0:
 // no tables); smem = the largest het_smem_bytes over the events
