@@ -2336,14 +2336,27 @@ __device__ void sky_ring_rotate(const double* x, double* y, int l1, int l2, doub
   y[7] = a;
 }
 
+// antenna patterns (psi = 0) of the two detectors at x's and at y's sky positions, and detector
+// l1's delay at both: all that sky_map needs of the geometry
+struct SkyPair {
+  double fp1x, fc1x, fp2x, fc2x, fp1y, fc1y, fp2y, fc2y, dt1x, dt1y;
+};
+__device__ SkyPair sky_pair(const double* x, const double* y, double GMST, int l1, int l2) {
+  SkyPair a;
+  sky_ant(l1, x[7], x[8], GMST, a.fp1x, a.fc1x);
+  sky_ant(l2, x[7], x[8], GMST, a.fp2x, a.fc2x);
+  sky_ant(l1, y[7], y[8], GMST, a.fp1y, a.fc1y);
+  sky_ant(l2, y[7], y[8], GMST, a.fp2y, a.fc2y);
+  a.dt1x = sky_delay(l1, x[7], x[8], GMST);
+  a.dt1y = sky_delay(l1, y[7], y[8], GMST);
+  return a;
+}
+
 // distance, polarisation, phase, inclination and geocentre time at y's sky position that keep the
 // strain in detectors l1 and l2 what it is at x
-__device__ void sky_map(const double* x, double* y, double GMST, int l1, int l2) {
-  double fp1x, fc1x, fp2x, fc2x, fp1y, fc1y, fp2y, fc2y;
-  sky_ant(l1, x[7], x[8], GMST, fp1x, fc1x);
-  sky_ant(l2, x[7], x[8], GMST, fp2x, fc2x);
-  sky_ant(l1, y[7], y[8], GMST, fp1y, fc1y);
-  sky_ant(l2, y[7], y[8], GMST, fp2y, fc2y);
+__device__ void sky_map(const double* x, double* y, const SkyPair& ap) {
+  const double fp1x = ap.fp1x, fc1x = ap.fc1x, fp2x = ap.fp2x, fc2x = ap.fc2x;
+  const double fp1y = ap.fp1y, fc1y = ap.fc1y, fp2y = ap.fp2y, fc2y = ap.fc2y;
   // the two polarisation amplitudes of x as (u, v, w, z)
   const double ci = x[10], Ap = 0.5 * (1.0 + ci * ci), ecc = -ci / Ap, A = Ap / exp(x[6]);
   double sphi, cphi, s2p, c2p;
@@ -2381,27 +2394,25 @@ __device__ void sky_map(const double* x, double* y, double GMST, int l1, int l2)
   y[10] = ciy;
   y[6] = log((1.0 + ciy * ciy) / (2.0 * Ay));
   y[4] = phiy;
-  y[5] = x[5] + sky_delay(l1, x[7], x[8], GMST) - sky_delay(l1, y[7], y[8], GMST);
+  y[5] = x[5] + ap.dt1x - ap.dt1y;
 }
 
-// log |det| of the 4 x 4 Jacobian of (ln D, psi, phi, cos iota) under sky_map at fixed sky positions
-__device__ double sky_log_jacobian(const double* x, const double* y, double GMST, int l1, int l2) {
-  const double ep = 1.0e-6;
-  const int idx[4] = {6, 9, 4, 10};
-  double J[4][4];
-  for (int i = 0; i < 4; i++) {
-    double xp[11], yp[11];
-    for (int j = 0; j < 11; j++) { xp[j] = x[j]; yp[j] = y[j]; }
-    xp[idx[i]] += ep;
-    sky_map(xp, yp, GMST, l1, l2);
-    // the other branch of the (psi, phi) solution maps back
-    if (fabs(yp[9] + 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] += 0.5 * kPi;
-    if (fabs(yp[9] - 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] -= 0.5 * kPi;
-    if (fabs(yp[4] + kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] += kPi;
-    if (fabs(yp[4] - kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] -= kPi;
-    for (int j = 0; j < 4; j++) J[i][j] = (yp[idx[j]] - y[idx[j]]) / ep;
-  }
-  // determinant by elimination with partial pivoting
+// parameters of the Jacobian: ln D, psi, phi, cos iota
+__device__ __forceinline__ int sky_jidx(int j) { return j == 0 ? 6 : (j == 1 ? 9 : (j == 2 ? 4 : 10)); }
+constexpr double kSkyEp = 1.0e-6;           // its difference step (skydensity_all)
+
+// row i of the Jacobian from the perturbed image yp, with the other branch of the (psi, phi)
+// solution mapped back onto y's
+__device__ void sky_jrow(double* yp, const double* y, double* row) {
+  if (fabs(yp[9] + 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] += 0.5 * kPi;
+  if (fabs(yp[9] - 0.5 * kPi - y[9]) < fabs(yp[9] - y[9])) yp[9] -= 0.5 * kPi;
+  if (fabs(yp[4] + kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] += kPi;
+  if (fabs(yp[4] - kPi - y[4]) < fabs(yp[4] - y[4])) yp[4] -= kPi;
+  for (int j = 0; j < 4; j++) row[j] = (yp[sky_jidx(j)] - y[sky_jidx(j)]) / kSkyEp;
+}
+
+// log |det| of a 4 x 4 matrix by elimination with partial pivoting
+__device__ double log_abs_det4(double (&J)[4][4]) {
   double d = 1.0;
   for (int c = 0; c < 4; c++) {
     int p = c;
@@ -2421,35 +2432,76 @@ __device__ double sky_log_jacobian(const double* x, const double* y, double GMST
   return log(fabs(d));
 }
 
-// ring rotation, signal-preserving map and log Jacobian of one proposal
-__device__ double sky_ring_move(const double* x, double* y, int l1, int l2, double GMST, double rot) {
-  for (int j = 0; j < 11; j++) y[j] = x[j];
-  sky_ring_rotate(x, y, l1, l2, GMST, rot);
-  sky_map(x, y, GMST, l1, l2);
-  return sky_log_jacobian(x, y, GMST, l1, l2);
+// One sky-ring proposal by a group of kSkyLanes lanes: lane 0 maps x, lanes 1..4 map x perturbed
+// along the Jacobian's parameters (independent: the sky positions are fixed), then lane 0 gathers
+// the rows by shuffles and takes log |det| (skydensity_all).  Every lane of the group must call it
+// (the shuffles), with the same l1, l2, rot; y and the return value are lane 0's.
+constexpr int kSkyLanes = 8;
+__device__ double sky_ring_group(const double* x, double* y, int l1, int l2, double GMST, double rot, int gl) {
+  double ys[11];
+  for (int j = 0; j < 11; j++) ys[j] = x[j];
+  sky_ring_rotate(x, ys, l1, l2, GMST, rot);
+  const SkyPair ap = sky_pair(x, ys, GMST, l1, l2);
+  double xp[11], yp[11];
+  for (int j = 0; j < 11; j++) { xp[j] = x[j]; yp[j] = ys[j]; }
+  if (gl >= 1 && gl <= 4) xp[sky_jidx(gl - 1)] += kSkyEp;
+  if (gl <= 4) sky_map(xp, yp, ap);
+  // lane 0's image to every lane of the group
+  double yb[11];
+  for (int j = 0; j < 11; j++) yb[j] = __shfl_sync(0xffffffffu, yp[j], 0, kSkyLanes);
+  double row[4] = {0.0, 0.0, 0.0, 0.0};
+  if (gl >= 1 && gl <= 4) sky_jrow(yp, yb, row);
+  double J[4][4];
+  for (int i = 0; i < 4; i++)
+    for (int k = 0; k < 4; k++) J[i][k] = __shfl_sync(0xffffffffu, row[k], i + 1, kSkyLanes);
+  for (int j = 0; j < 11; j++) y[j] = yb[j];
+  return log_abs_det4(J);
 }
 
+// sky-ring proposals of the step: kSkyLanes lanes per chain, all lanes reach every shuffle
 __global__ void k_pt_skyring(PtRun* __restrict__ runs, PtChains c, int B) {
-  const int b = blockIdx.x * blockDim.x + threadIdx.x;
-  if (b >= B || c.kind[b] != kKindSkyRing) return;
-  const PtRun& r = runs[c.run[b]];
-  Xoshiro g;
-  g.load(c.rng + (size_t)b * 4);
-  int id1 = 0, id2 = 1;
-  if (r.nifo > 2) {                  // a random pair of the network's detectors
-    id1 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
-    id2 = id1;
-    for (int k = 0; id2 == id1 && k < 64; k++) id2 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
-    if (id2 == id1) id2 = (id1 + 1) % r.nifo;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int b = t / kSkyLanes, gl = t % kSkyLanes;
+  const bool ring = b < B && c.kind[b] == kKindSkyRing;
+  // the group's draws, by lane 0 from the chain's stream
+  int l1 = 0, l2 = 1;
+  double rot = 0.0, half = 0.0, GMST = 0.0;
+  const double* x = nullptr;
+  if (ring) {
+    const PtRun& r = runs[c.run[b]];
+    GMST = r.GMST;
+    x = c.x + (size_t)b * 11;
+    if (gl == 0) {
+      Xoshiro g;
+      g.load(c.rng + (size_t)b * 4);
+      int id1 = 0, id2 = 1;
+      if (r.nifo > 2) {              // a random pair of the network's detectors
+        id1 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
+        id2 = id1;
+        for (int k = 0; id2 == id1 && k < 64; k++) id2 = min((int)(r.nifo * g.uniform()), r.nifo - 1);
+        if (id2 == id1) id2 = (id1 + 1) % r.nifo;
+      }
+      l1 = r.labels[id1];
+      l2 = r.labels[id2];
+      rot = kTwoPi * g.uniform();
+      half = g.uniform();
+      g.store(c.rng + (size_t)b * 4);
+    }
   }
+  l1 = __shfl_sync(0xffffffffu, l1, 0, kSkyLanes);
+  l2 = __shfl_sync(0xffffffffu, l2, 0, kSkyLanes);
+  rot = __shfl_sync(0xffffffffu, rot, 0, kSkyLanes);
+  half = __shfl_sync(0xffffffffu, half, 0, kSkyLanes);
+  double xl[11];
+  for (int j = 0; j < 11; j++) xl[j] = ring ? x[j] : 0.5;   // lanes of other chains map a dummy point
   double y[11];
-  const double lj = sky_ring_move(c.x + (size_t)b * 11, y, r.labels[id1], r.labels[id2], r.GMST,
-                                  kTwoPi * g.uniform());
-  if (g.uniform() > 0.5) {           // the other half of the (phi, psi) range
+  const double lj = sky_ring_group(xl, y, l1, l2, GMST, rot, gl);
+  if (!ring || gl != 0) return;
+  const PtRun& r = runs[c.run[b]];
+  if (half > 0.5) {                  // the other half of the (phi, psi) range
     y[4] += kPi;
     y[9] += 0.5 * kPi;
   }
-  g.store(c.rng + (size_t)b * 4);
   pt_wrap_angles(y);
   for (int j = 0; j < 11; j++) c.y[(size_t)b * 11 + j] = y[j];
   c.jack[b] = lj;
@@ -2457,12 +2509,20 @@ __global__ void k_pt_skyring(PtRun* __restrict__ runs, PtChains c, int B) {
 }
 
 void launch_pt_skyring(PtRun* d_runs, PtChains c, int B, cudaStream_t s) {
-  if (B > 0) k_pt_skyring<<<(B + 127) / 128, 128, 0, s>>>(d_runs, c, B);
+  if (B > 0) k_pt_skyring<<<(B * kSkyLanes + 127) / 128, 128, 0, s>>>(d_runs, c, B);
 }
 
+// one point: the first group of the one warp maps it, the other groups map a dummy point
 __global__ void k_sky_ring_map(const double* __restrict__ x, double* __restrict__ y, double GMST, int l1, int l2,
                                double rot, double* __restrict__ lj) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) *lj = sky_ring_move(x, y, l1, l2, GMST, rot);
+  const int gl = threadIdx.x % kSkyLanes;
+  double xl[11], yl[11];
+  for (int j = 0; j < 11; j++) xl[j] = threadIdx.x < kSkyLanes ? x[j] : 0.5;
+  const double v = sky_ring_group(xl, yl, l1, l2, GMST, rot, gl);
+  if (threadIdx.x == 0) {
+    for (int j = 0; j < 11; j++) y[j] = yl[j];
+    *lj = v;
+  }
 }
 
 void launch_sky_ring_map(const double* d_x, double* d_y, double GMST, int l1, int l2, double rot, double* d_lj,
