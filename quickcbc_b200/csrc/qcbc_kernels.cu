@@ -325,7 +325,7 @@ __device__ __forceinline__ void phd_taylorf2(PhdRec& c, const PhdMass& m, double
   v[6] = (11583.231236531 / 4.694215680 - 640.0 / 3.0 * kPi * kPi - 6848.0 / 21.0 * kGammaE) +
          et * (-15737.765635 / 3.048192 + 2255. / 12. * kPi * kPi) + et * et * 76055.0 / 1728.0 -
          et * et * et * 127825.0 / 1296.0;
-  v[6] += (-6848.0 / 21.0) * MO::log(4.);
+  v[6] += (-6848.0 / 21.0) * 1.3862943611198906;     // log 4
   vl[6] = -6848.0 / 21.0;
   v[7] = kPi * (77096675.0 / 254016.0 + 378515.0 / 1512.0 * et - 74045.0 / 756.0 * et * et);
   double sig = et * (721.0 / 48.0 * chi1 * chi2 - 247.0 / 48.0 * chi1 * chi2);
@@ -509,8 +509,10 @@ __device__ __forceinline__ SetPhys set_phys(const double* p) {
   return s;
 }
 
-// Per-detector projection: |F|, polarisation phase lambda, geocentre delay (QuickCBC.c:3724-3750).
-__device__ __forceinline__ void set_projection(PhdRec& c, const double* p, const NetGeom& g) {
+// Per-detector projection: |F|, polarisation phase lambda, geocentre delay (QuickCBC.c:3724-3750),
+// for detectors [id0, id1) of the network.
+__device__ __forceinline__ void set_projection(PhdRec& c, const double* p, const NetGeom& g, int id0 = 0,
+                                               int id1 = kMaxIfo) {
   double Ap = (1.0 + p[10] * p[10]) / 2.0, Ac = -p[10];
   double cd = sqrt(1.0 - p[8] * p[8]);
   double sa, ca, sps, cps;
@@ -518,7 +520,7 @@ __device__ __forceinline__ void set_projection(PhdRec& c, const double* p, const
   MO::sincos(p[9], &sps, &cps);
   double mp[21], mx[18];
   antenna_basis(cps, sps, cd, p[8], ca, -sa, mp, mx);
-  for (int id = 0; id < g.nifo; id++) {
+  for (int id = id0; id < min(id1, g.nifo); id++) {
     int l = g.labels[id];
     double fp = 0.0, fx = 0.0;
 #pragma unroll
@@ -679,25 +681,20 @@ __device__ __forceinline__ void mix_amp(PhdRec& c) {
   P.amrd.fg2 = (float)(fg * fg);
 }
 
-// first bins of the intermediate / ringdown pieces (needs Msec, fmax, fRD)
-__device__ __forceinline__ void mix_bins(PhdRec& c, const NetGeom& g) {
-  MixPoly& P = c.mix;
-  P.iA = first_bin_mf_at_least(g, c.Msec, kAmpJoin);
-  P.iF = first_bin_mf_at_least(g, c.Msec, c.fmax);
-  P.iP = first_bin_mf_at_least(g, c.Msec, kPhiJoin);
-  P.iM = first_bin_mf_at_least(g, c.Msec, 0.5 * c.fRD);
-}
-
 // ---- cooperative setup: a block of 4 warps builds the records of 32 parameter sets, lane l
 // of every warp working on set l.  Each warp takes a different independent piece of the
 // record in each of four phases, so the dependency chain of one record is about a third of
 // the serial one and the lanes of a warp still run the same code:
-//   phase 1  w0 masses/scales        w1 fbegin head, ts      w2 antenna projection   w3 -
+//   phase 1  w0 masses/scales        w1 fbegin head, ts      w2 projection, det 0-1   w3 projection, det 2
 //                                                            (or detector offsets)
-//   phase 2  w0 fRD, fDM             w1 fits, fbegin, lo     w2 a0, ai[0..4], mdf     w3 TaylorF2, MfRef, hi
-//   phase 3  w0 fmax, intermediate   w1 join int, phi(fRef)  w2 MRD join pieces       w3 t0
-//   phase 4  w0 MRD join, phi_pre,   w1 mixed-kernel phase    w2 mixed-kernel          w3 mixed-kernel
-//            mixed-kernel constants                              amplitude                piece bins
+//   phase 2  w0 fRD, fDM             w1 fits, fbegin tail    w2 a0, ai[0..4], mdf, hi w3 TaylorF2, MfRef
+//   phase 3  w0 fmax, intermediate,  w1 join int, phi(fRef)  w2 MRD join pieces       w3 t0, bin iP
+//            bin iA
+//   phase 4  w0 MRD join, phi_pre,   w1 mixed-kernel phase,   w2 mixed-kernel          w3 first bin lo
+//            mixed-kernel constants      bin iM                  amplitude, bin iF
+// Each piece runs in the first phase whose inputs exist, spread so that the longest warp of each
+// phase is as short as the dependencies allow (measured per warp with clock64: the four phases'
+// longest pieces went from 7.1k + 11.5k + 7.1k + 7.5k to 6.2k + 8.0k + 7.6k + 4.3k cycles).
 struct SetupScratch {
   double p[kMaxParams];
   PhdMass m;
@@ -705,7 +702,7 @@ struct SetupScratch {
   double v2, s[4], pv[8], pvl[8];
   MrdJoin mj;
   double phr_raw;
-  int phr_branch, st, lo, hi, live;
+  int phr_branch, st, hi, live;
 };
 
 constexpr int kSetupSets = 32;
@@ -764,7 +761,9 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
       c.sqT = sqrt(s_g[lane].Tobs);
     } else if (w == 2) {
       if (model == kModelIntrinsic) set_offsets(c, p, s_g[lane].nifo);
-      else set_projection(c, p, s_g[lane]);
+      else set_projection(c, p, s_g[lane], 0, 2);
+    } else if (model != kModelIntrinsic) {
+      set_projection(c, p, s_g[lane], 2, kMaxIfo);     // the third detector, if any
     }
   }
   __syncthreads();
@@ -776,14 +775,13 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     } else if (w == 1) {
       phd_fits(c, x.m.eta, x.m.chi, x.v2, x.s);
       c.fs = fbegin_tail(x.fb, x.p[2], x.p[3]);
-      x.lo = first_bin_above(g, c.fs);
     } else if (w == 2) {
       phd_amp_prefactors(c, x.m);
       set_mdf(c, g);
+      x.hi = last_bin_below(g, c.fCut);
     } else {
       phd_taylorf2(c, x.m, x.pv, x.pvl);
       c.MfRef = c.Msec * kFref;
-      x.hi = last_bin_below(g, c.fCut);
     }
   }
   __syncthreads();
@@ -792,6 +790,7 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     if (w == 0) {
       c.fmax = phd_fmax(c);
       phd_amp_int(c, x.v2);
+      c.mix.iA = first_bin_mf_at_least(s_g[lane], c.Msec, kAmpJoin);
     } else if (w == 1) {
       phd_pq_sigma(c, x.s);
       phd_join_int(c, x.pv, x.pvl, x.s);
@@ -800,14 +799,21 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
       x.mj = phd_mrd_pieces(c);
     } else {
       c.t0 = dphi_mrd<MO>(c, phd_fmax(c));
+      c.mix.iP = first_bin_mf_at_least(s_g[lane], c.Msec, kPhiJoin);
     }
   }
   __syncthreads();
   // phase 4
   if (on && w != 0) {
-    if (w == 1) mix_phase_main(c);
-    else if (w == 2) mix_amp(c);
-    else mix_bins(c, s_g[lane]);
+    if (w == 1) {
+      mix_phase_main(c);
+      c.mix.iM = first_bin_mf_at_least(s_g[lane], c.Msec, 0.5 * c.fRD);
+    } else if (w == 2) {
+      mix_amp(c);
+      c.mix.iF = first_bin_mf_at_least(s_g[lane], c.Msec, c.fmax);
+    } else {
+      c.i_lo = first_bin_above(s_g[lane], c.fs);
+    }
   }
   if (w == 0 && lane < nb) {
     int st;
@@ -817,7 +823,6 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
       mix_phase_join(c);
       st = x.st;
       c.flags = (st == kStOK) ? kRecValid : 0;
-      c.i_lo = x.lo;
       c.i_hi = x.hi;
       c.event = s_ev[lane];
     } else {
@@ -828,12 +833,12 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
       c.i_hi = 0;
     }
     status[b] = st;
-    if (ntile) {
-      int bins = (st == kStOK) ? c.i_hi - c.i_lo + 1 : 0;
-      ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
-    }
   }
   __syncthreads();
+  if (ntile && w == 0 && lane < nb) {  // needs i_lo from warp 3
+    const int bins = (c.flags & kRecValid) ? c.i_hi - c.i_lo + 1 : 0;
+    ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+  }
   // the block's records are contiguous in shared and in global memory
   const int4* src = reinterpret_cast<const int4*>(s_rec);
   int4* dst = reinterpret_cast<int4*>(recs + b0);
