@@ -514,11 +514,17 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   EventData ed = event_data(ev);
   launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
   if (k0) cudaEventRecord(k0, s);
-  launch_lnl_full(w->d_recs, B, g, ed, prec == QCBC_MIXED ? kMixed : kFP64, L, w->d_part, s);
-  if (k1) cudaEventRecord(k1, s);
-  launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, prec == QCBC_MIXED ? kMixed : kFP64,
-                       d_lnl, d_rho, s, model);
-  tls_launches += 3;
+  const Precision kp = prec == QCBC_MIXED ? kMixed : kFP64;
+  if (L.tiles == 1) {   // one tile per set: the lnL kernel finalises the set itself
+    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, s);
+    if (k1) cudaEventRecord(k1, s);
+    tls_launches += 2;
+  } else {
+    launch_lnl_full(w->d_recs, B, g, ed, kp, L, w->d_part, s);
+    if (k1) cudaEventRecord(k1, s);
+    launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, kp, d_lnl, d_rho, s, model);
+    tls_launches += 3;
+  }
   CU(cudaGetLastError());
   return QCBC_OK;
 }

@@ -1159,9 +1159,71 @@ __device__ __forceinline__ void tile_range(const PhdRec& c, int tiles, int t, in
   }
 }
 
+// lnL (and rho, or the per-detector SNR^2 of the intrinsic model) of one set from its per-detector
+// sums sd[id] = S[2 id], sh[id] = S[2 id + 1]; rho_b may be null
+__device__ __noinline__ void finalize_set(const PhdRec& c, const double* S, const NetGeom& g, const EventData& ev, int mixed,
+                             int model, double* lnl_b, double* rho_b) {
+  double L = 0.0;
+  int loud = 0;
+  for (int id = 0; id < g.nifo; id++) {
+    const double sd = S[2 * id], sh = S[2 * id + 1];
+    double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * ev.inv_sigma[id];
+    if (mixed) K *= c.a0 * c.mdf_m76;       // the mixed kernel sums the amplitude without this factor
+    double HD = K * sd, HH = K * K * sh;
+    double x = HD - 0.5 * HH;
+    if (model == kModelIntrinsic) {
+      if (rho_b) rho_b[id] = 2.0 * x;
+      loud += 2.0 * x > 25.0;
+    } else if (rho_b) {
+      rho_b[id] = HD / sqrt(HH);
+    }
+    L += x;
+  }
+  if (model == kModelIntrinsic && g.nifo > 1 && loud < 2) L = 0.0;   // a signal in at least two detectors
+  *lnl_b = L;
+}
+
+// the lnL of a set whose record failed the setup: the reference's rejected-sample value
+// (QuickCBC.c:2366), rho 0
+__device__ void reject_set(const NetGeom& g, double* lnl_b, double* rho_b) {
+  *lnl_b = -1.0e20;
+  if (rho_b)
+    for (int id = 0; id < g.nifo; id++) rho_b[id] = 0.0;
+}
+
+// Where a one-tile launch writes its result itself: lnl != null makes thread 0 finalise the set
+// (finalize_set) instead of writing the tile's partial sums.
+struct FinalOut {
+  double* lnl;
+  double* rho;
+  int mixed, model;
+};
+
+// thread 0's block sums of a set's only tile: its lnL, or its partials
+template <int NIFO>
+__device__ __forceinline__ void finish_tile(const PhdRec& rec, const double* acc, const NetGeom& g,
+                                            const EventData& ev, const FinalOut& fo, int b, int tiles, int t,
+                                            double* partials) {
+  if (fo.lnl) {
+    double* rho_b = fo.rho ? fo.rho + (size_t)b * g.nifo : nullptr;
+    if (!(rec.flags & kRecValid)) {
+      reject_set(g, fo.lnl + b, rho_b);
+      return;
+    }
+    double S[2 * kMaxIfo];
+#pragma unroll
+    for (int k = 0; k < 2 * kMaxIfo; k++) S[k] = k < 2 * NIFO ? acc[k] : 0.0;
+    finalize_set(rec, S, g, ev, fo.mixed, fo.model, fo.lnl + b, rho_b);
+  } else {
+    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+#pragma unroll
+    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  }
+}
+
 template <int PREC, int NIFO>
 __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ recs, NetGeom g, EventData ev, int tiles,
-                                                  double* __restrict__ partials) {
+                                                  double* __restrict__ partials, FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
@@ -1174,11 +1236,7 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
   for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
   tile_fp64<NIFO>(rec, g, ev, i0, i1, acc);
   block_sum<2 * NIFO>(acc, red);
-  if (threadIdx.x == 0) {
-    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
-#pragma unroll
-    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
-  }
+  if (threadIdx.x == 0) finish_tile<NIFO>(rec, acc, g, ev, fo, b, tiles, t, partials);
 }
 
 #ifndef QCBC_MIXED_MINBLOCKS
@@ -1210,7 +1268,8 @@ __device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][
 template <int NIFO>
 __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
                                                                                EventData ev, int tiles,
-                                                                               double* __restrict__ partials) {
+                                                                               double* __restrict__ partials,
+                                                                               FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ float2 s_rot[];   // [NIFO][nk]
@@ -1224,11 +1283,7 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
   tile_mixed<NIFO>(rec, g, ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
   group_sum<2 * NIFO>(acc, red, blockDim.x);
-  if (threadIdx.x == 0) {
-    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
-#pragma unroll
-    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
-  }
+  if (threadIdx.x == 0) finish_tile<NIFO>(rec, acc, g, ev, fo, b, tiles, t, partials);
 }
 
 // rotation-table length per block for a launch: ceil(max bins per tile / threads)
@@ -1240,37 +1295,53 @@ static int mixed_nk(const NetGeom& g, const FullLaunch& L) {
 
 template <int NIFO>
 static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
-                           double* part, cudaStream_t s) {
+                           double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
-  k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part);
+  k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
 static void launch_full_mixed(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
-                              double* part, cudaStream_t s) {
+                              double* part, const FinalOut& fo, cudaStream_t s) {
   switch (g.nifo) {
-    case 1: launch_mixed_n<1>(r, B, g, ev, L, part, s); break;
-    case 2: launch_mixed_n<2>(r, B, g, ev, L, part, s); break;
-    default: launch_mixed_n<3>(r, B, g, ev, L, part, s); break;
+    case 1: launch_mixed_n<1>(r, B, g, ev, L, part, fo, s); break;
+    case 2: launch_mixed_n<2>(r, B, g, ev, L, part, fo, s); break;
+    default: launch_mixed_n<3>(r, B, g, ev, L, part, fo, s); break;
   }
 }
 
 template <int PREC>
 static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
-                             double* part, cudaStream_t s) {
+                             double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   switch (g.nifo) {
-    case 1: k_lnl_full<PREC, 1><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
-    case 2: k_lnl_full<PREC, 2><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
-    default: k_lnl_full<PREC, 3><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part); break;
+    case 1: k_lnl_full<PREC, 1><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
+    case 2: k_lnl_full<PREC, 2><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
+    default: k_lnl_full<PREC, 3><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
   }
 }
 
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, s);
-  else launch_full_mixed(d_recs, B, g, ev, L, d_partials, s);
+  const FinalOut none{nullptr, nullptr, 0, 0};
+  if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, none, s);
+  else launch_full_mixed(d_recs, B, g, ev, L, d_partials, none, s);
+}
+
+bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
+                           Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
+                           int model, cudaStream_t s) {
+  if (B <= 0) return true;
+  if (L.tiles != 1) {
+    launch_lnl_full(d_recs, B, g, ev, prec, L, d_partials, s);
+    launch_finalize_full(d_partials, d_recs, d_status, B, L.tiles, g, ev, prec, d_lnl, d_rho, s, model);
+    return false;
+  }
+  const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model};
+  if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, fo, s);
+  else launch_full_mixed(d_recs, B, g, ev, L, d_partials, fo, s);
+  return true;
 }
 
 __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRec* __restrict__ recs,
@@ -1278,35 +1349,18 @@ __global__ void k_finalize_full(const double* __restrict__ partials, const PhdRe
                                 int mixed, int model, double* __restrict__ lnl, double* __restrict__ rho) {
   int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= B) return;
-  const PhdRec& c = recs[b];
+  double* rho_b = rho ? rho + (size_t)b * g.nifo : nullptr;
   if (status[b] != kStOK) {
-    lnl[b] = -1.0e20;                      // the reference's rejected-sample value (QuickCBC.c:2366)
-    if (rho) for (int id = 0; id < g.nifo; id++) rho[(size_t)b * g.nifo + id] = 0.0;
+    reject_set(g, lnl + b, rho_b);
     return;
   }
-  double L = 0.0;
-  int loud = 0;
-  for (int id = 0; id < g.nifo; id++) {
-    double sd = 0.0, sh = 0.0;
-    for (int t = 0; t < tiles; t++) {
-      const double* p = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
-      sd += p[2 * id];
-      sh += p[2 * id + 1];
-    }
-    double K = c.Fs[id] * kH22fac * c.amp_scale / c.sqT * ev.inv_sigma[id];
-    if (mixed) K *= c.a0 * c.mdf_m76;       // the mixed kernel sums the amplitude without this factor
-    double HD = K * sd, HH = K * K * sh;
-    double x = HD - 0.5 * HH;
-    if (model == kModelIntrinsic) {
-      if (rho) rho[(size_t)b * g.nifo + id] = 2.0 * x;
-      loud += 2.0 * x > 25.0;
-    } else if (rho) {
-      rho[(size_t)b * g.nifo + id] = HD / sqrt(HH);
-    }
-    L += x;
+  double S[2 * kMaxIfo];
+  for (int k = 0; k < 2 * kMaxIfo; k++) S[k] = 0.0;
+  for (int t = 0; t < tiles; t++) {
+    const double* p = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+    for (int k = 0; k < 2 * g.nifo; k++) S[k] += p[k];
   }
-  if (model == kModelIntrinsic && g.nifo > 1 && loud < 2) L = 0.0;   // a signal in at least two detectors
-  lnl[b] = L;
+  finalize_set(recs[b], S, g, ev, mixed, model, lnl + b, rho_b);
 }
 
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,

@@ -78,6 +78,11 @@ void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventD
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
                           const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
                           cudaStream_t s, int model = kModelFull);
+// lnL of B sets with the finaliser folded into the lnL kernel when each set is one tile (L.tiles == 1);
+// otherwise the lnL kernel and launch_finalize_full.  Returns true when one launch did both.
+bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
+                           Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
+                           int model, cudaStream_t s);
 // fill the per-bin tables for bins [0, n)
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
