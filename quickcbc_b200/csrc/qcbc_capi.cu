@@ -58,6 +58,7 @@ struct DeviceState {
   // per-bin constants for the mixed kernel: (i^{1/3}, i^{-1/3}) and (log i, i^{3/4})
   double2* d_tabA = nullptr;
   double2* d_tabB = nullptr;
+  float2* d_tabC = nullptr;
   int tab_n = 0;
   int* d_bucket = nullptr;   // QNM interval index per 0.001 of final spin
 };
@@ -128,15 +129,19 @@ static int ensure_bin_tables(DeviceState& ds, int n) {
   if (ds.tab_n >= n) return QCBC_OK;
   int want = std::max(n, 1 << 20);
   double2 *a = nullptr, *b = nullptr;
+  float2* c = nullptr;
   CU(cudaMalloc(&a, (size_t)want * sizeof(double2)));
   CU(cudaMalloc(&b, (size_t)want * sizeof(double2)));
-  launch_fill_bin_tables(a, b, want, 0);
+  CU(cudaMalloc(&c, (size_t)want * sizeof(float2)));
+  launch_fill_bin_tables(a, b, c, want, 0);
   tls_launches += 1;
   CU(cudaDeviceSynchronize());
   cudaFree(ds.d_tabA);
   cudaFree(ds.d_tabB);
+  cudaFree(ds.d_tabC);
   ds.d_tabA = a;
   ds.d_tabB = b;
+  ds.d_tabC = c;
   ds.tab_n = want;
   return QCBC_OK;
 }
@@ -303,6 +308,7 @@ static EventData event_data(const qcbc_event* ev) {
   d.tab_n = ds.tab_n;
   d.tabA = ds.d_tabA;
   d.tabB = ds.d_tabB;
+  d.tabC = ds.d_tabC;
   return d;
 }
 

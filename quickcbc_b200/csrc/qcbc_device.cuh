@@ -44,24 +44,29 @@ constexpr int kRecValid = 1;
 // Mf = m i with m = Msec df: every power of m and the factor 1/(2 pi) are folded into
 // per-set coefficients (computed in FP64 by the setup), so a bin needs only i, t = i^{1/3},
 // u = i^{-1/3}, L = log i and s = i^{3/4} (per-device tables) and no Mf at all.
-//   phase in cycles (FP64), the three pieces of IMRPhenomD.c:169-186 / internals.c:1540-1584,
-//   each minus t0 (Mf - MfRef) + phi_pre:
-//     inspiral      A0 + t (At + t Att) + L (AL + t AtL) + u (Au + u (Auu + u (Au3 + u^2 Au5)))
-//                   + i (Ai + t (Ait + t Aitt) + i Aii)
-//     intermediate  B0 + i Bi + u^9 Bu9 + L BL
-//     ringdown      R0 + i Ri + u^3 Ru3 + s Rs + Rat atan(i D1 - D0)
+//   phase in cycles, the three pieces of IMRPhenomD.c:169-186 / internals.c:1540-1584, each
+//   minus t0 (Mf - MfRef) + phi_pre, written as the ringdown's linear part R0 + i Ri plus a rest:
+//     inspiral      R0 + i Ri + A0 + t (At + t Att) + L (AL + t AtL) + u (Au + u (Auu + u (Au3 + u^2 Au5)))
+//                                 + i (Ai + t (Ait + t Aitt) + i Aii)
+//     intermediate  R0 + i Ri + B0 + i Bi + u^9 Bu9 + L BL
+//     ringdown      R0 + i Ri + Ru3 / i + Rs s + Rat atan(i D1 - D0)
+//   The kernel applies R0 + i Ri through its FP64-built rotation tables. The inspiral and
+//   intermediate rests are evaluated in FP64; the ringdown rest is a few cycles and is evaluated
+//   in FP32, with every coefficient split into a pair hi + lo of floats so that its rounding
+//   adds no error that is the same in every bin.
 //   amplitude (FP32) relative to a0 (Msec df)^{-7/6} i^{-7/6}, IMRPhenomD_internals.c:576-707:
 //     inspiral      1 + t^2 al0 + i (al1 + t (al2 + t al3) + i (al4 + t (al5 + t al6) + i al7))
-//     intermediate  Newton form in x = m i - hx1 (nodes hx1, hx1, hx2, hx3, hx3), x in FP64
-//     ringdown      exp(-dfr g2/fg) fg g1 / (dfr^2 + fg^2), dfr = m i - fRD in FP64
+//     intermediate  Newton form in x = m i - hx1 (nodes hx1, hx1, hx2, hx3, hx3)
+//     ringdown      exp(-dfr g2/fg) fg g1 / (dfr^2 + fg^2), dfr = m i - fRD
+//   with m, hx1 and fRD as float pairs.
 //   iA, iF, iP, iM: first bins of the intermediate amplitude, ringdown amplitude, intermediate
 //   phase and ringdown phase (Msec f_i compared with 0.014, fmax, 0.018, fRD/2 in FP64).
 struct MixPhIns { double A0, At, Att, AtL, AL, Au, Auu, Au3, Au5, Ai, Ait, Aitt, Aii; };
 struct MixPhInt { double B0, Bi, Bu9, BL; };
-struct MixPhMrd { double R0, Ri, Ru3, Rs, Rat, D1, D0; };
+struct MixPhMrd { double R0, Ri; float Ru3[2], Rs[2], Rat[2], D1[2], D0[2]; };
 struct MixAmpIns { float al[8]; };
-struct MixAmpInt { double m, hx1; float hc[5], h21, h31; };
-struct MixAmpMrd { double m, fRD; float g2_over_fg, fg_g1, fg2; };
+struct MixAmpInt { float m[2], hx1[2]; float hc[5], h21, h31; };
+struct MixAmpMrd { float m[2], fRD[2]; float g2_over_fg, fg_g1, fg2; };
 struct MixPoly {
   MixPhIns pins;
   MixPhInt pint;
@@ -70,6 +75,7 @@ struct MixPoly {
   MixAmpInt aint;
   MixAmpMrd amrd;
   int iA, iF, iP, iM;
+  int pad[2];
 };
 
 struct PhdRec {

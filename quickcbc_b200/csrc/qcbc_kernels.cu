@@ -613,6 +613,12 @@ __device__ __forceinline__ int first_bin_mf_at_least(const NetGeom& g, double Ms
   return i;
 }
 
+// v as a pair of floats hi + lo (hi = v rounded, lo = the remainder rounded)
+__device__ __forceinline__ void split_f2(double v, float (&p)[2]) {
+  p[0] = (float)v;
+  p[1] = (float)(v - (double)p[0]);
+}
+
 // inspiral phase but its constant, and the intermediate / ringdown pieces but the parts that
 // need the ringdown join (needs pq, alpha/beta, the intermediate join, t0, the mdf scales)
 __device__ __forceinline__ void mix_phase_main(PhdRec& c) {
@@ -636,12 +642,12 @@ __device__ __forceinline__ void mix_phase_main(PhdRec& c) {
   P.pint.Bi = K * (c.b1 * m * ie + c.C2Int * m - c.t0 * m);
   P.pint.Bu9 = K * (-(c.b3 * third) * U9 * ie);
   P.pint.BL = K * (c.b2 * ie);
-  P.pmrd.Ru3 = K * (-c.al2 * U3 * ie);
-  P.pmrd.Rs = K * ((4.0 / 3.0) * c.al3 * c.mdf_34 * ie);
-  P.pmrd.Rat = K * (c.al4 * ie);
+  split_f2(K * (-c.al2 * U3 * ie), P.pmrd.Ru3);
+  split_f2(K * ((4.0 / 3.0) * c.al3 * c.mdf_34 * ie), P.pmrd.Rs);
+  split_f2(K * (c.al4 * ie), P.pmrd.Rat);
   const double rdm = 1.0 / c.fDM;
-  P.pmrd.D1 = m * rdm;
-  P.pmrd.D0 = c.al5 * c.fRD * rdm;
+  split_f2(m * rdm, P.pmrd.D1);
+  split_f2(c.al5 * c.fRD * rdm, P.pmrd.D0);
 }
 
 // the rest of the phase pieces: constants (phi_pre) and the ringdown slope (C2MRD)
@@ -649,10 +655,17 @@ __device__ __forceinline__ void mix_phase_join(PhdRec& c) {
   MixPoly& P = c.mix;
   const double K = kInv2PiD, m = c.mdf, ie = c.inv_eta;
   const double shift = c.t0 * c.MfRef - c.phi_pre;
-  P.pins.A0 = K * (c.pq[0] + c.pq[4] * ((c.mdf_log + kLnPi) * (1.0 / 3.0)) + shift);
-  P.pint.B0 = K * (c.b2 * ie * c.mdf_log + c.C1Int + shift);
   P.pmrd.R0 = K * (c.C1MRD + shift);
   P.pmrd.Ri = K * (c.al1 * m * ie + c.C2MRD * m - c.t0 * m);
+  P.pins.A0 = K * (c.pq[0] + c.pq[4] * ((c.mdf_log + kLnPi) * (1.0 / 3.0)) + shift) - P.pmrd.R0;
+  P.pint.B0 = K * (c.b2 * ie * c.mdf_log + c.C1Int + shift) - P.pmrd.R0;
+}
+
+// the inspiral and intermediate slopes relative to the ringdown's (after mix_phase_main and
+// mix_phase_join)
+__device__ __forceinline__ void mix_phase_slopes(PhdRec& c) {
+  c.mix.pins.Ai -= c.mix.pmrd.Ri;
+  c.mix.pint.Bi -= c.mix.pmrd.Ri;
 }
 
 // FP32 amplitude coefficients (needs ai, the intermediate Newton form, g1..g3, fDM)
@@ -668,14 +681,14 @@ __device__ __forceinline__ void mix_amp(PhdRec& c) {
   al[5] = (float)(c.ai[5] * m2 * T);
   al[6] = (float)(c.ai[6] * m2 * T2);
   al[7] = (float)(c.ai[7] * m2 * m);
-  P.aint.m = m;
-  P.aint.hx1 = c.hx1;
+  split_f2(m, P.aint.m);
+  split_f2(c.hx1, P.aint.hx1);
   P.aint.h21 = (float)(c.hx2 - c.hx1);
   P.aint.h31 = (float)(c.hx3 - c.hx1);
   for (int k = 0; k < 5; k++) P.aint.hc[k] = (float)c.hc[k];
   const double fg = c.fDM * c.g3;
-  P.amrd.m = m;
-  P.amrd.fRD = c.fRD;
+  split_f2(m, P.amrd.m);
+  split_f2(c.fRD, P.amrd.fRD);
   P.amrd.g2_over_fg = (float)(c.g2 / fg);
   P.amrd.fg_g1 = (float)(fg * c.g1);
   P.amrd.fg2 = (float)(fg * fg);
@@ -839,6 +852,8 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     const int bins = (c.flags & kRecValid) ? c.i_hi - c.i_lo + 1 : 0;
     ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
   }
+  if (on && w == 1) mix_phase_slopes(c);   // needs Ri from warp 0
+  __syncthreads();
   // the block's records are contiguous in shared and in global memory
   const int4* src = reinterpret_cast<const int4*>(s_rec);
   int4* dst = reinterpret_cast<int4*>(recs + b0);
@@ -916,12 +931,15 @@ __device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, con
   }
 }
 
-// Mixed form.  Per bin i (f = i df, Mf = Msec f):
-//  * phase in FP64 from per-bin tables: Mf^{1/3} = (Msec df)^{1/3} i^{1/3}, Mf^{-1/3} likewise,
-//    log Mf = log(Msec df) + log i, Mf^{3/4} likewise; reduced to one cycle in FP64, then one FP32
-//    sincospi gives e^{-i phi(f)};
-//  * detector rotation e^{2 pi i (f (ts - td) + lambda/2pi)} = base(thread) x R[k] with a per-tile
-//    FP32 table R[k] = e^{2 pi i k (blockDim df)(ts - td)} built in FP64;
+// Mixed form.  Per bin i (f = i df, Mf = Msec f), with the phase written as the ringdown's linear
+// part R0 + i Ri plus a rest (MixPoly):
+//  * the rest of the inspiral and intermediate pieces in FP64 from per-bin tables:
+//    Mf^{1/3} = (Msec df)^{1/3} i^{1/3}, Mf^{-1/3} likewise, log Mf = log(Msec df) + log i,
+//    reduced to one cycle in FP64; the rest of the ringdown piece (a few cycles) in FP32 from
+//    1/i and i^{3/4}; then one FP32 sincos gives e^{-2 pi i rest};
+//  * detector rotation and linear phase e^{2 pi i (f (ts - td) + lambda/2pi - R0 - i Ri)}
+//    = base(thread) x R[k] with a per-tile FP32 table R[k] = e^{2 pi i k blockDim (df (ts - td) - Ri)},
+//    both built in FP64;
 //  * amplitude in FP32 without the constant a0 (Msec df)^{-7/6} (applied in FP64 by the finaliser);
 //  * FP32 partial sums over 8 bins, accumulated in FP64.
 // ---- mixed-precision tile body (coefficients: MixPoly in the record)
@@ -955,9 +973,18 @@ __device__ __forceinline__ double mph_int(const MixPhInt& q, double xi, double u
   double u3 = u * u * u;
   return fma(xi, sld(q.Bi), sld(q.B0)) + fma(L, sld(q.BL), (u3 * u3 * u3) * sld(q.Bu9));
 }
-__device__ __forceinline__ double mph_mrd(const MixPhMrd& q, double xi, double u, double s) {
-  const double at = (double)atanf((float)fma(xi, sld(q.D1), -sld(q.D0)));
-  return fma(xi, sld(q.Ri), sld(q.R0)) + fma(u * u * u, sld(q.Ru3), fma(s, sld(q.Rs), sld(q.Rat) * at));
+// the ringdown rest in FP32 (cycles, a few at most): Ru3 / i + Rs s + Rat atan(i D1 - D0) with
+// tc = (1/i, s = i^{3/4}); each coefficient is a float pair applied hi after lo
+__device__ __forceinline__ float mph_mrd(const MixPhMrd& q, float xf, float2 tc) {
+  const float z = fmaf(xf, sld(q.D1[0]), fmaf(xf, sld(q.D1[1]), -sld(q.D0[0]))) - sld(q.D0[1]);
+  const float at = atanf(z);
+  float ph = fmaf(at, sld(q.Rat[0]), at * sld(q.Rat[1]));
+  ph = fmaf(tc.y, sld(q.Rs[0]), fmaf(tc.y, sld(q.Rs[1]), ph));
+  return fmaf(tc.x, sld(q.Ru3[0]), fmaf(tc.x, sld(q.Ru3[1]), ph));
+}
+// x minus the nearest integer, for |x| < 2^22, in FP32 adds
+__device__ __forceinline__ float frac_cyc(float x) {
+  return __fsub_rn(x, __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f));
 }
 __device__ __forceinline__ float mamp_ins(const MixAmpIns& a, float xf, float tf) {
   const float* al = a.al;
@@ -965,14 +992,14 @@ __device__ __forceinline__ float mamp_ins(const MixAmpIns& a, float xf, float tf
   float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, sld(al[3]), sld(al[2])), sld(al[1])));
   return fmaf(xf, mid, fmaf(tf * tf, sld(al[0]), 1.0f));
 }
-__device__ __forceinline__ float mamp_int(const MixAmpInt& a, double xi) {
-  float x = (float)fma(xi, sld(a.m), -sld(a.hx1));
+__device__ __forceinline__ float mamp_int(const MixAmpInt& a, float xf) {
+  const float x = fmaf(xf, sld(a.m[0]), fmaf(xf, sld(a.m[1]), -sld(a.hx1[0]))) - sld(a.hx1[1]);
   return sld(a.hc[0]) +
          x * (sld(a.hc[1]) +
               x * (sld(a.hc[2]) + (x - sld(a.h21)) * (sld(a.hc[3]) + (x - sld(a.h31)) * sld(a.hc[4]))));
 }
-__device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, double xi) {
-  float dfr = (float)fma(xi, sld(a.m), -sld(a.fRD));
+__device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, float xf) {
+  const float dfr = fmaf(xf, sld(a.m[0]), fmaf(xf, sld(a.m[1]), -sld(a.fRD[0]))) - sld(a.fRD[1]);
   return __fdividef(__expf(-dfr * sld(a.g2_over_fg)) * sld(a.fg_g1), dfr * dfr + sld(a.fg2));
 }
 
@@ -1033,35 +1060,47 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
   double xi = (double)i;
   float xf = (float)i;
   int b = i;
+  // tables a row needs: tabA for the inspiral amplitude and the FP64 phase pieces, tabB for the
+  // FP64 phase pieces, tabC for the ringdown phase
+  constexpr bool kTabA = AP <= 0 || PP != 2, kTabB = PP != 2, kTabC = PP == 2 || PP < 0;
   for (int r = 0; r < n; r += 8) {
     const int m = min(8, n - r);
     MixAcc<NIFO> A;
     A.zero();
 #pragma unroll 1
     for (int j = 0; j < m; j++) {
-      const double2 tA = __ldg(ev.tabA + b), tB = __ldg(ev.tabB + b);
+      double2 tA = make_double2(0.0, 0.0), tB = make_double2(0.0, 0.0);
+      float2 tC = make_float2(0.f, 0.f);
+      if (kTabA) tA = __ldg(ev.tabA + b);
+      if (kTabB) tB = __ldg(ev.tabB + b);
+      if (kTabC) tC = __ldg(ev.tabC + b);
       float4 wv[NIFO];
 #pragma unroll
       for (int id = 0; id < NIFO; id++) wv[id] = __ldg(ev.w4 + id * nh + b);
-      double ph;
-      float a;
-      if (PP == 0) ph = mph_ins(qi, xi, tA.x, tA.y, tB.x);
-      else if (PP == 1) ph = mph_int(qn, xi, tA.y, tB.x);
-      else if (PP == 2) ph = mph_mrd(qm, xi, tA.y, tB.y);
-      else {
+      float cyc, a;
+      if (PP == 2) {
+        cyc = frac_cyc(mph_mrd(qm, xf, tC));
+      } else if (PP >= 0) {
+        const double ph = PP == 0 ? mph_ins(qi, xi, tA.x, tA.y, tB.x) : mph_int(qn, xi, tA.y, tB.x);
+        cyc = (float)(ph - rint(ph));
+      } else {
         const int pp = ph_piece(P, b);
-        ph = pp == 0 ? mph_ins(P.pins, xi, tA.x, tA.y, tB.x)
-                     : (pp == 1 ? mph_int(P.pint, xi, tA.y, tB.x) : mph_mrd(P.pmrd, xi, tA.y, tB.y));
+        if (pp == 2) {
+          cyc = frac_cyc(mph_mrd(P.pmrd, xf, tC));
+        } else {
+          const double ph = pp == 0 ? mph_ins(P.pins, xi, tA.x, tA.y, tB.x) : mph_int(P.pint, xi, tA.y, tB.x);
+          cyc = (float)(ph - rint(ph));
+        }
       }
       if (AP == 0) a = mamp_ins(ai, xf, (float)tA.x);
-      else if (AP == 1) a = mamp_int(an, xi);
-      else if (AP == 2) a = mamp_mrd(am, xi);
+      else if (AP == 1) a = mamp_int(an, xf);
+      else if (AP == 2) a = mamp_mrd(am, xf);
       else {
         const int ap = amp_piece(P, b);
         a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x)
-                    : (ap == 1 ? mamp_int(P.aint, xi) : mamp_mrd(P.amrd, xi));
+                    : (ap == 1 ? mamp_int(P.aint, xf) : mamp_mrd(P.amrd, xf));
       }
-      A.add(wv[0].w * a, (float)(ph - rint(ph)), wv, pr, nk);
+      A.add(wv[0].w * a, cyc, wv, pr, nk);
       b += bs;
       pr++;
       xi += dbs;
@@ -1084,10 +1123,11 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
   const int nk = mixed_table_len(i0, i1, bs);
   constexpr double kInv2Pi = 0.15915494309189533577;
   const double Dstep = (double)bs * g.df;
+  const double Ri = c.mix.pmrd.Ri, R0 = c.mix.pmrd.R0;    // the phase's linear part R0 + i Ri
   for (int k = tid; k < nk; k += bs) {
 #pragma unroll
     for (int id = 0; id < NIFO; id++) {
-      double cyc = (double)k * (Dstep * (c.ts - c.td[id]));
+      double cyc = (double)k * (Dstep * (c.ts - c.td[id]) - (double)bs * Ri);
       double sv, cv;
       sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
       s_rot[id * nk + k] = make_float2((float)cv, (float)sv);
@@ -1100,7 +1140,7 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
   float2 base[NIFO];
 #pragma unroll
   for (int id = 0; id < NIFO; id++) {
-    double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi;
+    double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi - fma((double)i, Ri, R0);
     double sv, cv;
     sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
     base[id] = make_float2((float)cv, (float)sv);
@@ -1371,17 +1411,18 @@ void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const 
                                                   prec == kMixed ? 1 : 0, model, d_lnl, d_rho);
 }
 
-__global__ void k_fill_bin_tables(double2* __restrict__ A, double2* __restrict__ Bt, int n) {
+__global__ void k_fill_bin_tables(double2* __restrict__ A, double2* __restrict__ Bt, float2* __restrict__ C, int n) {
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double x = (double)(i > 0 ? i : 1);
-    double c3 = cbrt(x);
+    double c3 = cbrt(x), s = pow(x, 0.75);
     A[i] = make_double2(c3, 1.0 / c3);
-    Bt[i] = make_double2(log(x), pow(x, 0.75));
+    Bt[i] = make_double2(log(x), s);
+    C[i] = make_float2((float)(1.0 / x), (float)s);
   }
 }
 
-void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s) {
-  k_fill_bin_tables<<<(n + 255) / 256, 256, 0, s>>>(d_tabA, d_tabB, n);
+void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, float2* d_tabC, int n, cudaStream_t s) {
+  k_fill_bin_tables<<<(n + 255) / 256, 256, 0, s>>>(d_tabA, d_tabB, d_tabC, n);
 }
 
 // ---------------------------------------------------------------- multi-event launches

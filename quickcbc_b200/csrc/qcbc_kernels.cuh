@@ -26,9 +26,10 @@ struct EventData {
   int nh;                // row length (N/2)
   double inv_sigma[kMaxIfo];
   // per-bin constants shared by all events on a device (index = bin number i >= 1):
-  // tabA = (i^{1/3}, i^{-1/3}), tabB = (log i, i^{3/4})
+  // tabA = (i^{1/3}, i^{-1/3}), tabB = (log i, i^{3/4}), tabC = (1/i, i^{3/4}) rounded to float
   const double2* tabA;
   const double2* tabB;
+  const float2* tabC;
   int tab_n;
 };
 
@@ -84,7 +85,7 @@ bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, con
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
                            int model, cudaStream_t s);
 // fill the per-bin tables for bins [0, n)
-void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, int n, cudaStream_t s);
+void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, float2* d_tabC, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
                     Precision prec, double* d_lnl, cudaStream_t s);
 // shared memory of one set's warp in the heterodyned kernels (its record and [3][nifo][M] doubles)
