@@ -233,6 +233,8 @@ struct Workspace {
   double* d_part = nullptr; size_t c_part = 0;
   double* d_lnl = nullptr; size_t c_lnl = 0;
   double* d_rho = nullptr; size_t c_rho = 0;
+  int* d_cls = nullptr; size_t c_cls = 0;         // launch order of the sets (launch_setup_ordered)
+  int* d_order = nullptr; size_t c_order = 0;
   double* h_params = nullptr; size_t ch_params = 0;
   double* h_lnl = nullptr; size_t ch_lnl = 0;
   double* h_rho = nullptr; size_t ch_rho = 0;
@@ -518,14 +520,19 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   if ((rc = grow(w->d_part, w->c_part, (size_t)B * L.tiles * 2 * kMaxIfo))) return rc;
   DeviceState& ds = g_dev[current_device()];
   EventData ed = event_data(ev);
-  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
-  if (k0) cudaEventRecord(k0, s);
   const Precision kp = prec == QCBC_MIXED ? kMixed : kFP64;
-  if (L.tiles == 1) {   // one tile per set: the lnL kernel finalises the set itself
-    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, s);
+  if (L.tiles == 1) {
+    // one tile per set: the sets run in order of length and the lnL kernel finalises each itself
+    if ((rc = grow(w->d_cls, w->c_cls, (size_t)B))) return rc;
+    if ((rc = grow(w->d_order, w->c_order, (size_t)B))) return rc;
+    launch_setup_ordered(d_params, B, g, ds.qnm, w->d_recs, w->d_status, SetOrder{w->d_cls, w->d_order}, s, model);
+    if (k0) cudaEventRecord(k0, s);
+    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, w->d_order, s);
     if (k1) cudaEventRecord(k1, s);
-    tls_launches += 2;
+    tls_launches += 3;
   } else {
+    launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
+    if (k0) cudaEventRecord(k0, s);
     launch_lnl_full(w->d_recs, B, g, ed, kp, L, w->d_part, s);
     if (k1) cudaEventRecord(k1, s);
     launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, kp, d_lnl, d_rho, s, model);

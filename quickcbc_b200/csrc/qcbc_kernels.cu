@@ -738,10 +738,20 @@ struct GeomTable {
   }
 };
 
+constexpr int kOrderBuckets = 64;
+
+// length class of a set of `bins` bins in a band of `band` bins, 0 .. kOrderBuckets - 1 (it only
+// orders the launch, so its rounding does not matter)
+__device__ __forceinline__ int length_class(int bins, int band) {
+  return min(kOrderBuckets - 1, __float2int_rz((float)bins * ((float)kOrderBuckets / (float)max(band, 1))));
+}
+
+// cls non-null: each set's length class (launch order, see k_order_sets)
 template <class Geom>
 __device__ __forceinline__ void setup_coop_block(const double* __restrict__ params, int B, const Geom& geo,
                                                  const QnmTable& q, int tile_bins, PhdRec* __restrict__ recs,
-                                                 int* __restrict__ status, int* __restrict__ ntile, int model) {
+                                                 int* __restrict__ status, int* __restrict__ ntile, int model,
+                                                 int* __restrict__ cls = nullptr) {
   __shared__ __align__(16) PhdRec s_rec[kSetupSets];
   __shared__ SetupScratch s_x[kSetupSets];
   __shared__ NetGeom s_g[kSetupSets];
@@ -848,9 +858,10 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     status[b] = st;
   }
   __syncthreads();
-  if (ntile && w == 0 && lane < nb) {  // needs i_lo from warp 3
-    const int bins = (c.flags & kRecValid) ? c.i_hi - c.i_lo + 1 : 0;
-    ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+  if ((ntile || cls) && w == 0 && lane < nb) {  // needs i_lo from warp 3
+    const int bins = (c.flags & kRecValid) ? max(0, c.i_hi - c.i_lo + 1) : 0;
+    if (ntile) ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+    if (cls) cls[b] = length_class(bins, s_g[lane].imax - s_g[lane].imin);
   }
   if (on && w == 1) mix_phase_slopes(c);   // needs Ri from warp 0
   __syncthreads();
@@ -861,17 +872,88 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
   for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
 }
 
+// Claims a slot of class c (c < 0: none) for each lane, one shared atomic per distinct class of
+// the warp; returns the lane's slot.  Every lane of the warp calls it.
+__device__ __forceinline__ int claim_slot(int* cnt, int c) {
+  const unsigned peers = __match_any_sync(0xffffffffu, c);
+  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
+  int base = 0;
+  if (lane == leader && c >= 0) base = atomicAdd(&cnt[c], __popc(peers));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return base + __popc(peers & ((1u << lane) - 1u));
+}
+
+constexpr int kOrderThreads = 1024;
+constexpr int kOrderChunk = 4;       // classes a thread holds at once
+static_assert(kOrderBuckets == 64, "k_order_sets scans two classes per lane of one warp");
+
+// Counting sort of the B sets by length class, longest first: order[k] = the set that lnL block
+// k evaluates (one block).
+__global__ void __launch_bounds__(kOrderThreads) k_order_sets(const int* __restrict__ cls, int* __restrict__ order,
+                                                              int B) {
+  __shared__ int cnt[kOrderBuckets];
+  if (threadIdx.x < kOrderBuckets) cnt[threadIdx.x] = 0;
+  __syncthreads();
+  constexpr int step = kOrderThreads * kOrderChunk;
+  int c[kOrderChunk];
+  for (int base = 0; base < B; base += step) {
+#pragma unroll
+    for (int j = 0; j < kOrderChunk; j++) {
+      const int s = base + j * kOrderThreads + threadIdx.x;
+      c[j] = s < B ? cls[s] : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kOrderChunk; j++) claim_slot(cnt, c[j]);
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {   // exclusive scan from the longest class: lane l holds classes 63-2l, 62-2l
+    const int l = threadIdx.x, v0 = cnt[kOrderBuckets - 1 - 2 * l], v1 = cnt[kOrderBuckets - 2 - 2 * l];
+    int x = v0 + v1;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, off);
+      if (l >= off) x += y;
+    }
+    const int start = x - v0 - v1;
+    cnt[kOrderBuckets - 1 - 2 * l] = start;
+    cnt[kOrderBuckets - 2 - 2 * l] = start + v0;
+  }
+  __syncthreads();
+  for (int base = 0; base < B; base += step) {
+    if (B > step) {   // one chunk: still in registers
+#pragma unroll
+      for (int j = 0; j < kOrderChunk; j++) {
+        const int s = base + j * kOrderThreads + threadIdx.x;
+        c[j] = s < B ? cls[s] : -1;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kOrderChunk; j++) {
+      const int pos = claim_slot(cnt, c[j]);
+      if (c[j] >= 0) order[pos] = base + j * kOrderThreads + threadIdx.x;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
                                                          QnmTable q, PhdRec* __restrict__ recs,
-                                                         int* __restrict__ status, int model) {
+                                                         int* __restrict__ status, int model, int* __restrict__ cls) {
   GeomOne geo{g};
-  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model);
+  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model, cls);
 }
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                   int* d_status, cudaStream_t s, int model) {
   if (B <= 0) return;
-  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model);
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
+                                                                      nullptr);
+}
+
+void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
+                          int* d_status, const SetOrder& o, cudaStream_t s, int model) {
+  if (B <= 0) return;
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
+                                                                      o.cls);
+  k_order_sets<<<1, kOrderThreads, 0, s>>>(o.cls, o.order, B);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -1237,6 +1319,7 @@ struct FinalOut {
   double* lnl;
   double* rho;
   int mixed, model;
+  const int* order;    // non-null: block k evaluates set order[k] (one tile per set)
 };
 
 // thread 0's block sums of a set's only tile: its lnL, or its partials
@@ -1266,7 +1349,8 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
                                                   double* __restrict__ partials, FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
-  int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
+  const int b = fo.order ? fo.order[bi] : bi;
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1304,7 +1388,6 @@ __device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][
 }
 
 // Mixed-precision full lnL over one tile of bins of one parameter set.
-// Mixed-precision full lnL over one tile of bins of one parameter set.
 template <int NIFO>
 __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
                                                                                EventData ev, int tiles,
@@ -1313,7 +1396,8 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ float2 s_rot[];   // [NIFO][nk]
-  const int b = blockIdx.x / tiles, t = blockIdx.x - b * tiles;
+  const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
+  const int b = fo.order ? fo.order[bi] : bi;
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1364,21 +1448,21 @@ static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const Eve
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  const FinalOut none{nullptr, nullptr, 0, 0};
+  const FinalOut none{nullptr, nullptr, 0, 0, nullptr};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, none, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, none, s);
 }
 
 bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
-                           int model, cudaStream_t s) {
+                           int model, const int* d_order, cudaStream_t s) {
   if (B <= 0) return true;
   if (L.tiles != 1) {
     launch_lnl_full(d_recs, B, g, ev, prec, L, d_partials, s);
     launch_finalize_full(d_partials, d_recs, d_status, B, L.tiles, g, ev, prec, d_lnl, d_rho, s, model);
     return false;
   }
-  const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model};
+  const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model, d_order};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, fo, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, fo, s);
   return true;

@@ -121,6 +121,37 @@ def test_launch_shapes_agree(cfg2):
     e.set_launch(0, 0)
 
 
+def test_length_ordered_batch_matches_unordered(cfg2, ora):
+    """At one tile per set (B >= 1184) the sets run in order of their bin count: every set's lnL
+    equals the same set in a multi-tile launch (which runs in index order), invalid sets at
+    scattered positions included, and repeat calls are bit-identical."""
+    ev, e = cfg2
+    rng = np.random.default_rng(2504)
+    P = synth.draw_params(rng, 2048, ev.inj)
+    bad = [5, 700, 2047]
+    P[bad, 2] = 1.5                    # spin outside [-1, 1]
+    assert e.get_launch(len(P), q.FP64)[0] == 1
+    for prec, tol in ((q.FP64, 1e-9), (q.MIXED, 2e-4)):
+        L = e.lnl_full(P, prec, allow_invalid=True)
+        assert np.array_equal(L, e.lnl_full(P, prec, allow_invalid=True)), "repeat calls must be bit-identical"
+        e.set_launch(4, 256)
+        Lu = e.lnl_full(P, prec, allow_invalid=True)
+        e.set_launch(0, 0)
+        assert np.all(L[bad] == -1e20) and np.all(Lu[bad] == -1e20)
+        np.testing.assert_allclose(L, Lu, rtol=0, atol=tol)
+    idx = np.array([0, 1, 511, 1024, 1500, 2046])
+    Lo, _ = ora.lnl_full_batch(ev, P[idx])
+    np.testing.assert_allclose(e.lnl_full(P, q.FP64, allow_invalid=True)[idx], Lo, rtol=0,
+                               atol=LNL_ATOL_FP64 * max(1.0, np.abs(Lo).max() / 100))
+    # more sets than the ordering kernel reads in one pass (1024 threads x 4)
+    P2 = synth.draw_params(rng, 4500, ev.inj)
+    L2 = e.lnl_full(P2, q.FP64)
+    e.set_launch(2, 256)
+    L2u = e.lnl_full(P2, q.FP64)
+    e.set_launch(0, 0)
+    np.testing.assert_allclose(L2, L2u, rtol=0, atol=1e-9)
+
+
 def test_invalid_parameter_sets_flagged(ev1):
     ev, z, e = ev1
     P = z["params"][:4].copy()
