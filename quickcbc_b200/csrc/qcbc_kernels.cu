@@ -872,6 +872,28 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
   for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
 }
 
+// Programmatic dependent launch: a kernel launched with launch_pdl may be scheduled while the
+// previous kernel of its stream still runs; pdl_wait() returns once that kernel has finished and
+// its writes are visible (immediately for a kernel launched the ordinary way).  A kernel that
+// calls pdl_trigger() lets its dependent be scheduled from then on.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+static void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // Claims a slot of class c (c < 0: none) for each lane, one shared atomic per distinct class of
 // the warp; returns the lane's slot.  Every lane of the warp calls it.
 __device__ __forceinline__ int claim_slot(int* cnt, int c) {
@@ -884,7 +906,7 @@ __device__ __forceinline__ int claim_slot(int* cnt, int c) {
 }
 
 constexpr int kOrderThreads = 1024;
-constexpr int kOrderChunk = 4;       // classes a thread holds at once
+constexpr int kOrderChunk = 2;       // classes a thread holds at once
 static_assert(kOrderBuckets == 64, "k_order_sets scans two classes per lane of one warp");
 
 // Counting sort of the B sets by length class, longest first: order[k] = the set that lnL block
@@ -892,6 +914,8 @@ static_assert(kOrderBuckets == 64, "k_order_sets scans two classes per lane of o
 __global__ void __launch_bounds__(kOrderThreads) k_order_sets(const int* __restrict__ cls, int* __restrict__ order,
                                                               int B) {
   __shared__ int cnt[kOrderBuckets];
+  pdl_wait();          // the setup's classes
+  pdl_trigger();       // the lnL launch may be scheduled; it waits for order[]
   if (threadIdx.x < kOrderBuckets) cnt[threadIdx.x] = 0;
   __syncthreads();
   constexpr int step = kOrderThreads * kOrderChunk;
@@ -937,6 +961,7 @@ __global__ void __launch_bounds__(kOrderThreads) k_order_sets(const int* __restr
 __global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
                                                          QnmTable q, PhdRec* __restrict__ recs,
                                                          int* __restrict__ status, int model, int* __restrict__ cls) {
+  pdl_trigger();       // a dependent launch (k_order_sets) may be scheduled; it waits for this grid
   GeomOne geo{g};
   setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model, cls);
 }
@@ -953,7 +978,7 @@ void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const
   if (B <= 0) return;
   k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
                                                                       o.cls);
-  k_order_sets<<<1, kOrderThreads, 0, s>>>(o.cls, o.order, B);
+  launch_pdl(k_order_sets, dim3(1), dim3(kOrderThreads), 0, s, (const int*)o.cls, o.order, B);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -1349,6 +1374,7 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
                                                   double* __restrict__ partials, FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
+  pdl_wait();          // records (and order) of the previous launch
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order ? fo.order[bi] : bi;
   load_record(rec, recs + b);
@@ -1396,6 +1422,7 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ float2 s_rot[];   // [NIFO][nk]
+  pdl_wait();          // records (and order) of the previous launch
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order ? fo.order[bi] : bi;
   load_record(rec, recs + b);
@@ -1422,7 +1449,8 @@ static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const Event
                            double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
-  k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
+  if (fo.order) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
+  else k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
 static void launch_full_mixed(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
@@ -1438,11 +1466,9 @@ template <int PREC>
 static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
                              double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
-  switch (g.nifo) {
-    case 1: k_lnl_full<PREC, 1><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
-    case 2: k_lnl_full<PREC, 2><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
-    default: k_lnl_full<PREC, 3><<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo); break;
-  }
+  auto k = g.nifo == 1 ? k_lnl_full<PREC, 1> : (g.nifo == 2 ? k_lnl_full<PREC, 2> : k_lnl_full<PREC, 3>);
+  if (fo.order) launch_pdl(k, grid, block, 0, s, r, g, ev, L.tiles, part, fo);
+  else k<<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
