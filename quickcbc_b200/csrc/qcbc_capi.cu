@@ -548,27 +548,25 @@ static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, do
   int rc = workspace(w);
   if (rc) return rc;
   const size_t ps = (size_t)param_stride(model, g.nifo);
-  if ((rc = grow(w->d_params, w->c_params, (size_t)B * ps))) return rc;
-  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
-  if ((rc = grow(w->d_rho, w->c_rho, (size_t)B * kMaxIfo))) return rc;
   if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * ps))) return rc;
   if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
   if ((rc = grow_host(w->h_rho, w->ch_rho, (size_t)B * kMaxIfo))) return rc;
-  if ((rc = grow_host(w->h_status, w->ch_status, (size_t)B))) return rc;
   memcpy(w->h_params, params, sizeof(double) * ps * (size_t)B);
   cudaStream_t s = w->stream;
-  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * ps * (size_t)B, cudaMemcpyHostToDevice, s));
-  if ((rc = enqueue_full(w, ev, w->d_params, B, w->d_lnl, rho ? w->d_rho : nullptr, prec, s, g, nullptr, nullptr,
-                         model)))
-    return rc;
-  CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
-  if (rho) CU(cudaMemcpyAsync(w->h_rho, w->d_rho, sizeof(double) * B * g.nifo, cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+  // The setup reads the parameters from, and the lnL kernel writes lnL (and rho) into, the pinned
+  // staging buffers directly (mapped host memory): the bytes cross the host link inside the
+  // kernels, with no copy calls and their latency.
+  double *m_params = nullptr, *m_lnl = nullptr, *m_rho = nullptr;
+  CU(cudaHostGetDevicePointer((void**)&m_params, w->h_params, 0));
+  CU(cudaHostGetDevicePointer((void**)&m_lnl, w->h_lnl, 0));
+  if (rho) CU(cudaHostGetDevicePointer((void**)&m_rho, w->h_rho, 0));
+  if ((rc = enqueue_full(w, ev, m_params, B, m_lnl, m_rho, prec, s, g, nullptr, nullptr, model))) return rc;
   CU(cudaStreamSynchronize(s));
   memcpy(lnl, w->h_lnl, sizeof(double) * B);
   if (rho) memcpy(rho, w->h_rho, sizeof(double) * B * g.nifo);
+  // a set fails the setup exactly when its lnL is the rejected-sample value
   int bad = 0;
-  for (int b = 0; b < B; b++) bad += w->h_status[b] != 0;
+  for (int b = 0; b < B; b++) bad += lnl[b] == -1.0e20;
   if (bad) return fail(QCBC_EDOM, "%d of %d parameter sets outside the waveform domain (lnL=-1e20)", bad, B);
   return QCBC_OK;
 }

@@ -722,14 +722,17 @@ constexpr int kSetupSets = 32;
 constexpr int kSetupThreads = 128;
 
 // geometry of set b: one shared NetGeom, or the event table of a multi-event launch
+// stride(model): doubles per parameter set in the launch's parameter array (the same for every set)
 struct GeomOne {
   NetGeom g;
   __device__ bool get(int, NetGeom& out, int& e) const { out = g; e = 0; return true; }
+  __device__ int stride(int model) const { return param_stride(model, g.nifo); }
 };
-struct GeomTable {
+struct GeomTable {            // multi-event launches: full model only
   const int* event_of;
   const EventDesc* events;
   int n_events;
+  __device__ int stride(int) const { return param_stride(kModelFull, kMaxIfo); }
   __device__ bool get(int b, NetGeom& out, int& e) const {
     e = event_of[b];
     if (e < 0 || e >= n_events || events[e].g.nifo == 0) return false;     // out of range or an empty slot
@@ -767,8 +770,24 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     x.live = geo.get(b, g, e);
     s_g[lane] = g;
     s_ev[lane] = e;
-    const int ps = x.live ? param_stride(model, g.nifo) : 0;
-    for (int k = 0; k < ps; k++) x.p[k] = params[(size_t)b * ps + k];
+  }
+  {
+    // The block's parameters are contiguous: every thread loads its share with independent loads
+    // (one round trip, also when they are read from mapped host memory), then stores them.
+    constexpr int kPer = (kSetupSets * kMaxParams + kSetupThreads - 1) / kSetupThreads;
+    const int ps = geo.stride(model), n = nb * ps;
+    const double* src = params + (size_t)b0 * ps;
+    double v[kPer];
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int i = threadIdx.x + j * kSetupThreads;
+      v[j] = i < n ? src[i] : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < kPer; j++) {
+      const int i = threadIdx.x + j * kSetupThreads;
+      if (i < n) s_x[i / ps].p[i - (i / ps) * ps] = v[j];
+    }
   }
   __syncthreads();
   const bool on = lane < nb && x.live;
