@@ -238,6 +238,10 @@ struct Workspace {
   double* h_params = nullptr; size_t ch_params = 0;
   double* h_lnl = nullptr; size_t ch_lnl = 0;
   double* h_rho = nullptr; size_t ch_rho = 0;
+  // device addresses of the pinned buffers above (mapped_ptr), and the capacity of the buffer
+  // each was taken from (a buffer is only reallocated to a larger capacity)
+  double *m_params = nullptr, *m_lnl = nullptr, *m_rho = nullptr;
+  size_t m_params_of = 0, m_lnl_of = 0, m_rho_of = 0;
   int* h_status = nullptr; size_t ch_status = 0;
   // generic scratch for the reference-signature entry points
   double* d_a = nullptr; size_t c_a = 0;
@@ -542,6 +546,15 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   return QCBC_OK;
 }
 
+// Device address of pinned buffer h of capacity cap, cached in m while the capacity is `of`.
+static int mapped_ptr(double* h, size_t cap, double*& m, size_t& of) {
+  if (of != cap || !m) {
+    CU(cudaHostGetDevicePointer((void**)&m, h, 0));
+    of = cap;
+  }
+  return QCBC_OK;
+}
+
 static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int prec,
                     const NetGeom& g, int model = kModelFull) {
   Workspace* w;
@@ -556,11 +569,12 @@ static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, do
   // The setup reads the parameters from, and the lnL kernel writes lnL (and rho) into, the pinned
   // staging buffers directly (mapped host memory): the bytes cross the host link inside the
   // kernels, with no copy calls and their latency.
-  double *m_params = nullptr, *m_lnl = nullptr, *m_rho = nullptr;
-  CU(cudaHostGetDevicePointer((void**)&m_params, w->h_params, 0));
-  CU(cudaHostGetDevicePointer((void**)&m_lnl, w->h_lnl, 0));
-  if (rho) CU(cudaHostGetDevicePointer((void**)&m_rho, w->h_rho, 0));
-  if ((rc = enqueue_full(w, ev, m_params, B, m_lnl, m_rho, prec, s, g, nullptr, nullptr, model))) return rc;
+  if ((rc = mapped_ptr(w->h_params, w->ch_params, w->m_params, w->m_params_of))) return rc;
+  if ((rc = mapped_ptr(w->h_lnl, w->ch_lnl, w->m_lnl, w->m_lnl_of))) return rc;
+  if (rho && (rc = mapped_ptr(w->h_rho, w->ch_rho, w->m_rho, w->m_rho_of))) return rc;
+  if ((rc = enqueue_full(w, ev, w->m_params, B, w->m_lnl, rho ? w->m_rho : nullptr, prec, s, g, nullptr, nullptr,
+                         model)))
+    return rc;
   CU(cudaStreamSynchronize(s));
   memcpy(lnl, w->h_lnl, sizeof(double) * B);
   if (rho) memcpy(rho, w->h_rho, sizeof(double) * B * g.nifo);
