@@ -139,6 +139,14 @@ def test_length_ordered_batch_matches_unordered(cfg2, ora):
         e.set_launch(0, 0)
         assert np.all(L[bad] == -1e20) and np.all(Lu[bad] == -1e20)
         np.testing.assert_allclose(L, Lu, rtol=0, atol=tol)
+    # rho from the one-tile kernel (written straight into the host staging buffer) against the
+    # multi-tile launch's
+    L1, R1 = e.lnl_full(P, q.FP64, rho=True, allow_invalid=True)
+    e.set_launch(4, 256)
+    _, R1u = e.lnl_full(P, q.FP64, rho=True, allow_invalid=True)
+    e.set_launch(0, 0)
+    assert np.all(R1[bad] == 0.0)
+    np.testing.assert_allclose(R1, R1u, rtol=1e-9, atol=1e-9)
     idx = np.array([0, 1, 511, 1024, 1500, 2046])
     Lo, _ = ora.lnl_full_batch(ev, P[idx])
     np.testing.assert_allclose(e.lnl_full(P, q.FP64, allow_invalid=True)[idx], Lo, rtol=0,
