@@ -133,7 +133,8 @@ void het_space(struct Net* net, struct Het* het, double* params, double* min, do
                double** SN, int N, double Tobs);
 
 /* The same functions under prefixed names, for a forwarding object that
- * gives an unchanged QuickCBC build strong definitions. */
+ * gives an unchanged QuickCBC build strong definitions: a small C file that
+ * defines each reference name as a call to its qcbc_gpu_ counterpart. */
 double qcbc_gpu_log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
                                     double* rho, int N, double Tobs);
 double qcbc_gpu_log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs);
