@@ -53,6 +53,25 @@ def test_lnl_intrinsic_vs_reference(ev1, sec):
     np.testing.assert_allclose(Lm, Lref, rtol=0, atol=1e-3)
 
 
+def test_lnl_intrinsic_large_batch_ordered_launch(ev1, sec):
+    """At one tile per set (B >= 1184) the intrinsic model runs in the length-ordered launch, with
+    the two-detector rule applied in the lnL kernel: lnL and SNR^2 equal the multi-tile launch's
+    and the fixture's for the sets it holds."""
+    _, e = ev1
+    base = sec["int_params"]
+    P = np.tile(base, (1500 // len(base) + 1, 1))[:1500].copy()
+    P[:, 6] += np.linspace(-0.01, 0.01, len(P))          # spread the sets' time offsets
+    assert e.get_launch(len(P), q.FP64)[0] == 1
+    L, S = e.lnl_intrinsic(P, q.FP64, snrsq=True)
+    e.set_launch(4, 256)
+    Lu, Su = e.lnl_intrinsic(P, q.FP64, snrsq=True)
+    e.set_launch(0, 0)
+    np.testing.assert_allclose(L, Lu, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(S, Su, rtol=1e-9, atol=1e-9)
+    Lf = e.lnl_intrinsic(base, q.FP64)
+    np.testing.assert_allclose(e.lnl_intrinsic(np.vstack([base, P]), q.FP64)[:len(base)], Lf, rtol=0, atol=1e-9)
+
+
 def test_lnl_intrinsic_rejects_wrong_layout(ev1, sec):
     _, e = ev1
     with pytest.raises(ValueError):
