@@ -662,8 +662,9 @@ def main():
                      "kernel_ms": kmean * 1e3, "bytes_per_launch": alg_bytes,
                      "note": "algorithmic bytes = 2048 sets x 3 det x 16064 bins x 12 B (FP32 weighted data); "
                              "one event's data serves all sets from L2, so DRAM traffic is the records plus one "
-                             "pass of the data; the kernel is bound by instruction issue and FP64 dependency "
-                             "latency (ncu: IPC 2.2 of 4, 110 instructions per set-bin; see profiles/)"},
+                             "pass of the data; the kernel is bound by instruction issue and dependency "
+                             "latency (ncu: IPC 2.58 of 4, about 145 thread instructions per set-bin; see "
+                             "profiles/k_lnl_full_mixed_cfg2.md)"},
         "clocks": clk.summary(),
         "fp64_batched": {"value": fp64_rate, "unit": "lnL evals/s", "ms_per_step": float(np.mean(ms64))},
         "fp64_per_call_dropin": {"value": percall_rate, "unit": "lnL evals/s",
