@@ -1254,9 +1254,9 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
 #pragma unroll
     for (int id = 0; id < NIFO; id++) {
       double cyc = (double)k * (Dstep * (c.ts - c.td[id]) - (double)bs * Ri);
-      double sv, cv;
-      sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
-      s_rot[id * nk + k] = make_float2((float)cv, (float)sv);
+      float sv, cv;                  // reduced to one cycle in FP64, the rotation itself in FP32
+      sincospif(2.0f * (float)(cyc - rint(cyc)), &sv, &cv);
+      s_rot[id * nk + k] = make_float2(cv, sv);
     }
   }
   __syncthreads();
@@ -1267,9 +1267,9 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
 #pragma unroll
   for (int id = 0; id < NIFO; id++) {
     double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi - fma((double)i, Ri, R0);
-    double sv, cv;
-    sincospi(2.0 * (cyc - rint(cyc)), &sv, &cv);
-    base[id] = make_float2((float)cv, (float)sv);
+    float sv, cv;
+    sincospif(2.0f * (float)(cyc - rint(cyc)), &sv, &cv);
+    base[id] = make_float2(cv, sv);
   }
   const MixPoly& P = c.mix;
   int k = 0;
