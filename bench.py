@@ -498,9 +498,8 @@ def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64",
 
 
 def run_profile(args):
-    """Warm-up then timed steps of the benchmark workload in one precision: k_setup, k_order_sets
-    and the lnL kernel per step (k_finalize_full in place of the sort when a set spans several
-    tiles)."""
+    """Warm-up then timed steps of the benchmark workload in one precision: k_setup and the lnL
+    kernel per step (and k_finalize_full when a set spans several tiles)."""
     import quickcbc_b200 as q
     from quickcbc_b200 import _lib
     _lib.check(_lib.lib().qcbc_init(0))

@@ -233,8 +233,11 @@ struct Workspace {
   double* d_part = nullptr; size_t c_part = 0;
   double* d_lnl = nullptr; size_t c_lnl = 0;
   double* d_rho = nullptr; size_t c_rho = 0;
-  int* d_cls = nullptr; size_t c_cls = 0;         // launch order of the sets (launch_setup_ordered)
-  int* d_order = nullptr; size_t c_order = 0;
+  // launch order of the sets (SetOrder): class counts of two calls, used by turns (the lnL launch
+  // of one call zeroes the other's), and the class lists
+  int* d_ocnt = nullptr; size_t c_ocnt = 0;
+  int* d_olist = nullptr; size_t c_olist = 0;
+  int ord_turn = 0;
   double* h_params = nullptr; size_t ch_params = 0;
   double* h_lnl = nullptr; size_t ch_lnl = 0;
   double* h_rho = nullptr; size_t ch_rho = 0;
@@ -527,13 +530,24 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   const Precision kp = prec == QCBC_MIXED ? kMixed : kFP64;
   if (L.tiles == 1) {
     // one tile per set: the sets run in order of length and the lnL kernel finalises each itself
-    if ((rc = grow(w->d_cls, w->c_cls, (size_t)B))) return rc;
-    if ((rc = grow(w->d_order, w->c_order, (size_t)B))) return rc;
-    launch_setup_ordered(d_params, B, g, ds.qnm, w->d_recs, w->d_status, SetOrder{w->d_cls, w->d_order}, s, model);
+    if (!w->d_ocnt) {
+      if ((rc = grow(w->d_ocnt, w->c_ocnt, (size_t)2 * kOrderClasses))) return rc;
+      CU(cudaMemsetAsync(w->d_ocnt, 0, sizeof(int) * 2 * kOrderClasses, s));
+    }
+    if ((rc = grow(w->d_olist, w->c_olist, (size_t)kOrderClasses * B))) return rc;
+    const SetOrder o{w->d_ocnt + kOrderClasses * w->ord_turn, w->d_olist,
+                     w->d_ocnt + kOrderClasses * (1 - w->ord_turn)};
+    launch_setup_ordered(d_params, B, g, ds.qnm, w->d_recs, w->d_status, o, s, model);
     if (k0) cudaEventRecord(k0, s);
-    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, w->d_order, s);
+    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, &o, s);
     if (k1) cudaEventRecord(k1, s);
-    tls_launches += 3;
+    const cudaError_t le = cudaGetLastError();
+    if (le != cudaSuccess) {         // a launch that did not run leaves counts behind: clear both turns
+      cudaMemsetAsync(w->d_ocnt, 0, sizeof(int) * 2 * kOrderClasses, s);
+      return fail(QCBC_ECUDA, "lnL launch: %s", cudaGetErrorString(le));
+    }
+    w->ord_turn ^= 1;
+    tls_launches += 2;
   } else {
     launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
     if (k0) cudaEventRecord(k0, s);

@@ -741,20 +741,18 @@ struct GeomTable {            // multi-event launches: full model only
   }
 };
 
-constexpr int kOrderBuckets = 64;
-
-// length class of a set of `bins` bins in a band of `band` bins, 0 .. kOrderBuckets - 1 (it only
+// length class of a set of `bins` bins in a band of `band` bins, 0 .. kOrderClasses - 1 (it only
 // orders the launch, so its rounding does not matter)
 __device__ __forceinline__ int length_class(int bins, int band) {
-  return min(kOrderBuckets - 1, __float2int_rz((float)bins * ((float)kOrderBuckets / (float)max(band, 1))));
+  return min(kOrderClasses - 1, __float2int_rz((float)bins * ((float)kOrderClasses / (float)max(band, 1))));
 }
 
-// cls non-null: each set's length class (launch order, see k_order_sets)
+// ocnt / olist non-null: each set is filed under its length class (SetOrder)
 template <class Geom>
 __device__ __forceinline__ void setup_coop_block(const double* __restrict__ params, int B, const Geom& geo,
                                                  const QnmTable& q, int tile_bins, PhdRec* __restrict__ recs,
                                                  int* __restrict__ status, int* __restrict__ ntile, int model,
-                                                 int* __restrict__ cls = nullptr) {
+                                                 int* __restrict__ ocnt = nullptr, int* __restrict__ olist = nullptr) {
   __shared__ __align__(16) PhdRec s_rec[kSetupSets];
   __shared__ SetupScratch s_x[kSetupSets];
   __shared__ NetGeom s_g[kSetupSets];
@@ -877,10 +875,20 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     status[b] = st;
   }
   __syncthreads();
-  if ((ntile || cls) && w == 0 && lane < nb) {  // needs i_lo from warp 3
-    const int bins = (c.flags & kRecValid) ? max(0, c.i_hi - c.i_lo + 1) : 0;
-    if (ntile) ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
-    if (cls) cls[b] = length_class(bins, s_g[lane].imax - s_g[lane].imin);
+  if (ntile && w == 0 && lane < nb) {  // needs i_lo from warp 3
+    const int bins = (c.flags & kRecValid) ? c.i_hi - c.i_lo + 1 : 0;
+    ntile[b] = bins > 0 ? (bins + tile_bins - 1) / tile_bins : 0;
+  }
+  if (ocnt && w == 0) {                // all lanes of warp 0: one global atomic per class present
+    int cl = -1;
+    if (lane < nb) cl = length_class((c.flags & kRecValid) ? max(0, c.i_hi - c.i_lo + 1) : 0,
+                                     s_g[lane].imax - s_g[lane].imin);
+    const unsigned peers = __match_any_sync(0xffffffffu, cl);
+    const int leader = __ffs(peers) - 1;
+    int first = 0;
+    if (lane == leader && cl >= 0) first = atomicAdd(ocnt + cl, __popc(peers));
+    first = __shfl_sync(0xffffffffu, first, leader);
+    if (cl >= 0) olist[(size_t)cl * B + first + __popc(peers & ((1u << lane) - 1u))] = b;
   }
   if (on && w == 1) mix_phase_slopes(c);   // needs Ri from warp 0
   __syncthreads();
@@ -913,91 +921,25 @@ static void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, 
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
-// Claims a slot of class c (c < 0: none) for each lane, one shared atomic per distinct class of
-// the warp; returns the lane's slot.  Every lane of the warp calls it.
-__device__ __forceinline__ int claim_slot(int* cnt, int c) {
-  const unsigned peers = __match_any_sync(0xffffffffu, c);
-  const int lane = threadIdx.x & 31, leader = __ffs(peers) - 1;
-  int base = 0;
-  if (lane == leader && c >= 0) base = atomicAdd(&cnt[c], __popc(peers));
-  base = __shfl_sync(0xffffffffu, base, leader);
-  return base + __popc(peers & ((1u << lane) - 1u));
-}
-
-constexpr int kOrderThreads = 1024;
-constexpr int kOrderChunk = 2;       // classes a thread holds at once
-static_assert(kOrderBuckets == 64, "k_order_sets scans two classes per lane of one warp");
-
-// Counting sort of the B sets by length class, longest first: order[k] = the set that lnL block
-// k evaluates (one block).
-__global__ void __launch_bounds__(kOrderThreads) k_order_sets(const int* __restrict__ cls, int* __restrict__ order,
-                                                              int B) {
-  __shared__ int cnt[kOrderBuckets];
-  pdl_wait();          // the setup's classes
-  pdl_trigger();       // the lnL launch may be scheduled; it waits for order[]
-  if (threadIdx.x < kOrderBuckets) cnt[threadIdx.x] = 0;
-  __syncthreads();
-  constexpr int step = kOrderThreads * kOrderChunk;
-  int c[kOrderChunk];
-  for (int base = 0; base < B; base += step) {
-#pragma unroll
-    for (int j = 0; j < kOrderChunk; j++) {
-      const int s = base + j * kOrderThreads + threadIdx.x;
-      c[j] = s < B ? cls[s] : -1;
-    }
-#pragma unroll
-    for (int j = 0; j < kOrderChunk; j++) claim_slot(cnt, c[j]);
-  }
-  __syncthreads();
-  if (threadIdx.x < 32) {   // exclusive scan from the longest class: lane l holds classes 63-2l, 62-2l
-    const int l = threadIdx.x, v0 = cnt[kOrderBuckets - 1 - 2 * l], v1 = cnt[kOrderBuckets - 2 - 2 * l];
-    int x = v0 + v1;
-    for (int off = 1; off < 32; off <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, x, off);
-      if (l >= off) x += y;
-    }
-    const int start = x - v0 - v1;
-    cnt[kOrderBuckets - 1 - 2 * l] = start;
-    cnt[kOrderBuckets - 2 - 2 * l] = start + v0;
-  }
-  __syncthreads();
-  for (int base = 0; base < B; base += step) {
-    if (B > step) {   // one chunk: still in registers
-#pragma unroll
-      for (int j = 0; j < kOrderChunk; j++) {
-        const int s = base + j * kOrderThreads + threadIdx.x;
-        c[j] = s < B ? cls[s] : -1;
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < kOrderChunk; j++) {
-      const int pos = claim_slot(cnt, c[j]);
-      if (c[j] >= 0) order[pos] = base + j * kOrderThreads + threadIdx.x;
-    }
-  }
-}
-
 __global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
                                                          QnmTable q, PhdRec* __restrict__ recs,
-                                                         int* __restrict__ status, int model, int* __restrict__ cls) {
-  pdl_trigger();       // a dependent launch (k_order_sets) may be scheduled; it waits for this grid
+                                                         int* __restrict__ status, int model, SetOrder o) {
+  pdl_trigger();       // a dependent launch (the lnL kernel) may be scheduled; it waits for this grid
   GeomOne geo{g};
-  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model, cls);
+  setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model, o.cnt, o.list);
 }
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                   int* d_status, cudaStream_t s, int model) {
   if (B <= 0) return;
   k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
-                                                                      nullptr);
+                                                                      SetOrder{nullptr, nullptr, nullptr});
 }
 
 void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                           int* d_status, const SetOrder& o, cudaStream_t s, int model) {
   if (B <= 0) return;
-  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
-                                                                      o.cls);
-  launch_pdl(k_order_sets, dim3(1), dim3(kOrderThreads), 0, s, (const int*)o.cls, o.order, B);
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model, o);
 }
 
 // ---------------------------------------------------------------- reductions
@@ -1363,8 +1305,36 @@ struct FinalOut {
   double* lnl;
   double* rho;
   int mixed, model;
-  const int* order;    // non-null: block k evaluates set order[k] (one tile per set)
+  SetOrder order;      // order.cnt non-null: block k evaluates the k-th set longest first (one tile per set)
+  int B;
 };
+
+// The set that block k of a one-tile launch evaluates: the k-th with the classes longest first
+// (SetOrder).  Warp 0 scans the class counts, two classes per lane, and the lane whose class holds
+// position k reads the set from the class's list.  Block 0 also zeroes the following call's
+// counts.  Contains __syncthreads(): every thread of the block calls it.
+__device__ int ordered_set(const FinalOut& fo, int k) {
+  __shared__ int s_set;
+  static_assert(kOrderClasses == 64, "two classes per lane of one warp");
+  if (threadIdx.x < 32) {
+    const int l = threadIdx.x, c0 = kOrderClasses - 1 - 2 * l, c1 = c0 - 1;
+    const int v0 = fo.order.cnt[c0], v1 = fo.order.cnt[c1];
+    int x = v0 + v1;
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, x, off);
+      if (l >= off) x += y;
+    }
+    const int s0 = x - v0 - v1, s1 = s0 + v0;
+    if (k >= s0 && k < s1) s_set = fo.order.list[(size_t)c0 * fo.B + (k - s0)];
+    if (k >= s1 && k < s1 + v1) s_set = fo.order.list[(size_t)c1 * fo.B + (k - s1)];
+    if (blockIdx.x == 0) {
+      fo.order.next_cnt[c0] = 0;
+      fo.order.next_cnt[c1] = 0;
+    }
+  }
+  __syncthreads();
+  return s_set;
+}
 
 // thread 0's block sums of a set's only tile: its lnL, or its partials
 template <int NIFO>
@@ -1393,9 +1363,9 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
                                                   double* __restrict__ partials, FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
-  pdl_wait();          // records (and order) of the previous launch
+  pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
-  const int b = fo.order ? fo.order[bi] : bi;
+  const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1441,9 +1411,9 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ float2 s_rot[];   // [NIFO][nk]
-  pdl_wait();          // records (and order) of the previous launch
+  pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
-  const int b = fo.order ? fo.order[bi] : bi;
+  const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1468,7 +1438,7 @@ static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const Event
                            double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
-  if (fo.order) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
+  if (fo.order.cnt) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
   else k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
@@ -1486,28 +1456,29 @@ static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const Eve
                              double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   auto k = g.nifo == 1 ? k_lnl_full<PREC, 1> : (g.nifo == 2 ? k_lnl_full<PREC, 2> : k_lnl_full<PREC, 3>);
-  if (fo.order) launch_pdl(k, grid, block, 0, s, r, g, ev, L.tiles, part, fo);
+  if (fo.order.cnt) launch_pdl(k, grid, block, 0, s, r, g, ev, L.tiles, part, fo);
   else k<<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  const FinalOut none{nullptr, nullptr, 0, 0, nullptr};
+  const FinalOut none{nullptr, nullptr, 0, 0, SetOrder{nullptr, nullptr, nullptr}, B};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, none, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, none, s);
 }
 
 bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
-                           int model, const int* d_order, cudaStream_t s) {
+                           int model, const SetOrder* order, cudaStream_t s) {
   if (B <= 0) return true;
   if (L.tiles != 1) {
     launch_lnl_full(d_recs, B, g, ev, prec, L, d_partials, s);
     launch_finalize_full(d_partials, d_recs, d_status, B, L.tiles, g, ev, prec, d_lnl, d_rho, s, model);
     return false;
   }
-  const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model, d_order};
+  const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model,
+                    order ? *order : SetOrder{nullptr, nullptr, nullptr}, B};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, fo, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, fo, s);
   return true;

@@ -72,12 +72,16 @@ __host__ __device__ constexpr int param_stride(int model, int nifo) {
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                   int* d_status, cudaStream_t s, int model = kModelFull);
-// Launch order of the sets: the setup writes each set's length class (its bin count in 64
-// classes of the band) to cls[B], and a one-block kernel sorts the sets by class, longest first,
-// into order[B] (two launches).
+// Launch order of the sets: the setup files each set under its length class (its bin count in
+// kOrderClasses classes of the band): cnt[c] counts class c, list[c * B + r] is its r-th set (r in
+// no particular order).  Block k of the one-tile lnL launch then takes the k-th set with the
+// classes longest first.  cnt must be zero before the setup; the lnL launch zeroes next_cnt, the
+// counts of the following call.
+constexpr int kOrderClasses = 64;
 struct SetOrder {
-  int* cls;
-  int* order;
+  int* cnt;        // [kOrderClasses]
+  int* list;       // [kOrderClasses][B]
+  int* next_cnt;   // [kOrderClasses], zeroed by the lnL launch
 };
 void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                           int* d_status, const SetOrder& o, cudaStream_t s, int model = kModelFull);
@@ -89,11 +93,11 @@ void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const 
                           const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
                           cudaStream_t s, int model = kModelFull);
 // lnL of B sets with the finaliser folded into the lnL kernel when each set is one tile (L.tiles == 1),
-// in the order d_order when given (launch_setup_ordered); otherwise the lnL kernel and
+// longest first when order is given (filled by launch_setup_ordered); otherwise the lnL kernel and
 // launch_finalize_full.  Returns true when one launch did both.
 bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
-                           int model, const int* d_order, cudaStream_t s);
+                           int model, const SetOrder* order, cudaStream_t s);
 // fill the per-bin tables for bins [0, n)
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, float2* d_tabC, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,
