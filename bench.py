@@ -87,13 +87,48 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def traffic_from_profiles(kernel="k_lnl_full"):
-    """Per-launch DRAM bytes of the kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_lnl_full_mixed_cfg2.md")
+def ncu_capture(name):
+    """Per-launch figures of one kernel from a committed ncu capture: profiles/<name>.csv holds the
+    `ncu -i <rep> --page raw --csv` rows of that capture (kernel name, grid, block and the DRAM
+    byte counters; the command is in its first line).  Returns the mean per launch, or None."""
+    import csv
+    p = os.path.join(ROOT, "profiles", name + ".csv")
     if not os.path.exists(p):
         return None
-    m = re.search(r"dram_bytes_per_launch:\s*([0-9.eE+]+)", open(p).read())
-    return float(m.group(1)) if m else None
+    with open(p) as f:
+        lines = [ln for ln in f if not ln.startswith("#")]
+    rows = list(csv.DictReader(lines))
+    units = rows[0] if rows and not rows[0].get("ID", "0").strip().isdigit() else None
+    rows = [r for r in rows if r.get("ID", "").strip().isdigit()]
+    if not rows:
+        return None
+
+    def num(r, k):
+        v = float(r[k].replace(",", ""))
+        u = (units or {}).get(k, "").strip().lower()
+        return v * {"kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9, "usecond": 1e-6, "msecond": 1e-3, "nsecond": 1e-9}.get(u, 1.0)
+    rd = [num(r, "dram__bytes_read.sum") for r in rows]
+    wr = [num(r, "dram__bytes_write.sum") for r in rows]
+    out = {"kernel": rows[0]["Kernel Name"], "grid": rows[0].get("Grid Size"), "block": rows[0].get("Block Size"),
+           "launches": len(rows), "dram_bytes": float(np.mean(np.add(rd, wr))), "file": f"profiles/{name}.csv"}
+    if "gpu__time_duration.sum" in rows[0]:
+        out["duration_s"] = float(np.mean([num(r, "gpu__time_duration.sum") for r in rows]))
+    return out
+
+
+def capture_traffic(name, kernel, grid, block, kernel_ms):
+    """roofline.traffic from the committed capture of this kernel, used only when the capture is of
+    the same kernel at the same launch shape (grid, block) as the timed launches; else null."""
+    cap = ncu_capture(name)
+    if cap is None:
+        return None, {"traffic_source": f"no capture profiles/{name}.csv"}
+    same = kernel in cap["kernel"] and str(cap["grid"]).replace(" ", "") == grid and \
+        str(cap["block"]).replace(" ", "") == block
+    info = {"traffic_source": cap["file"], "traffic_capture_launches": cap["launches"],
+            "traffic_capture_matches_launch": bool(same)}
+    if "duration_s" in cap:
+        info["capture_ms_cold"] = cap["duration_s"] * 1e3
+    return (cap["dram_bytes"] if same else None), info
 
 
 def load_peaks():
@@ -102,6 +137,20 @@ def load_peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def fp32_peak_tflops(sm_mhz):
+    """FP32 FMA peak of a B200 at the given SM clock: 148 SMs x 128 FP32 lanes x 2 flops per FMA.
+    MEASURED_PEAKS.json carries only HBM and bf16 figures, so this one is derived from the spec at
+    the clock sampled during the run."""
+    return 148 * 128 * 2 * (sm_mhz or 1965.0) * 1e6 / 1e12
+
+
+# Algorithmic FP32 work of one full-likelihood evaluation per in-band bin (the per-unit figures of
+# the path): one IMRPhenomD point (~60 flops: the piecewise amplitude and phase polynomials) plus,
+# per detector, the projection and the two multiply-accumulates of <d|h> and <h|h> (~14 flops).
+WF_FLOPS_PER_BIN = 60
+PROJ_FLOPS_PER_DET_BIN = 14
 
 
 def make_workload(seed_offset=0):
@@ -124,10 +173,11 @@ def cpu_baseline_reference(ev, P, budget_s=12.0, impl_note=""):
         from oracle import ref
         if not ref.available():
             raise FileNotFoundError
-        net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+        net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST, L=ref.native_lib())
         S = ev.SN.copy()
         S[:, int(16.0 * ev.Tobs):int(ev.fmin * ev.Tobs)] = np.inf   # reference built with fmin = 16 Hz
-        kind, cores = "reference", ref.max_threads()
+        kind, cores = "reference", ref.max_threads(net.L)
+        impl_note += f", build {ref.native_variant()}"
         run = lambda X, nt=cores: ref.lnl_full_batch(net, ev.D, X, ev.freq, S, ev.N, ev.Tobs, nthreads=nt)  # noqa: E731
     except Exception:
         from oracle import ora
@@ -172,14 +222,15 @@ def run_reference_arm(args):
     sample = 128   # parameter sets per timed step (bounded sample of the 2048-set step)
     try:
         from oracle import ref
-        net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+        net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST, L=ref.native_lib())
         S = ev.SN.copy()
         S[:, int(16.0 * ev.Tobs):int(ev.fmin * ev.Tobs)] = np.inf
         run = lambda X: ref.lnl_full_batch(net, ev.D, X, ev.freq, S, ev.N, ev.Tobs)  # noqa: E731
-        kind, cores = "reference", ref.max_threads()
+        kind, cores = "reference", ref.max_threads(net.L)
+        build = ref.native_variant()
     except Exception:
         run = lambda X: ora.lnl_full_batch(ev, X)  # noqa: E731
-        kind, cores = "port", os.cpu_count()
+        kind, cores, build = "port", os.cpu_count(), "oracle/_build"
     for w in range(args.warmup):
         run(P[:sample])
     secs = 0.0
@@ -193,7 +244,8 @@ def run_reference_arm(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic coloured Gaussian noise + IMRPhenomD injection", "config": dict(CONFIG),
             "cpu_baseline": {"value": v, "unit": "lnL evals/s", "cores": int(cores), "kind": kind,
-                             "sample": f"{sample} of the 2048 parameter sets per step, OpenMP over sets"},
+                             "sample": f"{sample} of the 2048 parameter sets per step, OpenMP over sets",
+                             "build": build},
             "e2e": {"value": v, "unit": "lnL evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -227,6 +279,88 @@ def bench_cfg1_percall(q, eng, _lib):
     q.set_band(16.0, 1024.0)
     return {"workload": "config 1: H1/L1, 4 s, 2048 Hz, 16 temperatures x 1 call, FP64 drop-in",
             "value": steps * 16 / dt, "unit": "lnL evals/s", "us_per_call": 1e6 * dt / (steps * 16)}
+
+
+def dropin_per_call_rates(q, ev, P, calls=96):
+    """log_likelihood_full under the reference's signature, one parameter set per call, from one host
+    thread and from 12 at once (ctypes releases the GIL during the call), with the data registered
+    by qcbc_bind_data and without (the unchanged program's path: each call checks that the cached
+    device copy still holds the caller's D and SN)."""
+    import ctypes as C
+    from quickcbc_b200 import _lib, engine as eng
+    L = _lib.lib()
+    nh = eng._NetHolder(ev.labels, ev.Tobs, ev.GMST)
+    Dr, Sr = eng._rows(ev.D), eng._rows(ev.SN)
+    fr, rv = eng._rv(ev.freq)
+    fn = L.log_likelihood_full
+    Pc = [np.ascontiguousarray(p) for p in P[:calls]]
+
+    def work(k0, n):
+        rho = np.zeros(4)
+        for j in range(n):
+            fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+
+    def rate(nthreads):
+        ts = [threading.Thread(target=work, args=(7 * t, 4)) for t in range(nthreads)]
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        ts = [threading.Thread(target=work, args=(7 * t, calls)) for t in range(nthreads)]
+        t0 = time.perf_counter()
+        for t in ts:
+            t.start()
+        for t in ts:
+            t.join()
+        return nthreads * calls / (time.perf_counter() - t0)
+
+    out = {"unit": "lnL evals/s", "note": "FP64, log_likelihood_full reference signature, one set per call"}
+    L.qcbc_unbind_all()
+    out["one_thread_unbound"] = {"value": rate(1)}
+    out["12_threads_unbound"] = {"value": rate(12)}
+    _lib.check(L.qcbc_bind_data(nh.ref, Dr, Sr, ev.N, ev.Tobs))
+    out["one_thread_bound"] = {"value": rate(1)}
+    out["12_threads_bound"] = {"value": rate(12)}
+    L.qcbc_unbind_all()
+    out["value"] = out["one_thread_bound"]["value"]
+    return out
+
+
+def cpu_baseline_het(ev, het_grid, P, budget_s=10.0):
+    """The reference's log_likelihood_het (QuickCBC.c:5303, its production hot loop) on its own
+    heterodyne tables for the same grid, under OpenMP over the sets on all host cores, on a bounded
+    sample of the config-3 sets; plus one thread."""
+    from oracle import ref
+    L = ref.native_lib()
+    net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST, L=L)
+    S = ev.SN.copy()
+    S[:, int(16.0 * ev.Tobs):int(ev.fmin * ev.Tobs)] = np.inf   # reference built with fmin = 16 Hz
+    het = ref.RefHet(net)
+    het.set_grid(het_grid["fgrid"], int(het_grid["MN"]), int(het_grid["MM"]), int(het_grid["J"]), ev.Tobs)
+    with _QuietCStdout():
+        het.heterodyne(ev.D, ev.inj, ev.freq, S, ev.N, ev.Tobs)
+    cores = ref.max_threads(L)
+
+    def sample(seconds, nt, chunk):
+        n, secs, k = 0, 0.0, 0
+        t_end = time.perf_counter() + seconds
+        while time.perf_counter() < t_end:
+            X = P[(k * chunk) % len(P):(k * chunk) % len(P) + chunk]
+            _, sec = het.lnl_batch(X, ev.Tobs, nthreads=nt)
+            n += len(X)
+            secs += sec
+            k += 1
+        return n, secs
+
+    n, secs = sample(budget_s, cores, 1024)
+    n1, s1 = sample(2.0, 1, 64)
+    het.lnl_batch(P[:1], ev.Tobs, nthreads=cores)          # restore the thread count
+    Lr, _ = het.lnl_batch(P[:256], ev.Tobs)
+    return {"value": n / secs, "unit": "lnL evals/s", "cores": int(cores), "kind": "reference",
+            "build": ref.native_variant(),
+            "sample": f"{n} of the config-3 sets in chunks of 1024, OpenMP over sets, {secs:.1f} s wall",
+            "single_thread": {"value": n1 / s1, "unit": "lnL evals/s", "sample": f"{n1} sets, 1 thread"},
+            "lnl_first256": Lr}
 
 
 def prior_box(Tobs):
@@ -301,21 +435,53 @@ def bench_cfg3_het(q):
     t1 = time.perf_counter()
     e.het_setup(ev.inj, fgrid, MN, MM, 2)
     t2 = time.perf_counter()
-    P = synth.jitter_params(np.random.default_rng(3000 + 500000), 4096, ev.inj, scale=1e-6)
+    # sets where sampler chains sit: Fisher steps (the device Fisher_Het at the injection) whose
+    # length is searched so that lnL falls by U[0.5, 10] (half the sets: posterior width),
+    # U[10, 60] and U[100, 400] (burn-in) below the injection
+    rng = np.random.default_rng(3000 + 500000)
+    F = e.het_fisher(ev.inj[None, :])[0]
+    ranges = ((0.5, 10.0, 2048), (10.0, 60.0, 1024), (100.0, 400.0, 1024))
+    drops = np.concatenate([rng.uniform(lo, hi, n) for lo, hi, n in ranges])
+    P = synth.cloud_at_drops(rng, ev.inj, F, drops, lambda X: e.lnl_het(X, q.FP64, allow_invalid=True))
+    group = np.repeat(np.arange(len(ranges)), [n for _, _, n in ranges])
     dP = q.DeviceBuffer(P.nbytes)
     dP.upload(P)
-    out = {"workload": "config 3: 3 det, 128 s, 4096 Hz, BNS 1.45+1.30, het grid M=%d" % len(fgrid),
+    out = {"workload": "config 3: 3 det, 128 s, 4096 Hz, BNS 1.45+1.30, het grid M=%d; 4096 sets whose "
+                       "lnL lies 0.5-10 (2048), 10-60 (1024) and 100-400 (1024) below the injection's"
+                       % len(fgrid),
            "het_space_s": t1 - t0, "heterodyne_s": t2 - t1,
            "grid_equals_reference": bool(np.array_equal(fgrid, g3["fgrid"])),
            "reference_het_space_heterodyne": reference_het_space_seconds()}
     Lh64 = e.lnl_het(P, q.FP64)
     Lhm = e.lnl_het(P, q.MIXED)
+    L0 = e.lnl_het(ev.inj[None, :], q.FP64)[0]
+    out["het_lnl_drop_range"] = [float(np.min(L0 - Lh64)), float(np.max(L0 - Lh64))]
+    out["het_max_abs_dlnL_mixed_vs_fp64_by_drop"] = {
+        "%g-%g" % (lo, hi): float(np.max(np.abs(Lh64 - Lhm)[group == k])) for k, (lo, hi, _) in enumerate(ranges)}
+    # the reference's own values on the fixture's 48 sets at the same three spreads
+    z3 = np.load(os.path.join(ROOT, "tests", "golden", "spread3.npz"))
+    if np.array_equal(fgrid, g3["fgrid"]) and ev.GMST == float(z3["GMST"]):
+        Pz = z3["params"]
+        out["vs_reference_spread_fixture"] = {
+            "sets": int(len(Pz)),
+            "het_mixed_max_abs": float(np.max(np.abs(e.lnl_het(Pz, q.MIXED) - z3["lnl_het"]))),
+            "het_fp64_max_abs": float(np.max(np.abs(e.lnl_het(Pz, q.FP64) - z3["lnl_het"]))),
+            "full_mixed_max_abs": float(np.max(np.abs(e.lnl_full(Pz, q.MIXED) - z3["lnl_full"]))),
+            "full_fp64_max_abs": float(np.max(np.abs(e.lnl_full(Pz, q.FP64) - z3["lnl_full"]))),
+        }
     for prec, name in ((q.MIXED, "het_mixed"), (q.FP64, "het_fp64")):
         q.time_lnl_het(e, dP, len(P), prec, 3, flush_l2=True)
         ms = q.time_lnl_het(e, dP, len(P), prec, 10, flush_l2=True)
         out[name] = {"value": len(P) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
     out["het_max_abs_dlnL_mixed_vs_fp64"] = float(np.max(np.abs(Lh64 - Lhm)))
-    Pf = P[:512]
+    try:
+        cb = cpu_baseline_het(ev, g3, P)
+        cb["max_abs_dlnL_gpu_fp64_vs_reference"] = float(np.max(np.abs(np.asarray(cb.pop("lnl_first256")) -
+                                                                       Lh64[:256])))
+        out["cpu_baseline_het"] = cb
+    except Exception as exc:
+        out["cpu_baseline_het"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
+    Pf = P[::8]                                          # 512 sets across the three spreads
     dPf = q.DeviceBuffer(Pf.nbytes)
     dPf.upload(Pf)
     Lf64 = e.lnl_full(Pf, q.FP64)
@@ -325,7 +491,7 @@ def bench_cfg3_het(q):
         ms, _ = q.time_lnl_full(e, dPf, len(Pf), prec, 5, flush_l2=True)
         out[name] = {"value": len(Pf) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
     out["full_max_abs_dlnL_mixed_vs_fp64"] = float(np.max(np.abs(Lf64 - Lfm)))
-    out["het_vs_full_fp64_max_abs"] = float(np.max(np.abs(Lh64[:512] - Lf64)))
+    out["het_vs_full_fp64_max_abs"] = float(np.max(np.abs(Lh64[::8] - Lf64)))
     e.close()
     return out
 
@@ -422,11 +588,13 @@ def interleaved_stream(q, b, evs, eo, P, Lm):
     nbytes = 0
     for e, ev in enumerate(evs):
         bins = min(int(ev.Tobs * 1024.0), ev.N // 2) - int(ev.Tobs * ev.fmin)
-        nbytes += int(np.sum(eo == e)) * len(ev.labels) * bins * 16
+        # useful bytes: FP32 (wr, wi, ws) per detector-bin and one FP32 bin factor per bin
+        nbytes += int(np.sum(eo == e)) * bins * (12 * len(ev.labels) + 4)
     t = float(np.median(ms)) * 1e-3
     peak, kind = load_peaks()
     return {"value": len(P_i) / t, "unit": "lnL evals/s", "ms": t * 1e3, "stream_bytes": nbytes,
             "achieved_GBs": nbytes / t / 1e9, "frac_hbm": nbytes / t / 1e9 / peak, "peak_kind": kind,
+            "bytes_note": "12 B per detector-bin + 4 B per bin of every set (each set reads its event's band)",
             "same_lnl_as_grouped_order": bool(np.array_equal(L_i, Lm[order]))}
 
 
@@ -472,8 +640,9 @@ def bench_cfg5_serving(q, n_runs=32, n_steps=20000, precisions=("mixed", "fp64",
     def tmpl(info, p):
         return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
     evs = [synth.make_event(tmpl, **s) for s in synth.uneven_event_specs(n_runs, seed=5000)]
-    out = {"workload": "config 5: %d runs, Poisson %.1f/s, 16 temps x 8 chains x %d steps, config-4 events, "
-                       "HBM budget 150 GB" % (n_runs, rate_hz, n_steps)}
+    arrivals = "all submitted at t = 0" if rate_hz is None else "Poisson %.1f/s" % rate_hz
+    out = {"workload": "config 5: %d runs, %s, 16 temps x 8 chains x %d steps, config-4 events, "
+                       "HBM budget 150 GB" % (n_runs, arrivals, n_steps)}
     for name in precisions:
         # "<precision>" samples the full lnL; "<precision>-het" builds each run's heterodyne grid and
         # tables on the GPU at admission and samples the heterodyned lnL, as the reference does;
@@ -622,52 +791,49 @@ def main():
            "unit": "lnL evals/s", "h2d_bytes_per_step": int(P.nbytes),
            "d2h_bytes_per_step": int(B * 8)}
 
-    # plain FP64 one-call-per-parameter-set drop-in (reference signature, data bound once)
-    ncall = 256
-    set_band = q.set_band
-    set_band(ev.fmin, 1024.0)
-    import ctypes as C
-    from quickcbc_b200 import engine as eng
-    nh = eng._NetHolder(ev.labels, ev.Tobs, ev.GMST)
-    Dr, Sr = eng._rows(ev.D), eng._rows(ev.SN)
-    fr, rv = eng._rv(ev.freq)
-    _lib.check(_lib.lib().qcbc_bind_data(nh.ref, Dr, Sr, ev.N, ev.Tobs))
-    rho = np.zeros(4)
-    fn = _lib.lib().log_likelihood_full
-    Pc = [np.ascontiguousarray(p) for p in P[:ncall]]
-    for p in Pc[:8]:
-        fn(nh.ref, Dr, eng._ptr(p), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
-    t0 = time.perf_counter()
-    for p in Pc:
-        fn(nh.ref, Dr, eng._ptr(p), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
-    percall_rate = ncall / (time.perf_counter() - t0)
-    _lib.lib().qcbc_unbind_all()
+    # plain FP64 one-call-per-parameter-set drop-in (reference signature): one host thread with the
+    # data bound once, and 12 host threads at once (the reference's NC = 12 OpenMP chains,
+    # QuickCBC.c:118, 2063-2067) bound and unbound
+    q.set_band(ev.fmin, 1024.0)
+    percall = dropin_per_call_rates(q, ev, P)
+    percall_rate = percall["one_thread_bound"]["value"]
 
-    # roofline of the fused kernel: algorithmic bytes = B x nifo x bins x 12 B (FP32 wr, wi, ws)
+    # roofline of the fused kernel: FP32 work per launch over its device time; the HBM view of the
+    # same launch (the path's algorithmic 24 B per detector-bin) for context
     bins = ev.imax - ev.imin
-    alg_bytes = B * ev.nifo * bins * 12
     kmean = float(np.mean(kms)) * 1e-3
-    peak, peak_kind = load_peaks()
-    achieved = alg_bytes / kmean / 1e9
-    traffic = traffic_from_profiles()
+    clocks = clk.summary()
+    fp32_peak = fp32_peak_tflops(clocks.get("sm_max_mhz"))
+    flops_bin = WF_FLOPS_PER_BIN + PROJ_FLOPS_PER_DET_BIN * ev.nifo
+    flops = B * bins * flops_bin
+    tiles, threads = e.get_launch(B, q.MIXED)
+    traffic, tinfo = capture_traffic("k_lnl_full_mixed_cfg2", "k_lnl_full_mixed", f"({B * tiles},1,1)",
+                                     f"({threads},1,1)", kmean * 1e3)
+    hbm_peak, peak_kind = load_peaks()
+    alg_bytes = B * ev.nifo * bins * 24
     out = {
         "metric": METRIC, "value": value, "unit": "lnL evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64/f32 mixed", "data": "synthetic coloured Gaussian noise + IMRPhenomD injection",
         "config": dict(CONFIG, parallelism=f"replicas x{world}"),
         "e2e": e2e, "gpu_launches": int(launches),
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_lnl_full_mixed<3>",
-                     "kernel_ms": kmean * 1e3, "bytes_per_launch": alg_bytes,
-                     "note": "algorithmic bytes = 2048 sets x 3 det x 16064 bins x 12 B (FP32 weighted data); "
-                             "one event's data serves all sets from L2, so DRAM traffic is the records plus one "
-                             "pass of the data; the kernel is bound by instruction issue and dependency "
-                             "latency (ncu: IPC 2.58 of 4, about 145 thread instructions per set-bin; see "
-                             "profiles/k_lnl_full_mixed_cfg2.md)"},
-        "clocks": clk.summary(),
+        "roofline": {
+            "bound": "issue", "achieved": flops / kmean / 1e12, "peak": fp32_peak, "unit": "TFLOP/s",
+            "frac": flops / kmean / 1e12 / fp32_peak, "traffic": traffic, "kernel": "k_lnl_full_mixed<3>",
+            "kernel_ms": kmean * 1e3, "flops_per_launch": flops, "flops_per_set_bin": flops_bin,
+            "peak_kind": "FP32 FMA peak derived from the spec at the sampled max SM clock (148 SMs x 128 lanes x 2)",
+            **tinfo,
+            "hbm": {"algorithmic_bytes_per_launch": alg_bytes, "achieved_GBs": alg_bytes / kmean / 1e9,
+                    "peak": hbm_peak, "peak_kind": peak_kind,
+                    "note": "the path's 24 B per detector-bin (FP64 D re, im, S); one event's 0.6 MB of "
+                            "weighted data serves all 2048 sets from L2, so DRAM carries only the "
+                            "records and one pass of the data (traffic); HBM does not bind"},
+            "note": "achieved = (%d + %d x %d) FP32 flops per set-bin x %d sets x %d bins / kernel time; the "
+                    "kernel is bound by instruction issue (ncu: profiles/k_lnl_full_mixed_cfg2.md)"
+                    % (WF_FLOPS_PER_BIN, PROJ_FLOPS_PER_DET_BIN, ev.nifo, B, bins)},
+        "clocks": clocks,
         "fp64_batched": {"value": fp64_rate, "unit": "lnL evals/s", "ms_per_step": float(np.mean(ms64))},
-        "fp64_per_call_dropin": {"value": percall_rate, "unit": "lnL evals/s",
-                                 "note": "log_likelihood_full reference signature, one call per set, data bound"},
+        "fp64_per_call_dropin": percall,
         "mixed_vs_fp64_per_call": value / percall_rate / world,
         "mixed_vs_fp64_batched": value / fp64_rate / world,
         "max_abs_dlnL_mixed_vs_fp64": dmax,
@@ -678,9 +844,16 @@ def main():
         out["config3"] = bench_cfg3_het(q)
         out["config4_uneven"] = bench_cfg4_uneven(q)
         out["input_stage"] = bench_input_stage(q)
-        out["config5_serving_reduced"] = bench_cfg5_serving(q, n_runs=16, n_steps=1000, rate_hz=2.0)
-        out["config5_serving_reduced"]["note"] = ("reduced: 16 runs x 1000 steps per run (config 5 specifies "
-                                                  "20000 steps; full run: bench.py --serve)")
+        # config 5 as specified (32 runs of 16 x 8 chains x 20000 steps, Poisson 2/s): mixed against
+        # plain FP64, heterodyned and full likelihood, chains stepped on the device
+        out["config5_serving"] = bench_cfg5_serving(q, n_runs=32, n_steps=20000, rate_hz=2.0,
+                                                    precisions=("mixed-het-dev", "fp64-het-dev", "mixed-dev",
+                                                                "fp64-dev"))
+        # the same service saturated (every run submitted at t = 0), so that the GPU, not the
+        # arrival stream, sets the pace: host-stepped and device-stepped, mixed and FP64
+        out["config5_serving_saturated"] = bench_cfg5_serving(q, n_runs=16, n_steps=1000, rate_hz=None,
+                                                              precisions=("mixed", "fp64", "mixed-dev", "fp64-dev",
+                                                                          "mixed-het-dev", "fp64-het-dev"))
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_reference(ev, P)
     if rank == 0:

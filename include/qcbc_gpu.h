@@ -75,7 +75,12 @@ long long qcbc_event_device_bytes(const qcbc_event* ev);
 /* Full likelihood for B parameter sets (host arrays).  rho may be NULL
  * ([B][nifo] otherwise, rho = <d|h>/sqrt(<h|h>) per detector). */
 int qcbc_lnl_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int precision);
-/* Same with device pointers on a caller stream (cudaStream_t passed as void*, NULL = the thread's stream). */
+/* Same with device pointers on a caller stream (cudaStream_t passed as void*, NULL = the thread's stream).
+ * The work is queued on that stream with no synchronisation.  Calls from one host thread share
+ * that thread's scratch, so calls on different streams from one thread must be ordered (each
+ * after the previous one's work).  A call may be captured into a CUDA graph once the same call
+ * (same B and precision) has run uncaptured on the thread, which sizes the scratch; replays
+ * reuse the scratch of the thread that captured it. */
 int qcbc_lnl_full_dev(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho, int precision,
                       void* stream);
 /* Batched log_likelihood_intrinsic (QuickCBC.c:4093-4140): params [B][7 + 3 (nifo - 1)] in the
@@ -185,7 +190,10 @@ int qcbc_het_fisher(qcbc_event* ev, const double* params, int B, double* fish);
  *    streams, or host threads without ordering) race and corrupt each other's
  *    results.  Serialise them, e.g. on one stream.
  *  - stream is a cudaStream_t passed as void* (NULL = the default stream);
- *    results are ready when the work on that stream completes. */
+ *    results are ready when the work on that stream completes.  NULL here is
+ *    the legacy default stream, unlike qcbc_lnl_full_dev, where NULL is the
+ *    calling thread's own non-blocking stream: a caller moving between the
+ *    two with NULL gets a different ordering against its other work. */
 #define QCBC_NOALLOC_MAX_SETS 4096
 #define QCBC_NOALLOC_MAX_TILE_SLOTS 16384
 #define QCBC_NOALLOC_SCRATCH_BYTES 4669440

@@ -9,11 +9,22 @@
  * QuickCBC.h / IMRPhenomD_internals.h uses its own definitions and only needs
  * the prototypes (define QCBC_HAVE_REFERENCE_TYPES before including this).
  *
- * Device residency: D, SN and freq are host arrays owned by the caller.  A
- * call uploads them unless they were registered with qcbc_bind_data(), in
- * which case the device copies made at registration are used (register again
- * after changing their contents).  No caller pointer is kept beyond a call
- * except as the registration key.
+ * Device residency: D, SN and freq are host arrays owned by the caller.
+ * Arrays registered with qcbc_bind_data() are used from the device copies made
+ * at registration (register again after changing their contents).  Otherwise a
+ * call compares the caller's D and SN rows with a host copy of the rows its
+ * cached device event was built from and uploads them only when a value
+ * differs (the reference rewrites SN in place when it redraws the PSD,
+ * QuickCBC.c:1994-2010), so results always follow the arrays' contents.  No
+ * caller pointer is kept beyond a call except as a cache key.  freq must be the
+ * reference's grid, freq[i] = i/Tobs (QuickCBC.c:419-420); another grid is
+ * refused (-1e20, qcbc_last_error()).
+ *
+ * Threading: every function may be called from several host threads at once,
+ * as the reference's OpenMP chains call the likelihoods (QuickCBC.c:2063-2067).
+ * Each thread has its own CUDA stream and scratch; a cached event that is
+ * replaced (new data, new heterodyne tables, a new binding) stays alive until
+ * the calls still using it return.
  *
  * Errors: the double-returning functions cannot report errors in-band; on a
  * failure they return -1e20 (the reference's rejected-sample value,
@@ -95,8 +106,12 @@ int qcbc_unbind_all(void);
 double log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN, double* rho,
                            int N, double Tobs);
 /* replaces QuickCBC.c:5303; the struct Het tables are uploaded on first use and
- * re-uploaded when het->IP, het->M or het->logLb change (re-heterodyne). */
+ * re-uploaded when het->IP, het->M or het->logLb change (re-heterodyne).  Tables
+ * of at most 32 structs stay on the device, least recently used evicted. */
 double log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs);
+/* Drop the device copy of het's tables now (e.g. next to freehet, QuickCBC.c:5096);
+ * optional. */
+int qcbc_het_forget(const struct Het* het);
 /* replaces QuickCBC.c:5112; needs het->M, MN, MM, J, NR, fgrid, freq from het_space.
  * Allocates the table arrays with the reference's row-pointer layout
  * (Utilities.c:2981-3015) so freehet() (QuickCBC.c:5096) releases them. */

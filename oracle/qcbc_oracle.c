@@ -4,7 +4,8 @@
  * TEST INFRASTRUCTURE ONLY: the checker for the CUDA kernels, never the
  * product.  Every routine below restates the reference algorithm at the
  * cited file:line; parity with the reference itself (oracle/_ref) is tested
- * in tests/test_oracle_vs_ref.py.
+ * in tests/test_oracle.py (against the golden fixtures the reference wrote and
+ * against the reference library on fresh seeds).
  *
  * Structure (not the reference's): one coefficient record per parameter set
  * (struct phd) holds everything frequency independent; phd_eval() maps one

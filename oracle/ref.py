@@ -33,7 +33,110 @@ def lib():
     if _lib is None:
         if not available():
             raise FileNotFoundError(f"reference oracle not built: {LIB_PATH} (make -C oracle ref)")
-        L = C.CDLL(LIB_PATH)
+        _lib = _declare(C.CDLL(LIB_PATH))
+    return _lib
+
+
+_native = None
+
+
+def _cpu_flags():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("flags"):
+                    return set(ln.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return set()
+
+
+def native_variant():
+    """The build of the reference library matched to this host's CPU: oracle/_ref/x86-64-v4 (AVX-512)
+    or x86-64-v3 (AVX2, FMA), both -O3 (make -C oracle ref-native), else the portable oracle/_ref."""
+    f = _cpu_flags()
+    for name, need in (("x86-64-v4", {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}),
+                       ("x86-64-v3", {"avx2", "fma", "bmi2", "movbe"})):
+        if need <= f and os.path.exists(os.path.join(_HERE, "_ref", name, "libqcbc_ref.so")):
+            return name
+    return "portable"
+
+
+def native_lib():
+    """The reference library built for this host's instruction set (native_variant); used by the
+    CPU baselines.  Tests use lib(), the portable build."""
+    global _native
+    if _native is None:
+        v = native_variant()
+        _native = lib() if v == "portable" else _declare(C.CDLL(os.path.join(_HERE, "_ref", v, "libqcbc_ref.so")))
+    return _native
+
+
+LINKED_PATH = os.path.join(_HERE, "_ref", "libquickcbc_linked.so")
+_linked = None
+
+
+def linked_available() -> bool:
+    return os.path.exists(LINKED_PATH)
+
+
+def linked():
+    """oracle/_ref/libquickcbc_linked.so: the reference's sources unmodified, their thirteen
+    replaced functions weakened and forwarded to libqcbc_gpu.so by include/qcbc_forward.c
+    (make -C oracle linked).  Same ref_* harness as lib(), plus lk_mcmc / lk_time_calls
+    (link_harness.c) and the stub's call counters qcbc_forward_calls[13]."""
+    global _linked
+    if _linked is None:
+        if not linked_available():
+            raise FileNotFoundError(f"linked reference not built: {LINKED_PATH} (make -C oracle linked)")
+        L = _declare(C.CDLL(LINKED_PATH))
+        vp, d, i = C.c_void_p, C.c_double, C.c_int
+        L.lk_data_new.restype = vp
+        L.lk_data_new.argtypes = [i, _dp, _dp, i, _dp, i, d]
+        L.lk_data_free.argtypes = [vp]
+        L.lk_lnl_full.restype = d
+        L.lk_lnl_full.argtypes = [vp, vp, _dp, _dp]
+        L.lk_bind.argtypes = [vp, vp]
+        L.lk_unbind.argtypes = []
+        L.lk_mcmc.restype = d
+        L.lk_mcmc.argtypes = [vp, vp, vp, _dp, _dp, _dp, i, i, C.c_ulong, _dp, _dp, _dp, _dp, _ip,
+                              C.POINTER(C.c_longlong)]
+        L.lk_time_calls.restype = d
+        L.lk_time_calls.argtypes = [vp, vp, vp, _dp, i, i, i, _dp]
+        _linked = L
+    return _linked
+
+
+FORWARD_NAMES = ("log_likelihood_full", "log_likelihood_het", "heterodyne", "fulltemplates", "fullphaseamp",
+                 "IMRPhenomDGenerateh22FDAmpPhase", "fourier_nwip", "log_likelihood_intrinsic", "templates",
+                 "AmpPhase", "het_diff", "Fisher_Het", "het_space")
+
+
+def forward_calls():
+    """The forwarding stub's call counts, by name (FORWARD_NAMES order)."""
+    arr = (C.c_longlong * len(FORWARD_NAMES)).in_dll(linked(), "qcbc_forward_calls")
+    return {n: int(arr[k]) for k, n in enumerate(FORWARD_NAMES)}
+
+
+class LinkedData:
+    """D, SN and freq held by the linked reference as QuickCBC holds them for a run: row-pointer
+    arrays made once over these numpy buffers (writes into SN are seen by the next call)."""
+
+    def __init__(self, net: RefNet, D, SN, freq, N, Tobs):
+        self.L = net.L
+        self.D, self.SN, self.freq = _f64(D).copy(), _f64(SN).copy(), _f64(freq).copy()
+        self.N, self.Tobs = int(N), float(Tobs)
+        self.ptr = self.L.lk_data_new(net.nifo, self.D, self.SN, self.SN.shape[1], self.freq, self.N, self.Tobs)
+
+    def __del__(self):
+        try:
+            self.L.lk_data_free(self.ptr)
+        except Exception:
+            pass
+
+
+def _declare(L):
+    if True:
         vp = C.c_void_p
         L.ref_net_new.restype = vp
         L.ref_net_new.argtypes = [C.c_int, _ip, C.c_double, C.c_double]
@@ -84,8 +187,7 @@ def lib():
         L.skymap_all.restype = None
         L.skydensity_all.argtypes = [_dp, _dp, C.c_double, C.c_int, C.c_int]
         L.skydensity_all.restype = C.c_double
-        _lib = L
-    return _lib
+    return L
 
 
 def _f64(a):
@@ -95,16 +197,17 @@ def _f64(a):
 class RefNet:
     """struct Net (QuickCBC.h:13-25) owned by the reference library."""
 
-    def __init__(self, labels, Tobs, GMST):
+    def __init__(self, labels, Tobs, GMST, L=None):
+        self.L = L if L is not None else lib()
         self.labels = np.ascontiguousarray(labels, dtype=np.int32)
         self.nifo = len(self.labels)
         self.Tobs = float(Tobs)
         self.GMST = float(GMST)
-        self.ptr = lib().ref_net_new(self.nifo, self.labels, self.Tobs, self.GMST)
+        self.ptr = self.L.ref_net_new(self.nifo, self.labels, self.Tobs, self.GMST)
 
     def __del__(self):
         try:
-            lib().ref_net_free(self.ptr)
+            self.L.ref_net_free(self.ptr)
         except Exception:
             pass
 
@@ -136,7 +239,7 @@ def Times(alpha, sindelta, GMST):
 def fulltemplates(net: RefNet, freq, params, N):
     h = np.zeros((net.nifo, N))
     f = _f64(freq)
-    lib().ref_fulltemplates(net.ptr, h, f, len(f), _f64(params).copy(), N)
+    net.L.ref_fulltemplates(net.ptr, h, f, len(f), _f64(params).copy(), N)
     return h
 
 
@@ -144,7 +247,7 @@ def fullphaseamp(net: RefNet, freq, params, N):
     a = np.zeros((net.nifo, N // 2))
     p = np.zeros((net.nifo, N // 2))
     f = _f64(freq)
-    lib().ref_fullphaseamp(net.ptr, a, p, f, len(f), _f64(params).copy(), N)
+    net.L.ref_fullphaseamp(net.ptr, a, p, f, len(f), _f64(params).copy(), N)
     return a, p
 
 
@@ -155,7 +258,7 @@ def fourier_nwip(a, b, S, imin, imax, N):
 def lnl_full(net: RefNet, D, params, freq, SN, N, Tobs):
     rho = np.zeros(net.nifo + 1)
     SN = _f64(SN)
-    L = lib().ref_lnl_full(net.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN, SN.shape[1], rho, N, Tobs)
+    L = net.L.ref_lnl_full(net.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN, SN.shape[1], rho, N, Tobs)
     return L, rho[: net.nifo]
 
 
@@ -163,13 +266,13 @@ def templates(net: RefNet, freq, params, N):
     """templates (QuickCBC.c:3527): intrinsic parameters, 7 + 3 (Nifo - 1) entries."""
     h = np.zeros((net.nifo, N))
     f = _f64(freq)
-    lib().ref_templates(net.ptr, h, f, len(f), _f64(params).copy(), N)
+    net.L.ref_templates(net.ptr, h, f, len(f), _f64(params).copy(), N)
     return h
 
 
 def lnl_intrinsic(net: RefNet, D, params, freq, SN, N, Tobs):
     SN = _f64(SN)
-    return lib().ref_lnl_intrinsic(net.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN, SN.shape[1], N, Tobs)
+    return net.L.ref_lnl_intrinsic(net.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN, SN.shape[1], N, Tobs)
 
 
 def AmpPhase(freq, params, N):
@@ -185,13 +288,13 @@ def lnl_full_batch(net: RefNet, D, params, freq, SN, N, Tobs, nthreads=0):
     P = _f64(params)
     out = np.zeros(P.shape[0])
     SN = _f64(SN)
-    secs = lib().ref_lnl_full_batch(net.ptr, _f64(D), P, P.shape[0], _f64(freq), SN, SN.shape[1], N,
+    secs = net.L.ref_lnl_full_batch(net.ptr, _f64(D), P, P.shape[0], _f64(freq), SN, SN.shape[1], N,
                                     Tobs, out, nthreads)
     return out, secs
 
 
-def max_threads():
-    return lib().ref_max_threads()
+def max_threads(L=None):
+    return (L if L is not None else lib()).ref_max_threads()
 
 
 class RefHet:
@@ -199,7 +302,8 @@ class RefHet:
 
     def __init__(self, net: RefNet):
         self.net = net
-        self.ptr = lib().ref_het_new()
+        self.L = net.L
+        self.ptr = self.L.ref_het_new()
 
     def space(self, params, pmin, pmax, freq, SN, N, Tobs, workdir):
         cwd = os.getcwd()
@@ -207,23 +311,23 @@ class RefHet:
         os.chdir(workdir)        # het_space writes diagnostic .dat files into the cwd
         try:
             SN = _f64(SN)
-            return lib().ref_het_space(self.net.ptr, self.ptr, _f64(params).copy(), _f64(pmin).copy(),
+            return self.L.ref_het_space(self.net.ptr, self.ptr, _f64(params).copy(), _f64(pmin).copy(),
                                        _f64(pmax).copy(), _f64(freq), SN, SN.shape[1], N, Tobs)
         finally:
             os.chdir(cwd)
 
     def set_grid(self, fgrid, MN, MM, J, Tobs):
         g = np.ascontiguousarray(fgrid, dtype=np.int32)
-        lib().ref_het_set_grid(self.ptr, g, len(g), MN, MM, J, Tobs)
+        self.L.ref_het_set_grid(self.ptr, g, len(g), MN, MM, J, Tobs)
 
     def heterodyne(self, D, params, freq, SN, N, Tobs):
         SN = _f64(SN)
-        lib().ref_heterodyne(self.net.ptr, self.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN,
+        self.L.ref_heterodyne(self.net.ptr, self.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN,
                              SN.shape[1], N, Tobs)
 
     def sizes(self):
         s = np.zeros(6, dtype=np.int32)
-        lib().ref_het_sizes(self.net.ptr, self.ptr, s)
+        self.L.ref_het_sizes(self.net.ptr, self.ptr, s)
         return dict(M=int(s[0]), MN=int(s[1]), MM=int(s[2]), J=int(s[3]), NR=int(s[4]), Nifo=int(s[5]))
 
     def export(self):
@@ -235,32 +339,32 @@ class RefHet:
             lc=np.zeros((NR, nI, J + 1)), ls=np.zeros((NR, nI, J + 1)), aa=np.zeros((nI, NR)),
             rc=np.zeros((nI, NR)), rs=np.zeros((nI, NR)), logLb=np.zeros(1),
         )
-        lib().ref_het_export(self.net.ptr, self.ptr, t["fgrid"], t["freq"], t["amp"], t["phase"], t["IP"],
+        self.L.ref_het_export(self.net.ptr, self.ptr, t["fgrid"], t["freq"], t["amp"], t["phase"], t["IP"],
                              t["SL"], t["lc"], t["ls"], t["aa"], t["rc"], t["rs"], t["logLb"])
         t["logLb"] = float(t["logLb"][0])
         t.update(z)
         return t
 
     def lnl(self, params, Tobs):
-        return lib().ref_lnl_het(self.net.ptr, self.ptr, _f64(params).copy(), Tobs)
+        return self.L.ref_lnl_het(self.net.ptr, self.ptr, _f64(params).copy(), Tobs)
 
     def lnl_batch(self, params, Tobs, nthreads=0):
         P = _f64(params)
         out = np.zeros(P.shape[0])
-        secs = lib().ref_lnl_het_batch(self.net.ptr, self.ptr, P, P.shape[0], Tobs, out, nthreads)
+        secs = self.L.ref_lnl_het_batch(self.net.ptr, self.ptr, P, P.shape[0], Tobs, out, nthreads)
         return out, secs
 
     def het_diff(self, params, dparams):
-        return lib().ref_het_diff(self.net.ptr, self.ptr, _f64(params).copy(), _f64(dparams).copy())
+        return self.L.ref_het_diff(self.net.ptr, self.ptr, _f64(params).copy(), _f64(dparams).copy())
 
     def fisher(self, params, Tobs):
         F = np.zeros((11, 11))
-        lib().ref_Fisher_Het(self.net.ptr, self.ptr, F, _f64(params).copy(), Tobs)
+        self.L.ref_Fisher_Het(self.net.ptr, self.ptr, F, _f64(params).copy(), Tobs)
         return F
 
     def lnl_test(self, D, params, freq, SN, N, Tobs):
         SN = _f64(SN)
-        return lib().ref_lnl_test(self.net.ptr, self.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN,
+        return self.L.ref_lnl_test(self.net.ptr, self.ptr, _f64(D), _f64(params).copy(), _f64(freq), SN,
                                   SN.shape[1], N, Tobs)
 
 

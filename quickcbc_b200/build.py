@@ -3,8 +3,9 @@
 Steps:
 1. Generate csrc/_gen/qnm_table.h: the IMRPhenomD quasi-normal-mode table
    (final spin, fring, fdamp; IMRPhenomD_internals.h:176-640 of the QuickCBC
-   reference) read from the reference tree given by QCBC_REFERENCE (default
-   /root/reference).  The generated file is a build output and is not committed.
+   reference) read from the reference tree given by QCBC_REFERENCE (default: a
+   `reference` directory beside this repository).  The generated file is a
+   build output and is not committed.
    When the reference tree is absent the existing generated file is reused.
 2. nvcc -gencode arch=compute_100a,code=sm_100a for the kernels and the C ABI.
 
@@ -28,7 +29,7 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", 
 
 
 def reference_dir() -> str:
-    return os.environ.get("QCBC_REFERENCE", "/root/reference")
+    return os.environ.get("QCBC_REFERENCE") or os.path.normpath(os.path.join(HERE, "..", "..", "reference"))
 
 
 def gen_qnm(force: bool = False) -> str:

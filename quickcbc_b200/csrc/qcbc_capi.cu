@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -233,11 +234,10 @@ struct Workspace {
   double* d_part = nullptr; size_t c_part = 0;
   double* d_lnl = nullptr; size_t c_lnl = 0;
   double* d_rho = nullptr; size_t c_rho = 0;
-  // launch order of the sets (SetOrder): class counts of two calls, used by turns (the lnL launch
-  // of one call zeroes the other's), and the class lists
+  // launch order of the sets (SetOrder): class counts, cleared on the call's stream before each
+  // ordered setup, and the class lists
   int* d_ocnt = nullptr; size_t c_ocnt = 0;
   int* d_olist = nullptr; size_t c_olist = 0;
-  int ord_turn = 0;
   double* h_params = nullptr; size_t ch_params = 0;
   double* h_lnl = nullptr; size_t ch_lnl = 0;
   double* h_rho = nullptr; size_t ch_rho = 0;
@@ -295,7 +295,7 @@ struct qcbc_event {
   double fmin = 16.0, fmax = 1024.0;
   int nh = 0;
   double* d_w64 = nullptr;
-  float4* d_w4 = nullptr;
+  float* d_wm = nullptr;     // FP32 planes of the mixed kernel (EventData::wm)
   double* d_D = nullptr;     // raw data [nifo][N] (heterodyne setup)
   double* d_S = nullptr;     // raw PSD [nifo][nh+1]
   double* d_freq = nullptr;  // canonical frequencies [nh]
@@ -310,7 +310,7 @@ struct qcbc_event {
 static EventData event_data(const qcbc_event* ev) {
   EventData d{};
   d.w64 = ev->d_w64;
-  d.w4 = ev->d_w4;
+  d.wm = ev->d_wm;
   d.nh = ev->nh;
   for (int k = 0; k < kMaxIfo; k++) d.inv_sigma[k] = ev->inv_sigma[k];
   const DeviceState& ds = g_dev[ev->device];
@@ -376,7 +376,9 @@ static int check_geom(int nifo, const int* labels, double Tobs, int N) {
   return QCBC_OK;
 }
 
-// Data upload: weighted FP64/FP32 copies plus raw D, S (rows gathered on the host).
+// Data upload: raw D, S (rows gathered on the host), then the weighted FP64 data and the mixed
+// kernel's FP32 planes built on the device by the kernel that rebuilds them after a PSD redraw
+// (launch_event_weights), so both ways give the same bits.
 static int event_upload(qcbc_event* ev, const double* const* Drows, const double* const* Srows) {
   const int nI = ev->g.nifo, N = ev->g.N, nh = N / 2;
   {
@@ -385,10 +387,9 @@ static int event_upload(qcbc_event* ev, const double* const* Drows, const double
     if (rc) return rc;
   }
   ev->nh = nh;
-  std::vector<double> w64((size_t)nI * 3 * nh, 0.0);
-  std::vector<float4> w4((size_t)nI * nh, make_float4(0.f, 0.f, 0.f, 0.f));
   std::vector<double> Dall((size_t)nI * N), Sall((size_t)nI * (nh + 1), 0.0);
-  int lo = std::max(ev->g.imin, 1), hi = std::min(ev->g.imax, nh);
+  const int lo = std::max(ev->g.imin, 1), hi = std::min(ev->g.imax, nh);
+  qcbc::Sigmas sg{{1.0, 1.0, 1.0}};
   for (int id = 0; id < nI; id++) {
     const double* D = Drows[id];
     const double* S = Srows[id];
@@ -399,50 +400,43 @@ static int event_upload(qcbc_event* ev, const double* const* Drows, const double
     for (int i = lo; i < hi; i++)
       if (S[i] > 0.0 && S[i] < smin) smin = S[i];
     if (!(smin < HUGE_VAL)) smin = 1.0;
-    double sigma = sqrt(smin);
-    ev->inv_sigma[id] = 1.0 / sigma;
-    double* wr = &w64[(size_t)id * 3 * nh];
-    double* wi = wr + nh;
-    double* ws = wi + nh;
-    for (int i = lo; i < hi; i++) {
-      double s = S[i];
-      wr[i] = 4.0 * sigma * D[i] / s;
-      wi[i] = 4.0 * sigma * D[N - i] / s;
-      ws[i] = 4.0 * sigma * sigma / s;
-    }
-    for (int i = 0; i < nh; i++) {
-      float4& v = w4[(size_t)id * nh + i];
-      v.x = (float)wr[i];
-      v.y = (float)wi[i];
-      v.z = (float)ws[i];
-      v.w = id == 0 ? (float)std::pow((double)(i > 0 ? i : 1), -7.0 / 6.0) : 0.0f;
-    }
+    sg.v[id] = sqrt(smin);
+    ev->inv_sigma[id] = 1.0 / sg.v[id];
   }
   std::vector<double> freq(nh);
   freq[0] = 1.0 / ev->g.Tobs;
   for (int i = 1; i < nh; i++) freq[i] = (double)i / ev->g.Tobs;
-  size_t b64 = w64.size() * 8, b32 = w4.size() * sizeof(float4), bD = Dall.size() * 8, bS = Sall.size() * 8, bf = freq.size() * 8;
+  const size_t b64 = (size_t)nI * 3 * nh * 8, bm = qcbc::mixed_plane_floats(nI, nh) * sizeof(float),
+               bD = Dall.size() * 8, bS = Sall.size() * 8, bf = freq.size() * 8;
   if (!ev->d_w64) {
     CU(cudaMalloc(&ev->d_w64, b64));
-    CU(cudaMalloc(&ev->d_w4, b32));
+    CU(cudaMalloc(&ev->d_wm, bm));
     CU(cudaMalloc(&ev->d_D, bD));
     CU(cudaMalloc(&ev->d_S, bS));
     CU(cudaMalloc(&ev->d_freq, bf));
   }
-  CU(cudaMemcpy(ev->d_w64, w64.data(), b64, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ev->d_w4, w4.data(), b32, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ev->d_D, Dall.data(), bD, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ev->d_S, Sall.data(), bS, cudaMemcpyHostToDevice));
-  CU(cudaMemcpy(ev->d_freq, freq.data(), bf, cudaMemcpyHostToDevice));
-  ev->bytes = (long long)(b64 + b32 + bD + bS + bf);
+  Workspace* w;
+  int rc = workspace(w);
+  if (rc) return rc;
+  cudaStream_t s = w->stream;     // the calling thread's stream: other threads' work goes on
+  CU(cudaMemsetAsync(ev->d_w64, 0, b64, s));
+  CU(cudaMemsetAsync(ev->d_wm, 0, bm, s));
+  CU(cudaMemcpyAsync(ev->d_D, Dall.data(), bD, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(ev->d_S, Sall.data(), bS, cudaMemcpyHostToDevice, s));
+  CU(cudaMemcpyAsync(ev->d_freq, freq.data(), bf, cudaMemcpyHostToDevice, s));
+  qcbc::launch_event_weights(ev->d_D, N, ev->d_S, nh + 1, nI, lo, hi, sg, ev->d_w64, ev->d_wm, s);
+  tls_launches += 1;
+  CU(cudaGetLastError());
+  CU(cudaStreamSynchronize(s));
+  ev->bytes = (long long)(b64 + bm + bD + bS + bf);
   ev->has_data = true;
   return QCBC_OK;
 }
 
 static void event_free_device(qcbc_event* ev) {
-  cudaFree(ev->d_w64); cudaFree(ev->d_w4); cudaFree(ev->d_D); cudaFree(ev->d_S); cudaFree(ev->d_freq);
+  cudaFree(ev->d_w64); cudaFree(ev->d_wm); cudaFree(ev->d_D); cudaFree(ev->d_S); cudaFree(ev->d_freq);
   cudaFree(ev->het.buf); cudaFree(ev->het.d_fgrid);
-  ev->d_w64 = nullptr; ev->d_w4 = nullptr; ev->d_D = nullptr; ev->d_S = nullptr; ev->d_freq = nullptr;
+  ev->d_w64 = nullptr; ev->d_wm = nullptr; ev->d_D = nullptr; ev->d_S = nullptr; ev->d_freq = nullptr;
   ev->het.buf = nullptr; ev->het.d_fgrid = nullptr;
 }
 
@@ -530,23 +524,18 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
   const Precision kp = prec == QCBC_MIXED ? kMixed : kFP64;
   if (L.tiles == 1) {
     // one tile per set: the sets run in order of length and the lnL kernel finalises each itself
-    if (!w->d_ocnt) {
-      if ((rc = grow(w->d_ocnt, w->c_ocnt, (size_t)2 * kOrderClasses))) return rc;
-      CU(cudaMemsetAsync(w->d_ocnt, 0, sizeof(int) * 2 * kOrderClasses, s));
-    }
+    // The counts start at zero on this call's stream, whatever ran before: repeated calls, calls
+    // on other streams and replays of a captured graph each clear their own.
+    if ((rc = grow(w->d_ocnt, w->c_ocnt, (size_t)kOrderClasses))) return rc;
     if ((rc = grow(w->d_olist, w->c_olist, (size_t)kOrderClasses * B))) return rc;
-    const SetOrder o{w->d_ocnt + kOrderClasses * w->ord_turn, w->d_olist,
-                     w->d_ocnt + kOrderClasses * (1 - w->ord_turn)};
+    CU(cudaMemsetAsync(w->d_ocnt, 0, sizeof(int) * kOrderClasses, s));
+    const SetOrder o{w->d_ocnt, w->d_olist};
     launch_setup_ordered(d_params, B, g, ds.qnm, w->d_recs, w->d_status, o, s, model);
     if (k0) cudaEventRecord(k0, s);
     launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, &o, s);
     if (k1) cudaEventRecord(k1, s);
     const cudaError_t le = cudaGetLastError();
-    if (le != cudaSuccess) {         // a launch that did not run leaves counts behind: clear both turns
-      cudaMemsetAsync(w->d_ocnt, 0, sizeof(int) * 2 * kOrderClasses, s);
-      return fail(QCBC_ECUDA, "lnL launch: %s", cudaGetErrorString(le));
-    }
-    w->ord_turn ^= 1;
+    if (le != cudaSuccess) return fail(QCBC_ECUDA, "lnL launch: %s", cudaGetErrorString(le));
     tls_launches += 2;
   } else {
     launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
@@ -1526,7 +1515,25 @@ struct BindKey {
     return N < o.N;
   }
 };
-static std::map<BindKey, qcbc_event*> g_bound;
+
+// The events the reference-signature entry points build from the caller's rows are held through
+// shared pointers.  A call copies the pointer under the cache's lock and keeps the event alive
+// while its kernels run, so replacing a cache entry (new data, new heterodyne tables, a new
+// binding) never frees or rewrites memory that a concurrent call reads: the old event is closed
+// when its last user returns.  Host threads may therefore call these entry points concurrently,
+// as the reference's OpenMP chains do (QuickCBC.c:2063-2067).
+struct EventRef {
+  qcbc_event* ev;
+  explicit EventRef(qcbc_event* e) : ev(e) {}
+  EventRef(const EventRef&) = delete;
+  EventRef& operator=(const EventRef&) = delete;
+  ~EventRef() { qcbc_event_close(ev); }
+};
+using EventPtr = std::shared_ptr<EventRef>;
+
+// The caches below live until the process exits and are never destroyed: destroying them would
+// close events after the CUDA runtime has shut down.
+static std::map<BindKey, EventPtr>& g_bound = *new std::map<BindKey, EventPtr>();   // qcbc_bind_data
 static std::mutex g_bind_mu;
 
 static qcbc_event* open_from_rows(struct Net* net, double** D, double** SN, int N, double Tobs) {
@@ -1542,24 +1549,118 @@ static qcbc_event* open_from_rows(struct Net* net, double** D, double** SN, int 
   return ev;
 }
 
+// Unbound calls: events cached by the rows' addresses together with a host copy of the rows they
+// were built from.  A call compares the caller's rows with that copy (the reference rewrites SN in
+// place when it redraws the PSD, QuickCBC.c:1994-2010) and reuses the event only when every value
+// is the same, so results never depend on stale data; anything else builds a new event.  At most
+// kRowsCacheMax entries, least recently used evicted.
+struct RowsSnap {
+  int nifo = 0, N = 0;
+  double Tobs = 0.0, GMST = 0.0, fmin = 0.0, fmax = 0.0;
+  std::vector<int> labels;
+  std::vector<double> D, S;     // [nifo][N], [nifo][N/2]
+  EventPtr ev;
+};
+struct RowsEntry {
+  std::shared_ptr<const RowsSnap> snap;
+  unsigned long long used = 0;
+};
+static std::map<BindKey, RowsEntry>& g_rows = *new std::map<BindKey, RowsEntry>();
+static unsigned long long g_rows_tick = 0;
+constexpr size_t kRowsCacheMax = 16;
+
+static bool rows_match(const RowsSnap& r, struct Net* net, double** D, double** SN, int N, double Tobs) {
+  if (r.nifo != net->Nifo || r.N != N || r.Tobs != Tobs || r.GMST != net->GMST || r.fmin != g_band_fmin ||
+      r.fmax != g_band_fmax)
+    return false;
+  const size_t nh = (size_t)N / 2;
+  for (int i = 0; i < r.nifo; i++) {
+    if (r.labels[i] != net->labels[i]) return false;
+    if (memcmp(&r.D[(size_t)i * N], D[i], sizeof(double) * (size_t)N) != 0) return false;
+    if (memcmp(&r.S[(size_t)i * nh], SN[i], sizeof(double) * nh) != 0) return false;
+  }
+  return true;
+}
+
+// The event holding (D, SN) for a reference-signature call: the bound one, else a cached one whose
+// rows equal the caller's, else a new one (which enters the cache).
+static EventPtr data_event(struct Net* net, double** D, double** SN, int N, double Tobs) {
+  const BindKey key{net, D, SN, N};
+  {
+    std::lock_guard<std::mutex> lk(g_bind_mu);
+    auto it = g_bound.find(key);
+    if (it != g_bound.end()) return it->second;
+  }
+  std::shared_ptr<const RowsSnap> snap;
+  {
+    std::lock_guard<std::mutex> lk(g_bind_mu);
+    auto it = g_rows.find(key);
+    if (it != g_rows.end()) {
+      it->second.used = ++g_rows_tick;
+      snap = it->second.snap;
+    }
+  }
+  if (snap && rows_match(*snap, net, D, SN, N, Tobs)) return snap->ev;   // compared outside the lock
+  qcbc_event* ev = open_from_rows(net, D, SN, N, Tobs);
+  if (!ev) return nullptr;
+  auto fresh = std::make_shared<RowsSnap>();
+  fresh->ev = std::make_shared<EventRef>(ev);
+  fresh->nifo = net->Nifo;
+  fresh->N = N;
+  fresh->Tobs = Tobs;
+  fresh->GMST = net->GMST;
+  fresh->fmin = g_band_fmin;
+  fresh->fmax = g_band_fmax;
+  fresh->labels.assign(net->labels, net->labels + net->Nifo);
+  const size_t nh = (size_t)N / 2;
+  fresh->D.resize((size_t)net->Nifo * N);
+  fresh->S.resize((size_t)net->Nifo * nh);
+  for (int i = 0; i < net->Nifo; i++) {
+    memcpy(&fresh->D[(size_t)i * N], D[i], sizeof(double) * (size_t)N);
+    memcpy(&fresh->S[(size_t)i * nh], SN[i], sizeof(double) * nh);
+  }
+  EventPtr out = fresh->ev;
+  std::lock_guard<std::mutex> lk(g_bind_mu);
+  g_rows[key] = RowsEntry{std::move(fresh), ++g_rows_tick};
+  while (g_rows.size() > kRowsCacheMax) {
+    auto lru = g_rows.begin();
+    for (auto it = g_rows.begin(); it != g_rows.end(); ++it)
+      if (it->second.used < lru->second.used) lru = it;
+    g_rows.erase(lru);
+  }
+  return out;
+}
+
+// The reference builds freq[i] = i/Tobs with freq[0] = 1/Tobs (QuickCBC.c:419-420) and the kernels
+// use that grid; another grid is refused rather than silently replaced.
+static bool reference_grid(const RealVector* freq, int N, double Tobs, int imin, int imax) {
+  const size_t nh = (size_t)N / 2;
+  if (!freq || !freq->data || freq->length < nh) return false;
+  const size_t probe[] = {1, (size_t)std::max(imin, 1), (size_t)std::max(imax - 1, 1), nh - 1};
+  for (size_t i : probe) {
+    if (i >= nh) continue;
+    const double want = (double)i / Tobs;
+    if (!(fabs(freq->data[i] - want) <= 1e-12 * want)) return false;
+  }
+  return true;
+}
+
 extern "C" int qcbc_bind_data(struct Net* net, double** D, double** SN, int N, double Tobs) {
   if (!net || !D || !SN) return fail(QCBC_EINVAL, "NULL argument");
   int rc = ensure_init();
   if (rc) return rc;
-  BindKey k{net, D, SN, N};
-  std::lock_guard<std::mutex> lk(g_bind_mu);
-  auto it = g_bound.find(k);
-  if (it != g_bound.end()) { qcbc_event_close(it->second); g_bound.erase(it); }
   qcbc_event* ev = open_from_rows(net, D, SN, N, Tobs);
   if (!ev) return QCBC_ENOMEM;
-  g_bound[k] = ev;
+  EventPtr p = std::make_shared<EventRef>(ev);
+  std::lock_guard<std::mutex> lk(g_bind_mu);
+  g_bound[BindKey{net, D, SN, N}] = std::move(p);    // a replaced binding closes after its last user
   return QCBC_OK;
 }
 
 extern "C" int qcbc_unbind_all(void) {
   std::lock_guard<std::mutex> lk(g_bind_mu);
-  for (auto& kv : g_bound) qcbc_event_close(kv.second);
   g_bound.clear();
+  g_rows.clear();
   return QCBC_OK;
 }
 
@@ -1575,52 +1676,52 @@ static int stage_freq(Workspace* w, const RealVector* freq, size_t n, double** d
 
 extern "C" double log_likelihood_full(struct Net* net, double** D, double* params, RealVector* freq, double** SN,
                                       double* rho, int N, double Tobs) {
-  (void)freq;   // the grid is i/Tobs, exactly what QuickCBC.c:419-420 builds
   if (!net || !D || !SN || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
   if (ensure_init()) return -1.0e20;
-  qcbc_event* ev = nullptr;
-  bool temp = false;
-  {
-    std::lock_guard<std::mutex> lk(g_bind_mu);
-    auto it = g_bound.find(BindKey{net, D, SN, N});
-    if (it != g_bound.end()) ev = it->second;
-  }
-  if (!ev) {
-    ev = open_from_rows(net, D, SN, N, Tobs);
-    if (!ev) return -1.0e20;
-    temp = true;
-  }
+  EventPtr ep = data_event(net, D, SN, N, Tobs);
+  if (!ep) return -1.0e20;
+  qcbc_event* ev = ep->ev;
   NetGeom g = ev->g;
   fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, ev->fmin, ev->fmax);
+  if (!reference_grid(freq, N, Tobs, g.imin, g.imax)) {
+    fail(QCBC_EINVAL, "freq is not the reference grid i/Tobs (QuickCBC.c:419-420)");
+    return -1.0e20;
+  }
   double lnl = -1.0e20, r[kMaxIfo];
   int rc = run_full(ev, params, 1, &lnl, r, QCBC_FP64, g);
   if (rho && rc == QCBC_OK)
     for (int i = 0; i < net->Nifo; i++) rho[i] = r[i];
-  if (temp) qcbc_event_close(ev);
   return rc == QCBC_OK ? lnl : -1.0e20;
 }
 
+// Heterodyne tables of the reference's struct Het, uploaded on first use and again when the
+// struct's tables change (another IP array, M or logLb: heterodyne() rebuilt them).  Entries are
+// keyed by the struct's address and evicted least recently used beyond kHetCacheMax, so the tables
+// of structs the caller has freed do not stay on the device for the life of the process.
 struct HetCacheEntry {
-  qcbc_event* ev = nullptr;
+  EventPtr ev;
   const void* ip = nullptr;
   int M = 0;
   double logLb = 0.0;
+  unsigned long long used = 0;
 };
-static std::map<const void*, HetCacheEntry> g_het_cache;
+static std::map<const void*, HetCacheEntry>& g_het_cache = *new std::map<const void*, HetCacheEntry>();
 static std::mutex g_het_mu;
+static unsigned long long g_het_tick = 0;
+constexpr size_t kHetCacheMax = 32;
 
-static qcbc_event* het_event_for(struct Net* net, struct Het* het) {
+static EventPtr het_event_for(struct Net* net, struct Het* het) {
   std::lock_guard<std::mutex> lk(g_het_mu);
   HetCacheEntry& e = g_het_cache[het];
+  e.used = ++g_het_tick;
   if (e.ev && e.ip == (const void*)het->IP && e.M == het->M && e.logLb == het->logLb) return e.ev;
-  if (!e.ev) {
-    e.ev = new qcbc_event();
-    e.ev->device = current_device();
-  }
-  qcbc_event* ev = e.ev;
-  fill_geom(ev->g, net->Nifo, net->labels, net->Tobs, net->GMST, 2 * het->M, 0.0, 1.0);
   int nI = net->Nifo, M = het->M, J = het->J, NR = het->NR, J1 = J + 1;
-  if (NR != (M - 1) / J) { fail(QCBC_EINVAL, "het NR inconsistent with M, J"); return nullptr; }
+  if (J < 1 || NR != (M - 1) / J) { fail(QCBC_EINVAL, "het NR inconsistent with M, J"); return nullptr; }
+  // a new event every time the tables change: calls still running on the old one keep it
+  qcbc_event* raw = new qcbc_event();
+  raw->device = current_device();
+  EventPtr ev = std::make_shared<EventRef>(raw);
+  fill_geom(raw->g, nI, net->labels, net->Tobs, net->GMST, 2 * het->M, 0.0, 1.0);
   std::vector<double> amp((size_t)nI * M), ph((size_t)nI * M), IP((size_t)NR * J1 * J1), SL((size_t)NR * nI * J1),
       lc(SL.size()), ls(SL.size()), aa((size_t)nI * NR), rcv(aa.size()), rsv(aa.size());
   for (int id = 0; id < nI; id++)
@@ -1641,21 +1742,36 @@ static qcbc_event* het_event_for(struct Net* net, struct Het* het) {
     }
   qcbc_het_tables t{M, het->MN, het->MM, J, NR, het->logLb, het->fgrid, het->freq->data, amp.data(), ph.data(),
                     IP.data(), SL.data(), lc.data(), ls.data(), aa.data(), rcv.data(), rsv.data()};
-  if (qcbc_het_set(ev, &t) != QCBC_OK) return nullptr;
+  if (qcbc_het_set(raw, &t) != QCBC_OK) return nullptr;
+  e.ev = ev;
   e.ip = het->IP;
   e.M = het->M;
   e.logLb = het->logLb;
+  while (g_het_cache.size() > kHetCacheMax) {
+    auto lru = g_het_cache.begin();
+    for (auto it = g_het_cache.begin(); it != g_het_cache.end(); ++it)
+      if (it->second.used < lru->second.used) lru = it;
+    g_het_cache.erase(lru);
+  }
   return ev;
+}
+
+// Forget the device copy of a struct Het's tables (e.g. before freehet); optional, since entries
+// are also evicted when the cache is full.
+extern "C" int qcbc_het_forget(const struct Het* het) {
+  std::lock_guard<std::mutex> lk(g_het_mu);
+  g_het_cache.erase(het);
+  return QCBC_OK;
 }
 
 extern "C" double log_likelihood_het(struct Net* net, struct Het* het, double* params, double Tobs) {
   (void)Tobs;   // fullphaseamp inside the reference's het lnL uses net->Tobs (QuickCBC.c:3797)
   if (!net || !het || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
   if (ensure_init()) return -1.0e20;
-  qcbc_event* ev = het_event_for(net, het);
+  EventPtr ev = het_event_for(net, het);
   if (!ev) return -1.0e20;
   double lnl = -1.0e20;
-  int rc = qcbc_lnl_het(ev, params, 1, &lnl, QCBC_FP64);
+  int rc = qcbc_lnl_het(ev->ev, params, 1, &lnl, QCBC_FP64);
   return rc == QCBC_OK ? lnl : -1.0e20;
 }
 
@@ -1834,26 +1950,19 @@ extern "C" double fourier_nwip(double* a, double* b, double* Sn, int imin, int i
 
 extern "C" double log_likelihood_intrinsic(struct Net* net, double** D, double* params, RealVector* freq,
                                            double** SN, int N, double Tobs) {
-  (void)freq;   // the grid is i/Tobs (QuickCBC.c:419-420)
   if (!net || !D || !SN || !params) { fail(QCBC_EINVAL, "NULL argument"); return -1.0e20; }
   if (ensure_init()) return -1.0e20;
-  qcbc_event* ev = nullptr;
-  bool temp = false;
-  {
-    std::lock_guard<std::mutex> lk(g_bind_mu);
-    auto it = g_bound.find(BindKey{net, D, SN, N});
-    if (it != g_bound.end()) ev = it->second;
-  }
-  if (!ev) {
-    ev = open_from_rows(net, D, SN, N, Tobs);
-    if (!ev) return -1.0e20;
-    temp = true;
-  }
+  EventPtr ep = data_event(net, D, SN, N, Tobs);
+  if (!ep) return -1.0e20;
+  qcbc_event* ev = ep->ev;
   NetGeom g = ev->g;
   fill_geom(g, net->Nifo, net->labels, Tobs, net->GMST, N, ev->fmin, ev->fmax);
+  if (!reference_grid(freq, N, Tobs, g.imin, g.imax)) {
+    fail(QCBC_EINVAL, "freq is not the reference grid i/Tobs (QuickCBC.c:419-420)");
+    return -1.0e20;
+  }
   double lnl = -1.0e20;
   int rc = run_full(ev, params, 1, &lnl, nullptr, QCBC_FP64, g, kModelIntrinsic);
-  if (temp) qcbc_event_close(ev);
   return rc == QCBC_OK ? lnl : -1.0e20;
 }
 
@@ -1917,20 +2026,20 @@ extern "C" void AmpPhase(double* Af, double* Pf, RealVector* freq, double* param
 extern "C" double het_diff(struct Net* net, struct Het* het, double* params, double* dparams) {
   if (!net || !het || !params || !dparams) { fail(QCBC_EINVAL, "NULL argument"); return 0.0; }
   if (ensure_init()) return 0.0;
-  qcbc_event* ev = het_event_for(net, het);
+  EventPtr ev = het_event_for(net, het);
   if (!ev) return 0.0;
   double out = 0.0;
-  return qcbc_het_diff(ev, params, dparams, 1, &out) == QCBC_OK ? out : 0.0;
+  return qcbc_het_diff(ev->ev, params, dparams, 1, &out) == QCBC_OK ? out : 0.0;
 }
 
 extern "C" void Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params, double Tobs) {
   (void)Tobs;   // fullphaseamp on the heterodyne grid uses net->Tobs (QuickCBC.c:3797)
   if (!net || !het || !fish || !params) { fail(QCBC_EINVAL, "NULL argument"); return; }
   if (ensure_init()) return;
-  qcbc_event* ev = het_event_for(net, het);
+  EventPtr ev = het_event_for(net, het);
   if (!ev) return;
   double F[11 * 11];
-  if (qcbc_het_fisher(ev, params, 1, F) != QCBC_OK) return;
+  if (qcbc_het_fisher(ev->ev, params, 1, F) != QCBC_OK) return;
   for (int i = 0; i < 11; i++)
     for (int j = 0; j < 11; j++) fish[i][j] = F[i * 11 + j];
 }
@@ -2101,7 +2210,7 @@ static int event_psd_changed(qcbc_event* ev, Workspace* w) {
     sg.v[id] = sqrt(m);
     ev->inv_sigma[id] = 1.0 / sg.v[id];
   }
-  qcbc::launch_event_weights(ev->d_D, ev->g.N, ev->d_S, nh + 1, nI, lo, hi, sg, ev->d_w64, ev->d_w4, s);
+  qcbc::launch_event_weights(ev->d_D, ev->g.N, ev->d_S, nh + 1, nI, lo, hi, sg, ev->d_w64, ev->d_wm, s);
   tls_launches += 2;
   CU(cudaGetLastError());
   CU(cudaStreamSynchronize(s));

@@ -237,7 +237,7 @@ __global__ void k_band_min(const double* __restrict__ S, int stride, int lo, int
 }
 
 __global__ void k_event_weights(const double* __restrict__ D, int N, const double* __restrict__ S, int stride, int lo,
-                                int hi, Sigmas sg, double* __restrict__ w64, float4* __restrict__ w4) {
+                                int hi, int nifo, Sigmas sg, double* __restrict__ w64, float* __restrict__ wm) {
   const int id = blockIdx.y;
   const int i = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= hi) return;
@@ -252,10 +252,29 @@ __global__ void k_event_weights(const double* __restrict__ D, int N, const doubl
   r[i] = wr;
   r[nh + i] = wi;
   r[2 * nh + i] = ws;
-  float4& v = w4[(size_t)id * nh + i];
-  v.x = (float)wr;
-  v.y = (float)wi;
-  v.z = (float)ws;
+  // the mixed kernel's planes (EventData::wm) carry the amplitude's bin factor i^{-7/6}
+  const double p = pow((double)i, -7.0 / 6.0);
+  const float fr = (float)(wr * p), fi = (float)(wi * p), fs = (float)(ws * (p * p));
+  const size_t n = (size_t)nh;
+  if (nifo == 1) {
+    wm[2 * (size_t)i] = fr;
+    wm[2 * (size_t)i + 1] = fi;
+    wm[2 * n + i] = fs;
+  } else {
+    // detectors 0 and 1: (wr, wi) pairs in the first float4 plane; detector 2's pair, then the
+    // ws of detectors 0 and 1, in the second plane (float4 for three detectors, float2 for two);
+    // detector 2's ws in the third
+    if (id < 2) {
+      wm[4 * (size_t)i + 2 * id] = fr;
+      wm[4 * (size_t)i + 2 * id + 1] = fi;
+      if (nifo == 3) wm[4 * n + 4 * (size_t)i + 2 + id] = fs;
+      else wm[4 * n + 2 * (size_t)i + id] = fs;
+    } else {
+      wm[4 * n + 4 * (size_t)i] = fr;
+      wm[4 * n + 4 * (size_t)i + 1] = fi;
+      wm[8 * n + i] = fs;
+    }
+  }
 }
 
 }  // namespace
@@ -265,10 +284,10 @@ void launch_band_min(const double* d_S, int stride, int nifo, int lo, int hi, do
 }
 
 void launch_event_weights(const double* d_D, int N, const double* d_S, int stride, int nifo, int lo, int hi,
-                          Sigmas sigma, double* d_w64, float4* d_w4, cudaStream_t s) {
+                          Sigmas sigma, double* d_w64, float* d_wm, cudaStream_t s) {
   if (hi <= lo) return;
   dim3 grid((hi - lo + 255) / 256, nifo);
-  k_event_weights<<<grid, 256, 0, s>>>(d_D, N, d_S, stride, lo, hi, sigma, d_w64, d_w4);
+  k_event_weights<<<grid, 256, 0, s>>>(d_D, N, d_S, stride, lo, hi, nifo, sigma, d_w64, d_wm);
 }
 
 }  // namespace qcbc

@@ -18,8 +18,9 @@ struct Sigmas {
   double v[3];
 };
 // Weighted data of bins [lo, hi) from D [nifo][N] and S rows: 4 sigma D/S (real, imaginary),
-// 4 sigma^2 / S, in FP64 ([nifo][3][nh]) and in the x, y, z lanes of the FP32 float4 copy.
+// 4 sigma^2 / S, in FP64 ([nifo][3][nh]) and, times the bin factors i^{-7/6}, i^{-7/6}, i^{-7/3},
+// in the mixed kernel's FP32 planes (EventData::wm).  Bins outside [lo, hi) are left as they are.
 void launch_event_weights(const double* d_D, int N, const double* d_S, int stride, int nifo, int lo, int hi,
-                          Sigmas sigma, double* d_w64, float4* d_w4, cudaStream_t s);
+                          Sigmas sigma, double* d_w64, float* d_wm, cudaStream_t s);
 
 }  // namespace qcbc

@@ -888,7 +888,8 @@ __device__ __forceinline__ void setup_coop_block(const double* __restrict__ para
     int first = 0;
     if (lane == leader && cl >= 0) first = atomicAdd(ocnt + cl, __popc(peers));
     first = __shfl_sync(0xffffffffu, first, leader);
-    if (cl >= 0) olist[(size_t)cl * B + first + __popc(peers & ((1u << lane) - 1u))] = b;
+    const int r = first + __popc(peers & ((1u << lane) - 1u));
+    if (cl >= 0 && r < B) olist[(size_t)cl * B + r] = b;   // r >= B only if the counts were not cleared
   }
   if (on && w == 1) mix_phase_slopes(c);   // needs Ri from warp 0
   __syncthreads();
@@ -933,7 +934,7 @@ void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTabl
                   int* d_status, cudaStream_t s, int model) {
   if (B <= 0) return;
   k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
-                                                                      SetOrder{nullptr, nullptr, nullptr});
+                                                                      SetOrder{nullptr, nullptr});
 }
 
 void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
@@ -1041,14 +1042,24 @@ __device__ __forceinline__ double mph_int(const MixPhInt& q, double xi, double u
   double u3 = u * u * u;
   return fma(xi, sld(q.Bi), sld(q.B0)) + fma(L, sld(q.BL), (u3 * u3 * u3) * sld(q.Bu9));
 }
+// How a piece's coefficients are read: from the block's record in shared memory at each use
+// (SmemRead, pins no registers), or from a copy the run keeps in registers (RegRead).
+struct SmemRead {
+  template <class T> static __device__ __forceinline__ T get(const T& x) { return sld(x); }
+};
+struct RegRead {
+  template <class T> static __device__ __forceinline__ T get(const T& x) { return x; }
+};
+
 // the ringdown rest in FP32 (cycles, a few at most): Ru3 / i + Rs s + Rat atan(i D1 - D0) with
 // tc = (1/i, s = i^{3/4}); each coefficient is a float pair applied hi after lo
+template <class R = SmemRead>
 __device__ __forceinline__ float mph_mrd(const MixPhMrd& q, float xf, float2 tc) {
-  const float z = fmaf(xf, sld(q.D1[0]), fmaf(xf, sld(q.D1[1]), -sld(q.D0[0]))) - sld(q.D0[1]);
+  const float z = fmaf(xf, R::get(q.D1[0]), fmaf(xf, R::get(q.D1[1]), -R::get(q.D0[0]))) - R::get(q.D0[1]);
   const float at = atanf(z);
-  float ph = fmaf(at, sld(q.Rat[0]), at * sld(q.Rat[1]));
-  ph = fmaf(tc.y, sld(q.Rs[0]), fmaf(tc.y, sld(q.Rs[1]), ph));
-  return fmaf(tc.x, sld(q.Ru3[0]), fmaf(tc.x, sld(q.Ru3[1]), ph));
+  float ph = fmaf(at, R::get(q.Rat[0]), at * R::get(q.Rat[1]));
+  ph = fmaf(tc.y, R::get(q.Rs[0]), fmaf(tc.y, R::get(q.Rs[1]), ph));
+  return fmaf(tc.x, R::get(q.Ru3[0]), fmaf(tc.x, R::get(q.Ru3[1]), ph));
 }
 // x minus the nearest integer, for |x| < 2^22, in FP32 adds
 __device__ __forceinline__ float frac_cyc(float x) {
@@ -1066,18 +1077,43 @@ __device__ __forceinline__ float mamp_int(const MixAmpInt& a, float xf) {
          x * (sld(a.hc[1]) +
               x * (sld(a.hc[2]) + (x - sld(a.h21)) * (sld(a.hc[3]) + (x - sld(a.h31)) * sld(a.hc[4]))));
 }
+template <class R = SmemRead>
 __device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, float xf) {
-  const float dfr = fmaf(xf, sld(a.m[0]), fmaf(xf, sld(a.m[1]), -sld(a.fRD[0]))) - sld(a.fRD[1]);
-  return __fdividef(__expf(-dfr * sld(a.g2_over_fg)) * sld(a.fg_g1), dfr * dfr + sld(a.fg2));
+  const float dfr = fmaf(xf, R::get(a.m[0]), fmaf(xf, R::get(a.m[1]), -R::get(a.fRD[0]))) - R::get(a.fRD[1]);
+  return __fdividef(__expf(-dfr * R::get(a.g2_over_fg)) * R::get(a.fg_g1), dfr * dfr + R::get(a.fg2));
 }
 
 // piece of bin i: 0 inspiral, 1 intermediate, 2 merger-ringdown
 __device__ __forceinline__ int amp_piece(const MixPoly& P, int i) { return i < P.iA ? 0 : (i >= P.iF ? 2 : 1); }
 __device__ __forceinline__ int ph_piece(const MixPoly& P, int i) { return i < P.iP ? 0 : (i >= P.iM ? 2 : 1); }
 
-// FP32 partial sums of up to 8 bins per detector: S = sum (wr - i wi) R_k amp e^{-i phi} and
-// sum amp^2 ws; flushed into the FP64 accumulators with the thread's rotation base applied,
-// so that acc[2 id] = sum amp (wr cos x + wi sin x), x = 2 pi f (ts - td) + lambda - phi.
+// The FP32 weighted data (wr', wi', ws') of NIFO detectors at bin b from the event's planes
+// (EventData::wm): three loads for three detectors, two for one or two.
+template <int NIFO>
+struct MixW {
+  float r[NIFO], i[NIFO], s[NIFO];
+  __device__ __forceinline__ void load(const float* __restrict__ wm, size_t nh, int b) {
+    if (NIFO == 3) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(wm) + b);
+      const float4 c = __ldg(reinterpret_cast<const float4*>(wm + 4 * nh) + b);
+      const float d = __ldg(wm + 8 * nh + b);
+      r[0] = a.x; i[0] = a.y; r[1 % NIFO] = a.z; i[1 % NIFO] = a.w;
+      r[2 % NIFO] = c.x; i[2 % NIFO] = c.y; s[0] = c.z; s[1 % NIFO] = c.w; s[2 % NIFO] = d;
+    } else if (NIFO == 2) {
+      const float4 a = __ldg(reinterpret_cast<const float4*>(wm) + b);
+      const float2 c = __ldg(reinterpret_cast<const float2*>(wm + 4 * nh) + b);
+      r[0] = a.x; i[0] = a.y; r[1 % NIFO] = a.z; i[1 % NIFO] = a.w; s[0] = c.x; s[1 % NIFO] = c.y;
+    } else {
+      const float2 a = __ldg(reinterpret_cast<const float2*>(wm) + b);
+      r[0] = a.x; i[0] = a.y; s[0] = __ldg(wm + 2 * nh + b);
+    }
+  }
+};
+
+// FP32 partial sums of up to 8 bins per detector: S = sum (wr' - i wi') R_k a e^{-i phi} and
+// sum a^2 ws' (a the amplitude without its bin factor i^{-7/6}, which the weighted data carry);
+// flushed into the FP64 accumulators with the thread's rotation base applied, so that
+// acc[2 id] = sum amp (wr cos x + wi sin x), x = 2 pi f (ts - td) + lambda - phi.
 template <int NIFO>
 struct MixAcc {
   float sx[NIFO], sy[NIFO], sh[NIFO];
@@ -1085,7 +1121,7 @@ struct MixAcc {
 #pragma unroll
     for (int id = 0; id < NIFO; id++) { sx[id] = 0.f; sy[id] = 0.f; sh[id] = 0.f; }
   }
-  __device__ __forceinline__ void add(float amp, float cyc, const float4* wv, const float2* rot, int nk) {
+  __device__ __forceinline__ void add(float amp, float cyc, const MixW<NIFO>& w, const float2* rot, int nk) {
     float sw, cw;
     __sincosf(6.28318530717958648f * cyc, &sw, &cw);     // |argument| <= pi
     const float ex = amp * cw, ey = -amp * sw, amp2 = amp * amp;
@@ -1093,9 +1129,9 @@ struct MixAcc {
     for (int id = 0; id < NIFO; id++) {
       const float2 R = rot[id * nk];
       const float qx = fmaf(R.x, ex, -R.y * ey), qy = fmaf(R.x, ey, R.y * ex);
-      sx[id] = fmaf(wv[id].x, qx, fmaf(wv[id].y, qy, sx[id]));
-      sy[id] = fmaf(wv[id].x, qy, fmaf(-wv[id].y, qx, sy[id]));
-      sh[id] = fmaf(amp2, wv[id].z, sh[id]);
+      sx[id] = fmaf(w.r[id], qx, fmaf(w.i[id], qy, sx[id]));
+      sy[id] = fmaf(w.r[id], qy, fmaf(-w.i[id], qx, sy[id]));
+      sh[id] = fmaf(amp2, w.s[id], sh[id]);
     }
   }
   __device__ __forceinline__ void flush(const float2* base, double* acc) {
@@ -1108,7 +1144,9 @@ struct MixAcc {
 };
 
 // Rows [k, k_end) of the thread's bins i = i0 + tid + k bs, all in amplitude piece AP and
-// phase piece PP (-1: decided per bin).  The coefficients of the pieces live in registers.
+// phase piece PP (-1: decided per bin).  The merger-ringdown pieces (most bins of heavy systems)
+// keep their coefficients in registers for the run; the others read theirs from the block's
+// record in shared memory at each use.
 template <int NIFO, int AP, int PP>
 __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot, int nk,
                                            const float2* base, int k, int k_end, int i, int i1, int bs,
@@ -1131,6 +1169,10 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
   // tables a row needs: tabA for the inspiral amplitude and the FP64 phase pieces, tabB for the
   // FP64 phase pieces, tabC for the ringdown phase
   constexpr bool kTabA = AP <= 0 || PP != 2, kTabB = PP != 2, kTabC = PP == 2 || PP < 0;
+  MixPhMrd qm_r;                    // register copies of the ringdown coefficients
+  MixAmpMrd am_r;
+  if (PP == 2) qm_r = qm;
+  if (AP == 2) am_r = am;
   for (int r = 0; r < n; r += 8) {
     const int m = min(8, n - r);
     MixAcc<NIFO> A;
@@ -1142,12 +1184,11 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       if (kTabA) tA = __ldg(ev.tabA + b);
       if (kTabB) tB = __ldg(ev.tabB + b);
       if (kTabC) tC = __ldg(ev.tabC + b);
-      float4 wv[NIFO];
-#pragma unroll
-      for (int id = 0; id < NIFO; id++) wv[id] = __ldg(ev.w4 + id * nh + b);
+      MixW<NIFO> w;
+      w.load(ev.wm, nh, b);
       float cyc, a;
       if (PP == 2) {
-        cyc = frac_cyc(mph_mrd(qm, xf, tC));
+        cyc = frac_cyc(mph_mrd<RegRead>(qm_r, xf, tC));
       } else if (PP >= 0) {
         const double ph = PP == 0 ? mph_ins(qi, xi, tA.x, tA.y, tB.x) : mph_int(qn, xi, tA.y, tB.x);
         cyc = (float)(ph - rint(ph));
@@ -1162,13 +1203,13 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       }
       if (AP == 0) a = mamp_ins(ai, xf, (float)tA.x);
       else if (AP == 1) a = mamp_int(an, xf);
-      else if (AP == 2) a = mamp_mrd(am, xf);
+      else if (AP == 2) a = mamp_mrd<RegRead>(am_r, xf);
       else {
         const int ap = amp_piece(P, b);
         a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x)
                     : (ap == 1 ? mamp_int(P.aint, xf) : mamp_mrd(P.amrd, xf));
       }
-      A.add(wv[0].w * a, cyc, wv, pr, nk);
+      A.add(a, cyc, w, pr, nk);
       b += bs;
       pr++;
       xi += dbs;
@@ -1311,13 +1352,16 @@ struct FinalOut {
 
 // The set that block k of a one-tile launch evaluates: the k-th with the classes longest first
 // (SetOrder).  Warp 0 scans the class counts, two classes per lane, and the lane whose class holds
-// position k reads the set from the class's list.  Block 0 also zeroes the following call's
-// counts.  Contains __syncthreads(): every thread of the block calls it.
+// position k reads the set from the class's list.  Returns -1 when the counts do not place a set
+// in [0, B) at position k (counts that were not cleared before the setup); the caller's block then
+// does nothing.  Contains __syncthreads(): every thread of the block calls it.
 __device__ int ordered_set(const FinalOut& fo, int k) {
   __shared__ int s_set;
   static_assert(kOrderClasses == 64, "two classes per lane of one warp");
   if (threadIdx.x < 32) {
     const int l = threadIdx.x, c0 = kOrderClasses - 1 - 2 * l, c1 = c0 - 1;
+    if (l == 0) s_set = -1;
+    __syncwarp();
     const int v0 = fo.order.cnt[c0], v1 = fo.order.cnt[c1];
     int x = v0 + v1;
     for (int off = 1; off < 32; off <<= 1) {
@@ -1325,12 +1369,10 @@ __device__ int ordered_set(const FinalOut& fo, int k) {
       if (l >= off) x += y;
     }
     const int s0 = x - v0 - v1, s1 = s0 + v0;
-    if (k >= s0 && k < s1) s_set = fo.order.list[(size_t)c0 * fo.B + (k - s0)];
-    if (k >= s1 && k < s1 + v1) s_set = fo.order.list[(size_t)c1 * fo.B + (k - s1)];
-    if (blockIdx.x == 0) {
-      fo.order.next_cnt[c0] = 0;
-      fo.order.next_cnt[c1] = 0;
-    }
+    int b = -1;
+    if (k >= s0 && k < s1 && k - s0 < fo.B) b = fo.order.list[(size_t)c0 * fo.B + (k - s0)];
+    if (k >= s1 && k < s1 + v1 && k - s1 < fo.B) b = fo.order.list[(size_t)c1 * fo.B + (k - s1)];
+    if (b >= 0 && b < fo.B) s_set = b;
   }
   __syncthreads();
   return s_set;
@@ -1366,6 +1408,7 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
   pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
+  if (b < 0) return;   // whole block
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1414,6 +1457,7 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
+  if (b < 0) return;   // whole block
   load_record(rec, recs + b);
   __syncthreads();
   int i0, i1;
@@ -1463,7 +1507,7 @@ static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const Eve
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  const FinalOut none{nullptr, nullptr, 0, 0, SetOrder{nullptr, nullptr, nullptr}, B};
+  const FinalOut none{nullptr, nullptr, 0, 0, SetOrder{nullptr, nullptr}, B};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, none, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, none, s);
 }
@@ -1478,7 +1522,7 @@ bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, con
     return false;
   }
   const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model,
-                    order ? *order : SetOrder{nullptr, nullptr, nullptr}, B};
+                    order ? *order : SetOrder{nullptr, nullptr}, B};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, fo, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, fo, s);
   return true;

@@ -22,7 +22,13 @@ struct NetGeom {
 //   wr = 4 sigma Re(D)/S,  wi = 4 sigma Im(D)/S,  ws = 4 sigma^2 / S  per bin.
 struct EventData {
   const double* w64;     // [nifo][3][nh]: wr, wi, ws rows (FP64 kernels)
-  const float4* w4;      // [nifo][nh]: (wr, wi, ws, x) with x = i^{-7/6} in detector 0 (mixed kernel)
+  // FP32 weighted data of the mixed kernel with the amplitude's bin factor folded in:
+  // wr' = wr i^{-7/6}, wi' = wi i^{-7/6}, ws' = ws i^{-7/3}, 12 B per detector-bin in planes that
+  // one thread reads with the fewest aligned loads (MixW):
+  //   nifo 3: float4 (wr0', wi0', wr1', wi1') | float4 (wr2', wi2', ws0', ws1') | float ws2'
+  //   nifo 2: float4 (wr0', wi0', wr1', wi1') | float2 (ws0', ws1')
+  //   nifo 1: float2 (wr0', wi0') | float ws0'
+  const float* wm;
   int nh;                // row length (N/2)
   double inv_sigma[kMaxIfo];
   // per-bin constants shared by all events on a device (index = bin number i >= 1):
@@ -32,6 +38,8 @@ struct EventData {
   const float2* tabC;
   int tab_n;
 };
+// Floats of the mixed kernel's planes for an event of nifo detectors: 3 per detector-bin over nh bins.
+inline size_t mixed_plane_floats(int nifo, size_t nh) { return (size_t)3 * nifo * nh; }
 
 // Heterodyne summary tables on the device (layouts as the reference's struct Het, flattened):
 //   freq[M], amp/phase[nifo][M], IP[NR][J+1][J+1], SL/lc/ls[NR][nifo][J+1], aa/rc/rs[nifo][NR].
@@ -75,13 +83,12 @@ void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTabl
 // Launch order of the sets: the setup files each set under its length class (its bin count in
 // kOrderClasses classes of the band): cnt[c] counts class c, list[c * B + r] is its r-th set (r in
 // no particular order).  Block k of the one-tile lnL launch then takes the k-th set with the
-// classes longest first.  cnt must be zero before the setup; the lnL launch zeroes next_cnt, the
-// counts of the following call.
+// classes longest first.  cnt must be zero before the setup (the caller clears it on the launch
+// stream).
 constexpr int kOrderClasses = 64;
 struct SetOrder {
   int* cnt;        // [kOrderClasses]
   int* list;       // [kOrderClasses][B]
-  int* next_cnt;   // [kOrderClasses], zeroed by the lnL launch
 };
 void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                           int* d_status, const SetOrder& o, cudaStream_t s, int model = kModelFull);

@@ -163,14 +163,18 @@ class Server:
 
 def serve_stream(server, events, rate_hz, seed=0, sampler=None, log=None):
     """Submit `events` as a Poisson stream (mean rate_hz arrivals per second, in
-    real time) and step the service until every run has finished.
+    real time; rate_hz=None submits every event at once, which saturates the
+    service) and step the service until every run has finished.
 
     Returns per-run times-to-posterior, their p50/p99, and the aggregate lnL
     evaluations per second over the whole session."""
     sampler = dict(sampler or {})
     rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, size=len(events)))
-    arrivals -= arrivals[0]
+    if rate_hz is None:
+        arrivals = np.zeros(len(events))
+    else:
+        arrivals = np.cumsum(rng.exponential(1.0 / rate_hz, size=len(events)))
+        arrivals -= arrivals[0]
     t0 = server.clock()
     ids, nxt = [], 0
     e0 = server.stats()["lnl_evals"]

@@ -189,6 +189,64 @@ def jitter_params(rng, B, center, scale=1e-3):
     return P
 
 
+def wrap_params(P):
+    """Parameter sets brought back into the reference's ranges: phase, alpha and psi wrapped,
+    sin(delta) and cos(iota) reflected into [-1, 1], spins clipped to the prior's +-0.85, and
+    eta = (Mc/Mt)^(5/3) above 0.25 reflected about 0.25 at fixed (well-measured) chirp mass."""
+    P = np.array(P, dtype=np.float64)
+    for k, period in ((4, 2 * np.pi), (7, 2 * np.pi), (9, np.pi)):
+        P[:, k] = np.mod(P[:, k], period)
+    for k in (8, 10):
+        x = np.mod(P[:, k] + 1.0, 4.0)
+        P[:, k] = np.where(x > 2.0, 4.0 - x, x) - 1.0
+    P[:, 2:4] = np.clip(P[:, 2:4], -0.85, 0.85)
+    eta = np.exp((P[:, 0] - P[:, 1]) / 0.6)
+    over = eta > 0.25
+    P[over, 1] = P[over, 0] - 0.6 * np.log(np.clip(0.5 - eta[over], 0.05, 0.25 - 1e-12))
+    return P
+
+
+def fisher_steps(rng, B, fisher):
+    """B Gaussian steps with covariance F^-1 for the 11 x 11 Fisher matrix F (e.g. Fisher_Het,
+    QuickCBC.c:5446), drawn along F's eigenvectors as the reference sampler's eigen-jumps are
+    (update, QuickCBC.c:2268-2282); eigenvalues below 10 are raised to 10, as the reference's
+    FisherEvec does (QuickCBC.c:2510-2516)."""
+    F = np.asarray(fisher, dtype=np.float64)
+    lam, V = np.linalg.eigh(0.5 * (F + F.T))
+    return (rng.normal(size=(B, NP)) / np.sqrt(np.maximum(lam, 10.0))) @ V.T
+
+
+def cloud_at_drops(rng, center, fisher, drops, lnl, iters=40):
+    """Parameter sets about ``center`` whose lnL lies the given amounts below lnL(center): set b
+    is center + t_b s_b (wrapped), s_b a Fisher step (fisher_steps) and t_b > 0 found by bisection
+    on lnL(center) - lnL(center + t s_b) = drops[b].  ``lnl(P) -> [B]`` evaluates a batch (sets
+    it rejects at -1e20 count as infinitely far).  Chains at the posterior's width sit 0.5-10
+    below the peak, wider ones tens below, and burn-in points hundreds below.  A high-SNR
+    likelihood is far from quadratic beyond a fraction of a Fisher step, which is why the
+    distance along each step is searched rather than scaled."""
+    drops = np.asarray(drops, dtype=np.float64)
+    B = len(drops)
+    c = np.asarray(center, dtype=np.float64)
+    S = fisher_steps(rng, B, fisher)
+    L0 = float(lnl(c[None, :])[0])
+
+    def drop(t):
+        return L0 - np.asarray(lnl(wrap_params(c[None, :] + t[:, None] * S)), dtype=np.float64)
+
+    lo, hi = np.zeros(B), np.full(B, 1.0)
+    for _ in range(20):                       # grow hi until it passes the target
+        short = drop(hi) < drops
+        if not short.any():
+            break
+        hi[short] *= 2.0
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        below = drop(mid) < drops
+        lo = np.where(below, mid, lo)
+        hi = np.where(below, hi, mid)
+    return wrap_params(c[None, :] + (0.5 * (lo + hi))[:, None] * S)
+
+
 # --- the synthetic workloads (sizes from the reference's usage) -------------
 CONFIGS = {
     1: dict(labels=[0, 1], Tobs=4.0, fs=2048.0, fmin=16.0, m1=36.0, m2=29.0, chi1=0.3, chi2=-0.1,

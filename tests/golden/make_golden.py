@@ -6,7 +6,7 @@ The reference ships no golden vectors or known-answer tests, so these
 fixtures pin the CPU oracle and the CUDA kernels on machines where the
 reference tree is absent.  Regenerate with:
 
-    make -C oracle ref && python tests/golden/make_golden.py [wave cfg1 het1 grid3 secondary1]
+    make -C oracle ref && python tests/golden/make_golden.py [wave cfg1 het1 grid3 spread3 secondary1 ingest1]
 
 Contents (float64 unless noted):
   wave.npz     amp/phase of IMRPhenomDGenerateh22FDAmpPhase for 6 systems on a
@@ -16,6 +16,9 @@ Contents (float64 unless noted):
   het1.npz     reference heterodyne grid (het_space) and tables for config 1,
                reference het lnL at 16 nearby parameter sets
   grid3.npz    reference heterodyne grid for config 3 (3 det, 128 s, 4096 Hz)
+  spread3.npz  config 3 away from the peak: 48 sets about the injection whose lnL lies
+               0.5-10, 10-60 and 100-400 below it (posterior width to burn-in), with the
+               reference's heterodyned, full and exact (log_likelihood_test) lnL of each
   secondary1.npz  config 1: templates and log_likelihood_intrinsic on intrinsic-layout
                parameter sets, AmpPhase, and het_diff / Fisher_Het on the reference's
                heterodyne tables of het1.npz's grid
@@ -141,6 +144,41 @@ def make_grid3():
                         logLb=t["logLb"], params=P, lnl=L, inj=ev.inj, GMST=ev.GMST)
 
 
+def make_spread3():
+    """Config 3 away from the peak.  Reference heterodyne tables on grid3's grid about the
+    injection, the reference's Fisher_Het there, and 48 sets from synth.cloud_at_drops (Fisher
+    steps, distance along each searched on the reference's heterodyned lnL) at lnL drops drawn
+    from U[0.5, 10] (chains at the posterior's width), U[10, 60] and U[100, 400] (burn-in), 16
+    each.  For each set the reference's log_likelihood_het, log_likelihood_full and
+    log_likelihood_test (the heterodyned lnL evaluated exactly from differenced full templates,
+    QuickCBC.c:5621-5667)."""
+    g = np.load(os.path.join(OUT, "grid3.npz"))
+    ev = synth.config_event(3, ref_template_factory())
+    net = ref.RefNet(ev.labels, ev.Tobs, ev.GMST)
+    S = band_psd(ev)
+    het = ref.RefHet(net)
+    het.set_grid(g["fgrid"], int(g["MN"]), int(g["MM"]), int(g["J"]), ev.Tobs)
+    het.heterodyne(ev.D, ev.inj, ev.freq, S, ev.N, ev.Tobs)
+    F = het.fisher(ev.inj, ev.Tobs)
+    rng = np.random.default_rng(3700)
+    ranges = np.array([[0.5, 10.0], [10.0, 60.0], [100.0, 400.0]])
+    drops = np.concatenate([rng.uniform(lo, hi, 16) for lo, hi in ranges])
+    group = np.repeat(np.arange(len(ranges)), 16).astype(np.int32)
+    P = synth.cloud_at_drops(rng, ev.inj, F, drops, lambda X: het.lnl_batch(X, ev.Tobs)[0])
+    Lh, _ = het.lnl_batch(P, ev.Tobs)
+    Lf, _ = ref.lnl_full_batch(net, ev.D, P, ev.freq, S, ev.N, ev.Tobs)
+    Lt = np.array([het.lnl_test(ev.D, p, ev.freq, S, ev.N, ev.Tobs) for p in P])
+    L0, _ = ref.lnl_full_batch(net, ev.D, ev.inj[None, :], ev.freq, S, ev.N, ev.Tobs)
+    np.savez_compressed(os.path.join(OUT, "spread3.npz"), params=P, group=group, drop_ranges=ranges,
+                        target_drops=drops, fisher=F, lnl_het=Lh, lnl_full=Lf, lnl_exact=Lt,
+                        lnl_inj_full=float(L0[0]), inj=ev.inj, GMST=ev.GMST, logLb=het.export()["logLb"])
+    for k, (lo, hi) in enumerate(ranges):
+        m = group == k
+        print("spread3 drops %g-%g: full lnL %.2f..%.2f (injection %.2f), |het-full| max %.3g, "
+              "|het-exact| max %.3g" % (lo, hi, Lf[m].min(), Lf[m].max(), L0[0], np.abs(Lh[m] - Lf[m]).max(),
+                                        np.abs(Lh[m] - Lt[m]).max()))
+
+
 def intrinsic_equivalent(p, labels, GMST):
     """Intrinsic-layout parameters (QuickCBC.c:3570-3582) of the template that equals the full
     template of p (QuickCBC.c:3722-3760) in every detector: detector 0's response |F0|,
@@ -225,7 +263,7 @@ def make_ingest1():
 
 
 if __name__ == "__main__":
-    which = set(sys.argv[1:]) or {"wave", "cfg1", "het1", "grid3", "secondary1", "ingest1"}
+    which = set(sys.argv[1:]) or {"wave", "cfg1", "het1", "grid3", "spread3", "secondary1", "ingest1"}
     if "wave" in which:
         make_wave()
     if which & {"cfg1", "het1"}:
@@ -234,6 +272,8 @@ if __name__ == "__main__":
             make_het1(ev, net)
     if "grid3" in which:
         make_grid3()
+    if "spread3" in which:
+        make_spread3()
     if "secondary1" in which:
         make_secondary1()
     if "ingest1" in which:
