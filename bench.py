@@ -122,8 +122,8 @@ def capture_traffic(name, kernel, grid, block, kernel_ms):
     cap = ncu_capture(name)
     if cap is None:
         return None, {"traffic_source": f"no capture profiles/{name}.csv"}
-    same = kernel in cap["kernel"] and str(cap["grid"]).replace(" ", "") == grid and \
-        str(cap["block"]).replace(" ", "") == block
+    same = kernel in cap["kernel"] and (grid is None or str(cap["grid"]).replace(" ", "") == grid) and \
+        (block is None or str(cap["block"]).replace(" ", "") == block)
     info = {"traffic_source": cap["file"], "traffic_capture_launches": cap["launches"],
             "traffic_capture_matches_launch": bool(same)}
     if "duration_s" in cap:
@@ -295,24 +295,29 @@ def dropin_per_call_rates(q, ev, P, calls=96):
     fn = L.log_likelihood_full
     Pc = [np.ascontiguousarray(p) for p in P[:calls]]
 
-    def work(k0, n):
-        rho = np.zeros(4)
-        for j in range(n):
-            fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
-
     def rate(nthreads):
-        ts = [threading.Thread(target=work, args=(7 * t, 4)) for t in range(nthreads)]
+        # each thread warms up (its stream and staging buffers are made on its first call), then all
+        # start the timed calls together
+        go, done = threading.Barrier(nthreads + 1), threading.Barrier(nthreads + 1)
+
+        def work(k0):
+            rho = np.zeros(4)
+            for j in range(4):
+                fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+            go.wait()
+            for j in range(calls):
+                fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+            done.wait()
+        ts = [threading.Thread(target=work, args=(7 * t,)) for t in range(nthreads)]
         for t in ts:
             t.start()
-        for t in ts:
-            t.join()
-        ts = [threading.Thread(target=work, args=(7 * t, calls)) for t in range(nthreads)]
+        go.wait()
         t0 = time.perf_counter()
-        for t in ts:
-            t.start()
+        done.wait()
+        dt = time.perf_counter() - t0
         for t in ts:
             t.join()
-        return nthreads * calls / (time.perf_counter() - t0)
+        return nthreads * calls / dt
 
     out = {"unit": "lnL evals/s", "note": "FP64, log_likelihood_full reference signature, one set per call"}
     L.qcbc_unbind_all()
@@ -589,12 +594,13 @@ def interleaved_stream(q, b, evs, eo, P, Lm):
     for e, ev in enumerate(evs):
         bins = min(int(ev.Tobs * 1024.0), ev.N // 2) - int(ev.Tobs * ev.fmin)
         # useful bytes: FP32 (wr, wi, ws) per detector-bin and one FP32 bin factor per bin
-        nbytes += int(np.sum(eo == e)) * bins * (12 * len(ev.labels) + 4)
+        nbytes += int(np.sum(eo == e)) * bins * 12 * len(ev.labels)
     t = float(np.median(ms)) * 1e-3
     peak, kind = load_peaks()
     return {"value": len(P_i) / t, "unit": "lnL evals/s", "ms": t * 1e3, "stream_bytes": nbytes,
             "achieved_GBs": nbytes / t / 1e9, "frac_hbm": nbytes / t / 1e9 / peak, "peak_kind": kind,
-            "bytes_note": "12 B per detector-bin + 4 B per bin of every set (each set reads its event's band)",
+            "bytes_note": "12 B per detector-bin of every set (each set reads its event's band; the bin factor "
+                          "i^-7/6 is folded into the weighted data)",
             "same_lnl_as_grouped_order": bool(np.array_equal(L_i, Lm[order]))}
 
 
@@ -684,6 +690,31 @@ def run_profile(args):
     e.close()
 
 
+def run_profile_cfg4(args):
+    """Profiling run of the config-4 interleaved launch (the HBM-streaming case): the 256 events and
+    65536 sets in round-robin event order, `warmup` untimed launches, then `steps` launches."""
+    import quickcbc_b200 as q
+    from quickcbc_b200 import _lib, synth
+    _lib.check(_lib.lib().qcbc_init(0))
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    evs = [synth.make_event(tmpl, **sp) for sp in synth.uneven_event_specs(256)]
+    hs = [q.Event.from_synthetic(x) for x in evs]
+    b = q.Batch(hs)
+    eo, P = synth.uneven_params(evs)
+    order = np.lexsort((eo, np.arange(len(eo)) - np.searchsorted(eo, eo)))
+    b.autotune(eo, P, q.MIXED)
+    b.lnl(eo[order], P[order], q.MIXED)
+    b.time(len(P), q.MIXED, iters=args.warmup, flush_l2=True)
+    ms = b.time(len(P), q.MIXED, iters=args.steps, flush_l2=True)
+    print(json.dumps({"profile": "config4 interleaved mixed", "B": len(P), "ms": [float(x) for x in ms],
+                      "tiling": list(b.tiling())}))
+    b.close()
+    for h in hs:
+        h.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -703,6 +734,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--profile-cfg4", action="store_true",
+                    help="profiling run of the config-4 interleaved launch (for ncu)")
     ap.add_argument("--ref-het-space-child", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -712,6 +745,8 @@ def main():
         return run_reference_arm(args)
     if args.profile:
         return run_profile(args)
+    if args.profile_cfg4:
+        return run_profile_cfg4(args)
     if args.serve:
         import quickcbc_b200 as q
         from quickcbc_b200 import _lib
@@ -843,6 +878,16 @@ def main():
         out["config1_per_call"] = bench_cfg1_percall(q, eng, _lib)
         out["config3"] = bench_cfg3_het(q)
         out["config4_uneven"] = bench_cfg4_uneven(q)
+        # the HBM-streaming case: the config-4 launch with the sets interleaved across all 256 events
+        st = out["config4_uneven"]["mixed_interleaved"]
+        tr, ti = capture_traffic("k_lnl_multi_cfg4", "k_lnl_multi", None, None, st["ms"])
+        out["roofline_stream"] = {
+            "bound": "hbm", "achieved": st["achieved_GBs"], "peak": hbm_peak, "unit": "GB/s",
+            "frac": st["frac_hbm"], "traffic": tr, "peak_kind": peak_kind, "kernel": "k_lnl_multi (mixed)",
+            "kernel_ms": st["ms"], "bytes_per_launch": st["stream_bytes"], **ti,
+            "note": "config 4, 65536 sets interleaved across 256 events (1-3 detectors): useful bytes = "
+                    "12 B (FP32 wr, wi, ws) per detector-bin of every set's band; the waveform's bin factor "
+                    "is folded into those values, so no per-bin table is streamed"}
         out["input_stage"] = bench_input_stage(q)
         # config 5 as specified (32 runs of 16 x 8 chains x 20000 steps, Poisson 2/s): mixed against
         # plain FP64, heterodyned and full likelihood, chains stepped on the device

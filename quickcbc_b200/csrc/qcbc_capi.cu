@@ -64,7 +64,8 @@ struct DeviceState {
   int* d_bucket = nullptr;   // QNM interval index per 0.001 of final spin
 };
 static std::mutex g_mu;
-static DeviceState g_dev[16];
+constexpr int kMaxDevices = 16;        // devices the library keeps state for (device ids 0..15)
+static DeviceState g_dev[kMaxDevices];
 static std::vector<double> g_qnm_host[3];   // a, fring, fdamp
 
 static void natural_spline_m2(const std::vector<double>& x, const std::vector<double>& y, std::vector<double>& M) {
@@ -154,7 +155,7 @@ static int current_device() {
 }
 
 extern "C" int qcbc_init(int device) {
-  if (device < 0 || device >= 16) return fail(QCBC_EINVAL, "device %d out of range", device);
+  if (device < 0 || device >= kMaxDevices) return fail(QCBC_EINVAL, "device %d out of range 0..%d", device, kMaxDevices - 1);
   int ndev = 0;
   cudaError_t e = cudaGetDeviceCount(&ndev);
   if (e != cudaSuccess || ndev == 0)
@@ -175,8 +176,11 @@ extern "C" int qcbc_init(int device) {
   return QCBC_OK;
 }
 
+// Every entry point calls this (directly or through workspace()) before it indexes per-device
+// state with the current device, so the index is checked here.
 static int ensure_init() {
   int d = current_device();
+  if (d < 0 || d >= kMaxDevices) return fail(QCBC_EINVAL, "current device %d out of range 0..%d", d, kMaxDevices - 1);
   if (g_dev[d].ready) return QCBC_OK;
   return qcbc_init(d);
 }
@@ -2139,7 +2143,7 @@ static_assert(kNaBytes == QCBC_NOALLOC_SCRATCH_BYTES, "header size constant out 
 // Device address of g_noalloc_scratch per device.  In host code the array's name
 // only stands in for the symbol; the address comes from cudaGetSymbolAddress,
 // taken once per device with that device current.
-static void* g_noalloc_addr[16] = {nullptr};
+static void* g_noalloc_addr[kMaxDevices] = {nullptr};
 static std::mutex g_noalloc_mu;
 
 extern "C" int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
@@ -2153,6 +2157,7 @@ extern "C" int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int
                 QCBC_NOALLOC_MAX_SETS);
   int dev = 0;
   CU(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(QCBC_EINVAL, "current device %d out of range", dev);
   if (dev != ev->device)
     return fail(QCBC_EINVAL, "event lives on device %d but device %d is current", ev->device, dev);
   if (!g_dev[dev].ready) return fail(QCBC_EINVAL, "device %d not initialised (open an event first)", dev);
