@@ -690,6 +690,32 @@ def run_profile(args):
     e.close()
 
 
+def run_profile_cfg3(args):
+    """Profiling run of the config-3 heterodyned step (k_setup then k_lnl_het) on 4096 sets spread
+    as in the bench: grid and tables built on the GPU, `warmup` untimed steps, then `steps`."""
+    import quickcbc_b200 as q
+    from quickcbc_b200 import _lib, synth
+    _lib.check(_lib.lib().qcbc_init(0))
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    g3 = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
+    ev = synth.config_event(3, tmpl)
+    e = q.Event.from_synthetic(ev)
+    e.het_setup(ev.inj, g3["fgrid"], int(g3["MN"]), int(g3["MM"]), int(g3["J"]))
+    rng = np.random.default_rng(3000 + 500000)
+    F = e.het_fisher(ev.inj[None, :])[0]
+    drops = np.concatenate([rng.uniform(0.5, 10.0, 2048), rng.uniform(10.0, 60.0, 1024), rng.uniform(100.0, 400.0, 1024)])
+    P = synth.cloud_at_drops(rng, ev.inj, F, drops, lambda X: e.lnl_het(X, q.FP64, allow_invalid=True))
+    d = q.DeviceBuffer(P.nbytes)
+    d.upload(P)
+    prec = q.MIXED if args.prec == "mixed" else q.FP64
+    q.time_lnl_het(e, d, len(P), prec, args.warmup, flush_l2=True)
+    ms = q.time_lnl_het(e, d, len(P), prec, args.steps, flush_l2=True)
+    print(json.dumps({"profile": "config3 heterodyned " + args.prec, "B": len(P), "ms": [float(x) for x in ms]}))
+    e.close()
+
+
 def run_profile_cfg4(args):
     """Profiling run of the config-4 interleaved launch (the HBM-streaming case): the 256 events and
     65536 sets in round-robin event order, `warmup` untimed launches, then `steps` launches."""
@@ -704,7 +730,7 @@ def run_profile_cfg4(args):
     b = q.Batch(hs)
     eo, P = synth.uneven_params(evs)
     order = np.lexsort((eo, np.arange(len(eo)) - np.searchsorted(eo, eo)))
-    b.autotune(eo, P, q.MIXED)
+    b.set_tiling(8192, 256)     # fixed, so that the launch count before the captured one is known
     b.lnl(eo[order], P[order], q.MIXED)
     b.time(len(P), q.MIXED, iters=args.warmup, flush_l2=True)
     ms = b.time(len(P), q.MIXED, iters=args.steps, flush_l2=True)
@@ -734,6 +760,8 @@ def main():
     ap.add_argument("--profile", action="store_true",
                     help="profiling run: warm-up and timed steps of one precision only (for ncu)")
     ap.add_argument("--prec", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--profile-cfg3", action="store_true",
+                    help="profiling run of the config-3 heterodyned step (for ncu)")
     ap.add_argument("--profile-cfg4", action="store_true",
                     help="profiling run of the config-4 interleaved launch (for ncu)")
     ap.add_argument("--ref-het-space-child", action="store_true", help=argparse.SUPPRESS)
@@ -745,6 +773,8 @@ def main():
         return run_reference_arm(args)
     if args.profile:
         return run_profile(args)
+    if args.profile_cfg3:
+        return run_profile_cfg3(args)
     if args.profile_cfg4:
         return run_profile_cfg4(args)
     if args.serve:

@@ -196,7 +196,7 @@ int qcbc_het_fisher(qcbc_event* ev, const double* params, int B, double* fish);
  *    two with NULL gets a different ordering against its other work. */
 #define QCBC_NOALLOC_MAX_SETS 4096
 #define QCBC_NOALLOC_MAX_TILE_SLOTS 16384
-#define QCBC_NOALLOC_SCRATCH_BYTES 4669440
+#define QCBC_NOALLOC_SCRATCH_BYTES 4734976
 int qcbc_lnl_full_noalloc(qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
                           int precision, void* stream);
 

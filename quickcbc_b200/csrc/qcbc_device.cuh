@@ -61,13 +61,15 @@ constexpr int kRecValid = 1;
 //   with m, hx1 and fRD as float pairs.
 //   iA, iF, iP, iM: first bins of the intermediate amplitude, ringdown amplitude, intermediate
 //   phase and ringdown phase (Msec f_i compared with 0.014, fmax, 0.018, fRD/2 in FP64).
-struct MixPhIns { double A0, At, Att, AtL, AL, Au, Auu, Au3, Au5, Ai, Ait, Aitt, Aii; };
-struct MixPhInt { double B0, Bi, Bu9, BL; };
-struct MixPhMrd { double R0, Ri; float Ru3[2], Rs[2], Rat[2], D1[2], D0[2]; };
-struct MixAmpIns { float al[8]; };
-struct MixAmpInt { float m[2], hx1[2]; float hc[5], h21, h31; };
-struct MixAmpMrd { float m[2], fRD[2]; float g2_over_fg, fg_g1, fg2; };
-struct MixPoly {
+//   Each piece's coefficients are 16-byte aligned and ordered as the kernel uses them, so that a
+//   bin reads them with 128-bit shared-memory loads: pairs of doubles, quadruples of floats.
+struct alignas(16) MixPhIns { double A0, At, Att, AtL, AL, Au, Auu, Au3, Au5, Ai, Ait, Aitt, Aii, pad; };
+struct alignas(16) MixPhInt { double B0, Bi, Bu9, BL; };
+struct alignas(16) MixPhMrd { double R0, Ri; float Ru3[2], Rs[2], Rat[2], D1[2], D0[2], pad[2]; };
+struct alignas(16) MixAmpIns { float al[8]; };
+struct alignas(16) MixAmpInt { float m[2], hx1[2]; float hc[5], h21, h31, pad; };
+struct alignas(16) MixAmpMrd { float m[2], fRD[2]; float g2_over_fg, fg_g1, fg2, pad; };
+struct alignas(16) MixPoly {
   MixPhIns pins;
   MixPhInt pint;
   MixPhMrd pmrd;
@@ -75,7 +77,6 @@ struct MixPoly {
   MixAmpInt aint;
   MixAmpMrd amrd;
   int iA, iF, iP, iM;
-  int pad[2];
 };
 
 struct PhdRec {

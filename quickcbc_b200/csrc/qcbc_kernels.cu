@@ -1014,73 +1014,69 @@ __device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, con
 // ---- mixed-precision tile body (coefficients: MixPoly in the record)
 
 // The piece coefficients of a parameter set stay in shared memory (the block's record) and are
-// re-read at every use: asm volatile keeps each load in the bin loop, so the coefficients pin no
-// registers and three blocks of 256 threads fit an SM (80 registers per thread).
-__device__ __forceinline__ double sld(const double& x) {
-  double v;
-  asm volatile("ld.shared.f64 %0, [%1];" : "=d"(v) : "r"((uint32_t)__cvta_generic_to_shared(&x)));
+// re-read at every use, 128 bits at a time: asm volatile keeps each load in the bin loop, so the
+// coefficients pin no registers and three blocks of 256 threads fit an SM (80 registers per
+// thread).  Every address is 16-byte aligned (the MixPoly pieces are).
+__device__ __forceinline__ double2 sld2(const double* x) {
+  double2 v;
+  asm volatile("ld.shared.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"((uint32_t)__cvta_generic_to_shared(x)));
   return v;
 }
-__device__ __forceinline__ float sld(const float& x) {
-  float v;
-  asm volatile("ld.shared.f32 %0, [%1];" : "=f"(v) : "r"((uint32_t)__cvta_generic_to_shared(&x)));
+__device__ __forceinline__ float4 sld4(const float* x) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+               : "r"((uint32_t)__cvta_generic_to_shared(x)));
   return v;
 }
 
 // the three phase pieces in cycles (FP64) and the three amplitude pieces (FP32) at bin xi
 __device__ __forceinline__ double mph_ins(const MixPhIns& q, double xi, double t, double u, double L) {
-  double ph = fma(t, fma(t, sld(q.Att), sld(q.At)), sld(q.A0));
-  ph = fma(L, fma(t, sld(q.AtL), sld(q.AL)), ph);
-  double pu = fma(u * u, sld(q.Au5), sld(q.Au3));
-  pu = fma(u, pu, sld(q.Auu));
-  pu = fma(u, pu, sld(q.Au));
+  const double2 c0 = sld2(&q.A0), c1 = sld2(&q.Att), c2 = sld2(&q.AL), c3 = sld2(&q.Auu), c4 = sld2(&q.Au5),
+                c5 = sld2(&q.Ait), c6 = sld2(&q.Aii);
+  // c0 = (A0, At), c1 = (Att, AtL), c2 = (AL, Au), c3 = (Auu, Au3), c4 = (Au5, Ai), c5 = (Ait, Aitt), c6 = (Aii, -)
+  double ph = fma(t, fma(t, c1.x, c0.y), c0.x);
+  ph = fma(L, fma(t, c1.y, c2.x), ph);
+  double pu = fma(u * u, c4.x, c3.y);
+  pu = fma(u, pu, c3.x);
+  pu = fma(u, pu, c2.y);
   ph = fma(u, pu, ph);
-  double pi = fma(xi, sld(q.Aii), fma(t, fma(t, sld(q.Aitt), sld(q.Ait)), sld(q.Ai)));
+  const double pi = fma(xi, c6.x, fma(t, fma(t, c5.y, c5.x), c4.y));
   return fma(xi, pi, ph);
 }
 __device__ __forceinline__ double mph_int(const MixPhInt& q, double xi, double u, double L) {
-  double u3 = u * u * u;
-  return fma(xi, sld(q.Bi), sld(q.B0)) + fma(L, sld(q.BL), (u3 * u3 * u3) * sld(q.Bu9));
+  const double2 c0 = sld2(&q.B0), c1 = sld2(&q.Bu9);     // (B0, Bi), (Bu9, BL)
+  const double u3 = u * u * u;
+  return fma(xi, c0.y, c0.x) + fma(L, c1.y, (u3 * u3 * u3) * c1.x);
 }
-// How a piece's coefficients are read: from the block's record in shared memory at each use
-// (SmemRead, pins no registers), or from a copy the run keeps in registers (RegRead).
-struct SmemRead {
-  template <class T> static __device__ __forceinline__ T get(const T& x) { return sld(x); }
-};
-struct RegRead {
-  template <class T> static __device__ __forceinline__ T get(const T& x) { return x; }
-};
-
 // the ringdown rest in FP32 (cycles, a few at most): Ru3 / i + Rs s + Rat atan(i D1 - D0) with
 // tc = (1/i, s = i^{3/4}); each coefficient is a float pair applied hi after lo
-template <class R = SmemRead>
 __device__ __forceinline__ float mph_mrd(const MixPhMrd& q, float xf, float2 tc) {
-  const float z = fmaf(xf, R::get(q.D1[0]), fmaf(xf, R::get(q.D1[1]), -R::get(q.D0[0]))) - R::get(q.D0[1]);
+  const float4 a = sld4(q.Ru3), b = sld4(q.Rat), d = sld4(q.D0);   // (Ru3, Rs), (Rat, D1), (D0, -)
+  const float z = fmaf(xf, b.z, fmaf(xf, b.w, -d.x)) - d.y;
   const float at = atanf(z);
-  float ph = fmaf(at, R::get(q.Rat[0]), at * R::get(q.Rat[1]));
-  ph = fmaf(tc.y, R::get(q.Rs[0]), fmaf(tc.y, R::get(q.Rs[1]), ph));
-  return fmaf(tc.x, R::get(q.Ru3[0]), fmaf(tc.x, R::get(q.Ru3[1]), ph));
+  float ph = fmaf(at, b.x, at * b.y);
+  ph = fmaf(tc.y, a.z, fmaf(tc.y, a.w, ph));
+  return fmaf(tc.x, a.x, fmaf(tc.x, a.y, ph));
 }
 // x minus the nearest integer, for |x| < 2^22, in FP32 adds
 __device__ __forceinline__ float frac_cyc(float x) {
   return __fsub_rn(x, __fsub_rn(__fadd_rn(x, 12582912.0f), 12582912.0f));
 }
 __device__ __forceinline__ float mamp_ins(const MixAmpIns& a, float xf, float tf) {
-  const float* al = a.al;
-  float inner = fmaf(xf, sld(al[7]), fmaf(tf, fmaf(tf, sld(al[6]), sld(al[5])), sld(al[4])));
-  float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, sld(al[3]), sld(al[2])), sld(al[1])));
-  return fmaf(xf, mid, fmaf(tf * tf, sld(al[0]), 1.0f));
+  const float4 l = sld4(a.al), h = sld4(a.al + 4);
+  const float inner = fmaf(xf, h.w, fmaf(tf, fmaf(tf, h.z, h.y), h.x));
+  const float mid = fmaf(xf, inner, fmaf(tf, fmaf(tf, l.w, l.z), l.y));
+  return fmaf(xf, mid, fmaf(tf * tf, l.x, 1.0f));
 }
 __device__ __forceinline__ float mamp_int(const MixAmpInt& a, float xf) {
-  const float x = fmaf(xf, sld(a.m[0]), fmaf(xf, sld(a.m[1]), -sld(a.hx1[0]))) - sld(a.hx1[1]);
-  return sld(a.hc[0]) +
-         x * (sld(a.hc[1]) +
-              x * (sld(a.hc[2]) + (x - sld(a.h21)) * (sld(a.hc[3]) + (x - sld(a.h31)) * sld(a.hc[4]))));
+  const float4 s = sld4(a.m), c = sld4(a.hc), e = sld4(a.hc + 4);   // (m, hx1), hc[0..3], (hc[4], h21, h31, -)
+  const float x = fmaf(xf, s.x, fmaf(xf, s.y, -s.z)) - s.w;
+  return c.x + x * (c.y + x * (c.z + (x - e.y) * (c.w + (x - e.z) * e.x)));
 }
-template <class R = SmemRead>
 __device__ __forceinline__ float mamp_mrd(const MixAmpMrd& a, float xf) {
-  const float dfr = fmaf(xf, R::get(a.m[0]), fmaf(xf, R::get(a.m[1]), -R::get(a.fRD[0]))) - R::get(a.fRD[1]);
-  return __fdividef(__expf(-dfr * R::get(a.g2_over_fg)) * R::get(a.fg_g1), dfr * dfr + R::get(a.fg2));
+  const float4 s = sld4(a.m), g = sld4(&a.g2_over_fg);   // (m, fRD), (g2/fg, fg g1, fg^2, -)
+  const float dfr = fmaf(xf, s.x, fmaf(xf, s.y, -s.z)) - s.w;
+  return __fdividef(__expf(-dfr * g.x) * g.y, dfr * dfr + g.z);
 }
 
 // piece of bin i: 0 inspiral, 1 intermediate, 2 merger-ringdown
@@ -1144,8 +1140,7 @@ struct MixAcc {
 };
 
 // Rows [k, k_end) of the thread's bins i = i0 + tid + k bs, all in amplitude piece AP and
-// phase piece PP (-1: decided per bin).  The merger-ringdown pieces (most bins of heavy systems)
-// keep their coefficients in registers for the run; the others read theirs from the block's
+// phase piece PP (-1: decided per bin).  The pieces' coefficients are read from the block's
 // record in shared memory at each use.
 template <int NIFO, int AP, int PP>
 __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot, int nk,
@@ -1169,10 +1164,6 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
   // tables a row needs: tabA for the inspiral amplitude and the FP64 phase pieces, tabB for the
   // FP64 phase pieces, tabC for the ringdown phase
   constexpr bool kTabA = AP <= 0 || PP != 2, kTabB = PP != 2, kTabC = PP == 2 || PP < 0;
-  MixPhMrd qm_r;                    // register copies of the ringdown coefficients
-  MixAmpMrd am_r;
-  if (PP == 2) qm_r = qm;
-  if (AP == 2) am_r = am;
   for (int r = 0; r < n; r += 8) {
     const int m = min(8, n - r);
     MixAcc<NIFO> A;
@@ -1188,7 +1179,7 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       w.load(ev.wm, nh, b);
       float cyc, a;
       if (PP == 2) {
-        cyc = frac_cyc(mph_mrd<RegRead>(qm_r, xf, tC));
+        cyc = frac_cyc(mph_mrd(qm, xf, tC));
       } else if (PP >= 0) {
         const double ph = PP == 0 ? mph_ins(qi, xi, tA.x, tA.y, tB.x) : mph_int(qn, xi, tA.y, tB.x);
         cyc = (float)(ph - rint(ph));
@@ -1203,7 +1194,7 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       }
       if (AP == 0) a = mamp_ins(ai, xf, (float)tA.x);
       else if (AP == 1) a = mamp_int(an, xf);
-      else if (AP == 2) a = mamp_mrd<RegRead>(am_r, xf);
+      else if (AP == 2) a = mamp_mrd(am, xf);
       else {
         const int ap = amp_piece(P, b);
         a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x)
