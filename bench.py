@@ -106,7 +106,8 @@ def ncu_capture(name):
     def num(r, k):
         v = float(r[k].replace(",", ""))
         u = (units or {}).get(k, "").strip().lower()
-        return v * {"kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9, "usecond": 1e-6, "msecond": 1e-3, "nsecond": 1e-9}.get(u, 1.0)
+        return v * {"kbyte": 1e3, "mbyte": 1e6, "gbyte": 1e9, "us": 1e-6, "usecond": 1e-6, "ms": 1e-3,
+                    "msecond": 1e-3, "ns": 1e-9, "nsecond": 1e-9}.get(u, 1.0)
     rd = [num(r, "dram__bytes_read.sum") for r in rows]
     wr = [num(r, "dram__bytes_write.sum") for r in rows]
     out = {"kernel": rows[0]["Kernel Name"], "grid": rows[0].get("Grid Size"), "block": rows[0].get("Block Size"),
