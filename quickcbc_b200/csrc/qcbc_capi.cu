@@ -138,9 +138,8 @@ static int ensure_bin_tables(DeviceState& ds, int n) {
   launch_fill_bin_tables(a, b, c, want, 0);
   tls_launches += 1;
   CU(cudaDeviceSynchronize());
-  cudaFree(ds.d_tabA);
-  cudaFree(ds.d_tabB);
-  cudaFree(ds.d_tabC);
+  // The smaller tables stay allocated: batches copy the table pointers into their device event
+  // descriptors when a slot is set, and they must keep pointing at valid tables.
   ds.d_tabA = a;
   ds.d_tabB = b;
   ds.d_tabC = c;
@@ -341,6 +340,10 @@ static HetData het_data(const qcbc_event* ev) {
   d.aa = p; p += (size_t)nI * h.NR;
   d.rc = p; p += (size_t)nI * h.NR;
   d.rs = p;
+  const DeviceState& ds = g_dev[ev->device];
+  d.tabA = ds.d_tabA;
+  d.tabB = ds.d_tabB;
+  d.tabC = ds.d_tabC;
   return d;
 }
 

@@ -235,55 +235,6 @@ __device__ __forceinline__ void phd_eval64(const PhdRec& c, double Mf, double& a
   phase = ph - (c.t0 * (Mf - c.MfRef) + c.phi_pre);
 }
 
-// Mixed precision: phase in FP64 (its magnitude reaches 1e4-1e6 rad), the
-// amplitude in FP32.  Mf^{-1/3} comes from an FP32 seed refined by two FP64
-// Newton steps r <- r (4 - x r^3)/3 (quadratic convergence: 1e-7 -> 1e-14 -> 1e-16).
-__device__ __forceinline__ void phd_eval_mixed(const PhdRec& c, double Mf, float& amp, double& phase) {
-  float mff = (float)Mf;
-  double r = (double)(1.0f / cbrtf(mff));
-  r = r * (4.0 - Mf * r * r * r) * (1.0 / 3.0);
-  r = r * (4.0 - Mf * r * r * r) * (1.0 / 3.0);
-  double r2 = r * r;                       // Mf^{-2/3}
-  double third = Mf * r2;                  // Mf^{1/3}
-  // amplitude, FP32
-  float rf = (float)r, thf = (float)third;
-  float sixth_inv = sqrtf(rf);             // Mf^{-1/6}
-  float pre = (float)c.a0 * rf * rf * rf * sixth_inv;   // a0 Mf^{-7/6}
-  float a;
-  if (Mf < kAmpJoin) {
-    float t2 = thf * thf, m = mff;
-    float p43 = m * thf, p53 = p43 * thf, p2 = m * m, p73 = thf * p2, p83 = t2 * p2;
-    a = 1.0f + t2 * (float)c.ai[0] + m * (float)c.ai[1] + p43 * (float)c.ai[2] + p53 * (float)c.ai[3] +
-        p2 * (float)c.ai[4] + p73 * (float)c.ai[5] + p83 * (float)c.ai[6] + m * p2 * (float)c.ai[7];
-  } else if (Mf >= c.fmax) {
-    float fg = (float)(c.fDM * c.g3), df = (float)(Mf - c.fRD);
-    a = __expf(-df * (float)c.g2 / fg) * (fg * (float)c.g1) / (df * df + fg * fg);
-  } else {
-    float x = (float)(Mf - c.hx1), x2 = (float)(Mf - c.hx2), x3 = (float)(Mf - c.hx3);
-    a = (float)c.hc[0] + x * ((float)c.hc[1] + x * ((float)c.hc[2] + x2 * ((float)c.hc[3] + x3 * (float)c.hc[4])));
-  }
-  amp = pre * a;
-  // phase, FP64
-  double ph;
-  if (Mf < kPhiJoin) {
-    const double* q = c.pq;
-    double logv = log(third * c.pi_third);
-    double r3 = r2 * r, r5 = r3 * r2;
-    ph = q[0] + q[1] * (third * third) + q[2] * third + q[3] * logv * third + q[4] * logv + q[5] * r + q[6] * r2 +
-         q[7] * r3 + q[8] * r5;
-    double p43 = Mf * third, p53 = p43 * third;
-    ph += (q[9] * Mf + q[10] * p43 + q[11] * p53 + q[12] * Mf * Mf) * c.inv_eta;
-  } else if (Mf >= c.fMRDJoin) {
-    double sq = sqrt(Mf), f34 = sqrt(Mf * sq);
-    double at = (double)atanf((float)((Mf - c.al5 * c.fRD) / c.fDM));
-    ph = (-(c.al2 / Mf) + (4.0 / 3.0) * (c.al3 * f34) + c.al1 * Mf + c.al4 * at) * c.inv_eta + c.C1MRD + c.C2MRD * Mf;
-  } else {
-    // b3/(3 Mf^3) with r^9 = Mf^{-3}; the beta2 log term reaches ~1e2 rad, so FP64 log
-    ph = (c.b1 * Mf - c.b3 * (1.0 / 3.0) * r2 * r2 * r2 * r2 * r + c.b2 * log(Mf)) * c.inv_eta + c.C1Int + c.C2Int * Mf;
-  }
-  phase = ph - (c.t0 * (Mf - c.MfRef) + c.phi_pre);
-}
-
 // Reduce x to [-pi, pi] in FP64 with a two-constant 2 pi (|x| < 1e9 keeps it exact to ~1e-15).
 __device__ __forceinline__ double reduce_2pi(double x) {
   constexpr double kInv2Pi = 0.15915494309189533577;

@@ -1764,6 +1764,30 @@ constexpr int kRecDoubles = (int)(sizeof(PhdRec) / 8);
 // doubles of shared memory one set's warp uses (a multiple of 2, so the next record stays 16-B aligned)
 __host__ __device__ inline int het_warp_doubles(int nifo, int M) { return kRecDoubles + (3 * nifo * M + 1) / 2 * 2; }
 
+// The mixed-precision waveform at bin i of the event (a heterodyne grid point, f = i/Tobs) from
+// the folded polynomials of the mixed full-likelihood kernel (MixPoly) and the per-bin tables:
+// phc = phase / 2 pi = R0 + i Ri + the piece's rest (FP64 for the inspiral and intermediate
+// rests, FP32 for the ringdown's few cycles), amp = a0 Mf^{-7/6} A(Mf) in FP32 (the piece's
+// amplitude times a0 (Msec df)^{-7/6} i^{-7/6}).  No log, cube root or FP64 division per point.
+// The record must be in shared memory (its coefficients are read with shared loads).
+__device__ __forceinline__ void mixed_point(const PhdRec& c, const HetData& h, int i, float& amp, double& phc) {
+  const MixPoly& P = c.mix;
+  const double2 tA = __ldg(h.tabA + i), tB = __ldg(h.tabB + i);
+  const float2 tC = __ldg(h.tabC + i);
+  const double xi = (double)i;
+  const float xf = (float)i;
+  const int pp = ph_piece(P, i), ap = amp_piece(P, i);
+  double rest;
+  if (pp == 0) rest = mph_ins(P.pins, xi, tA.x, tA.y, tB.x);
+  else if (pp == 1) rest = mph_int(P.pint, xi, tA.y, tB.x);
+  else rest = (double)mph_mrd(P.pmrd, xf, tC);
+  const double2 r = sld2(&P.pmrd.R0);                          // (R0, Ri)
+  phc = fma(xi, r.y, r.x) + rest;
+  const float a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x) : (ap == 1 ? mamp_int(P.aint, xf) : mamp_mrd(P.amrd, xf));
+  const float u = (float)tA.y;                                // i^{-1/3}
+  amp = a * (u * u * u) * sqrtf(u) * (float)(c.a0 * c.mdf_m76);
+}
+
 template <int PREC>
 __device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm,
                                          double* out) {
@@ -1794,9 +1818,8 @@ __device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, cons
       }
     } else {
       float amp = 0.f;
-      double ph = 0.0;
-      if (!(f > c.fCut)) phd_eval_mixed(c, c.Msec * f, amp, ph);
-      double phc = ph * kInv2Pi;
+      double phc = 0.0;
+      if (!(f > c.fCut)) mixed_point(c, h, (int)rint(f * g.Tobs), amp, phc);
       for (int id = 0; id < nifo; id++) {
         double aref = __ldg(h.amp + id * M + j), pref = __ldg(h.phase + id * M + j);
         float ratio = amp * (float)(c.Fs[id] * kH22fac * c.amp_scale / c.sqT * y / aref);

@@ -47,6 +47,11 @@ struct HetData {
   int M, J, NR, MN, MM;
   double logLb;
   const double *freq, *amp, *phase, *IP, *SL, *lc, *ls, *aa, *rc, *rs;
+  // the device's per-bin tables (EventData::tabA/B/C): the mixed form evaluates the waveform at
+  // the grid's bins with the folded polynomials of the mixed full-likelihood kernel
+  const double2* tabA;
+  const double2* tabB;
+  const float2* tabC;
 };
 
 enum Precision { kFP64 = 0, kMixed = 1 };
