@@ -282,54 +282,66 @@ def bench_cfg1_percall(q, eng, _lib):
             "value": steps * 16 / dt, "unit": "lnL evals/s", "us_per_call": 1e6 * dt / (steps * 16)}
 
 
-def dropin_per_call_rates(q, ev, P, calls=96):
+def _native_rate(which, net, het, D, rv, SN, N, Tobs, P, calls, nthreads):
+    """Reference-signature calls per second from `nthreads` native host threads started together
+    (qcbc_time_dropin: C++ threads, no interpreter between calls)."""
+    import ctypes as C
+    from quickcbc_b200 import _lib, engine as eng
+    Pc = np.ascontiguousarray(P, dtype=np.float64)
+    secs, last = C.c_double(0.0), np.zeros(nthreads)
+    _lib.check(_lib.lib().qcbc_time_dropin(which, net, het, D, rv, SN, N, Tobs, eng._ptr(Pc), len(Pc), calls,
+                                           nthreads, C.byref(secs), eng._ptr(last)))
+    return {"value": nthreads * calls / secs.value, "us_per_call_per_thread": secs.value / calls * 1e6}
+
+
+def dropin_per_call_rates(q, ev, P, calls=400):
     """log_likelihood_full under the reference's signature, one parameter set per call, from one host
-    thread and from 12 at once (ctypes releases the GIL during the call), with the data registered
-    by qcbc_bind_data and without (the unchanged program's path: each call checks that the cached
-    device copy still holds the caller's D and SN)."""
+    thread and from 12 at once (the reference's NC = 12 OpenMP chains, QuickCBC.c:118, 2063-2067;
+    native threads), with the data registered by qcbc_bind_data and without (the unchanged
+    program's path: each call checks that the cached device copy still holds the caller's D and
+    SN).  Concurrent calls on one event are merged into shared launches."""
     import ctypes as C
     from quickcbc_b200 import _lib, engine as eng
     L = _lib.lib()
     nh = eng._NetHolder(ev.labels, ev.Tobs, ev.GMST)
-    Dr, Sr = eng._rows(ev.D), eng._rows(ev.SN)
+    D, SN = eng._f64(ev.D), eng._f64(ev.SN)
+    Dr, Sr = eng._rows(D), eng._rows(SN)
     fr, rv = eng._rv(ev.freq)
-    fn = L.log_likelihood_full
-    Pc = [np.ascontiguousarray(p) for p in P[:calls]]
+    Pc = np.ascontiguousarray(P[:96])
 
     def rate(nthreads):
-        # each thread warms up (its stream and staging buffers are made on its first call), then all
-        # start the timed calls together
-        go, done = threading.Barrier(nthreads + 1), threading.Barrier(nthreads + 1)
+        return _native_rate(0, nh.ref, None, Dr, C.byref(rv), Sr, ev.N, ev.Tobs, Pc, calls, nthreads)
 
-        def work(k0):
-            rho = np.zeros(4)
-            for j in range(4):
-                fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
-            go.wait()
-            for j in range(calls):
-                fn(nh.ref, Dr, eng._ptr(Pc[(k0 + j) % len(Pc)]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
-            done.wait()
-        ts = [threading.Thread(target=work, args=(7 * t,)) for t in range(nthreads)]
-        for t in ts:
-            t.start()
-        go.wait()
-        t0 = time.perf_counter()
-        done.wait()
-        dt = time.perf_counter() - t0
-        for t in ts:
-            t.join()
-        return nthreads * calls / dt
-
-    out = {"unit": "lnL evals/s", "note": "FP64, log_likelihood_full reference signature, one set per call"}
+    out = {"unit": "lnL evals/s", "note": "FP64, log_likelihood_full reference signature, one set per call, "
+                                          "native host threads"}
     L.qcbc_unbind_all()
-    out["one_thread_unbound"] = {"value": rate(1)}
-    out["12_threads_unbound"] = {"value": rate(12)}
+    out["one_thread_unbound"] = rate(1)
+    out["12_threads_unbound"] = rate(12)
     _lib.check(L.qcbc_bind_data(nh.ref, Dr, Sr, ev.N, ev.Tobs))
-    out["one_thread_bound"] = {"value": rate(1)}
-    out["12_threads_bound"] = {"value": rate(12)}
+    out["one_thread_bound"] = rate(1)
+    out["12_threads_bound"] = rate(12)
     L.qcbc_unbind_all()
     out["value"] = out["one_thread_bound"]["value"]
     return out
+
+
+def dropin_het_per_call_rates(q, ev, het_grid, P, calls=1000):
+    """log_likelihood_het under the reference's signature (its sampler's hot call, QuickCBC.c:2372),
+    one set per call, from one native host thread and from 12 at once: the rate an unchanged
+    QuickCBC linked against the library sees.  The tables come from the drop-in heterodyne on the
+    same grid."""
+    import ctypes as C
+    from quickcbc_b200 import engine as eng
+    H = eng.LegacyHet(ev.labels, ev.GMST, ev.Tobs, het_grid["fgrid"], int(het_grid["MN"]), int(het_grid["MM"]),
+                      int(het_grid["J"]))
+    H.heterodyne(ev.D, ev.inj, ev.freq, ev.SN, ev.N)
+    Pc = np.ascontiguousarray(P[:200])
+
+    def rate(nthreads):
+        return _native_rate(1, H.nh.ref, C.byref(H.het), None, None, None, ev.N, ev.Tobs, Pc, calls, nthreads)
+
+    return {"unit": "lnL evals/s", "note": "FP64, log_likelihood_het reference signature, one set per call, "
+                                          "native host threads", "one_thread": rate(1), "12_threads": rate(12)}
 
 
 def cpu_baseline_het(ev, het_grid, P, budget_s=10.0):
@@ -480,6 +492,10 @@ def bench_cfg3_het(q):
         ms = q.time_lnl_het(e, dP, len(P), prec, 10, flush_l2=True)
         out[name] = {"value": len(P) / (np.median(ms) * 1e-3), "unit": "lnL evals/s", "ms": float(np.median(ms))}
     out["het_max_abs_dlnL_mixed_vs_fp64"] = float(np.max(np.abs(Lh64 - Lhm)))
+    try:
+        out["het_per_call_dropin"] = dropin_het_per_call_rates(q, ev, g3, P)
+    except Exception as exc:
+        out["het_per_call_dropin"] = {"unavailable": f"{type(exc).__name__}: {exc}"}
     try:
         cb = cpu_baseline_het(ev, g3, P)
         cb["max_abs_dlnL_gpu_fp64_vs_reference"] = float(np.max(np.abs(np.asarray(cb.pop("lnl_first256")) -

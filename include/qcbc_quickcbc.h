@@ -24,7 +24,11 @@
  * as the reference's OpenMP chains call the likelihoods (QuickCBC.c:2063-2067).
  * Each thread has its own CUDA stream and scratch; a cached event that is
  * replaced (new data, new heterodyne tables, a new binding) stays alive until
- * the calls still using it return.
+ * the calls still using it return.  Concurrent log_likelihood_het calls on the
+ * same tables, and log_likelihood_full calls on the same data and geometry,
+ * are merged: a caller that finds no launch running for that event takes the
+ * sets of the callers waiting meanwhile into its own launch.  Each caller gets
+ * the value it would get alone, bit for bit.
  *
  * Errors: the double-returning functions cannot report errors in-band; on a
  * failure they return -1e20 (the reference's rejected-sample value,
@@ -146,6 +150,17 @@ void Fisher_Het(struct Net* net, struct Het* het, double** fish, double* params,
  * allocates them); writes no diagnostic files */
 void het_space(struct Net* net, struct Het* het, double* params, double* min, double* max, RealVector* freq,
                double** SN, int N, double Tobs);
+
+/* Times the reference-signature likelihood from `nthreads` native host threads
+ * started together, as the reference's OpenMP chains call it: each thread makes
+ * 4 untimed calls, then `calls` timed ones with parameter set (7 t + k) mod nsets
+ * of params[nsets][11].  which = 0: log_likelihood_full(net, D, ., freq, SN, rho,
+ * N, Tobs); which = 1: log_likelihood_het(net, het, ., Tobs).  *seconds is the
+ * wall time of the timed calls of all threads; lnl_last[t] (optional) the last
+ * lnL of thread t. */
+int qcbc_time_dropin(int which, struct Net* net, struct Het* het, double** D, RealVector* freq, double** SN, int N,
+                     double Tobs, const double* params, int nsets, int calls, int nthreads, double* seconds,
+                     double* lnl_last);
 
 /* The same functions under prefixed names, for a forwarding object that
  * gives an unchanged QuickCBC build strong definitions: a small C file that

@@ -120,6 +120,9 @@ def lib():
         L.log_likelihood_full.argtypes = [C.POINTER(Net), _PPD, _PD, C.POINTER(RealVector), _PPD, _PD, i, d]
         L.log_likelihood_het.restype = d
         L.log_likelihood_het.argtypes = [C.POINTER(Net), C.POINTER(Het), _PD, d]
+        L.qcbc_time_dropin.restype = i
+        L.qcbc_time_dropin.argtypes = [i, C.POINTER(Net), C.POINTER(Het), _PPD, C.POINTER(RealVector), _PPD, i, d, _PD,
+                                       i, i, i, _PD, _PD]
         L.heterodyne.restype = None
         L.heterodyne.argtypes = [C.POINTER(Net), C.POINTER(Het), _PPD, _PD, C.POINTER(RealVector), _PPD, i, d]
         L.fulltemplates.restype = None

@@ -12,6 +12,9 @@
 #include <string>
 #include <vector>
 #include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <thread>
 
 #include "qcbc_kernels.cuh"
 #include "qcbc_hetspace.h"
@@ -520,8 +523,8 @@ extern "C" int qcbc_get_full_launch(qcbc_event* ev, int B, int precision, int* t
 // ------------------------------------------------------------------ full likelihood
 static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, int B, double* d_lnl, double* d_rho,
                         int prec, cudaStream_t s, const NetGeom& g, cudaEvent_t k0 = nullptr,
-                        cudaEvent_t k1 = nullptr, int model = kModelFull) {
-  FullLaunch L = choose_launch(ev, B, prec);
+                        cudaEvent_t k1 = nullptr, int model = kModelFull, const FullLaunch* shape = nullptr) {
+  FullLaunch L = shape ? *shape : choose_launch(ev, B, prec);
   int rc;
   if ((rc = grow(w->d_recs, w->c_recs, (size_t)B))) return rc;
   if ((rc = grow(w->d_status, w->c_status, (size_t)B))) return rc;
@@ -566,7 +569,7 @@ static int mapped_ptr(double* h, size_t cap, double*& m, size_t& of) {
 }
 
 static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, double* rho, int prec,
-                    const NetGeom& g, int model = kModelFull) {
+                    const NetGeom& g, int model = kModelFull, const FullLaunch* shape = nullptr) {
   Workspace* w;
   int rc = workspace(w);
   if (rc) return rc;
@@ -583,7 +586,7 @@ static int run_full(qcbc_event* ev, const double* params, int B, double* lnl, do
   if ((rc = mapped_ptr(w->h_lnl, w->ch_lnl, w->m_lnl, w->m_lnl_of))) return rc;
   if (rho && (rc = mapped_ptr(w->h_rho, w->ch_rho, w->m_rho, w->m_rho_of))) return rc;
   if ((rc = enqueue_full(w, ev, w->m_params, B, w->m_lnl, rho ? w->m_rho : nullptr, prec, s, g, nullptr, nullptr,
-                         model)))
+                         model, shape)))
     return rc;
   CU(cudaStreamSynchronize(s));
   memcpy(lnl, w->h_lnl, sizeof(double) * B);
@@ -849,21 +852,20 @@ extern "C" int qcbc_lnl_het(qcbc_event* ev, const double* params, int B, double*
   Workspace* w;
   int rc = workspace(w);
   if (rc) return rc;
-  if ((rc = grow(w->d_params, w->c_params, (size_t)B * 11))) return rc;
-  if ((rc = grow(w->d_lnl, w->c_lnl, (size_t)B))) return rc;
   if ((rc = grow_host(w->h_params, w->ch_params, (size_t)B * 11))) return rc;
   if ((rc = grow_host(w->h_lnl, w->ch_lnl, (size_t)B))) return rc;
-  if ((rc = grow_host(w->h_status, w->ch_status, (size_t)B))) return rc;
   memcpy(w->h_params, params, sizeof(double) * 11 * (size_t)B);
   cudaStream_t s = w->stream;
-  CU(cudaMemcpyAsync(w->d_params, w->h_params, sizeof(double) * 11 * (size_t)B, cudaMemcpyHostToDevice, s));
-  if ((rc = enqueue_het(w, ev, w->d_params, B, w->d_lnl, precision, s, ev->g))) return rc;
-  CU(cudaMemcpyAsync(w->h_lnl, w->d_lnl, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
-  CU(cudaMemcpyAsync(w->h_status, w->d_status, sizeof(int) * B, cudaMemcpyDeviceToHost, s));
+  // as for the full likelihood: the setup reads the parameters from, and the heterodyned kernel
+  // writes lnL into, the pinned staging buffers through their mapped addresses (no copy calls)
+  if ((rc = mapped_ptr(w->h_params, w->ch_params, w->m_params, w->m_params_of))) return rc;
+  if ((rc = mapped_ptr(w->h_lnl, w->ch_lnl, w->m_lnl, w->m_lnl_of))) return rc;
+  if ((rc = enqueue_het(w, ev, w->m_params, B, w->m_lnl, precision, s, ev->g))) return rc;
   CU(cudaStreamSynchronize(s));
   memcpy(lnl, w->h_lnl, sizeof(double) * B);
+  // a set fails the setup exactly when its lnL is the rejected-sample value
   int bad = 0;
-  for (int b = 0; b < B; b++) bad += w->h_status[b] != 0;
+  for (int b = 0; b < B; b++) bad += lnl[b] == -1.0e20;
   if (bad) return fail(QCBC_EDOM, "%d of %d parameter sets outside the waveform domain (lnL=-1e20)", bad, B);
   return QCBC_OK;
 }
@@ -1529,14 +1531,146 @@ struct BindKey {
 // binding) never frees or rewrites memory that a concurrent call reads: the old event is closed
 // when its last user returns.  Host threads may therefore call these entry points concurrently,
 // as the reference's OpenMP chains do (QuickCBC.c:2063-2067).
+struct MergeReq;
 struct EventRef {
   qcbc_event* ev;
+  // calls waiting to be merged into one launch on this event (merge_call)
+  std::mutex mu;                     // guards queue
+  std::vector<MergeReq*> queue;
+  std::atomic<int> queued{0};        // queue.size(), readable without the lock
+  std::atomic<bool> busy{false};     // a caller is leading a batch
+  std::atomic<int> last_batch{1};    // size of the previous batch: how many callers to wait for
   explicit EventRef(qcbc_event* e) : ev(e) {}
   EventRef(const EventRef&) = delete;
   EventRef& operator=(const EventRef&) = delete;
   ~EventRef() { qcbc_event_close(ev); }
 };
 using EventPtr = std::shared_ptr<EventRef>;
+
+// ------------------------------------------------------------------ merging of concurrent calls
+// The reference's sampler calls log_likelihood_het (QuickCBC.c:2372) and, while it sets up,
+// log_likelihood_full (QuickCBC.c:948-1016) one parameter set at a time from each of its OpenMP
+// threads.  Calls that arrive for the same event while a launch for it is running are merged:
+// the first caller that finds no launch running takes every waiting set of its kind into one
+// batch, runs it and hands each caller its lnL; the others wait, and when their set was not in
+// that batch one of them leads the next.  A lone caller runs its set alone with no wait.  A set's
+// lnL does not depend on the batch it runs in (the heterodyned kernel gives each set its own
+// warp; a merged full-likelihood batch keeps the tiling of a one-set call), so a merged call
+// returns the bits of a lone one.
+struct MergeReq {
+  int kind = 0;                  // kMergeHet or kMergeFull
+  int device = 0;                // the calling thread's device (its batch runs there)
+  const double* params = nullptr;
+  const NetGeom* g = nullptr;    // full likelihood: the call's geometry (sets merge only when equal)
+  double lnl = -1.0e20;
+  double rho[kMaxIfo] = {0.0, 0.0, 0.0};
+  int rc = QCBC_OK;
+  std::string err;
+  std::atomic<int> done{0};      // set by the batch's leader once lnl, rho, rc and err are written
+};
+constexpr int kMergeHet = 0, kMergeFull = 1;
+constexpr int kMergeMax = 256;
+
+// One launch for the sets of `batch` (same kind, device and geometry), each caller's result and
+// error written into its request.
+static void merge_launch(qcbc_event* ev, const std::vector<MergeReq*>& batch) {
+  const int B = (int)batch.size();
+  const MergeReq& lead = *batch[0];
+  std::vector<double> P((size_t)B * 11), L((size_t)B, -1.0e20), R((size_t)B * kMaxIfo, 0.0);
+  for (int b = 0; b < B; b++) memcpy(&P[(size_t)b * 11], batch[b]->params, 11 * sizeof(double));
+  int rc;
+  if (lead.kind == kMergeHet) {
+    rc = qcbc_lnl_het(ev, P.data(), B, L.data(), QCBC_FP64);
+  } else {
+    const FullLaunch one = choose_launch(ev, 1, QCBC_FP64);
+    rc = run_full(ev, P.data(), B, L.data(), R.data(), QCBC_FP64, *lead.g, kModelFull, &one);
+  }
+  const std::string err = rc ? tls_err : std::string();
+  const int nifo = lead.g ? lead.g->nifo : 0;
+  for (int b = 0; b < B; b++) {
+    MergeReq& r = *batch[b];
+    r.lnl = L[b];
+    for (int i = 0; i < nifo; i++) r.rho[i] = R[(size_t)b * nifo + i];
+    if (rc == QCBC_EDOM) {
+      // only the sets outside the waveform domain fail, as each would alone
+      r.rc = L[b] == -1.0e20 ? QCBC_EDOM : QCBC_OK;
+      if (r.rc) r.err = "1 of 1 parameter sets outside the waveform domain (lnL=-1e20)";
+    } else {
+      r.rc = rc;
+      r.err = err;
+    }
+  }
+}
+
+// How long a new leader waits for as many callers as the previous batch had (the reference's
+// chains call again a few microseconds after their previous results come back).
+constexpr double kMergeGatherSeconds = 20e-6;
+
+static inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+  __builtin_ia32_pause();
+#endif
+}
+
+// Lead one batch: wait briefly for the callers of the previous batch, take this request and the
+// waiting ones of the same kind, device and geometry, run them, publish each result.
+static void merge_lead(EventRef& er, MergeReq& me) {
+  const int target = std::min(er.last_batch.load(std::memory_order_relaxed), kMergeMax);
+  if (target > 1 && er.queued.load(std::memory_order_acquire) < target) {
+    const auto t_end = std::chrono::steady_clock::now() + std::chrono::duration<double>(kMergeGatherSeconds);
+    while (er.queued.load(std::memory_order_acquire) < target && std::chrono::steady_clock::now() < t_end)
+      cpu_relax();
+  }
+  std::vector<MergeReq*> batch{&me};
+  {
+    std::lock_guard<std::mutex> lk(er.mu);
+    std::vector<MergeReq*> rest;
+    for (MergeReq* r : er.queue) {
+      if (r == &me) continue;
+      const bool same = r->kind == me.kind && r->device == me.device &&
+                        (me.kind == kMergeHet || memcmp(r->g, me.g, sizeof(NetGeom)) == 0);
+      if (same && (int)batch.size() < kMergeMax) batch.push_back(r);
+      else rest.push_back(r);
+    }
+    er.queue.swap(rest);
+    er.queued.store((int)er.queue.size(), std::memory_order_release);
+  }
+  merge_launch(er.ev, batch);
+  er.last_batch.store((int)batch.size(), std::memory_order_relaxed);
+  // a follower may return (and its request go out of scope) as soon as its flag is set
+  for (MergeReq* r : batch) r->done.store(1, std::memory_order_release);
+  er.busy.store(false, std::memory_order_release);
+}
+
+// Run request `me` on event `er`, merged with the requests of other threads that arrive meanwhile.
+// Waiting callers spin (a launch takes tens of microseconds, shorter than a sleep and wake-up),
+// yielding the core after the first few thousand rounds.  Returns the request's status, with its
+// error message in this thread's error slot.
+static int merge_call(EventRef& er, MergeReq& me) {
+  {
+    std::lock_guard<std::mutex> lk(er.mu);
+    er.queue.push_back(&me);
+    er.queued.store((int)er.queue.size(), std::memory_order_release);
+  }
+  for (unsigned spin = 0;; spin++) {
+    if (me.done.load(std::memory_order_acquire)) break;
+    bool idle = false;
+    if (!er.busy.load(std::memory_order_relaxed) &&
+        er.busy.compare_exchange_strong(idle, true, std::memory_order_acq_rel)) {
+      // the previous leader may have taken and finished this request before releasing the flag
+      if (me.done.load(std::memory_order_acquire)) {
+        er.busy.store(false, std::memory_order_release);
+        break;
+      }
+      merge_lead(er, me);
+      break;
+    }
+    if (spin < 4096) cpu_relax();
+    else std::this_thread::yield();
+  }
+  if (me.rc) tls_err = me.err;
+  return me.rc;
+}
 
 // The caches below live until the process exits and are never destroyed: destroying them would
 // close events after the CUDA runtime has shut down.
@@ -1694,11 +1828,15 @@ extern "C" double log_likelihood_full(struct Net* net, double** D, double* param
     fail(QCBC_EINVAL, "freq is not the reference grid i/Tobs (QuickCBC.c:419-420)");
     return -1.0e20;
   }
-  double lnl = -1.0e20, r[kMaxIfo];
-  int rc = run_full(ev, params, 1, &lnl, r, QCBC_FP64, g);
+  MergeReq me;
+  me.kind = kMergeFull;
+  me.device = current_device();
+  me.params = params;
+  me.g = &g;
+  const int rc = merge_call(*ep, me);
   if (rho && rc == QCBC_OK)
-    for (int i = 0; i < net->Nifo; i++) rho[i] = r[i];
-  return rc == QCBC_OK ? lnl : -1.0e20;
+    for (int i = 0; i < net->Nifo; i++) rho[i] = me.rho[i];
+  return rc == QCBC_OK ? me.lnl : -1.0e20;
 }
 
 // Heterodyne tables of the reference's struct Het, uploaded on first use and again when the
@@ -1777,9 +1915,52 @@ extern "C" double log_likelihood_het(struct Net* net, struct Het* het, double* p
   if (ensure_init()) return -1.0e20;
   EventPtr ev = het_event_for(net, het);
   if (!ev) return -1.0e20;
-  double lnl = -1.0e20;
-  int rc = qcbc_lnl_het(ev->ev, params, 1, &lnl, QCBC_FP64);
-  return rc == QCBC_OK ? lnl : -1.0e20;
+  MergeReq me;
+  me.kind = kMergeHet;
+  me.device = current_device();
+  me.params = params;
+  const int rc = merge_call(*ev, me);
+  return rc == QCBC_OK ? me.lnl : -1.0e20;
+}
+
+extern "C" int qcbc_time_dropin(int which, struct Net* net, struct Het* het, double** D, RealVector* freq,
+                                double** SN, int N, double Tobs, const double* params, int nsets, int calls,
+                                int nthreads, double* seconds, double* lnl_last) {
+  if (!net || !params || !seconds || (which == 1 && !het) || (which == 0 && (!D || !SN || !freq)))
+    return fail(QCBC_EINVAL, "NULL argument");
+  if (which != 0 && which != 1) return fail(QCBC_EINVAL, "which=%d (0 full, 1 heterodyned)", which);
+  if (nsets < 1 || calls < 1 || nthreads < 1 || nthreads > 256) return fail(QCBC_EINVAL, "nsets, calls, nthreads");
+  int rc = ensure_init();
+  if (rc) return rc;
+  const int dev = current_device();
+  std::atomic<int> ready{0}, bad{0};
+  std::atomic<bool> go{false};
+  std::vector<double> last((size_t)nthreads, -1.0e20);
+  auto work = [&](int t) {
+    cudaSetDevice(dev);
+    double p[11], rho[kMaxIfo + 1];
+    auto call = [&](int k) {
+      memcpy(p, params + (size_t)((7 * t + k) % nsets) * 11, sizeof(p));
+      return which ? log_likelihood_het(net, het, p, Tobs) : log_likelihood_full(net, D, p, freq, SN, rho, N, Tobs);
+    };
+    for (int k = 0; k < 4; k++) call(k);
+    ready.fetch_add(1);
+    while (!go.load(std::memory_order_acquire)) std::this_thread::yield();
+    double x = -1.0e20;
+    for (int k = 0; k < calls; k++) x = call(k);
+    last[(size_t)t] = x;
+    if (x == -1.0e20) bad.fetch_add(1);
+  };
+  std::vector<std::thread> ts;
+  for (int t = 0; t < nthreads; t++) ts.emplace_back(work, t);
+  while (ready.load() < nthreads) std::this_thread::yield();
+  const auto t0 = std::chrono::steady_clock::now();
+  go.store(true, std::memory_order_release);
+  for (auto& th : ts) th.join();
+  *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (lnl_last)
+    for (int t = 0; t < nthreads; t++) lnl_last[t] = last[(size_t)t];
+  return bad.load() ? fail(QCBC_EDOM, "%d threads ended on lnL=-1e20", bad.load()) : QCBC_OK;
 }
 
 // Allocation helpers with the reference's layout (Utilities.c:2941-3015): N+1 rows of M+1 entries.

@@ -1895,6 +1895,7 @@ __global__ void __launch_bounds__(128, QCBC_HET_MINBLOCKS) k_lnl_het(const PhdRe
                                                  NetGeom g, HetData h, int B, int warp_doubles,
                                                  double* __restrict__ lnl) {
   extern __shared__ __align__(16) double sm[];
+  pdl_wait();          // records of the setup (immediate when launched the ordinary way)
   const int w = threadIdx.x >> 5;
   const int b = blockIdx.x * (blockDim.x >> 5) + w;
   if (b >= B) return;                // the whole warp leaves; no block barrier follows
@@ -1937,6 +1938,8 @@ size_t het_smem_bytes(const NetGeom& g, const HetData& h) {
   return (size_t)het_warp_doubles(g.nifo, h.M) * sizeof(double);
 }
 
+constexpr int kHetPdlMaxSets = 128;
+
 // sets per block: four warps while their shared memory stays within 96 KB
 static int het_sets_per_block(size_t warp_bytes) {
   int n = 4;
@@ -1963,8 +1966,12 @@ void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetG
   const int spb = het_sets_per_block(smem);
   const int wd = het_warp_doubles(g.nifo, h.M);
   const unsigned grid = (unsigned)((B + spb - 1) / spb);
-  if (prec == kFP64) k_lnl_het<kFP64><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
-  else k_lnl_het<kMixed><<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
+  auto k = prec == kFP64 ? k_lnl_het<kFP64> : k_lnl_het<kMixed>;
+  // A small batch (the reference-signature calls, merged or not) is launched with programmatic
+  // dependent launch after the setup, so its few blocks wait on the SMs instead of behind a launch
+  // gap; a large one is launched the ordinary way (early blocks holding SMs slowed it).
+  if (B <= kHetPdlMaxSets) launch_pdl(k, dim3(grid), dim3(32 * spb), spb * smem, s, d_recs, d_status, g, h, B, wd, d_lnl);
+  else k<<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
 }
 
 // ---------------------------------------------------------------- heterodyne-grid waveforms, het_diff, Fisher_Het

@@ -301,6 +301,66 @@ def test_reference_signature_heterodyne(ev1, golden):
         assert abs(H.lnl(h["params"][k]) - h["lnl"][k]) < LNL_ATOL_FP64
 
 
+def _from_threads(nthreads, calls, fn):
+    """fn(k) from `nthreads` host threads at once (ctypes releases the GIL in the call), thread t
+    starting at call 5t: (results [thread][call], launches made by each thread)."""
+    import threading
+    from quickcbc_b200 import _lib
+    out, launches = np.zeros((nthreads, calls)), np.zeros(nthreads, dtype=np.int64)
+    go = threading.Barrier(nthreads)
+
+    def work(t):
+        go.wait()
+        n0 = _lib.launch_count()
+        for j in range(calls):
+            k = (j + 5 * t) % calls
+            out[t, k] = fn(k)
+        launches[t] = _lib.launch_count() - n0
+    ts = [threading.Thread(target=work, args=(t,)) for t in range(nthreads)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join()
+    return out, launches
+
+
+def test_concurrent_reference_calls_merge_bit_exact(ev1, golden):
+    """12 threads calling log_likelihood_het and log_likelihood_full at once, as the reference's
+    OpenMP chains do: their calls share launches (fewer launches than a lone caller makes) and each
+    returns the bits of the same call made alone."""
+    import ctypes as C
+    from quickcbc_b200 import _lib, engine as eng
+    ev, z, _ = ev1
+    h = golden("het1.npz")
+    H = q.LegacyHet(ev.labels, ev.GMST, ev.Tobs, h["fgrid"], int(h["MN"]), int(h["MM"]), int(h["J"]))
+    H.heterodyne(ev.D, h["pref"], ev.freq, ev.SN, ev.N)
+    P = [np.ascontiguousarray(p) for p in synth.jitter_params(np.random.default_rng(5), 40, h["pref"], 1e-3)]
+    P[7][2] = 1.5                                  # spin outside [-1, 1]: -1e20 alone and merged
+    lone = np.array([H.lnl(p) for p in P])
+    assert lone[7] == -1e20 and np.all(lone[np.arange(40) != 7] > -1e20)
+    out, launches = _from_threads(12, len(P), lambda k: H.lnl(P[k]))
+    assert np.array_equal(out, np.broadcast_to(lone, out.shape))
+    assert launches.sum() < 2 * out.size           # two launches per lone call: some calls merged
+
+    q.set_band(16.0, 1024.0)
+    nh = eng._NetHolder(ev.labels, ev.Tobs, ev.GMST)
+    D, SN = eng._f64(ev.D), eng._f64(ev.SN)
+    Dr, Sr = eng._rows(D), eng._rows(SN)
+    f, rv = eng._rv(ev.freq)
+    L = _lib.lib()
+
+    def full(k):
+        rho = np.zeros(4)
+        return L.log_likelihood_full(nh.ref, Dr, eng._ptr(P[k]), C.byref(rv), Sr, eng._ptr(rho), ev.N, ev.Tobs)
+    lone = np.array([full(k) for k in range(len(P))])
+    assert lone[7] == -1e20
+    np.testing.assert_allclose(lone[:5], [q.log_likelihood_full(ev.labels, ev.GMST, ev.D, P[k], ev.freq, ev.SN,
+                                                                ev.N, ev.Tobs)[0] for k in range(5)], rtol=0, atol=0)
+    out, launches = _from_threads(12, len(P), full)
+    assert np.array_equal(out, np.broadcast_to(lone, out.shape))
+    assert launches.sum() < 2 * out.size
+
+
 def test_cfg3_heterodyne_long_signal(ora):
     """Config 3 (3 det, 128 s, 4096 Hz, BNS): reference het grid, tables set up on
     the GPU in FP64, het lnL against the reference's value and the oracle."""
