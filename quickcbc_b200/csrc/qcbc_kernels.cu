@@ -1130,22 +1130,35 @@ struct MixAcc {
       sh[id] = fmaf(amp2, w.s[id], sh[id]);
     }
   }
-  __device__ __forceinline__ void flush(const float2* base, double* acc) {
+  template <class State>
+  __device__ __forceinline__ void flush(State& S) {
 #pragma unroll
     for (int id = 0; id < NIFO; id++) {
-      acc[2 * id] += (double)(base[id].x * sx[id] - base[id].y * sy[id]);
-      acc[2 * id + 1] += (double)sh[id];
+      const float2 bs = S.base(id);
+      S.acc(2 * id) += (double)(bs.x * sx[id] - bs.y * sy[id]);
+      S.acc(2 * id + 1) += (double)sh[id];
     }
   }
+};
+
+// The mixed kernels keep a thread's rotation base and FP64 sums in its column of two shared-memory
+// arrays rather than in registers: 18 registers fewer at three detectors, so that four blocks of
+// 256 threads fit an SM (64 registers; 157.7 us against 165.9 us at three blocks for the config-2
+// launch).
+struct MixSmemState {
+  float2* b;     // [NIFO][st], this thread's column
+  double* a;     // [2 NIFO][st]
+  int st;
+  __device__ __forceinline__ float2& base(int id) { return b[id * st]; }
+  __device__ __forceinline__ double& acc(int k) { return a[k * st]; }
 };
 
 // Rows [k, k_end) of the thread's bins i = i0 + tid + k bs, all in amplitude piece AP and
 // phase piece PP (-1: decided per bin).  The pieces' coefficients are read from the block's
 // record in shared memory at each use.
-template <int NIFO, int AP, int PP>
+template <int NIFO, int AP, int PP, class State>
 __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot, int nk,
-                                           const float2* base, int k, int k_end, int i, int i1, int bs,
-                                           double* acc) {
+                                           State& S, int k, int k_end, int i, int i1, int bs) {
   if (i > i1) return;
   const int n = min(k_end - k, (i1 - i) / bs + 1);     // rows of this thread in the run
   const MixPhIns& qi = P.pins;      // in shared memory, read per use (sld)
@@ -1206,7 +1219,7 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
       xi += dbs;
       xf += fbs;
     }
-    A.flush(base, acc);
+    A.flush(S);
   }
 }
 
@@ -1217,9 +1230,9 @@ __device__ __forceinline__ int mixed_table_len(int i0, int i1, int bs) {
 // Builds the rotation table (shared), then runs the bin loop in runs of rows that share their
 // waveform pieces.  The tile is walked by bs threads (tid = 0..bs-1).  Contains
 // __syncthreads(): every thread of the block must call it.
-template <int NIFO>
+template <int NIFO, class State>
 __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
-                                           int tid, int bs, float2* s_rot, double* acc) {
+                                           int tid, int bs, float2* s_rot, State& S) {
   const int nk = mixed_table_len(i0, i1, bs);
   constexpr double kInv2Pi = 0.15915494309189533577;
   const double Dstep = (double)bs * g.df;
@@ -1237,13 +1250,12 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
   int i = i0 + tid;
   if (i > i1) return;
   double f = g.div_exact ? (double)i * g.df : (double)i / g.Tobs;
-  float2 base[NIFO];
 #pragma unroll
   for (int id = 0; id < NIFO; id++) {
     double cyc = f * (c.ts - c.td[id]) + c.lam[id] * kInv2Pi - fma((double)i, Ri, R0);
     float sv, cv;
     sincospif(2.0f * (float)(cyc - rint(cyc)), &sv, &cv);
-    base[id] = make_float2(cv, sv);
+    S.base(id) = make_float2(cv, sv);
   }
   const MixPoly& P = c.mix;
   int k = 0;
@@ -1254,7 +1266,7 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
     int k_end;
     if (a0 != amp_piece(P, r1) || p0 != ph_piece(P, r1)) {
       k_end = k + 1;
-      mixed_rows<NIFO, -1, -1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc);
+      mixed_rows<NIFO, -1, -1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs);
     } else {
       int nxt = i1 + 1;              // the pieces can only change at a threshold
       if (P.iA > r0 && P.iA < nxt) nxt = P.iA;
@@ -1263,20 +1275,50 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
       if (P.iM > r0 && P.iM < nxt) nxt = P.iM;
       k_end = nxt > i1 ? nk : max(k + 1, (nxt - i0 - bs) / bs + 1);
       switch (a0 * 3 + p0) {
-        case 0: mixed_rows<NIFO, 0, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 1: mixed_rows<NIFO, 0, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 2: mixed_rows<NIFO, 0, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 3: mixed_rows<NIFO, 1, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 4: mixed_rows<NIFO, 1, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 5: mixed_rows<NIFO, 1, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 6: mixed_rows<NIFO, 2, 0>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        case 7: mixed_rows<NIFO, 2, 1>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
-        default: mixed_rows<NIFO, 2, 2>(P, ev, s_rot, nk, base, k, k_end, i, i1, bs, acc); break;
+        case 0: mixed_rows<NIFO, 0, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 1: mixed_rows<NIFO, 0, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 2: mixed_rows<NIFO, 0, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 3: mixed_rows<NIFO, 1, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 4: mixed_rows<NIFO, 1, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 5: mixed_rows<NIFO, 1, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 6: mixed_rows<NIFO, 2, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 7: mixed_rows<NIFO, 2, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        default: mixed_rows<NIFO, 2, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
       }
     }
     k = k_end;
     i = i0 + tid + k * bs;
   }
+}
+
+// rotation-table entries per detector that a block of a launch needs: ceil(max bins per tile /
+// threads) + 1
+__host__ __device__ __forceinline__ int mixed_nk_cap(int band, int tiles, int threads) {
+  const int bins = band > 1 ? band : 1;
+  const int chunk = (bins + tiles - 1) / tiles;
+  return (chunk + threads - 1) / threads + 1;
+}
+
+// tile_mixed with the thread's state in shared memory after the rotation table (nk_cap entries for
+// each of nifo_cap detectors): the thread's column of base [nifo_cap][threads] float2 and of
+// sums [2 nifo_cap][threads] double (threads x nifo_cap x 24 bytes).  acc[0 .. 2 NIFO) receives
+// the thread's FP64 sums.
+template <int NIFO>
+__device__ __forceinline__ void tile_mixed_smem(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
+                                                float2* s_rot, int nk_cap, int nifo_cap, double* acc) {
+  float2* s_base = s_rot + (size_t)nifo_cap * nk_cap;
+  double* s_acc = reinterpret_cast<double*>(s_base + (size_t)nifo_cap * blockDim.x);
+  MixSmemState S{s_base + threadIdx.x, s_acc + threadIdx.x, (int)blockDim.x};
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) S.acc(k) = 0.0;
+  tile_mixed<NIFO>(c, g, ev, i0, i1, threadIdx.x, blockDim.x, s_rot, S);
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) acc[k] = S.acc(k);
+}
+
+// bytes of shared memory a mixed block keeps its threads' state in (tile_mixed_smem)
+__host__ __device__ __forceinline__ size_t mixed_state_bytes(int threads, int nifo) {
+  return (size_t)threads * nifo * (sizeof(float2) + 2 * sizeof(double));
 }
 
 __device__ __forceinline__ void load_record(PhdRec& dst, const PhdRec* src) {
@@ -1413,7 +1455,7 @@ __global__ void __launch_bounds__(256) k_lnl_full(const PhdRec* __restrict__ rec
 }
 
 #ifndef QCBC_MIXED_MINBLOCKS
-#define QCBC_MIXED_MINBLOCKS 3     // 80 registers: the piece coefficients are read from shared memory
+#define QCBC_MIXED_MINBLOCKS 4     // 64 registers: coefficients and the thread's sums in shared memory
 #endif
 // Sums over the threads of each group of gs threads (gs a multiple of 32) in a fixed order;
 // the first thread of each group holds its group's sums.
@@ -1454,25 +1496,20 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   int i0, i1;
   tile_range(rec, tiles, t, i0, i1);
   double acc[2 * NIFO];
-#pragma unroll
-  for (int k = 0; k < 2 * NIFO; k++) acc[k] = 0.0;
-  tile_mixed<NIFO>(rec, g, ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
+  tile_mixed_smem<NIFO>(rec, g, ev, i0, i1, s_rot, mixed_nk_cap(g.imax - g.imin, tiles, blockDim.x), NIFO, acc);
   group_sum<2 * NIFO>(acc, red, blockDim.x);
   if (threadIdx.x == 0) finish_tile<NIFO>(rec, acc, g, ev, fo, b, tiles, t, partials);
 }
 
 // rotation-table length per block for a launch: ceil(max bins per tile / threads)
-static int mixed_nk(const NetGeom& g, const FullLaunch& L) {
-  int bins = max(1, g.imax - g.imin);
-  int chunk = (bins + L.tiles - 1) / L.tiles;
-  return (chunk + L.threads - 1) / L.threads + 1;
-}
+static int mixed_nk(const NetGeom& g, const FullLaunch& L) { return mixed_nk_cap(g.imax - g.imin, L.tiles, L.threads); }
 
 template <int NIFO>
 static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
                            double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
+  smem += mixed_state_bytes(L.threads, NIFO);
   if (fo.order.cnt) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
   else k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
 }
@@ -1621,10 +1658,11 @@ void launch_scan_expand(const int* d_ntile, int B, int* d_off, int* d_items, int
 }
 
 #ifndef QCBC_MULTI_MINBLOCKS
-#define QCBC_MULTI_MINBLOCKS 3
+#define QCBC_MULTI_MINBLOCKS 4
 #endif
-// Both bodies are held to the register budget of three or more blocks per SM: the FP64 body is
-// light on registers, the mixed body reads its piece coefficients from shared memory.
+// Both bodies are held to the register budget of four blocks per SM: the FP64 body is light on
+// registers, the mixed body reads its piece coefficients from shared memory and keeps each
+// thread's sums there (tile_mixed_smem).
 template <int PREC>
 __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS) k_lnl_multi(const PhdRec* __restrict__ recs,
                                                       const EventDesc* __restrict__ events,
@@ -1663,9 +1701,10 @@ __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS)
       else if (nifo == 2) tile_fp64<2>(rec, evd.g, evd.ev, i0, i1, acc);
       else tile_fp64<3>(rec, evd.g, evd.ev, i0, i1, acc);
     } else {
-      if (nifo == 1) tile_mixed<1>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
-      else if (nifo == 2) tile_mixed<2>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
-      else tile_mixed<3>(rec, evd.g, evd.ev, i0, i1, threadIdx.x, blockDim.x, s_rot, acc);
+      const int nk = (tile_bins + blockDim.x - 1) / blockDim.x + 1;
+      if (nifo == 1) tile_mixed_smem<1>(rec, evd.g, evd.ev, i0, i1, s_rot, nk, kMaxIfo, acc);
+      else if (nifo == 2) tile_mixed_smem<2>(rec, evd.g, evd.ev, i0, i1, s_rot, nk, kMaxIfo, acc);
+      else tile_mixed_smem<3>(rec, evd.g, evd.ev, i0, i1, s_rot, nk, kMaxIfo, acc);
     }
     block_sum<2 * kMaxIfo>(acc, red);
     if (threadIdx.x == 0) {
@@ -1680,7 +1719,7 @@ __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS)
 static size_t multi_smem(Precision prec, int threads, int tile_bins) {
   if (prec == kFP64) return 0;
   int nk = (tile_bins + threads - 1) / threads + 1;
-  return (size_t)nk * kMaxIfo * sizeof(float2);
+  return (size_t)nk * kMaxIfo * sizeof(float2) + mixed_state_bytes(threads, kMaxIfo);
 }
 
 int multi_blocks_per_sm(Precision prec, int threads, int tile_bins) {
