@@ -1054,7 +1054,11 @@ extern "C" int qcbc_time_lnl_full(qcbc_event* ev, const double* d_params, int B,
   for (int it = 0; it < iters; it++) {
     if (flush && (rc = flush_l2(w, s))) return rc;
     CU(cudaEventRecord(w->e0, s));
-    if ((rc = enqueue_full(w, ev, d_params, B, w->d_lnl, nullptr, precision, s, ev->g, w->e2, w->e3))) return rc;
+    // the kernel's own events only when its time is asked for: an event recorded between the setup
+    // and the lnL kernel also ends the programmatic overlap of the two launches
+    if ((rc = enqueue_full(w, ev, d_params, B, w->d_lnl, nullptr, precision, s, ev->g, kernel_ms ? w->e2 : nullptr,
+                           kernel_ms ? w->e3 : nullptr)))
+      return rc;
     CU(cudaEventRecord(w->e1, s));
     CU(cudaEventSynchronize(w->e1));
     CU(cudaEventElapsedTime(&ms[it], w->e0, w->e1));

@@ -299,12 +299,15 @@ class DeviceBuffer:
             pass
 
 
-def time_lnl_full(event: Event, dbuf: DeviceBuffer, B, precision, iters, flush_l2=True):
+def time_lnl_full(event: Event, dbuf: DeviceBuffer, B, precision, iters, flush_l2=True, kernel_times=True):
+    """Device times (ms) of `iters` full-likelihood steps, and of their lnL kernels when
+    kernel_times (events recorded around the kernel; without them the step runs as a plain call
+    does, the lnL kernel overlapping the setup's tail)."""
     ms = (C.c_float * iters)()
     kms = (C.c_float * iters)()
     check(lib().qcbc_time_lnl_full(event.handle, dbuf.ptr, B, precision_code(precision), iters, int(flush_l2), ms,
-                                   kms))
-    return np.array(ms[:]), np.array(kms[:])
+                                   kms if kernel_times else None))
+    return np.array(ms[:]), (np.array(kms[:]) if kernel_times else None)
 
 
 def time_lnl_het(event: Event, dbuf: DeviceBuffer, B, precision, iters, flush_l2=True):
