@@ -244,6 +244,9 @@ struct Workspace {
   // ordered setup, and the class lists
   int* d_ocnt = nullptr; size_t c_ocnt = 0;
   int* d_olist = nullptr; size_t c_olist = 0;
+  // per-set tile counts of multi-tile launches that finalise in their last tile (FinalOut::done):
+  // zeroed when allocated, left zero by every launch
+  int* d_done = nullptr; size_t c_done = 0;
   double* h_params = nullptr; size_t ch_params = 0;
   double* h_lnl = nullptr; size_t ch_lnl = 0;
   double* h_rho = nullptr; size_t ch_rho = 0;
@@ -487,6 +490,13 @@ static FullLaunch heuristic_launch(const qcbc_event* ev, int B, int prec) {
   FullLaunch L;
   L.threads = 256;
   int bins = std::max(1, ev->g.imax - ev->g.imin);
+  // a few sets (the reference-signature calls, alone or merged): one row of bins per thread while
+  // the launch still fits one wave of four blocks per SM, for the shortest latency
+  const int rows1 = (bins + L.threads - 1) / L.threads;
+  if ((long long)B * rows1 <= 148 * 4) {
+    L.tiles = rows1;
+    return L;
+  }
   int want_blocks = 148 * 8;
   int tiles = (want_blocks + B - 1) / B;
   int max_tiles = std::max(1, bins / 512);
@@ -548,12 +558,16 @@ static int enqueue_full(Workspace* w, qcbc_event* ev, const double* d_params, in
     if (le != cudaSuccess) return fail(QCBC_ECUDA, "lnL launch: %s", cudaGetErrorString(le));
     tls_launches += 2;
   } else {
+    // several tiles per set: the last tile of each set to finish finalises it
+    const size_t had = w->c_done;
+    if ((rc = grow(w->d_done, w->c_done, (size_t)B))) return rc;
+    if (w->c_done != had) CU(cudaMemsetAsync(w->d_done, 0, sizeof(int) * w->c_done, s));
     launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, model);
     if (k0) cudaEventRecord(k0, s);
-    launch_lnl_full(w->d_recs, B, g, ed, kp, L, w->d_part, s);
+    launch_lnl_full_final(w->d_recs, w->d_status, B, g, ed, kp, L, w->d_part, d_lnl, d_rho, model, nullptr, s,
+                          w->d_done);
     if (k1) cudaEventRecord(k1, s);
-    launch_finalize_full(w->d_part, w->d_recs, w->d_status, B, L.tiles, g, ed, kp, d_lnl, d_rho, s, model);
-    tls_launches += 3;
+    tls_launches += 2;
   }
   CU(cudaGetLastError());
   return QCBC_OK;

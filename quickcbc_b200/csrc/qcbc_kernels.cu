@@ -1373,14 +1373,18 @@ __device__ void reject_set(const NetGeom& g, double* lnl_b, double* rho_b) {
     for (int id = 0; id < g.nifo; id++) rho_b[id] = 0.0;
 }
 
-// Where a one-tile launch writes its result itself: lnl != null makes thread 0 finalise the set
-// (finalize_set) instead of writing the tile's partial sums.
+// Where a launch writes its results itself: lnl != null makes the set's last tile finalise it
+// (finalize_set).  At one tile per set that tile's thread 0 does so from its block sums; at several
+// tiles each tile writes its partial sums and counts itself in done[b], and the block that counts
+// last sums the set's partials in tile order and finalises it (then clears done[b] for the next
+// launch).  lnl == null: every tile writes its partials for k_finalize_full.
 struct FinalOut {
   double* lnl;
   double* rho;
   int mixed, model;
   SetOrder order;      // order.cnt non-null: block k evaluates the k-th set longest first (one tile per set)
   int B;
+  int* done;           // several tiles per set: per-set tile counts, zero before the launch
 };
 
 // The set that block k of a one-tile launch evaluates: the k-th with the classes longest first
@@ -1411,13 +1415,14 @@ __device__ int ordered_set(const FinalOut& fo, int k) {
   return s_set;
 }
 
-// thread 0's block sums of a set's only tile: its lnL, or its partials
+// thread 0's block sums of tile t of set b: the set's lnL (its only tile, or its last to finish), or
+// the tile's partials (FinalOut)
 template <int NIFO>
 __device__ __forceinline__ void finish_tile(const PhdRec& rec, const double* acc, const NetGeom& g,
                                             const EventData& ev, const FinalOut& fo, int b, int tiles, int t,
                                             double* partials) {
-  if (fo.lnl) {
-    double* rho_b = fo.rho ? fo.rho + (size_t)b * g.nifo : nullptr;
+  double* rho_b = fo.rho ? fo.rho + (size_t)b * g.nifo : nullptr;
+  if (fo.lnl && tiles == 1) {
     if (!(rec.flags & kRecValid)) {
       reject_set(g, fo.lnl + b, rho_b);
       return;
@@ -1426,11 +1431,30 @@ __device__ __forceinline__ void finish_tile(const PhdRec& rec, const double* acc
 #pragma unroll
     for (int k = 0; k < 2 * kMaxIfo; k++) S[k] = k < 2 * NIFO ? acc[k] : 0.0;
     finalize_set(rec, S, g, ev, fo.mixed, fo.model, fo.lnl + b, rho_b);
-  } else {
-    double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
-#pragma unroll
-    for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+    return;
   }
+  double* out = partials + ((size_t)b * tiles + t) * (2 * kMaxIfo);
+#pragma unroll
+  for (int k = 0; k < 2 * NIFO; k++) out[k] = acc[k];
+  if (!fo.lnl || !fo.done) return;
+  __threadfence();                               // the partials before the count
+  if (atomicAdd(fo.done + b, 1) != tiles - 1) return;
+  __threadfence();                               // every tile's partials after the count
+  fo.done[b] = 0;
+  if (!(rec.flags & kRecValid)) {
+    reject_set(g, fo.lnl + b, rho_b);
+    return;
+  }
+  // the same sum in the same order as k_finalize_full
+  double S[2 * kMaxIfo];
+#pragma unroll
+  for (int k = 0; k < 2 * kMaxIfo; k++) S[k] = 0.0;
+  for (int u = 0; u < tiles; u++) {
+    const double* p = partials + ((size_t)b * tiles + u) * (2 * kMaxIfo);
+#pragma unroll
+    for (int k = 0; k < 2 * NIFO; k++) S[k] += __ldcg(p + k);
+  }
+  finalize_set(rec, S, g, ev, fo.mixed, fo.model, fo.lnl + b, rho_b);
 }
 
 template <int PREC, int NIFO>
@@ -1510,7 +1534,7 @@ static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const Event
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
   smem += mixed_state_bytes(L.threads, NIFO);
-  if (fo.order.cnt) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
+  if (fo.order.cnt || fo.done) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
   else k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
@@ -1528,29 +1552,30 @@ static void launch_full_prec(const PhdRec* r, int B, const NetGeom& g, const Eve
                              double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
   auto k = g.nifo == 1 ? k_lnl_full<PREC, 1> : (g.nifo == 2 ? k_lnl_full<PREC, 2> : k_lnl_full<PREC, 3>);
-  if (fo.order.cnt) launch_pdl(k, grid, block, 0, s, r, g, ev, L.tiles, part, fo);
+  if (fo.order.cnt || fo.done) launch_pdl(k, grid, block, 0, s, r, g, ev, L.tiles, part, fo);
   else k<<<grid, block, 0, s>>>(r, g, ev, L.tiles, part, fo);
 }
 
 void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventData& ev, Precision prec,
                      const FullLaunch& L, double* d_partials, cudaStream_t s) {
   if (B <= 0) return;
-  const FinalOut none{nullptr, nullptr, 0, 0, SetOrder{nullptr, nullptr}, B};
+  const FinalOut none{nullptr, nullptr, 0, 0, SetOrder{nullptr, nullptr}, B, nullptr};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, none, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, none, s);
 }
 
 bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
-                           int model, const SetOrder* order, cudaStream_t s) {
+                           int model, const SetOrder* order, cudaStream_t s, int* d_done) {
   if (B <= 0) return true;
-  if (L.tiles != 1) {
+  if (L.tiles != 1 && !d_done) {
     launch_lnl_full(d_recs, B, g, ev, prec, L, d_partials, s);
     launch_finalize_full(d_partials, d_recs, d_status, B, L.tiles, g, ev, prec, d_lnl, d_rho, s, model);
     return false;
   }
   const FinalOut fo{d_lnl, d_rho, prec == kMixed ? 1 : 0, model,
-                    order ? *order : SetOrder{nullptr, nullptr}, B};
+                    (order && L.tiles == 1) ? *order : SetOrder{nullptr, nullptr}, B,
+                    L.tiles == 1 ? nullptr : d_done};
   if (prec == kFP64) launch_full_prec<kFP64>(d_recs, B, g, ev, L, d_partials, fo, s);
   else launch_full_mixed(d_recs, B, g, ev, L, d_partials, fo, s);
   return true;

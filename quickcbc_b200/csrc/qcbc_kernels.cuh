@@ -104,12 +104,14 @@ void launch_lnl_full(const PhdRec* d_recs, int B, const NetGeom& g, const EventD
 void launch_finalize_full(const double* d_partials, const PhdRec* d_recs, const int* d_status, int B, int tiles,
                           const NetGeom& g, const EventData& ev, Precision prec, double* d_lnl, double* d_rho,
                           cudaStream_t s, int model = kModelFull);
-// lnL of B sets with the finaliser folded into the lnL kernel when each set is one tile (L.tiles == 1),
-// longest first when order is given (filled by launch_setup_ordered); otherwise the lnL kernel and
-// launch_finalize_full.  Returns true when one launch did both.
+// lnL of B sets with the finaliser folded into the lnL kernel: when each set is one tile (L.tiles ==
+// 1), longest first when order is given (filled by launch_setup_ordered); at several tiles per set
+// when d_done (B ints, zero before the launch and left zero after it) is given, the set's last
+// tile to finish finalises it.  Otherwise the lnL kernel and launch_finalize_full.  Returns true
+// when one launch did both.
 bool launch_lnl_full_final(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const EventData& ev,
                            Precision prec, const FullLaunch& L, double* d_partials, double* d_lnl, double* d_rho,
-                           int model, const SetOrder* order, cudaStream_t s);
+                           int model, const SetOrder* order, cudaStream_t s, int* d_done = nullptr);
 // fill the per-bin tables for bins [0, n)
 void launch_fill_bin_tables(double2* d_tabA, double2* d_tabB, float2* d_tabC, int n, cudaStream_t s);
 void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetGeom& g, const HetData& h,

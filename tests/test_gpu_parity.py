@@ -121,6 +121,38 @@ def test_launch_shapes_agree(cfg2):
     e.set_launch(0, 0)
 
 
+def test_multi_tile_sets_finalised_in_their_last_tile(cfg2):
+    """At several tiles per set, the last tile of each set to finish sums the set's partials in tile
+    order and finalises it (no finaliser launch).  The result equals, bit for bit, the allocation-free
+    entry point's separate finaliser over the same partials; repeat calls agree (each set's tile count
+    is back at zero after a launch); an invalid set among them gets -1e20 and rho 0."""
+    from quickcbc_b200 import _lib
+    ev, e = cfg2
+    P = synth.draw_params(np.random.default_rng(2506), 40, ev.inj)
+    P[3, 2] = 1.5                      # spin outside [-1, 1]
+    B = len(P)
+    dP = q.DeviceBuffer(P.nbytes)
+    dP.upload(P)
+    dL, dR = q.DeviceBuffer(B * 8), q.DeviceBuffer(B * 8 * e.nifo)
+    L = _lib.lib()
+
+    def run(fn, prec):
+        rc = fn(e.handle, dP.ptr, B, dL.ptr, dR.ptr, prec, None)
+        assert rc == 0, _lib.last_error()
+        assert L.qcbc_synchronize() == 0
+        return dL.download((B,)), dR.download((B, e.nifo))
+    try:
+        for tiles in (2, 7, 63):
+            e.set_launch(tiles, 256)
+            for prec in (q.FP64, q.MIXED):
+                a = run(L.qcbc_lnl_full_dev, prec)
+                assert a[0][3] == -1e20 and np.all(a[1][3] == 0.0)
+                for x in (run(L.qcbc_lnl_full_dev, prec), run(L.qcbc_lnl_full_noalloc, prec)):
+                    assert np.array_equal(a[0], x[0]) and np.array_equal(a[1], x[1]), (tiles, prec)
+    finally:
+        e.set_launch(0, 0)
+
+
 def test_length_ordered_batch_matches_unordered(cfg2, ora):
     """At one tile per set (B >= 1184) the sets run in order of their bin count: every set's lnL
     equals the same set in a multi-tile launch (which runs in index order), invalid sets at
