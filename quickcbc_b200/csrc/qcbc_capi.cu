@@ -490,13 +490,6 @@ static FullLaunch heuristic_launch(const qcbc_event* ev, int B, int prec) {
   FullLaunch L;
   L.threads = 256;
   int bins = std::max(1, ev->g.imax - ev->g.imin);
-  // a few sets (the reference-signature calls, alone or merged): one row of bins per thread while
-  // the launch still fits one wave of four blocks per SM, for the shortest latency
-  const int rows1 = (bins + L.threads - 1) / L.threads;
-  if ((long long)B * rows1 <= 148 * 4) {
-    L.tiles = rows1;
-    return L;
-  }
   int want_blocks = 148 * 8;
   int tiles = (want_blocks + B - 1) / B;
   int max_tiles = std::max(1, bins / 512);

@@ -1852,16 +1852,17 @@ __device__ __forceinline__ void mixed_point(const PhdRec& c, const HetData& h, i
   amp = a * (u * u * u) * sqrtf(u) * (float)(c.a0 * c.mdf_m76);
 }
 
+// Phase 1 of a set: the waveform at grid points j0, j0 + jstep, ... and the per-detector ratios
+// to the reference into the set's shared memory sm ([3][nifo][M]: hc, hs, cc).
 template <int PREC>
-__device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm,
-                                         double* out) {
-  const int lane = threadIdx.x & 31;
+__device__ __forceinline__ void het_points(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm, int j0,
+                                           int jstep) {
   const int M = h.M, nifo = g.nifo;
   double* s_hc = sm;                 // [nifo][M]
   double* s_hs = sm + nifo * M;
   double* s_cc = sm + 2 * nifo * M;
   constexpr double kInv2Pi = 0.15915494309189533577;
-  for (int j = lane; j < M; j += 32) {
+  for (int j = j0; j < M; j += jstep) {
     double f = __ldg(h.freq + j);
     double y = 1.0;
     if (f < c.fs) y = exp(10.0 * (f - c.fs) / c.fs);          // taper below fbegin (QuickCBC.c:3859)
@@ -1898,7 +1899,16 @@ __device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, cons
       }
     }
   }
-  __syncwarp();
+}
+
+// Phase 2 of a set, by one warp once phase 1 is in sm: the region contractions (lane r takes
+// regions r, r + 32, ...), a butterfly warp sum, and lane 0 writes lnL to *out.
+__device__ __forceinline__ void het_regions(const NetGeom& g, const HetData& h, const double* sm, double* out) {
+  const int lane = threadIdx.x & 31;
+  const int M = h.M, nifo = g.nifo;
+  const double* s_hc = sm;
+  const double* s_hs = sm + nifo * M;
+  const double* s_cc = sm + 2 * nifo * M;
   const int J = h.J, J1 = J + 1, NR = h.NR;
   double acc[4 * kMaxIfo];           // per detector: HH, HR, x, y
 #pragma unroll
@@ -1945,6 +1955,15 @@ __device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, cons
     }
     *out = L;
   }
+}
+
+// lnL of one set by one warp: phase 1 over the warp's lanes, then phase 2
+template <int PREC>
+__device__ __forceinline__ void het_warp(const PhdRec& c, const NetGeom& g, const HetData& h, double* sm,
+                                         double* out) {
+  het_points<PREC>(c, g, h, sm, threadIdx.x & 31, 32);
+  __syncwarp();
+  het_regions(g, h, sm, out);
 }
 
 // the warp's record into its shared memory
@@ -2002,7 +2021,31 @@ size_t het_smem_bytes(const NetGeom& g, const HetData& h) {
   return (size_t)het_warp_doubles(g.nifo, h.M) * sizeof(double);
 }
 
-constexpr int kHetPdlMaxSets = 128;
+// Heterodyned lnL of a few sets (the reference-signature calls, alone or merged): one block per
+// set, phase 1 over all the block's threads (one grid point each while M <= blockDim), then phase 2
+// by warp 0 exactly as k_lnl_het's warp does it, so both kernels give the same bits.  The block's
+// shared memory: the record, then [3][nifo][M] doubles.
+template <int PREC>
+__global__ void __launch_bounds__(128) k_lnl_het_wide(const PhdRec* __restrict__ recs, const int* __restrict__ status,
+                                                     NetGeom g, HetData h, int B, double* __restrict__ lnl) {
+  extern __shared__ __align__(16) double sm[];
+  pdl_wait();          // records of the setup
+  const int b = blockIdx.x;
+  if (b >= B) return;
+  if (status[b] != kStOK) {
+    if (threadIdx.x == 0) lnl[b] = -1.0e20;
+    return;
+  }
+  const double* src = reinterpret_cast<const double*>(recs + b);
+  for (int k = threadIdx.x; k < kRecDoubles; k += blockDim.x) sm[k] = src[k];
+  __syncthreads();
+  het_points<PREC>(*reinterpret_cast<const PhdRec*>(sm), g, h, sm + kRecDoubles, threadIdx.x, blockDim.x);
+  __syncthreads();
+  if (threadIdx.x < 32) het_regions(g, h, sm + kRecDoubles, lnl + b);
+}
+
+// batches up to this size take k_lnl_het_wide
+constexpr int kHetWideMaxSets = 128;
 
 // sets per block: four warps while their shared memory stays within 96 KB
 static int het_sets_per_block(size_t warp_bytes) {
@@ -2030,12 +2073,18 @@ void launch_lnl_het(const PhdRec* d_recs, const int* d_status, int B, const NetG
   const int spb = het_sets_per_block(smem);
   const int wd = het_warp_doubles(g.nifo, h.M);
   const unsigned grid = (unsigned)((B + spb - 1) / spb);
+  // A small batch (the reference-signature calls, merged or not) takes a block per set and is
+  // launched with programmatic dependent launch after the setup, so its blocks wait on the SMs
+  // instead of behind a launch gap; a large one takes a warp per set, launched the ordinary way
+  // (early blocks holding SMs slowed it).
+  if (B <= kHetWideMaxSets) {
+    auto kw = prec == kFP64 ? k_lnl_het_wide<kFP64> : k_lnl_het_wide<kMixed>;
+    const int threads = std::min(128, std::max(32, (h.M + 31) / 32 * 32));
+    launch_pdl(kw, dim3((unsigned)B), dim3(threads), smem, s, d_recs, d_status, g, h, B, d_lnl);
+    return;
+  }
   auto k = prec == kFP64 ? k_lnl_het<kFP64> : k_lnl_het<kMixed>;
-  // A small batch (the reference-signature calls, merged or not) is launched with programmatic
-  // dependent launch after the setup, so its few blocks wait on the SMs instead of behind a launch
-  // gap; a large one is launched the ordinary way (early blocks holding SMs slowed it).
-  if (B <= kHetPdlMaxSets) launch_pdl(k, dim3(grid), dim3(32 * spb), spb * smem, s, d_recs, d_status, g, h, B, wd, d_lnl);
-  else k<<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
+  k<<<grid, 32 * spb, spb * smem, s>>>(d_recs, d_status, g, h, B, wd, d_lnl);
 }
 
 // ---------------------------------------------------------------- heterodyne-grid waveforms, het_diff, Fisher_Het
@@ -2877,6 +2926,8 @@ void allow_dynamic_smem() {
   allow((const void*)k_lnl_het_multi<kMixed>);
   allow((const void*)k_lnl_het<kFP64>);
   allow((const void*)k_lnl_het<kMixed>);
+  allow((const void*)k_lnl_het_wide<kFP64>);
+  allow((const void*)k_lnl_het_wide<kMixed>);
 }
 
 }  // namespace qcbc

@@ -321,6 +321,22 @@ def test_lnl_het_vs_reference(ev1, golden):
     assert np.max(np.abs(Lm - h["lnl"])) <= LNL_ATOL_MIXED
 
 
+def test_het_small_batches_match_large_bit_for_bit(ev1, golden):
+    """Up to 128 sets the heterodyned lnL takes a block per set (the grid points spread over the
+    block), above that a warp per set: a set gets the same bits either way, invalid sets -1e20."""
+    ev, _, e = ev1
+    h = golden("het1.npz")
+    e.het_set(h)
+    P = synth.jitter_params(np.random.default_rng(2507), 300, h["pref"], 1e-3)
+    P[[4, 250], 2] = 1.5               # spin outside [-1, 1]
+    for prec in (q.FP64, q.MIXED):
+        big = e.lnl_het(P, prec, allow_invalid=True)                 # 300 sets: a warp per set
+        assert big[4] == -1e20 and big[250] == -1e20
+        small = np.concatenate([e.lnl_het(P[k:k + 100], prec, allow_invalid=True) for k in (0, 100, 200)])
+        assert np.array_equal(big, small), prec
+        assert np.array_equal(big[:3], [e.lnl_het(P[k:k + 1], prec)[0] for k in range(3)])
+
+
 def test_reference_signature_heterodyne(ev1, golden):
     ev, _, _ = ev1
     h = golden("het1.npz")
