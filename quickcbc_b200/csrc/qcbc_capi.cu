@@ -1736,12 +1736,31 @@ static bool rows_match(const RowsSnap& r, struct Net* net, double** D, double** 
 
 // The event holding (D, SN) for a reference-signature call: the bound one, else a cached one whose
 // rows equal the caller's, else a new one (which enters the cache).
+// The bound event this thread last used, valid while no binding was made or dropped since
+// (g_bind_gen): a chain calling with the same registered arrays skips the cache's lock.
+struct TlsBound {
+  BindKey key{nullptr, nullptr, nullptr, 0};
+  unsigned long long gen = 0;
+  std::weak_ptr<EventRef> ev;
+};
+static thread_local TlsBound tls_bound;
+static std::atomic<unsigned long long> g_bind_gen{1};
+
 static EventPtr data_event(struct Net* net, double** D, double** SN, int N, double Tobs) {
   const BindKey key{net, D, SN, N};
+  TlsBound& t = tls_bound;
+  const unsigned long long gen = g_bind_gen.load(std::memory_order_acquire);
+  if (t.gen == gen && !(t.key < key) && !(key < t.key))
+    if (EventPtr ev = t.ev.lock()) return ev;
   {
     std::lock_guard<std::mutex> lk(g_bind_mu);
     auto it = g_bound.find(key);
-    if (it != g_bound.end()) return it->second;
+    if (it != g_bound.end()) {
+      t.key = key;
+      t.gen = gen;
+      t.ev = it->second;
+      return it->second;
+    }
   }
   std::shared_ptr<const RowsSnap> snap;
   {
@@ -1806,6 +1825,7 @@ extern "C" int qcbc_bind_data(struct Net* net, double** D, double** SN, int N, d
   EventPtr p = std::make_shared<EventRef>(ev);
   std::lock_guard<std::mutex> lk(g_bind_mu);
   g_bound[BindKey{net, D, SN, N}] = std::move(p);    // a replaced binding closes after its last user
+  g_bind_gen.fetch_add(1, std::memory_order_acq_rel);
   return QCBC_OK;
 }
 
@@ -1813,6 +1833,7 @@ extern "C" int qcbc_unbind_all(void) {
   std::lock_guard<std::mutex> lk(g_bind_mu);
   g_bound.clear();
   g_rows.clear();
+  g_bind_gen.fetch_add(1, std::memory_order_acq_rel);
   return QCBC_OK;
 }
 
@@ -1866,7 +1887,42 @@ static std::mutex g_het_mu;
 static unsigned long long g_het_tick = 0;
 constexpr size_t kHetCacheMax = 32;
 
+// The last struct Het this thread used and a weak reference to its event: a chain that calls with
+// the same tables again skips the cache's lock (twelve chains calling at once contend for it).
+// Valid while the struct's IP, M and logLb are unchanged and the cache still holds the event.
+struct TlsHet {
+  const void* het = nullptr;
+  const void* ip = nullptr;
+  int M = 0;
+  double logLb = 0.0;
+  unsigned long long gen = 0;
+  std::weak_ptr<EventRef> ev;
+};
+static thread_local TlsHet tls_het;
+// bumped whenever the cache drops or replaces an entry: thread-local references older than that
+// go back through the cache
+static std::atomic<unsigned long long> g_het_gen{1};
+
+static EventPtr het_event_locked(struct Net* net, struct Het* het);
+
 static EventPtr het_event_for(struct Net* net, struct Het* het) {
+  TlsHet& t = tls_het;
+  const unsigned long long gen = g_het_gen.load(std::memory_order_acquire);
+  if (t.gen == gen && t.het == het && t.ip == (const void*)het->IP && t.M == het->M && t.logLb == het->logLb)
+    if (EventPtr ev = t.ev.lock()) return ev;
+  EventPtr ev = het_event_locked(net, het);
+  if (ev) {
+    t.gen = gen;
+    t.het = het;
+    t.ip = het->IP;
+    t.M = het->M;
+    t.logLb = het->logLb;
+    t.ev = ev;
+  }
+  return ev;
+}
+
+static EventPtr het_event_locked(struct Net* net, struct Het* het) {
   std::lock_guard<std::mutex> lk(g_het_mu);
   HetCacheEntry& e = g_het_cache[het];
   e.used = ++g_het_tick;
@@ -1899,6 +1955,7 @@ static EventPtr het_event_for(struct Net* net, struct Het* het) {
   qcbc_het_tables t{M, het->MN, het->MM, J, NR, het->logLb, het->fgrid, het->freq->data, amp.data(), ph.data(),
                     IP.data(), SL.data(), lc.data(), ls.data(), aa.data(), rcv.data(), rsv.data()};
   if (qcbc_het_set(raw, &t) != QCBC_OK) return nullptr;
+  if (e.ev) g_het_gen.fetch_add(1, std::memory_order_acq_rel);   // replaces an entry's tables
   e.ev = ev;
   e.ip = het->IP;
   e.M = het->M;
@@ -1908,6 +1965,7 @@ static EventPtr het_event_for(struct Net* net, struct Het* het) {
     for (auto it = g_het_cache.begin(); it != g_het_cache.end(); ++it)
       if (it->second.used < lru->second.used) lru = it;
     g_het_cache.erase(lru);
+    g_het_gen.fetch_add(1, std::memory_order_acq_rel);
   }
   return ev;
 }
@@ -1917,6 +1975,7 @@ static EventPtr het_event_for(struct Net* net, struct Het* het) {
 extern "C" int qcbc_het_forget(const struct Het* het) {
   std::lock_guard<std::mutex> lk(g_het_mu);
   g_het_cache.erase(het);
+  g_het_gen.fetch_add(1, std::memory_order_acq_rel);
   return QCBC_OK;
 }
 
