@@ -1542,11 +1542,28 @@ struct BindKey {
 // binding) never frees or rewrites memory that a concurrent call reads: the old event is closed
 // when its last user returns.  Host threads may therefore call these entry points concurrently,
 // as the reference's OpenMP chains do (QuickCBC.c:2063-2067).
+static inline void cpu_relax() {
+#if defined(__x86_64__) || defined(__i386__)
+  __builtin_ia32_pause();
+#endif
+}
+
+// A spin lock for sections of a few instructions that many threads enter at once: a thread that
+// finds std::mutex taken may sleep in the kernel and wake tens of microseconds later.
+struct SpinLock {
+  std::atomic<bool> taken{false};
+  void lock() {
+    while (taken.exchange(true, std::memory_order_acquire))
+      while (taken.load(std::memory_order_relaxed)) cpu_relax();
+  }
+  void unlock() { taken.store(false, std::memory_order_release); }
+};
+
 struct MergeReq;
 struct EventRef {
   qcbc_event* ev;
   // calls waiting to be merged into one launch on this event (merge_call)
-  std::mutex mu;                     // guards queue
+  SpinLock mu;                       // guards queue
   std::vector<MergeReq*> queue;
   std::atomic<int> queued{0};        // queue.size(), readable without the lock
   std::atomic<bool> busy{false};     // a caller is leading a batch
@@ -1587,7 +1604,10 @@ constexpr int kMergeMax = 256;
 static void merge_launch(qcbc_event* ev, const std::vector<MergeReq*>& batch) {
   const int B = (int)batch.size();
   const MergeReq& lead = *batch[0];
-  std::vector<double> P((size_t)B * 11), L((size_t)B, -1.0e20), R((size_t)B * kMaxIfo, 0.0);
+  static thread_local std::vector<double> P, L, R;
+  P.resize((size_t)B * 11);
+  L.assign((size_t)B, -1.0e20);
+  R.assign((size_t)B * kMaxIfo, 0.0);
   for (int b = 0; b < B; b++) memcpy(&P[(size_t)b * 11], batch[b]->params, 11 * sizeof(double));
   int rc;
   if (lead.kind == kMergeHet) {
@@ -1617,12 +1637,6 @@ static void merge_launch(qcbc_event* ev, const std::vector<MergeReq*>& batch) {
 // chains call again a few microseconds after their previous results come back).
 constexpr double kMergeGatherSeconds = 20e-6;
 
-static inline void cpu_relax() {
-#if defined(__x86_64__) || defined(__i386__)
-  __builtin_ia32_pause();
-#endif
-}
-
 // Lead one batch: wait briefly for the callers of the previous batch, take this request and the
 // waiting ones of the same kind, device and geometry, run them, publish each result.
 static void merge_lead(EventRef& er, MergeReq& me) {
@@ -1632,19 +1646,23 @@ static void merge_lead(EventRef& er, MergeReq& me) {
     while (er.queued.load(std::memory_order_acquire) < target && std::chrono::steady_clock::now() < t_end)
       cpu_relax();
   }
-  std::vector<MergeReq*> batch{&me};
+  static thread_local std::vector<MergeReq*> batch;
+  batch.clear();
+  batch.reserve(kMergeMax);
+  batch.push_back(&me);
   {
-    std::lock_guard<std::mutex> lk(er.mu);
-    std::vector<MergeReq*> rest;
-    for (MergeReq* r : er.queue) {
+    std::lock_guard<SpinLock> lk(er.mu);
+    size_t keep = 0;                 // the requests left for a later batch stay in place
+    for (size_t i = 0; i < er.queue.size(); i++) {
+      MergeReq* r = er.queue[i];
       if (r == &me) continue;
       const bool same = r->kind == me.kind && r->device == me.device &&
                         (me.kind == kMergeHet || memcmp(r->g, me.g, sizeof(NetGeom)) == 0);
       if (same && (int)batch.size() < kMergeMax) batch.push_back(r);
-      else rest.push_back(r);
+      else er.queue[keep++] = r;
     }
-    er.queue.swap(rest);
-    er.queued.store((int)er.queue.size(), std::memory_order_release);
+    er.queue.resize(keep);
+    er.queued.store((int)keep, std::memory_order_release);
   }
   merge_launch(er.ev, batch);
   er.last_batch.store((int)batch.size(), std::memory_order_relaxed);
@@ -1659,7 +1677,7 @@ static void merge_lead(EventRef& er, MergeReq& me) {
 // error message in this thread's error slot.
 static int merge_call(EventRef& er, MergeReq& me) {
   {
-    std::lock_guard<std::mutex> lk(er.mu);
+    std::lock_guard<SpinLock> lk(er.mu);
     er.queue.push_back(&me);
     er.queued.store((int)er.queue.size(), std::memory_order_release);
   }

@@ -1010,7 +1010,7 @@ __device__ __forceinline__ void tile_fp64(const PhdRec& c, const NetGeom& g, con
 //    = base(thread) x R[k] with a per-tile FP32 table R[k] = e^{2 pi i k blockDim (df (ts - td) - Ri)},
 //    both built in FP64;
 //  * amplitude in FP32 without the constant a0 (Msec df)^{-7/6} (applied in FP64 by the finaliser);
-//  * FP32 partial sums over 8 bins, accumulated in FP64.
+//  * FP32 partial sums over 16 bins, accumulated in FP64.
 // ---- mixed-precision tile body (coefficients: MixPoly in the record)
 
 // The piece coefficients of a parameter set stay in shared memory (the block's record) and are
@@ -1106,10 +1106,17 @@ struct MixW {
   }
 };
 
-// FP32 partial sums of up to 8 bins per detector: S = sum (wr' - i wi') R_k a e^{-i phi} and
+// FP32 partial sums of up to 16 bins per detector: S = sum (wr' - i wi') R_k a e^{-i phi} and
 // sum a^2 ws' (a the amplitude without its bin factor i^{-7/6}, which the weighted data carry);
 // flushed into the FP64 accumulators with the thread's rotation base applied, so that
 // acc[2 id] = sum amp (wr cos x + wi sin x), x = 2 pi f (ts - td) + lambda - phi.
+// bins of one thread summed in FP32 between flushes into its FP64 sums
+constexpr int kMixFlushBins = 16;
+
+// Row stride (float2 entries) of the rotation table, whose row k holds R_k of every detector:
+// padded to 4 at three detectors so that a row is two aligned loads.
+__host__ __device__ constexpr int mix_rs(int nifo) { return nifo == 1 ? 1 : (nifo == 2 ? 2 : 4); }
+
 template <int NIFO>
 struct MixAcc {
   float sx[NIFO], sy[NIFO], sh[NIFO];
@@ -1117,13 +1124,22 @@ struct MixAcc {
 #pragma unroll
     for (int id = 0; id < NIFO; id++) { sx[id] = 0.f; sy[id] = 0.f; sh[id] = 0.f; }
   }
-  __device__ __forceinline__ void add(float amp, float cyc, const MixW<NIFO>& w, const float2* rot, int nk) {
+  __device__ __forceinline__ void add(float amp, float cyc, const MixW<NIFO>& w, const float2* rot) {
     float sw, cw;
     __sincosf(6.28318530717958648f * cyc, &sw, &cw);     // |argument| <= pi
     const float ex = amp * cw, ey = -amp * sw, amp2 = amp * amp;
+    float2 Rr[NIFO];                 // this row's rotations: one 128-bit load for detectors 0 and 1
+    if (NIFO >= 2) {
+      const float4 q = *reinterpret_cast<const float4*>(rot);
+      Rr[0] = make_float2(q.x, q.y);
+      Rr[1 % NIFO] = make_float2(q.z, q.w);
+      if (NIFO == 3) Rr[2 % NIFO] = rot[2];
+    } else {
+      Rr[0] = rot[0];
+    }
 #pragma unroll
     for (int id = 0; id < NIFO; id++) {
-      const float2 R = rot[id * nk];
+      const float2 R = Rr[id];
       const float qx = fmaf(R.x, ex, -R.y * ey), qy = fmaf(R.x, ey, R.y * ex);
       sx[id] = fmaf(w.r[id], qx, fmaf(w.i[id], qy, sx[id]));
       sy[id] = fmaf(w.r[id], qy, fmaf(-w.i[id], qx, sy[id]));
@@ -1157,7 +1173,7 @@ struct MixSmemState {
 // phase piece PP (-1: decided per bin).  The pieces' coefficients are read from the block's
 // record in shared memory at each use.
 template <int NIFO, int AP, int PP, class State>
-__device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot, int nk,
+__device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev, const float2* s_rot,
                                            State& S, int k, int k_end, int i, int i1, int bs) {
   if (i > i1) return;
   const int n = min(k_end - k, (i1 - i) / bs + 1);     // rows of this thread in the run
@@ -1168,7 +1184,8 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
   const MixAmpInt& an = P.aint;
   const MixAmpMrd& am = P.amrd;
   const size_t nh = (size_t)ev.nh;
-  const float2* pr = s_rot + k;
+  constexpr int RS = mix_rs(NIFO);
+  const float2* pr = s_rot + (size_t)k * RS;
   const double dbs = (double)bs;
   const float fbs = (float)bs;
   double xi = (double)i;
@@ -1177,8 +1194,8 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
   // tables a row needs: tabA for the inspiral amplitude and the FP64 phase pieces, tabB for the
   // FP64 phase pieces, tabC for the ringdown phase
   constexpr bool kTabA = AP <= 0 || PP != 2, kTabB = PP != 2, kTabC = PP == 2 || PP < 0;
-  for (int r = 0; r < n; r += 8) {
-    const int m = min(8, n - r);
+  for (int r = 0; r < n; r += kMixFlushBins) {
+    const int m = min(kMixFlushBins, n - r);
     MixAcc<NIFO> A;
     A.zero();
 #pragma unroll 1
@@ -1213,9 +1230,9 @@ __device__ __forceinline__ void mixed_rows(const MixPoly& P, const EventData& ev
         a = ap == 0 ? mamp_ins(P.ains, xf, (float)tA.x)
                     : (ap == 1 ? mamp_int(P.aint, xf) : mamp_mrd(P.amrd, xf));
       }
-      A.add(a, cyc, w, pr, nk);
+      A.add(a, cyc, w, pr);
       b += bs;
-      pr++;
+      pr += RS;
       xi += dbs;
       xf += fbs;
     }
@@ -1243,7 +1260,7 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
       double cyc = (double)k * (Dstep * (c.ts - c.td[id]) - (double)bs * Ri);
       float sv, cv;                  // reduced to one cycle in FP64, the rotation itself in FP32
       sincospif(2.0f * (float)(cyc - rint(cyc)), &sv, &cv);
-      s_rot[id * nk + k] = make_float2(cv, sv);
+      s_rot[k * mix_rs(NIFO) + id] = make_float2(cv, sv);
     }
   }
   __syncthreads();
@@ -1266,7 +1283,7 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
     int k_end;
     if (a0 != amp_piece(P, r1) || p0 != ph_piece(P, r1)) {
       k_end = k + 1;
-      mixed_rows<NIFO, -1, -1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs);
+      mixed_rows<NIFO, -1, -1>(P, ev, s_rot, S, k, k_end, i, i1, bs);
     } else {
       int nxt = i1 + 1;              // the pieces can only change at a threshold
       if (P.iA > r0 && P.iA < nxt) nxt = P.iA;
@@ -1275,15 +1292,15 @@ __device__ __forceinline__ void tile_mixed(const PhdRec& c, const NetGeom& g, co
       if (P.iM > r0 && P.iM < nxt) nxt = P.iM;
       k_end = nxt > i1 ? nk : max(k + 1, (nxt - i0 - bs) / bs + 1);
       switch (a0 * 3 + p0) {
-        case 0: mixed_rows<NIFO, 0, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 1: mixed_rows<NIFO, 0, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 2: mixed_rows<NIFO, 0, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 3: mixed_rows<NIFO, 1, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 4: mixed_rows<NIFO, 1, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 5: mixed_rows<NIFO, 1, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 6: mixed_rows<NIFO, 2, 0>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        case 7: mixed_rows<NIFO, 2, 1>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
-        default: mixed_rows<NIFO, 2, 2>(P, ev, s_rot, nk, S, k, k_end, i, i1, bs); break;
+        case 0: mixed_rows<NIFO, 0, 0>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 1: mixed_rows<NIFO, 0, 1>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 2: mixed_rows<NIFO, 0, 2>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 3: mixed_rows<NIFO, 1, 0>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 4: mixed_rows<NIFO, 1, 1>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 5: mixed_rows<NIFO, 1, 2>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 6: mixed_rows<NIFO, 2, 0>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        case 7: mixed_rows<NIFO, 2, 1>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
+        default: mixed_rows<NIFO, 2, 2>(P, ev, s_rot, S, k, k_end, i, i1, bs); break;
       }
     }
     k = k_end;
@@ -1306,7 +1323,7 @@ __host__ __device__ __forceinline__ int mixed_nk_cap(int band, int tiles, int th
 template <int NIFO>
 __device__ __forceinline__ void tile_mixed_smem(const PhdRec& c, const NetGeom& g, const EventData& ev, int i0, int i1,
                                                 float2* s_rot, int nk_cap, int nifo_cap, double* acc) {
-  float2* s_base = s_rot + (size_t)nifo_cap * nk_cap;
+  float2* s_base = s_rot + (size_t)mix_rs(nifo_cap) * nk_cap;
   double* s_acc = reinterpret_cast<double*>(s_base + (size_t)nifo_cap * blockDim.x);
   MixSmemState S{s_base + threadIdx.x, s_acc + threadIdx.x, (int)blockDim.x};
 #pragma unroll
@@ -1510,7 +1527,7 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
                                                                                FinalOut fo) {
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
-  extern __shared__ float2 s_rot[];   // [NIFO][nk]
+  extern __shared__ __align__(16) float2 s_rot[];   // [nk][mix_rs(NIFO)], then the threads' state
   pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
@@ -1532,7 +1549,7 @@ template <int NIFO>
 static void launch_mixed_n(const PhdRec* r, int B, const NetGeom& g, const EventData& ev, const FullLaunch& L,
                            double* part, const FinalOut& fo, cudaStream_t s) {
   dim3 grid((unsigned)(B * L.tiles)), block(L.threads);
-  size_t smem = (size_t)mixed_nk(g, L) * NIFO * sizeof(float2);
+  size_t smem = (size_t)mixed_nk(g, L) * mix_rs(NIFO) * sizeof(float2);
   smem += mixed_state_bytes(L.threads, NIFO);
   if (fo.order.cnt || fo.done) launch_pdl(k_lnl_full_mixed<NIFO>, grid, block, smem, s, r, g, ev, L.tiles, part, fo);
   else k_lnl_full_mixed<NIFO><<<grid, block, smem, s>>>(r, g, ev, L.tiles, part, fo);
@@ -1698,7 +1715,7 @@ __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS)
   __shared__ EventDesc evd;
   __shared__ int s_item, s_b;
   __shared__ double red[32 * 2 * kMaxIfo];
-  extern __shared__ float2 s_rot[];   // mixed: rotation table [3][nk]
+  extern __shared__ __align__(16) float2 s_rot[];   // mixed: rotation table [nk][4], then the threads' state
   int total = off[B];
   if (total > items_cap) total = items_cap;
   for (;;) {
@@ -1744,7 +1761,7 @@ __global__ void __launch_bounds__(256, PREC == kFP64 ? 4 : QCBC_MULTI_MINBLOCKS)
 static size_t multi_smem(Precision prec, int threads, int tile_bins) {
   if (prec == kFP64) return 0;
   int nk = (tile_bins + threads - 1) / threads + 1;
-  return (size_t)nk * kMaxIfo * sizeof(float2) + mixed_state_bytes(threads, kMaxIfo);
+  return (size_t)nk * mix_rs(kMaxIfo) * sizeof(float2) + mixed_state_bytes(threads, kMaxIfo);
 }
 
 int multi_blocks_per_sm(Precision prec, int threads, int tile_bins) {
