@@ -707,6 +707,56 @@ def run_profile(args):
     e.close()
 
 
+def run_percall(args):
+    """The reference-signature drop-ins called one parameter set at a time, as QuickCBC's sampler
+    calls them: device time of a B = 1 and a B = 12 step (the sizes of a lone call and of twelve
+    merged ones), the host-buffer call's time, and the native-thread call rates from 1 and 12
+    threads.  Config 2 for the full likelihood (FP64), config 3 for the heterodyned one (FP64)."""
+    import quickcbc_b200 as q
+    from quickcbc_b200 import _lib, synth
+    _lib.check(_lib.lib().qcbc_init(0))
+
+    def step_times(timer, call, P, B):
+        d = q.DeviceBuffer(P[:B].nbytes)
+        d.upload(P[:B])
+        timer(d, B, 20)
+        ms = timer(d, B, 200)
+        for _ in range(20):
+            call(P[:B])
+        t0 = time.perf_counter()
+        for _ in range(300):
+            call(P[:B])
+        return {"device_us_median": float(np.median(ms) * 1e3), "host_call_us": (time.perf_counter() - t0) / 300 * 1e6}
+
+    out = {"metric": "reference-signature calls, one parameter set per call (FP64)"}
+    ev, P = make_workload()
+    q.set_band(ev.fmin, 1024.0)
+    e = q.Event.from_synthetic(ev)
+    full = {"workload": "config 2: 3 det, 16 s, 4096 Hz"}
+    for B in (1, 12):
+        full[f"B{B}"] = step_times(lambda d, b, n: q.time_lnl_full(e, d, b, q.FP64, n, flush_l2=False,
+                                                                    kernel_times=False)[0],
+                                   lambda X: e.lnl_full(X, q.FP64), P, B)
+        full[f"B{B}"]["tiles_threads"] = e.get_launch(B, q.FP64)
+    full["per_call"] = dropin_per_call_rates(q, ev, P)
+    out["full"] = full
+
+    def tmpl(info, p):
+        return q.fulltemplates(info["labels"], info["GMST"], info["freq"], p, info["N"])
+    g3 = np.load(os.path.join(ROOT, "tests", "golden", "grid3.npz"))
+    ev3 = synth.config_event(3, tmpl)
+    e3 = q.Event.from_synthetic(ev3)
+    e3.het_setup(ev3.inj, g3["fgrid"], int(g3["MN"]), int(g3["MM"]), 2)
+    P3 = synth.jitter_params(np.random.default_rng(3100), 256, ev3.inj, 1e-4)
+    het = {"workload": "config 3: 3 det, 128 s, BNS, het grid M = %d" % len(g3["fgrid"])}
+    for B in (1, 12):
+        het[f"B{B}"] = step_times(lambda d, b, n: q.time_lnl_het(e3, d, b, q.FP64, n, flush_l2=False),
+                                  lambda X: e3.lnl_het(X, q.FP64), P3, B)
+    het["per_call"] = dropin_het_per_call_rates(q, ev3, g3, P3)
+    out["het"] = het
+    print(json.dumps(out))
+
+
 def run_profile_cfg3(args):
     """Profiling run of the config-3 heterodyned step (k_setup then k_lnl_het) on 4096 sets spread
     as in the bench: grid and tables built on the GPU, `warmup` untimed steps, then `steps`."""
@@ -781,6 +831,8 @@ def main():
                     help="profiling run of the config-3 heterodyned step (for ncu)")
     ap.add_argument("--profile-cfg4", action="store_true",
                     help="profiling run of the config-4 interleaved launch (for ncu)")
+    ap.add_argument("--percall", action="store_true",
+                    help="reference-signature drop-ins, one set per call: step latencies and 1/12-thread rates")
     ap.add_argument("--ref-het-space-child", action="store_true", help=argparse.SUPPRESS)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -792,6 +844,8 @@ def main():
         return run_profile(args)
     if args.profile_cfg3:
         return run_profile_cfg3(args)
+    if args.percall:
+        return run_percall(args)
     if args.profile_cfg4:
         return run_profile_cfg4(args)
     if args.serve:

@@ -78,7 +78,9 @@ def lib():
         L.qcbc_event_close.argtypes = [vp]
         L.qcbc_event_device_bytes.restype = ll
         L.qcbc_event_device_bytes.argtypes = [vp]
-        L.qcbc_lnl_full.argtypes = [vp, _PD, i, _PD, _PD, i]
+        # host arrays as plain addresses (a numpy array's .ctypes.data): the batched calls are
+        # made per sampler step, and building a typed pointer per argument costs microseconds
+        L.qcbc_lnl_full.argtypes = [vp, vp, i, vp, vp, i]
         L.qcbc_lnl_full_dev.argtypes = [vp, vp, i, vp, vp, i, vp]
         L.qcbc_lnl_full_noalloc.argtypes = [vp, vp, i, vp, vp, i, vp]
         L.qcbc_synchronize.argtypes = []
@@ -95,7 +97,7 @@ def lib():
         L.qcbc_het_setup.argtypes = [vp, _PD, pi, i, i, i, i]
         L.qcbc_het_sizes.argtypes = [vp, pi, pi, pi, pi, pi]
         L.qcbc_het_export.argtypes = [vp, pi] + [_PD] * 11
-        L.qcbc_lnl_het.argtypes = [vp, _PD, i, _PD, i]
+        L.qcbc_lnl_het.argtypes = [vp, vp, i, vp, i]
         L.qcbc_lnl_intrinsic.argtypes = [vp, _PD, i, _PD, _PD, i]
         L.qcbc_het_diff.argtypes = [vp, _PD, _PD, i, _PD]
         L.qcbc_het_fisher.argtypes = [vp, _PD, i, _PD]

@@ -82,9 +82,9 @@ class Event:
     def lnl_full(self, params, precision=FP64, rho=False, allow_invalid=False):
         P = _f64(np.atleast_2d(params))
         B = P.shape[0]
-        out = np.zeros(B)
-        r = np.zeros((B, self.nifo)) if rho else None
-        rc = lib().qcbc_lnl_full(self._h, _ptr(P), B, _ptr(out), _ptr(r) if rho else None,
+        out = np.empty(B)
+        r = np.empty((B, self.nifo)) if rho else None
+        rc = lib().qcbc_lnl_full(self._h, P.ctypes.data, B, out.ctypes.data, r.ctypes.data if rho else None,
                                  precision_code(precision))
         if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
             check(rc)
@@ -144,8 +144,8 @@ class Event:
 
     def lnl_het(self, params, precision=FP64, allow_invalid=False):
         P = _f64(np.atleast_2d(params))
-        out = np.zeros(P.shape[0])
-        rc = lib().qcbc_lnl_het(self._h, _ptr(P), P.shape[0], _ptr(out), precision_code(precision))
+        out = np.empty(P.shape[0])
+        rc = lib().qcbc_lnl_het(self._h, P.ctypes.data, P.shape[0], out.ctypes.data, precision_code(precision))
         if rc != 0 and not (allow_invalid and rc == _lib.QCBC_EDOM):
             check(rc)
         return out
