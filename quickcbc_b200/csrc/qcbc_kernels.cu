@@ -1519,6 +1519,40 @@ __device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][
   }
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// While the setup runs (before pdl_wait), the first blocks of the lnL launch pull the band's FP32
+// planes and bin tables into L2, one 128-byte line per thread, so that the first rows of every
+// block find them there instead of in HBM.
+template <int NIFO>
+__device__ __forceinline__ void mixed_prefetch(const NetGeom& g, const EventData& ev) {
+  const size_t nh = (size_t)ev.nh, lo = (size_t)max(g.imin, 0), n = (size_t)max(g.imax - g.imin, 0);
+  const char* base[6];
+  size_t len[6];
+  int ns = 0;
+  auto seg = [&](const void* p, size_t elem) {
+    base[ns] = static_cast<const char*>(p) + lo * elem;
+    len[ns++] = n * elem;
+  };
+  if (NIFO == 3) {
+    seg(ev.wm, 16); seg(ev.wm + 4 * nh, 16); seg(ev.wm + 8 * nh, 4);
+  } else if (NIFO == 2) {
+    seg(ev.wm, 16); seg(ev.wm + 4 * nh, 8);
+  } else {
+    seg(ev.wm, 8); seg(ev.wm + 2 * nh, 4);
+  }
+  seg(ev.tabA, 16); seg(ev.tabB, 16); seg(ev.tabC, 8);
+  size_t line = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  for (int k = 0; k < ns; k++) {
+    const size_t lines = (len[k] + 127) / 128;
+    if (line < lines) {
+      prefetch_l2(base[k] + line * 128);
+      return;
+    }
+    line -= lines;
+  }
+}
+
 // Mixed-precision full lnL over one tile of bins of one parameter set.
 template <int NIFO>
 __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(const PhdRec* __restrict__ recs, NetGeom g,
@@ -1528,6 +1562,7 @@ __global__ void __launch_bounds__(256, QCBC_MIXED_MINBLOCKS) k_lnl_full_mixed(co
   __shared__ PhdRec rec;
   __shared__ double red[32 * 2 * kMaxIfo];
   extern __shared__ __align__(16) float2 s_rot[];   // [nk][mix_rs(NIFO)], then the threads' state
+  mixed_prefetch<NIFO>(g, ev);
   pdl_wait();          // records (and class lists) of the setup
   const int bi = blockIdx.x / tiles, t = blockIdx.x - bi * tiles;
   const int b = fo.order.cnt ? ordered_set(fo, bi) : bi;
