@@ -1664,7 +1664,15 @@ static void merge_lead(EventRef& er, MergeReq& me) {
     er.queue.resize(keep);
     er.queued.store((int)keep, std::memory_order_release);
   }
-  merge_launch(er.ev, batch);
+  try {
+    merge_launch(er.ev, batch);
+  } catch (...) {                    // an allocation failed: every caller of the batch gets the error
+    for (MergeReq* r : batch) {
+      r->lnl = -1.0e20;
+      r->rc = QCBC_ENOMEM;
+      r->err = "host allocation failed in a merged likelihood call";
+    }
+  }
   er.last_batch.store((int)batch.size(), std::memory_order_relaxed);
   // a follower may return (and its request go out of scope) as soon as its flag is set
   for (MergeReq* r : batch) r->done.store(1, std::memory_order_release);

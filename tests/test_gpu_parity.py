@@ -409,6 +409,27 @@ def test_concurrent_reference_calls_merge_bit_exact(ev1, golden):
     assert launches.sum() < 2 * out.size
 
 
+def test_native_thread_timer(ev1, golden):
+    """qcbc_time_dropin (the bench's per-call rates): 3 native threads x 5 merged calls each end on
+    the lone call's lnL; a bad `which` is refused."""
+    import ctypes as C
+    from quickcbc_b200 import _lib, engine as eng
+    ev, _, _ = ev1
+    h = golden("het1.npz")
+    H = q.LegacyHet(ev.labels, ev.GMST, ev.Tobs, h["fgrid"], int(h["MN"]), int(h["MM"]), int(h["J"]))
+    H.heterodyne(ev.D, h["pref"], ev.freq, ev.SN, ev.N)
+    P = np.ascontiguousarray(h["params"][:1])
+    L = _lib.lib()
+    secs, last = C.c_double(0.0), np.zeros(3)
+    rc = L.qcbc_time_dropin(1, H.nh.ref, C.byref(H.het), None, None, None, ev.N, ev.Tobs, eng._ptr(P), 1, 5, 3,
+                            C.byref(secs), eng._ptr(last))
+    assert rc == 0, _lib.last_error()
+    assert secs.value > 0 and np.all(last == H.lnl(P[0]))
+    rc = L.qcbc_time_dropin(2, H.nh.ref, C.byref(H.het), None, None, None, ev.N, ev.Tobs, eng._ptr(P), 1, 5, 3,
+                            C.byref(secs), None)
+    assert rc == -1 and "which" in _lib.last_error()
+
+
 def test_cfg3_heterodyne_long_signal(ora):
     """Config 3 (3 det, 128 s, 4096 Hz, BNS): reference het grid, tables set up on
     the GPU in FP64, het lnL against the reference's value and the oracle."""
