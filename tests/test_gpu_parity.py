@@ -193,50 +193,52 @@ def test_length_ordered_batch_matches_unordered(cfg2, ora):
 
 
 def test_device_call_captured_in_graph_and_on_two_streams(cfg2):
-    """qcbc_lnl_full_dev at one tile per set on a caller's stream: captured into a CUDA graph and
-    replayed three times, and alternated between two streams, it gives the uncaptured result bit
-    for bit (each call clears its own launch-order counts on its stream)."""
+    """qcbc_lnl_full_dev on a caller's stream, at one tile per set (2048 sets) and at several tiles
+    per set (40 sets, each finalised by its last tile): captured into a CUDA graph and replayed three
+    times, and alternated between two streams, it gives the uncaptured result bit for bit (each call
+    clears its own launch-order counts on its stream; the per-set tile counts are left at zero by
+    every launch)."""
     import ctypes as C
     import torch
     from quickcbc_b200 import _lib
     ev, e = cfg2
-    P = synth.draw_params(np.random.default_rng(2505), 2048, ev.inj)
-    B = len(P)
-    assert e.get_launch(B, q.MIXED)[0] == 1
-    dP, dL = q.DeviceBuffer(P.nbytes), q.DeviceBuffer(B * 8)
-    dP.upload(P)
     L = _lib.lib()
     s1, s2 = torch.cuda.Stream(), torch.cuda.Stream()
+    for B, one_tile in ((2048, True), (40, False)):
+        P = synth.draw_params(np.random.default_rng(2505), B, ev.inj)
+        assert (e.get_launch(B, q.MIXED)[0] == 1) == one_tile
+        dP, dL = q.DeviceBuffer(P.nbytes), q.DeviceBuffer(B * 8)
+        dP.upload(P)
 
-    def clear():                             # pageable uploads may finish after cudaMemcpy returns
-        dL.upload(np.full(B, np.nan))
-        assert L.qcbc_synchronize() == 0
+        def clear():                         # pageable uploads may finish after cudaMemcpy returns
+            dL.upload(np.full(B, np.nan))
+            assert L.qcbc_synchronize() == 0
 
-    def call(prec, s):
-        rc = L.qcbc_lnl_full_dev(e.handle, dP.ptr, B, dL.ptr, None, prec, C.c_void_p(s.cuda_stream))
-        assert rc == 0, _lib.last_error()
+        def call(prec, s):
+            rc = L.qcbc_lnl_full_dev(e.handle, dP.ptr, B, dL.ptr, None, prec, C.c_void_p(s.cuda_stream))
+            assert rc == 0, _lib.last_error()
 
-    for prec in (q.FP64, q.MIXED):
-        call(prec, s1)                       # grows the thread's scratch before capture
-        s1.synchronize()
-        want = dL.download((B,))
-        np.testing.assert_allclose(want, e.lnl_full(P, prec), rtol=0, atol=0)
-        for s in (s2, s1, s2):               # alternate streams, each call ordered after the last
-            clear()
-            call(prec, s)
-            s.synchronize()
-            assert np.array_equal(dL.download((B,)), want)
-        g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g, stream=s1, capture_error_mode="thread_local"):
-            call(prec, s1)
-        for rep in range(3):
-            clear()
-            g.replay()
-            torch.cuda.synchronize()
-            assert np.array_equal(dL.download((B,)), want), f"replay {rep}"
-        del g
-    dP.free()
-    dL.free()
+        for prec in (q.FP64, q.MIXED):
+            call(prec, s1)                   # grows the thread's scratch before capture
+            s1.synchronize()
+            want = dL.download((B,))
+            np.testing.assert_allclose(want, e.lnl_full(P, prec), rtol=0, atol=0)
+            for s in (s2, s1, s2):           # alternate streams, each call ordered after the last
+                clear()
+                call(prec, s)
+                s.synchronize()
+                assert np.array_equal(dL.download((B,)), want)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g, stream=s1, capture_error_mode="thread_local"):
+                call(prec, s1)
+            for rep in range(3):
+                clear()
+                g.replay()
+                torch.cuda.synchronize()
+                assert np.array_equal(dL.download((B,)), want), f"B {B} replay {rep}"
+            del g
+        dP.free()
+        dL.free()
 
 
 def test_invalid_parameter_sets_flagged(ev1):
