@@ -844,8 +844,22 @@ static int enqueue_het(Workspace* w, qcbc_event* ev, const double* d_params, int
   if ((rc = grow(w->d_recs, w->c_recs, (size_t)B))) return rc;
   if ((rc = grow(w->d_status, w->c_status, (size_t)B))) return rc;
   DeviceState& ds = g_dev[current_device()];
-  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s);
-  launch_lnl_het(w->d_recs, w->d_status, B, g, het_data(ev), prec == QCBC_MIXED ? kMixed : kFP64, d_lnl, s);
+  const HetData hd = het_data(ev);
+  // the setup's threads pull the heterodyne tables (and, for the mixed form, the bin tables at the
+  // grid's bins) into L2 for the heterodyned launch
+  SetupPrefetch pf;
+  pf.buf = ev->het.buf;
+  pf.bytes = het_doubles(ev->g.nifo, ev->het.M, ev->het.J) * sizeof(double);
+  if (prec == QCBC_MIXED) {
+    pf.bins = ev->het.d_fgrid;
+    pf.nbins = ev->het.M;
+    pf.tabA = hd.tabA;
+    pf.tabB = hd.tabB;
+    pf.tabC = hd.tabC;
+    pf.tab_n = g_dev[ev->device].tab_n;
+  }
+  launch_setup(d_params, B, g, ds.qnm, w->d_recs, w->d_status, s, kModelFull, pf);
+  launch_lnl_het(w->d_recs, w->d_status, B, g, hd, prec == QCBC_MIXED ? kMixed : kFP64, d_lnl, s);
   tls_launches += 2;
   CU(cudaGetLastError());
   return QCBC_OK;

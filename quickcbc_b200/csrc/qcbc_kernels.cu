@@ -922,25 +922,49 @@ static void launch_pdl(void (*k)(KArgs...), dim3 grid, dim3 block, size_t smem, 
   cudaLaunchKernelEx(&cfg, k, args...);
 }
 
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
+
+// One line of the following launch's tables per thread (SetupPrefetch); every address lies inside
+// its array.
+__device__ __forceinline__ void setup_prefetch(const SetupPrefetch& pf) {
+  size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t lines = (pf.bytes + 127) / 128;
+  if (t < lines) {
+    prefetch_l2(static_cast<const char*>(pf.buf) + t * 128);
+    return;
+  }
+  t -= lines;
+  if (t < (size_t)pf.nbins) {
+    const int i = pf.bins[t];
+    if (i < 0 || i >= pf.tab_n) return;
+    if (pf.tabA) prefetch_l2(pf.tabA + i);
+    if (pf.tabB) prefetch_l2(pf.tabB + i);
+    if (pf.tabC) prefetch_l2(pf.tabC + i);
+  }
+}
+
 __global__ void __launch_bounds__(kSetupThreads) k_setup(const double* __restrict__ params, int B, NetGeom g,
                                                          QnmTable q, PhdRec* __restrict__ recs,
-                                                         int* __restrict__ status, int model, SetOrder o) {
+                                                         int* __restrict__ status, int model, SetOrder o,
+                                                         SetupPrefetch pf) {
   pdl_trigger();       // a dependent launch (the lnL kernel) may be scheduled; it waits for this grid
+  setup_prefetch(pf);
   GeomOne geo{g};
   setup_coop_block(params, B, geo, q, 1, recs, status, nullptr, model, o.cnt, o.list);
 }
 
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
-                  int* d_status, cudaStream_t s, int model) {
+                  int* d_status, cudaStream_t s, int model, const SetupPrefetch& pf) {
   if (B <= 0) return;
   k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model,
-                                                                      SetOrder{nullptr, nullptr});
+                                                                      SetOrder{nullptr, nullptr}, pf);
 }
 
 void launch_setup_ordered(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
                           int* d_status, const SetOrder& o, cudaStream_t s, int model) {
   if (B <= 0) return;
-  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model, o);
+  k_setup<<<(B + kSetupSets - 1) / kSetupSets, kSetupThreads, 0, s>>>(d_params, B, g, q, d_recs, d_status, model, o,
+                                                                      SetupPrefetch{});
 }
 
 // ---------------------------------------------------------------- reductions
@@ -1518,8 +1542,6 @@ __device__ __forceinline__ void group_sum(double (&v)[NV], double* smem /* [32][
     }
   }
 }
-
-__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 
 // While the setup runs (before pdl_wait), the first blocks of the lnL launch pull the band's FP32
 // planes and bin tables into L2, one 128-byte line per thread, so that the first rows of every

@@ -83,8 +83,21 @@ __host__ __device__ constexpr int param_stride(int model, int nifo) {
   return model == kModelIntrinsic ? kNX + 3 * (nifo - 1) : 11;
 }
 
+// Tables of the launch that follows the setup, which the setup's threads pull into L2 while they
+// start (one 128-byte line each): a contiguous range, and the per-bin table entries at `nbins`
+// bins listed in `bins` (device memory).  Empty by default.
+struct SetupPrefetch {
+  const void* buf = nullptr;
+  size_t bytes = 0;
+  const int* bins = nullptr;
+  int nbins = 0;
+  const double2* tabA = nullptr;
+  const double2* tabB = nullptr;
+  const float2* tabC = nullptr;
+  int tab_n = 0;                     // entries of each table; bins outside [0, tab_n) are skipped
+};
 void launch_setup(const double* d_params, int B, const NetGeom& g, const QnmTable& q, PhdRec* d_recs,
-                  int* d_status, cudaStream_t s, int model = kModelFull);
+                  int* d_status, cudaStream_t s, int model = kModelFull, const SetupPrefetch& pf = SetupPrefetch{});
 // Launch order of the sets: the setup files each set under its length class (its bin count in
 // kOrderClasses classes of the band): cnt[c] counts class c, list[c * B + r] is its r-th set (r in
 // no particular order).  Block k of the one-tile lnL launch then takes the k-th set with the
